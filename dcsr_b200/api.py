@@ -1,0 +1,317 @@
+"""Python host binding of the DCSR C ABI (include/dcsr_b200.h).
+
+Device memory is held in torch CUDA tensors; every call passes raw pointers
+and the current torch CUDA stream to libdcsr_b200.so through ctypes.  There is
+no CPU fallback: if the shared library is missing or fails to load, the first
+call raises.
+
+``DcsrMatrix`` is the handle class; ``dcsr_b200.device`` mirrors the
+reference's free-function operator names on top of it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libdcsr_b200.so")
+
+F32, F64 = 0, 1
+MERGE, APPEND = 0, 1
+OK, POOL_EXHAUSTED, LAYER_OVERFLOW, BAD_INDEX, OOM, BAD_ARG, TIMEOUT, CUDA_ERROR, NOT_SUPPORTED = range(9)
+REDUCE_SUM, REDUCE_MAX, REDUCE_MIN, REDUCE_COUNT = range(4)
+
+_TORCH_DT = {F32: torch.float32, F64: torch.float64}
+
+
+class DcsrError(RuntimeError):
+    def __init__(self, status: int, what: str):
+        self.status = status
+        super().__init__(f"{what}: {status_string(status)} ({status})")
+
+
+class Opts(C.Structure):
+    _fields_ = [(n, C.c_int32) for n in (
+        "max_segs", "factor_x16", "min_cap", "align", "alpha", "spare_x16", "min_spare", "mode", "reloc_min")]
+
+    def as_dict(self):
+        return {n: getattr(self, n) for n, _ in self._fields_}
+
+
+class Info(C.Structure):
+    _fields_ = [("n_rows", C.c_int32), ("n_cols", C.c_int32), ("dtype", C.c_int32), ("pitch", C.c_int32),
+                ("pool_cap", C.c_int64), ("row_sizes", C.c_void_p), ("seg", C.c_void_p), ("cols", C.c_void_p),
+                ("vals", C.c_void_p), ("opts", Opts)]
+
+
+_lib = None
+_vp, _i32, _i64, _dbl = C.c_void_p, C.c_int32, C.c_int64, C.c_double
+
+_SIGS = {
+    "dcsr_default_opts": (None, [C.POINTER(Opts), _i32]),
+    "dcsr_create": (_i32, [C.POINTER(_vp), _i32, _i32, _i32, C.POINTER(Opts)]),
+    "dcsr_destroy": (_i32, [_vp]),
+    "dcsr_info": (_i32, [_vp, C.POINTER(Info)]),
+    "dcsr_get_layout": (_i32, [_vp, _vp, _vp, _vp]),
+    "dcsr_from_csr": (_i32, [_vp, _vp, _vp, _vp, _i64, _vp]),
+    "dcsr_from_coo": (_i32, [_vp, _vp, _vp, _vp, _i64, _vp]),
+    "dcsr_from_hyb": (_i32, [_vp, _vp, _vp, _i32, _i64, _vp, _vp, _vp, _i64, _vp]),
+    "dcsr_nnz": (_i32, [_vp, C.POINTER(_i64), _vp]),
+    "dcsr_to_csr": (_i32, [_vp, _vp, _vp, _vp, _vp]),
+    "dcsr_to_coo": (_i32, [_vp, _vp, _vp, _vp, _vp]),
+    "dcsr_update": (_i32, [_vp, _vp, _vp, _vp, _i64, _vp]),
+    "dcsr_update_sync": (_i32, [_vp, _vp, _vp, _vp, _i64, _vp]),
+    "dcsr_get_status": (_i32, [_vp, _vp, C.POINTER(_i32)]),
+    "dcsr_compact": (_i32, [_vp, _vp]),
+    "dcsr_reserve": (_i32, [_vp, _i64, _vp]),
+    "dcsr_bin_rows": (_i32, [_vp, _vp]),
+    "dcsr_spmv": (_i32, [_vp, _vp, _i32, _i64, _vp, _i64, _dbl, _dbl, _vp]),
+    "dcsr_row_reduce": (_i32, [_vp, _i32, _vp, _vp]),
+    "dcsr_spgemm": (_i32, [_vp, _vp, _vp, _vp]),
+    "dcsr_count_sorted_indices": (_i32, [_vp, _i64, _vp, _vp]),
+    "dcsr_reduce_by_key": (_i32, [_vp, _vp, _i64, _i32, _vp, _vp, _vp, _vp]),
+    "dcsr_status_string": (C.c_char_p, [_i32]),
+    "dcsr_launch_count": (C.c_uint64, []),
+    "dcsr_version": (C.c_char_p, []),
+}
+
+
+def lib():
+    """Load libdcsr_b200.so (raises if it is missing: there is no fallback)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with `python -m dcsr_b200.build`")
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in _SIGS.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def status_string(st: int) -> str:
+    return lib().dcsr_status_string(st).decode()
+
+
+def launch_count() -> int:
+    return int(lib().dcsr_launch_count())
+
+
+def _check(st: int, what: str):
+    if st != OK:
+        raise DcsrError(st, what)
+
+
+def _stream(stream=None):
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return C.c_void_p(s.cuda_stream)
+
+
+def _ptr(t: torch.Tensor | None):
+    if t is None:
+        return None
+    if not t.is_cuda:
+        raise ValueError("device tensor expected")
+    if not t.is_contiguous():
+        raise ValueError("contiguous tensor expected")
+    return C.c_void_p(t.data_ptr())
+
+
+def default_opts(mode: int = MERGE, **kw) -> Opts:
+    o = Opts()
+    lib().dcsr_default_opts(C.byref(o), mode)
+    for k, v in kw.items():
+        setattr(o, k, int(v))
+    return o
+
+
+def _dtype_code(dtype) -> int:
+    if dtype in (torch.float32, F32, "f32", "float32"):
+        return F32
+    if dtype in (torch.float64, F64, "f64", "float64"):
+        return F64
+    raise ValueError(f"unsupported dtype {dtype}")
+
+
+@dataclass
+class Layout:
+    row_sizes: np.ndarray
+    seg: np.ndarray
+    pitch: int
+    max_segs: int
+    pool_cap: int
+
+
+class DcsrMatrix:
+    """A DCSR matrix resident on the current CUDA device."""
+
+    def __init__(self, n_rows: int, n_cols: int, dtype=torch.float32, mode: int = MERGE, opts: Opts | None = None,
+                 **kw):
+        self.h = None
+        o = opts if opts is not None else default_opts(mode, **kw)
+        self.opts = o
+        self.n_rows, self.n_cols = int(n_rows), int(n_cols)
+        self.dtype_code = _dtype_code(dtype)
+        self.dtype = _TORCH_DT[self.dtype_code]
+        h = C.c_void_p()
+        _check(lib().dcsr_create(C.byref(h), self.n_rows, self.n_cols, self.dtype_code, C.byref(o)), "dcsr_create")
+        self.h = h
+
+    def close(self):
+        if self.h is not None and _lib is not None:
+            lib().dcsr_destroy(self.h)
+        self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---------------------------------------------------------- loading
+    def from_csr(self, row_ptr, cols, vals, stream=None):
+        row_ptr, cols, vals = self._i(row_ptr), self._i(cols), self._v(vals)
+        _check(lib().dcsr_from_csr(self.h, _ptr(row_ptr), _ptr(cols), _ptr(vals), cols.numel(), _stream(stream)),
+               "dcsr_from_csr")
+        return self
+
+    def from_coo(self, rows, cols, vals, stream=None):
+        rows, cols, vals = self._i(rows), self._i(cols), self._v(vals)
+        _check(lib().dcsr_from_coo(self.h, _ptr(rows), _ptr(cols), _ptr(vals), rows.numel(), _stream(stream)),
+               "dcsr_from_coo")
+        return self
+
+    def from_hyb(self, ell_cols, ell_vals, coo_rows, coo_cols, coo_vals, stream=None):
+        """ell_cols/ell_vals: [width, pitch] column-major ELL (-1 = padding)."""
+        ell_cols, ell_vals = self._i(ell_cols), self._v(ell_vals)
+        coo_rows, coo_cols, coo_vals = self._i(coo_rows), self._i(coo_cols), self._v(coo_vals)
+        width = ell_cols.shape[0] if ell_cols.dim() == 2 else 0
+        pitch = ell_cols.shape[1] if ell_cols.dim() == 2 else self.n_rows
+        _check(lib().dcsr_from_hyb(self.h, _ptr(ell_cols), _ptr(ell_vals), width, pitch, _ptr(coo_rows),
+                                   _ptr(coo_cols), _ptr(coo_vals), coo_rows.numel(), _stream(stream)),
+               "dcsr_from_hyb")
+        return self
+
+    # ---------------------------------------------------------- updates
+    def update(self, rows, cols, vals, sync: bool = True, stream=None) -> int:
+        """Batch update; sync=True applies the repair policy and returns the
+        final status, sync=False enqueues only (status via get_status())."""
+        rows, cols, vals = self._i(rows), self._i(cols), self._v(vals)
+        fn = lib().dcsr_update_sync if sync else lib().dcsr_update
+        st = fn(self.h, _ptr(rows), _ptr(cols), _ptr(vals), rows.numel(), _stream(stream))
+        if st in (BAD_ARG, OOM, CUDA_ERROR):
+            raise DcsrError(st, "dcsr_update")
+        return st
+
+    def get_status(self, stream=None) -> int:
+        s = C.c_int32()
+        _check(lib().dcsr_get_status(self.h, _stream(stream), C.byref(s)), "dcsr_get_status")
+        return s.value
+
+    def compact(self, stream=None):
+        _check(lib().dcsr_compact(self.h, _stream(stream)), "dcsr_compact")
+
+    def reserve(self, cap: int, stream=None):
+        _check(lib().dcsr_reserve(self.h, cap, _stream(stream)), "dcsr_reserve")
+
+    def bin_rows(self, stream=None):
+        _check(lib().dcsr_bin_rows(self.h, _stream(stream)), "dcsr_bin_rows")
+
+    # ----------------------------------------------------------- export
+    def nnz(self, stream=None) -> int:
+        v = C.c_int64()
+        _check(lib().dcsr_nnz(self.h, C.byref(v), _stream(stream)), "dcsr_nnz")
+        return v.value
+
+    def to_csr(self, stream=None):
+        nnz = self.nnz(stream)
+        dev = torch.device("cuda", torch.cuda.current_device())
+        rp = torch.empty(self.n_rows + 1, dtype=torch.int32, device=dev)
+        c = torch.empty(max(nnz, 1), dtype=torch.int32, device=dev)
+        v = torch.empty(max(nnz, 1), dtype=self.dtype, device=dev)
+        _check(lib().dcsr_to_csr(self.h, _ptr(rp), _ptr(c), _ptr(v), _stream(stream)), "dcsr_to_csr")
+        return rp, c[:nnz], v[:nnz]
+
+    def to_coo(self, stream=None):
+        nnz = self.nnz(stream)
+        dev = torch.device("cuda", torch.cuda.current_device())
+        r = torch.empty(max(nnz, 1), dtype=torch.int32, device=dev)
+        c = torch.empty(max(nnz, 1), dtype=torch.int32, device=dev)
+        v = torch.empty(max(nnz, 1), dtype=self.dtype, device=dev)
+        _check(lib().dcsr_to_coo(self.h, _ptr(r), _ptr(c), _ptr(v), _stream(stream)), "dcsr_to_coo")
+        return r[:nnz], c[:nnz], v[:nnz]
+
+    def layout(self, stream=None) -> Layout:
+        info = self.info()
+        rs = np.zeros(self.n_rows + 1, np.int32)
+        seg = np.zeros(info.pitch * info.opts.max_segs, np.int32)
+        _check(lib().dcsr_get_layout(self.h, C.c_void_p(rs.ctypes.data), C.c_void_p(seg.ctypes.data),
+                                     _stream(stream)), "dcsr_get_layout")
+        return Layout(rs, seg, info.pitch, info.opts.max_segs, info.pool_cap)
+
+    def info(self) -> Info:
+        i = Info()
+        _check(lib().dcsr_info(self.h, C.byref(i)), "dcsr_info")
+        return i
+
+    # -------------------------------------------------------- operators
+    def spmv(self, x: torch.Tensor, y: torch.Tensor | None = None, alpha: float = 1.0, beta: float = 0.0,
+             stream=None) -> torch.Tensor:
+        """y = alpha*A@x + beta*y; x is [n_cols] or [n_cols, k] (row-major)."""
+        x = self._v(x)
+        k = 1 if x.dim() == 1 else x.shape[1]
+        if y is None:
+            y = torch.empty((self.n_rows,) if x.dim() == 1 else (self.n_rows, k), dtype=self.dtype, device=x.device)
+            beta = 0.0
+        _check(lib().dcsr_spmv(self.h, _ptr(x), k, k, _ptr(y), k, alpha, beta, _stream(stream)), "dcsr_spmv")
+        return y
+
+    def row_reduce(self, op: int = REDUCE_SUM, y: torch.Tensor | None = None, stream=None) -> torch.Tensor:
+        if y is None:
+            y = torch.empty(self.n_rows, dtype=self.dtype, device=torch.device("cuda", torch.cuda.current_device()))
+        _check(lib().dcsr_row_reduce(self.h, op, _ptr(y), _stream(stream)), "dcsr_row_reduce")
+        return y
+
+    def spgemm(self, B: "DcsrMatrix", C_out: "DcsrMatrix | None" = None, stream=None, **kw) -> "DcsrMatrix":
+        if C_out is None:
+            C_out = DcsrMatrix(self.n_rows, B.n_cols, self.dtype, **kw)
+        _check(lib().dcsr_spgemm(self.h, B.h, C_out.h, _stream(stream)), "dcsr_spgemm")
+        return C_out
+
+    # ---------------------------------------------------------- helpers
+    def _i(self, t):
+        t = torch.as_tensor(t)
+        if not t.is_cuda:
+            t = t.cuda()
+        return t.to(torch.int32).contiguous()
+
+    def _v(self, t):
+        t = torch.as_tensor(t)
+        if not t.is_cuda:
+            t = t.cuda()
+        return t.to(self.dtype).contiguous()
+
+
+def count_sorted_indices(I: torch.Tensor, X: torch.Tensor, stream=None) -> torch.Tensor:
+    """X[I[n]] += 1 (in place) for a sorted int32 index tensor I."""
+    _check(lib().dcsr_count_sorted_indices(_ptr(I), I.numel(), _ptr(X), _stream(stream)),
+           "dcsr_count_sorted_indices")
+    return X
+
+
+def reduce_by_key(keys: torch.Tensor, vals: torch.Tensor, stream=None):
+    """Unique sorted keys and their left-to-right sums."""
+    n = keys.numel()
+    ko = torch.empty(max(n, 1), dtype=torch.int32, device=keys.device)
+    vo = torch.empty(max(n, 1), dtype=vals.dtype, device=keys.device)
+    cnt = torch.zeros(1, dtype=torch.int64, device=keys.device)
+    _check(lib().dcsr_reduce_by_key(_ptr(keys), _ptr(vals), n, _dtype_code(vals.dtype), _ptr(ko), _ptr(vo),
+                                    _ptr(cnt), _stream(stream)), "dcsr_reduce_by_key")
+    m = int(cnt.item())
+    return ko[:m], vo[:m]

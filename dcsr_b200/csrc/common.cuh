@@ -1,0 +1,251 @@
+// common.cuh -- shared internals of the DCSR library: the handle, the device
+// view of a matrix, layout policy, status words, the scratch arena and warp
+// helpers.  sm_100a only.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <atomic>
+#include <cstdio>
+#include <cstdlib>
+
+#include "../../include/dcsr_b200.h"
+
+namespace dcsr {
+
+constexpr int WARP = 32;
+constexpr unsigned FULL = 0xffffffffu;
+
+extern std::atomic<uint64_t> g_launches;
+inline void count_launch(uint64_t n = 1) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
+#define DCSR_CUDA(call)                                                                         \
+  do {                                                                                          \
+    cudaError_t _e = (call);                                                                    \
+    if (_e != cudaSuccess) {                                                                    \
+      fprintf(stderr, "dcsr: CUDA error %s at %s:%d\n", cudaGetErrorString(_e), __FILE__, __LINE__); \
+      return _e == cudaErrorMemoryAllocation ? DCSR_OOM : DCSR_CUDA_ERROR;                      \
+    }                                                                                           \
+  } while (0)
+
+#define DCSR_TRY(call)             \
+  do {                             \
+    int _s = (call);               \
+    if (_s != DCSR_OK) return _s;  \
+  } while (0)
+
+// Launch with the launch counter and an error check.
+#define DCSR_LAUNCH(kernel, grid, block, smem, stream, ...)          \
+  do {                                                               \
+    kernel<<<(grid), (block), (smem), (stream)>>>(__VA_ARGS__);      \
+    ::dcsr::count_launch();                                          \
+    DCSR_CUDA(cudaGetLastError());                                   \
+  } while (0)
+
+__host__ __device__ inline int64_t align_up(int64_t x, int64_t a) { return (x + a - 1) / a * a; }
+__host__ __device__ inline int64_t div_up(int64_t x, int64_t a) { return (x + a - 1) / a; }
+
+// Row capacity for a logical length under the layout policy (integer-only so
+// the oracle restates it exactly).
+__host__ __device__ inline int64_t policy_cap(const dcsr_opts &o, int64_t len) {
+  int64_t c = (len * o.factor_x16 + 15) / 16;
+  if (c < o.min_cap) c = o.min_cap;
+  if (c < len) c = len;
+  return align_up(c, o.align);
+}
+__host__ __device__ inline int64_t pool_capacity(const dcsr_opts &o, int64_t top) {
+  int64_t spare = top * o.spare_x16 / 16;
+  if (spare < o.min_spare) spare = o.min_spare;
+  return top + spare;
+}
+
+// Device status block of a handle (int64 words).
+enum StatWord {
+  ST_STATUS = 0,   // dcsr_status of the last rejected operation (sticky until read)
+  ST_GO = 1,       // 1 when the current update plan was accepted
+  ST_NEED = 2,     // pool top the current update requires
+  ST_TOUCHED = 3,  // touched rows of the current batch
+  ST_TILES = 4,    // relocation tiles of the current batch
+  ST_TOTAL = 5,    // scratch total (scan results)
+  ST_AUX = 6,
+  ST_WORDS = 8
+};
+
+// Device view of a matrix passed by value to kernels.
+template <typename V>
+struct Mat {
+  int32_t n_rows, n_cols, max_segs, pitch;
+  int64_t pool_cap;
+  int32_t *row_sizes;
+  int32_t *seg;
+  int32_t *cols;
+  V *vals;
+  long long *stat;
+  dcsr_opts o;
+};
+
+// Stream-ordered scratch arena: one device buffer, bump-allocated per
+// operation, grown (stream-ordered free + malloc) when an operation needs more.
+struct Arena {
+  char *base = nullptr;
+  size_t cap = 0, used = 0;
+  int reserve(size_t bytes, cudaStream_t s) {
+    used = 0;
+    if (bytes <= cap) return DCSR_OK;
+    if (base) DCSR_CUDA(cudaFreeAsync(base, s));
+    base = nullptr;
+    cap = 0;
+    size_t want = bytes + bytes / 4 + (1 << 20);
+    DCSR_CUDA(cudaMallocAsync((void **)&base, want, s));
+    cap = want;
+    return DCSR_OK;
+  }
+  template <typename T>
+  T *take(size_t n) {
+    size_t off = align_up((int64_t)used, 256);
+    used = off + n * sizeof(T);
+    if (used > cap) {  // a sizing bug in the library: stop before any kernel sees the pointer
+      fprintf(stderr, "dcsr: scratch arena overflow (%zu > %zu bytes)\n", used, cap);
+      abort();
+    }
+    return (T *)(base + off);
+  }
+  void release(cudaStream_t s) {
+    if (base) cudaFreeAsync(base, s);
+    base = nullptr;
+    cap = used = 0;
+  }
+};
+
+inline size_t arena_bytes(size_t n, size_t elem) { return align_up((int64_t)(n * elem), 256) + 256; }
+
+}  // namespace dcsr
+
+// The opaque handle.
+struct dcsr_matrix_s {
+  int32_t n_rows = 0, n_cols = 0, dtype = 0, pitch = 0;
+  dcsr_opts o{};
+  int64_t pool_cap = 0;
+  int32_t *row_sizes = nullptr;
+  int32_t *seg = nullptr;
+  int32_t *cols = nullptr;
+  void *vals = nullptr;
+  long long *stat = nullptr;
+  // SpMV row bins (handle-local; the reference used a global __constant__).
+  int32_t *bin_perm = nullptr;   // [n_rows] row ids grouped by class
+  int32_t *bin_info = nullptr;   // [32]: class offsets [0..8], unit offsets [16..24]
+  bool bins_valid = false;
+  dcsr::Arena scratch;
+  int device = 0;
+
+  template <typename V>
+  dcsr::Mat<V> view() const {
+    dcsr::Mat<V> m;
+    m.n_rows = n_rows;
+    m.n_cols = n_cols;
+    m.max_segs = o.max_segs;
+    m.pitch = pitch;
+    m.pool_cap = pool_cap;
+    m.row_sizes = row_sizes;
+    m.seg = seg;
+    m.cols = cols;
+    m.vals = (V *)vals;
+    m.stat = stat;
+    m.o = o;
+    return m;
+  }
+  size_t vsize() const { return dtype == DCSR_F64 ? 8 : 4; }
+};
+
+namespace dcsr {
+
+// ---------------------------------------------------------- warp helpers
+
+__device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
+
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
+  return v;
+}
+template <typename T>
+__device__ __forceinline__ T warp_min(T v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    T w = __shfl_xor_sync(FULL, v, o);
+    v = w < v ? w : v;
+  }
+  return v;
+}
+// Inclusive prefix sum within a warp.
+template <typename T>
+__device__ __forceinline__ T warp_incl_scan(T v) {
+  int l = lane_id();
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    T w = __shfl_up_sync(FULL, v, o);
+    if (l >= o) v += w;
+  }
+  return v;
+}
+
+// A row's linked segments (at most 8), read from the segment table.
+struct Chain {
+  int32_t st[8];
+  int32_t cp[8];
+  int ns;
+  int64_t total;
+  __device__ __forceinline__ int64_t phys(int64_t p) const {
+#pragma unroll 1
+    for (int i = 0; i < ns; i++) {
+      if (p < cp[i]) return (int64_t)st[i] + p;
+      p -= cp[i];
+    }
+    return -1;
+  }
+};
+
+template <typename V>
+__device__ __forceinline__ Chain load_chain(const Mat<V> &m, int32_t r) {
+  Chain c;
+  c.ns = 0;
+  c.total = 0;
+#pragma unroll 1
+  for (int l = 0; l < m.max_segs; l++) {
+    int2 p = *reinterpret_cast<const int2 *>(m.seg + (int64_t)l * m.pitch + 2 * (int64_t)r);
+    if (p.x < 0) break;
+    c.st[c.ns] = p.x;
+    c.cp[c.ns] = p.y - p.x;
+    c.total += p.y - p.x;
+    c.ns++;
+  }
+  return c;
+}
+
+// Persistent-grid size for a kernel: blocks resident across all SMs.
+int persistent_grid(const void *kernel, int block, size_t smem);
+int sm_count();
+
+// -------------------------------------------------------------- primitives
+// (scan.cu / radix.cu)
+
+// Exclusive scan of int64 values; out may alias in; *total (device) = sum.
+int scan_i64(const long long *in, long long *out, int64_t n, long long *total, Arena &ar, cudaStream_t s);
+size_t scan_scratch_bytes(int64_t n);
+
+// Stable LSD radix sort of (uint64 key, uint32 value) pairs on bits [0, bits).
+// Sorted output lands in (*keys, *vals) -- the pointers are swapped with the
+// tmp buffers as passes ping-pong.
+int radix_sort_pairs(unsigned long long **keys, unsigned **vals, unsigned long long **keys_tmp,
+                     unsigned **vals_tmp, int64_t n, int bits, Arena &ar, cudaStream_t s);
+size_t radix_scratch_bytes(int64_t n);
+
+inline int bits_for(int64_t n) {  // bits to represent values in [0, n)
+  int b = 1;
+  while (b < 62 && (int64_t(1) << b) < n) b++;
+  return b;
+}
+
+}  // namespace dcsr

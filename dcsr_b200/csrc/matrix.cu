@@ -1,0 +1,672 @@
+// matrix.cu -- DCSR handle lifecycle, CSR/COO/HYB -> DCSR loading, DCSR ->
+// CSR/COO export, compaction (defragmentation), pool growth, SpMV row bins,
+// the synchronous update repair policy and the status API.
+#include <cstring>
+#include <vector>
+
+#include "internal.cuh"
+
+namespace dcsr {
+
+enum { AUX_BAD_INDEX = 1, AUX_NONCANON = 4, AUX_BAD_ROWPTR = 8 };
+
+// ------------------------------------------------------------- kernels
+
+// caps[r] = policy_cap(len_r) with len_r from an int64 row pointer, caps[n] = 0.
+__global__ void k_caps_from_rp(const long long *rp, int32_t n, dcsr_opts o, long long *caps) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r <= n; r += stride)
+    caps[r] = r < n ? policy_cap(o, rp[r + 1] - rp[r]) : 0;
+}
+__global__ void k_caps_from_sizes(const int32_t *row_sizes, int32_t n, dcsr_opts o, long long *caps) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r <= n; r += stride)
+    caps[r] = r < n ? policy_cap(o, row_sizes[r]) : 0;
+}
+
+// Layer 0 = (off, off+cap), other layers cleared; row_sizes from lens (rp
+// diff) when rp != nullptr; pool top = offs[n].
+__global__ void k_layout(int32_t *seg, int32_t *row_sizes, int32_t n, int32_t pitch, int max_segs,
+                         const long long *offs, const long long *rp) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r <= n; r += stride) {
+    if (r == n) {
+      row_sizes[n] = (int32_t)offs[n];
+      continue;
+    }
+    *reinterpret_cast<int2 *>(seg + 2 * r) = make_int2((int32_t)offs[r], (int32_t)offs[r + 1]);
+    for (int l = 1; l < max_segs; l++) *reinterpret_cast<int2 *>(seg + (int64_t)l * pitch + 2 * r) = make_int2(-1, -1);
+    if (rp) row_sizes[r] = (int32_t)(rp[r + 1] - rp[r]);
+  }
+}
+
+// Copy CSR rows into their new layer-0 segments (warp per row, grid-stride).
+template <typename V>
+__global__ void k_copy_csr(int32_t n, const long long *offs, const long long *rp, const int32_t *cols,
+                           const V *vals, int32_t *pcols, V *pvals) {
+  const int lane = threadIdx.x & 31;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t r = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < n; r += nw) {
+    const int64_t s = rp[r], e = rp[r + 1], d = offs[r];
+    for (int64_t j = s + lane; j < e; j += 32) {
+      pcols[d + (j - s)] = cols[j];
+      pvals[d + (j - s)] = vals[j];
+    }
+  }
+}
+
+// CSR input check: row pointer monotone, columns in range, rows strictly
+// ascending (canonical); converts row_ptr to int64.
+__global__ void k_csr_check(const int32_t *row_ptr, const int32_t *cols, int32_t n, int32_t n_cols, long long *rp64,
+                            long long *stat) {
+  const int lane = threadIdx.x & 31;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  unsigned long long flags = 0;
+  for (int64_t r = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < n; r += nw) {
+    const int32_t s = row_ptr[r], e = row_ptr[r + 1];
+    if (lane == 0) {
+      rp64[r] = s;
+      if (r == n - 1) rp64[n] = e;
+      if (e < s || (r == 0 && s != 0)) flags |= AUX_BAD_ROWPTR;
+    }
+    if (e < s) continue;
+    for (int32_t j = s + lane; j < e; j += 32) {
+      const int32_t c = cols[j];
+      if (c < 0 || c >= n_cols) flags |= AUX_BAD_INDEX;
+      if (j > s && cols[j - 1] >= c) flags |= AUX_NONCANON;
+    }
+  }
+  flags = __reduce_or_sync(FULL, (unsigned)flags);
+  if (lane == 0 && flags) atomicOr((unsigned long long *)&stat[ST_AUX], flags);
+}
+
+__global__ void k_expand_rows(const long long *rp, int32_t n, int32_t *rows) {
+  const int lane = threadIdx.x & 31;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t r = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < n; r += nw)
+    for (int64_t j = rp[r] + lane; j < rp[r + 1]; j += 32) rows[j] = (int32_t)r;
+}
+
+__global__ void k_lens(const int32_t *row_sizes, int32_t n, long long *out) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r <= n; r += stride)
+    out[r] = r < n ? row_sizes[r] : 0;
+}
+
+// Export: warp per row follows the chain; writes row_ptr, (rows), cols, vals.
+template <typename V>
+__global__ void k_export(Mat<V> m, const long long *rp, int32_t *row_ptr, int32_t *rows, int32_t *cols, V *vals) {
+  const int lane = threadIdx.x & 31;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (gw == 0 && lane == 0 && row_ptr) row_ptr[m.n_rows] = (int32_t)rp[m.n_rows];
+  for (int64_t r = gw; r < m.n_rows; r += nw) {
+    const Chain ch = load_chain(m, (int32_t)r);
+    const int64_t L = m.row_sizes[r], d = rp[r];
+    if (lane == 0 && row_ptr) row_ptr[r] = (int32_t)d;
+    int64_t p = 0;
+    for (int s = 0; s < ch.ns && p < L; s++) {
+      const int64_t take = ch.cp[s] < L - p ? ch.cp[s] : L - p;
+      for (int64_t j = lane; j < take; j += 32) {
+        cols[d + p + j] = m.cols[ch.st[s] + j];
+        vals[d + p + j] = m.vals[ch.st[s] + j];
+        if (rows) rows[d + p + j] = (int32_t)r;
+      }
+      p += take;
+    }
+  }
+}
+
+// Compaction copy: each row's chain -> contiguous at offs[r] in the new pool.
+template <typename V>
+__global__ void k_compact_copy(Mat<V> m, const long long *offs, int32_t *ncols, V *nvals) {
+  const int lane = threadIdx.x & 31;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t r = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < m.n_rows; r += nw) {
+    const Chain ch = load_chain(m, (int32_t)r);
+    const int64_t L = m.row_sizes[r], d = offs[r];
+    int64_t p = 0;
+    for (int s = 0; s < ch.ns && p < L; s++) {
+      const int64_t take = ch.cp[s] < L - p ? ch.cp[s] : L - p;
+      for (int64_t j = lane; j < take; j += 32) {
+        ncols[d + p + j] = m.cols[ch.st[s] + j];
+        nvals[d + p + j] = m.vals[ch.st[s] + j];
+      }
+      p += take;
+    }
+  }
+}
+
+__global__ void k_sum_lens(const int32_t *row_sizes, int32_t n, long long *out) {
+  long long s = 0;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += stride) s += row_sizes[r];
+  s = warp_sum(s);
+  if ((threadIdx.x & 31) == 0 && s) atomicAdd((unsigned long long *)out, (unsigned long long)s);
+}
+
+// HYB -> COO: valid ELL slots (column-major, -1 padding) in (row, slot)
+// order, then the COO overflow in its given order.
+__global__ void k_ell_flags(const int32_t *ell_cols, int32_t n, int32_t width, int64_t pitch, long long *flag) {
+  const int64_t total = (int64_t)n * width;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += stride) {
+    const int64_t r = i / width, j = i % width;
+    flag[i] = ell_cols[j * pitch + r] >= 0 ? 1 : 0;
+  }
+}
+template <typename V>
+__global__ void k_ell_emit(const int32_t *ell_cols, const V *ell_vals, int32_t n, int32_t width, int64_t pitch,
+                           const long long *pos, int32_t *rows, int32_t *cols, V *vals) {
+  const int64_t total = (int64_t)n * width;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += stride) {
+    const int64_t r = i / width, j = i % width;
+    const int32_t c = ell_cols[j * pitch + r];
+    if (c < 0) continue;
+    rows[pos[i]] = (int32_t)r;
+    cols[pos[i]] = c;
+    vals[pos[i]] = ell_vals[j * pitch + r];
+  }
+}
+
+// Row bins: 7 length classes {<2,<4,<8,<16,<32,<512,>=512} (reference SetBins,
+// include/sparse_update.inl:1121-1150).
+__device__ __forceinline__ int row_class(int32_t len) {
+  return len < 2 ? 0 : len < 4 ? 1 : len < 8 ? 2 : len < 16 ? 3 : len < 32 ? 4 : len < 512 ? 5 : 6;
+}
+__global__ void k_bin_keys(const int32_t *row_sizes, int32_t n, unsigned long long *keys, unsigned *vals) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += stride) {
+    keys[r] = (unsigned long long)row_class(row_sizes[r]);
+    vals[r] = (unsigned)r;
+  }
+}
+// bin_info: [c] = class start (c = 0..7, [7] = n); [8 + s] = first unit of
+// processing slot s (slot 0 = class 6 ... slot 6 = class 0); [15] = units.
+__global__ void k_bin_info(const unsigned long long *keys, int32_t n, int32_t *info) {
+  __shared__ int32_t start[8];
+  const int c = threadIdx.x;
+  if (c < 8) {
+    int64_t lo = 0, hi = n;
+    while (lo < hi) {
+      int64_t mid = (lo + hi) >> 1;
+      if (keys[mid] < (unsigned long long)c) lo = mid + 1;
+      else hi = mid;
+    }
+    start[c] = c == 7 ? n : (int32_t)lo;
+  }
+  __syncthreads();
+  if (c == 0) {
+    int32_t u = 0;
+    for (int s = 0; s < 7; s++) {
+      const int cls = 6 - s;
+      const int32_t cnt = start[cls + 1] - start[cls];
+      const int32_t rows_per_unit = cls == 6 ? 1 : 256 >> cls;
+      info[8 + s] = u;
+      u += (cnt + rows_per_unit - 1) / rows_per_unit;
+    }
+    info[15] = u;
+    for (int k = 0; k < 8; k++) info[k] = start[k];
+  }
+}
+
+static int grid_for(int64_t n, int block) {
+  int64_t g = div_up(n, block);
+  int64_t cap = (int64_t)sm_count() * 16;
+  return (int)(g < 1 ? 1 : (g > cap ? cap : g));
+}
+
+// ------------------------------------------------------------ host side
+
+static int alloc_pool(dcsr_handle h, int64_t cap, int32_t **cols, void **vals, cudaStream_t s) {
+  if (cap < 1) cap = 1;
+  DCSR_CUDA(cudaMallocAsync((void **)cols, cap * sizeof(int32_t), s));
+  DCSR_CUDA(cudaMallocAsync(vals, cap * h->vsize(), s));
+  return DCSR_OK;
+}
+static void free_pool(dcsr_handle h, cudaStream_t s) {
+  if (h->cols) cudaFreeAsync(h->cols, s);
+  if (h->vals) cudaFreeAsync(h->vals, s);
+  h->cols = nullptr;
+  h->vals = nullptr;
+}
+
+size_t load_scratch_bytes(dcsr_handle h) { return arena_bytes(h->n_rows + 2, 8) + scan_scratch_bytes(h->n_rows + 1); }
+
+int load_from_csr64(dcsr_handle h, const long long *rp, const int32_t *cols, const void *vals, cudaStream_t s) {
+  Arena &ar = h->scratch;  // caller reserved load_scratch_bytes() beyond its own use
+  const int32_t n = h->n_rows;
+  long long *caps = ar.take<long long>(n + 2);
+  DCSR_LAUNCH(k_caps_from_rp, grid_for(n + 1, 256), 256, 0, s, rp, n, h->o, caps);
+  DCSR_TRY(scan_i64(caps, caps, n + 1, h->stat + ST_TOTAL, ar, s));
+  long long host[ST_WORDS];
+  DCSR_CUDA(cudaMemcpyAsync(host, h->stat, sizeof(host), cudaMemcpyDeviceToHost, s));
+  DCSR_CUDA(cudaStreamSynchronize(s));
+  if (host[ST_AUX] & AUX_BAD_INDEX) {
+    DCSR_CUDA(cudaMemsetAsync(h->stat + ST_AUX, 0, sizeof(long long), s));
+    return DCSR_BAD_INDEX;
+  }
+  const int64_t top = host[ST_TOTAL];
+  if (top > 0x7fffffffLL) return DCSR_OOM;
+  int64_t cap = pool_capacity(h->o, top);
+  if (cap > 0x7fffffffLL) cap = 0x7fffffffLL;
+  int32_t *nc;
+  void *nv;
+  DCSR_TRY(alloc_pool(h, cap, &nc, &nv, s));
+  free_pool(h, s);
+  h->cols = nc;
+  h->vals = nv;
+  h->pool_cap = cap;
+  DCSR_LAUNCH(k_layout, grid_for(n + 1, 256), 256, 0, s, h->seg, h->row_sizes, n, h->pitch, h->o.max_segs, caps, rp);
+  if (h->dtype == DCSR_F32)
+    DCSR_LAUNCH(k_copy_csr<float>, grid_for((int64_t)n * 32, 256), 256, 0, s, n, caps, rp, cols, (const float *)vals,
+                h->cols, (float *)h->vals);
+  else
+    DCSR_LAUNCH(k_copy_csr<double>, grid_for((int64_t)n * 32, 256), 256, 0, s, n, caps, rp, cols,
+                (const double *)vals, h->cols, (double *)h->vals);
+  h->bins_valid = false;
+  return DCSR_OK;
+}
+
+int reserve(dcsr_handle h, int64_t cap, cudaStream_t s) {
+  if (cap <= h->pool_cap && h->vals) return DCSR_OK;
+  if (cap > 0x7fffffffLL) return DCSR_OOM;
+  int32_t *nc;
+  void *nv;
+  DCSR_TRY(alloc_pool(h, cap, &nc, &nv, s));
+  if (h->vals && h->pool_cap > 0) {
+    DCSR_CUDA(cudaMemcpyAsync(nc, h->cols, h->pool_cap * sizeof(int32_t), cudaMemcpyDeviceToDevice, s));
+    DCSR_CUDA(cudaMemcpyAsync(nv, h->vals, h->pool_cap * h->vsize(), cudaMemcpyDeviceToDevice, s));
+  }
+  free_pool(h, s);
+  h->cols = nc;
+  h->vals = nv;
+  h->pool_cap = cap;
+  return DCSR_OK;
+}
+
+int compact(dcsr_handle h, cudaStream_t s) {
+  const int32_t n = h->n_rows;
+  Arena &ar = h->scratch;
+  DCSR_TRY(ar.reserve(arena_bytes(n + 2, 8) + scan_scratch_bytes(n + 1), s));
+  long long *caps = ar.take<long long>(n + 2);
+  DCSR_LAUNCH(k_caps_from_sizes, grid_for(n + 1, 256), 256, 0, s, h->row_sizes, n, h->o, caps);
+  DCSR_TRY(scan_i64(caps, caps, n + 1, h->stat + ST_TOTAL, ar, s));
+  long long top;
+  DCSR_CUDA(cudaMemcpyAsync(&top, h->stat + ST_TOTAL, sizeof(top), cudaMemcpyDeviceToHost, s));
+  DCSR_CUDA(cudaStreamSynchronize(s));
+  if (top > 0x7fffffffLL) return DCSR_OOM;
+  int64_t cap = pool_capacity(h->o, top);
+  if (cap < h->pool_cap) cap = h->pool_cap;
+  if (cap > 0x7fffffffLL) cap = 0x7fffffffLL;
+  int32_t *nc;
+  void *nv;
+  DCSR_TRY(alloc_pool(h, cap, &nc, &nv, s));
+  if (h->dtype == DCSR_F32)
+    DCSR_LAUNCH(k_compact_copy<float>, grid_for((int64_t)n * 32, 256), 256, 0, s, h->view<float>(), caps, nc,
+                (float *)nv);
+  else
+    DCSR_LAUNCH(k_compact_copy<double>, grid_for((int64_t)n * 32, 256), 256, 0, s, h->view<double>(), caps, nc,
+                (double *)nv);
+  DCSR_LAUNCH(k_layout, grid_for(n + 1, 256), 256, 0, s, h->seg, h->row_sizes, n, h->pitch, h->o.max_segs, caps,
+              (const long long *)nullptr);
+  free_pool(h, s);
+  h->cols = nc;
+  h->vals = nv;
+  h->pool_cap = cap;
+  h->bins_valid = false;
+  return DCSR_OK;
+}
+
+int bin_rows(dcsr_handle h, cudaStream_t s) {
+  const int32_t n = h->n_rows;
+  Arena &ar = h->scratch;
+  DCSR_TRY(ar.reserve(2 * arena_bytes(n + 1, 8) + arena_bytes(n + 1, 4) + radix_scratch_bytes(n), s));
+  unsigned long long *k0 = ar.take<unsigned long long>(n + 1), *k1 = ar.take<unsigned long long>(n + 1);
+  unsigned *v0 = ar.take<unsigned>(n + 1);
+  unsigned *v1 = (unsigned *)h->bin_perm;
+  if (n > 0) {
+    DCSR_LAUNCH(k_bin_keys, grid_for(n, 256), 256, 0, s, h->row_sizes, n, k0, v0);
+    if (n > 1) {
+      DCSR_TRY(radix_sort_pairs(&k0, &v0, &k1, &v1, n, 3, ar, s));  // one 8-bit pass: result in k1/bin_perm
+    } else {
+      DCSR_CUDA(cudaMemcpyAsync(h->bin_perm, v0, sizeof(unsigned), cudaMemcpyDeviceToDevice, s));
+    }
+  }
+  DCSR_LAUNCH(k_bin_info, 1, 32, 0, s, k0, n, h->bin_info);
+  h->bins_valid = true;
+  return DCSR_OK;
+}
+
+static int read_stat(dcsr_handle h, cudaStream_t s, long long *host) {
+  DCSR_CUDA(cudaMemcpyAsync(host, h->stat, sizeof(long long) * ST_WORDS, cudaMemcpyDeviceToHost, s));
+  DCSR_CUDA(cudaStreamSynchronize(s));
+  return DCSR_OK;
+}
+static int clear_status(dcsr_handle h, cudaStream_t s) {
+  DCSR_CUDA(cudaMemsetAsync(h->stat + ST_STATUS, 0, sizeof(long long), s));
+  return DCSR_OK;
+}
+
+}  // namespace dcsr
+
+using namespace dcsr;
+
+// ------------------------------------------------------------------ C ABI
+
+extern "C" {
+
+void dcsr_default_opts(dcsr_opts *o, int32_t mode) {
+  if (!o) return;
+  o->max_segs = 4;
+  o->mode = mode;
+  o->alpha = 4;
+  o->spare_x16 = 16;
+  o->min_spare = 4096;
+  o->reloc_min = 2048;
+  if (mode == DCSR_APPEND) {
+    o->factor_x16 = 16;
+    o->min_cap = 0;
+    o->align = 1;
+  } else {
+    o->factor_x16 = 32;
+    o->min_cap = 4;
+    o->align = 4;
+  }
+}
+
+int dcsr_create(dcsr_handle *out, int32_t n_rows, int32_t n_cols, int32_t dtype, const dcsr_opts *opts) {
+  if (!out || n_rows < 0 || n_cols < 0 || (dtype != DCSR_F32 && dtype != DCSR_F64)) return DCSR_BAD_ARG;
+  dcsr_opts o;
+  if (opts) o = *opts;
+  else dcsr_default_opts(&o, DCSR_MERGE);
+  if (o.max_segs < 1 || o.max_segs > 8 || o.factor_x16 < 16 || o.align < 1 || (o.align & (o.align - 1)) ||
+      o.min_cap < 0 || o.alpha < 0 || o.spare_x16 < 0 || o.min_spare < 0 || (o.mode != DCSR_MERGE && o.mode != DCSR_APPEND))
+    return DCSR_BAD_ARG;
+  dcsr_matrix_s *h = new dcsr_matrix_s;
+  h->n_rows = n_rows;
+  h->n_cols = n_cols;
+  h->dtype = dtype;
+  h->o = o;
+  h->pitch = (int32_t)align_up(2 * (int64_t)n_rows, 32);
+  cudaGetDevice(&h->device);
+  const size_t nseg = (size_t)h->pitch * o.max_segs;
+  int st = DCSR_OK;
+  if (cudaMalloc((void **)&h->row_sizes, sizeof(int32_t) * (n_rows + 1)) != cudaSuccess ||
+      cudaMalloc((void **)&h->seg, sizeof(int32_t) * (nseg ? nseg : 1)) != cudaSuccess ||
+      cudaMalloc((void **)&h->stat, sizeof(long long) * ST_WORDS) != cudaSuccess ||
+      cudaMalloc((void **)&h->bin_perm, sizeof(int32_t) * (n_rows + 1)) != cudaSuccess ||
+      cudaMalloc((void **)&h->bin_info, sizeof(int32_t) * 32) != cudaSuccess)
+    st = DCSR_OOM;
+  if (st == DCSR_OK) {
+    cudaMemset(h->row_sizes, 0, sizeof(int32_t) * (n_rows + 1));
+    cudaMemset(h->seg, 0xff, sizeof(int32_t) * (nseg ? nseg : 1));
+    cudaMemset(h->stat, 0, sizeof(long long) * ST_WORDS);
+    cudaMemset(h->bin_info, 0, sizeof(int32_t) * 32);
+    st = reserve(h, pool_capacity(o, 0), 0);
+    if (cudaDeviceSynchronize() != cudaSuccess) st = DCSR_CUDA_ERROR;
+  }
+  if (st != DCSR_OK) {
+    dcsr_destroy(h);
+    return st;
+  }
+  *out = h;
+  return DCSR_OK;
+}
+
+int dcsr_destroy(dcsr_handle h) {
+  if (!h) return DCSR_BAD_ARG;
+  cudaDeviceSynchronize();
+  h->scratch.release(0);
+  free_pool(h, 0);
+  cudaFree(h->row_sizes);
+  cudaFree(h->seg);
+  cudaFree(h->stat);
+  cudaFree(h->bin_perm);
+  cudaFree(h->bin_info);
+  cudaDeviceSynchronize();
+  delete h;
+  return DCSR_OK;
+}
+
+int dcsr_info(dcsr_handle h, dcsr_info_t *info) {
+  if (!h || !info) return DCSR_BAD_ARG;
+  info->n_rows = h->n_rows;
+  info->n_cols = h->n_cols;
+  info->dtype = h->dtype;
+  info->pitch = h->pitch;
+  info->pool_cap = h->pool_cap;
+  info->row_sizes = h->row_sizes;
+  info->seg = h->seg;
+  info->cols = h->cols;
+  info->vals = h->vals;
+  info->opts = h->o;
+  return DCSR_OK;
+}
+
+int dcsr_get_layout(dcsr_handle h, int32_t *row_sizes, int32_t *seg, void *stream) {
+  if (!h) return DCSR_BAD_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  if (row_sizes)
+    DCSR_CUDA(cudaMemcpyAsync(row_sizes, h->row_sizes, sizeof(int32_t) * (h->n_rows + 1), cudaMemcpyDefault, s));
+  if (seg)
+    DCSR_CUDA(cudaMemcpyAsync(seg, h->seg, sizeof(int32_t) * (size_t)h->pitch * h->o.max_segs, cudaMemcpyDefault, s));
+  DCSR_CUDA(cudaStreamSynchronize(s));
+  return DCSR_OK;
+}
+
+int dcsr_from_csr(dcsr_handle h, const int32_t *row_ptr, const int32_t *cols, const void *vals, int64_t nnz,
+                  void *stream) {
+  if (!h || !row_ptr || (nnz > 0 && (!cols || !vals)) || nnz < 0 || nnz > 0x7fffffffLL) return DCSR_BAD_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  const int32_t n = h->n_rows;
+  Arena &ar = h->scratch;
+  DCSR_TRY(ar.reserve(arena_bytes(n + 2, 8) + load_scratch_bytes(h), s));
+  long long *rp = ar.take<long long>(n + 2);
+  DCSR_CUDA(cudaMemsetAsync(h->stat + ST_AUX, 0, sizeof(long long), s));
+  if (n > 0) DCSR_LAUNCH(k_csr_check, grid_for((int64_t)n * 32, 256), 256, 0, s, row_ptr, cols, n, h->n_cols, rp, h->stat);
+  else DCSR_CUDA(cudaMemsetAsync(rp, 0, sizeof(long long), s));
+  long long host[ST_WORDS], total = 0;
+  DCSR_CUDA(cudaMemcpyAsync(&total, rp + n, sizeof(total), cudaMemcpyDeviceToHost, s));
+  DCSR_TRY(read_stat(h, s, host));
+  const long long aux = host[ST_AUX];
+  if (total != nnz) {
+    DCSR_CUDA(cudaMemsetAsync(h->stat + ST_AUX, 0, sizeof(long long), s));
+    return DCSR_BAD_ARG;
+  }
+  DCSR_CUDA(cudaMemsetAsync(h->stat + ST_AUX, 0, sizeof(long long), s));
+  if (aux & AUX_BAD_ROWPTR) return DCSR_BAD_ARG;
+  if (aux & AUX_BAD_INDEX) return DCSR_BAD_INDEX;
+  if ((aux & AUX_NONCANON) && h->o.mode == DCSR_MERGE) {
+    // canonicalise through the COO path (sort by (row,col), sum duplicates)
+    DCSR_TRY(ar.reserve(arena_bytes(n + 2, 8) + arena_bytes(nnz + 1, 4) + coo_to_csr_scratch(h, nnz) +
+                            load_scratch_bytes(h), s));
+    long long *rp2 = ar.take<long long>(n + 2);
+    int32_t *rows = ar.take<int32_t>(nnz + 1);
+    DCSR_LAUNCH(k_csr_check, grid_for((int64_t)n * 32, 256), 256, 0, s, row_ptr, cols, n, h->n_cols, rp2, h->stat);
+    DCSR_LAUNCH(k_expand_rows, grid_for((int64_t)n * 32, 256), 256, 0, s, rp2, n, rows);
+    DCSR_CUDA(cudaMemsetAsync(h->stat + ST_AUX, 0, sizeof(long long), s));
+    long long *crp;
+    int32_t *cc;
+    void *cv;
+    DCSR_TRY(coo_to_csr64(h, rows, cols, vals, nnz, true, ar, &crp, &cc, &cv, nullptr, s));
+    return load_from_csr64(h, crp, cc, cv, s);
+  }
+  return load_from_csr64(h, rp, cols, vals, s);
+}
+
+int dcsr_from_coo(dcsr_handle h, const int32_t *rows, const int32_t *cols, const void *vals, int64_t nnz,
+                  void *stream) {
+  if (!h || nnz < 0 || nnz > 0x7fffffffLL || (nnz > 0 && (!rows || !cols || !vals))) return DCSR_BAD_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  Arena &ar = h->scratch;
+  DCSR_TRY(ar.reserve(coo_to_csr_scratch(h, nnz) + load_scratch_bytes(h), s));
+  DCSR_CUDA(cudaMemsetAsync(h->stat + ST_AUX, 0, sizeof(long long), s));
+  long long *rp;
+  int32_t *cc;
+  void *cv;
+  DCSR_TRY(coo_to_csr64(h, rows, cols, vals, nnz, h->o.mode == DCSR_MERGE, ar, &rp, &cc, &cv, nullptr, s));
+  return load_from_csr64(h, rp, cc, cv, s);
+}
+
+int dcsr_from_hyb(dcsr_handle h, const int32_t *ell_cols, const void *ell_vals, int32_t ell_width, int64_t ell_pitch,
+                  const int32_t *coo_rows, const int32_t *coo_cols, const void *coo_vals, int64_t coo_nnz,
+                  void *stream) {
+  if (!h || ell_width < 0 || coo_nnz < 0 || (ell_width > 0 && (!ell_cols || !ell_vals || ell_pitch < h->n_rows)))
+    return DCSR_BAD_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  const int64_t slots = (int64_t)h->n_rows * ell_width;
+  const int64_t T = slots + coo_nnz;
+  if (T > 0x7fffffffLL) return DCSR_BAD_ARG;
+  // stage 1: ELL -> COO triples (separate scratch so the COO path can reserve its own)
+  int32_t *rows = nullptr, *cols = nullptr;
+  void *vals = nullptr;
+  long long *flag = nullptr;
+  DCSR_CUDA(cudaMallocAsync((void **)&rows, sizeof(int32_t) * (T + 1), s));
+  DCSR_CUDA(cudaMallocAsync((void **)&cols, sizeof(int32_t) * (T + 1), s));
+  DCSR_CUDA(cudaMallocAsync(&vals, h->vsize() * (T + 1), s));
+  DCSR_CUDA(cudaMallocAsync((void **)&flag, sizeof(long long) * (slots + 1), s));
+  Arena tmp;
+  DCSR_TRY(tmp.reserve(scan_scratch_bytes(slots + 1), s));
+  long long nell = 0;
+  if (slots > 0) {
+    DCSR_LAUNCH(k_ell_flags, grid_for(slots, 256), 256, 0, s, ell_cols, h->n_rows, ell_width, ell_pitch, flag);
+    DCSR_TRY(scan_i64(flag, flag, slots, h->stat + ST_TOTAL, tmp, s));
+    if (h->dtype == DCSR_F32)
+      DCSR_LAUNCH(k_ell_emit<float>, grid_for(slots, 256), 256, 0, s, ell_cols, (const float *)ell_vals, h->n_rows,
+                  ell_width, ell_pitch, flag, rows, cols, (float *)vals);
+    else
+      DCSR_LAUNCH(k_ell_emit<double>, grid_for(slots, 256), 256, 0, s, ell_cols, (const double *)ell_vals, h->n_rows,
+                  ell_width, ell_pitch, flag, rows, cols, (double *)vals);
+    DCSR_CUDA(cudaMemcpyAsync(&nell, h->stat + ST_TOTAL, sizeof(nell), cudaMemcpyDeviceToHost, s));
+    DCSR_CUDA(cudaStreamSynchronize(s));
+  }
+  if (coo_nnz > 0) {
+    DCSR_CUDA(cudaMemcpyAsync(rows + nell, coo_rows, sizeof(int32_t) * coo_nnz, cudaMemcpyDeviceToDevice, s));
+    DCSR_CUDA(cudaMemcpyAsync(cols + nell, coo_cols, sizeof(int32_t) * coo_nnz, cudaMemcpyDeviceToDevice, s));
+    DCSR_CUDA(cudaMemcpyAsync((char *)vals + nell * h->vsize(), coo_vals, h->vsize() * coo_nnz,
+                              cudaMemcpyDeviceToDevice, s));
+  }
+  int st = dcsr_from_coo(h, rows, cols, vals, nell + coo_nnz, stream);
+  tmp.release(s);
+  cudaFreeAsync(rows, s);
+  cudaFreeAsync(cols, s);
+  cudaFreeAsync(vals, s);
+  cudaFreeAsync(flag, s);
+  return st;
+}
+
+int dcsr_nnz(dcsr_handle h, int64_t *nnz, void *stream) {
+  if (!h || !nnz) return DCSR_BAD_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  DCSR_CUDA(cudaMemsetAsync(h->stat + ST_AUX + 1, 0, sizeof(long long), s));
+  if (h->n_rows > 0)
+    DCSR_LAUNCH(k_sum_lens, grid_for(h->n_rows, 256), 256, 0, s, h->row_sizes, h->n_rows, h->stat + ST_AUX + 1);
+  long long v = 0;
+  DCSR_CUDA(cudaMemcpyAsync(&v, h->stat + ST_AUX + 1, sizeof(v), cudaMemcpyDeviceToHost, s));
+  DCSR_CUDA(cudaStreamSynchronize(s));
+  *nnz = v;
+  return DCSR_OK;
+}
+
+static int export_impl(dcsr_handle h, int32_t *row_ptr, int32_t *rows, int32_t *cols, void *vals, cudaStream_t s) {
+  const int32_t n = h->n_rows;
+  Arena &ar = h->scratch;
+  DCSR_TRY(ar.reserve(arena_bytes(n + 2, 8) + scan_scratch_bytes(n + 1), s));
+  long long *rp = ar.take<long long>(n + 2);
+  DCSR_LAUNCH(k_lens, grid_for(n + 1, 256), 256, 0, s, h->row_sizes, n, rp);
+  DCSR_TRY(scan_i64(rp, rp, n + 1, nullptr, ar, s));
+  const int g = grid_for((int64_t)(n > 0 ? n : 1) * 32, 256);
+  if (h->dtype == DCSR_F32)
+    DCSR_LAUNCH(k_export<float>, g, 256, 0, s, h->view<float>(), rp, row_ptr, rows, cols, (float *)vals);
+  else
+    DCSR_LAUNCH(k_export<double>, g, 256, 0, s, h->view<double>(), rp, row_ptr, rows, cols, (double *)vals);
+  return DCSR_OK;
+}
+
+int dcsr_to_csr(dcsr_handle h, int32_t *row_ptr, int32_t *cols, void *vals, void *stream) {
+  if (!h || !row_ptr) return DCSR_BAD_ARG;
+  return export_impl(h, row_ptr, nullptr, cols, vals, (cudaStream_t)stream);
+}
+
+int dcsr_to_coo(dcsr_handle h, int32_t *rows, int32_t *cols, void *vals, void *stream) {
+  if (!h) return DCSR_BAD_ARG;
+  return export_impl(h, nullptr, rows, cols, vals, (cudaStream_t)stream);
+}
+
+int dcsr_update(dcsr_handle h, const int32_t *rows, const int32_t *cols, const void *vals, int64_t nnz, void *stream) {
+  if (!h || nnz < 0 || (nnz > 0 && (!rows || !cols || !vals))) return DCSR_BAD_ARG;
+  return update_async(h, rows, cols, vals, nnz, (cudaStream_t)stream);
+}
+
+int dcsr_update_sync(dcsr_handle h, const int32_t *rows, const int32_t *cols, const void *vals, int64_t nnz,
+                     void *stream) {
+  if (!h || nnz < 0 || (nnz > 0 && (!rows || !cols || !vals))) return DCSR_BAD_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  long long host[ST_WORDS];
+  DCSR_TRY(clear_status(h, s));
+  DCSR_TRY(update_async(h, rows, cols, vals, nnz, s));
+  DCSR_TRY(read_stat(h, s, host));
+  int st = (int)host[ST_STATUS];
+  if (st == DCSR_POOL_EXHAUSTED || st == DCSR_LAYER_OVERFLOW) {
+    DCSR_TRY(clear_status(h, s));
+    DCSR_TRY(compact(h, s));
+    DCSR_TRY(update_async(h, rows, cols, vals, nnz, s));
+    DCSR_TRY(read_stat(h, s, host));
+    st = (int)host[ST_STATUS];
+    if (st == DCSR_POOL_EXHAUSTED) {
+      DCSR_TRY(clear_status(h, s));
+      DCSR_TRY(reserve(h, pool_capacity(h->o, host[ST_NEED]), s));
+      DCSR_TRY(update_async(h, rows, cols, vals, nnz, s));
+      DCSR_TRY(read_stat(h, s, host));
+      st = (int)host[ST_STATUS];
+    }
+  }
+  DCSR_TRY(clear_status(h, s));
+  return st;
+}
+
+int dcsr_get_status(dcsr_handle h, void *stream, int32_t *status) {
+  if (!h || !status) return DCSR_BAD_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  long long host[ST_WORDS];
+  DCSR_TRY(read_stat(h, s, host));
+  *status = (int32_t)host[ST_STATUS];
+  return clear_status(h, s);
+}
+
+int dcsr_compact(dcsr_handle h, void *stream) {
+  if (!h) return DCSR_BAD_ARG;
+  return compact(h, (cudaStream_t)stream);
+}
+
+int dcsr_reserve(dcsr_handle h, int64_t pool_cap, void *stream) {
+  if (!h || pool_cap < 0) return DCSR_BAD_ARG;
+  return reserve(h, pool_cap, (cudaStream_t)stream);
+}
+
+int dcsr_bin_rows(dcsr_handle h, void *stream) {
+  if (!h) return DCSR_BAD_ARG;
+  return bin_rows(h, (cudaStream_t)stream);
+}
+
+const char *dcsr_status_string(int st) {
+  switch (st) {
+    case DCSR_OK: return "OK";
+    case DCSR_POOL_EXHAUSTED: return "POOL_EXHAUSTED";
+    case DCSR_LAYER_OVERFLOW: return "LAYER_OVERFLOW";
+    case DCSR_BAD_INDEX: return "BAD_INDEX";
+    case DCSR_OOM: return "OOM";
+    case DCSR_BAD_ARG: return "BAD_ARG";
+    case DCSR_TIMEOUT: return "TIMEOUT";
+    case DCSR_CUDA_ERROR: return "CUDA_ERROR";
+    case DCSR_NOT_SUPPORTED: return "NOT_SUPPORTED";
+    default: return "UNKNOWN";
+  }
+}
+
+uint64_t dcsr_launch_count(void) { return g_launches.load(); }
+const char *dcsr_version(void) { return "dcsr_b200 0.1 (sm_100a)"; }
+
+}  // extern "C"

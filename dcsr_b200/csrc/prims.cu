@@ -1,0 +1,327 @@
+// prims.cu -- device-wide primitives: exclusive scan, stable LSD radix sort of
+// (key, value) pairs, and the public segmented primitives
+// (count_sorted_indices, reduce_by_key).  All hand-written for sm_100a.
+#include <algorithm>
+
+#include "common.cuh"
+
+namespace dcsr {
+
+std::atomic<uint64_t> g_launches{0};
+
+int sm_count() {
+  static int n = 0;
+  if (!n) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    if (n <= 0) n = 148;
+  }
+  return n;
+}
+
+int persistent_grid(const void *kernel, int block, size_t smem) {
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, block, smem) != cudaSuccess || per_sm < 1)
+    per_sm = 1;
+  return per_sm * sm_count();
+}
+
+// ------------------------------------------------------------------ scan
+
+constexpr int SCAN_THREADS = 256;
+constexpr int SCAN_ITEMS = 8;
+constexpr int SCAN_TILE = SCAN_THREADS * SCAN_ITEMS;
+
+// Block-wide exclusive scan of one value per thread; returns the block total.
+template <typename T>
+__device__ __forceinline__ T block_excl_scan(T v, T *total) {
+  __shared__ T wsum[33];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  T inc = warp_incl_scan(v);
+  if (lane == 31) wsum[warp] = inc;
+  __syncthreads();
+  if (warp == 0) {
+    T w = lane < nw ? wsum[lane] : T(0);
+    T wi = warp_incl_scan(w);
+    if (lane < nw) wsum[lane] = wi - w;
+    if (lane == nw - 1) wsum[32] = wi;
+  }
+  __syncthreads();
+  T out = inc - v + wsum[warp];
+  *total = wsum[32];
+  __syncthreads();
+  return out;
+}
+
+__global__ void k_scan_reduce(const long long *in, int64_t n, long long *partial) {
+  const int64_t base = (int64_t)blockIdx.x * SCAN_TILE;
+  long long s = 0;
+#pragma unroll
+  for (int j = 0; j < SCAN_ITEMS; j++) {
+    int64_t i = base + j * SCAN_THREADS + threadIdx.x;
+    if (i < n) s += in[i];
+  }
+  s = warp_sum(s);
+  __shared__ long long ws[SCAN_THREADS / 32];
+  if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    long long t = 0;
+    for (int w = 0; w < SCAN_THREADS / 32; w++) t += ws[w];
+    partial[blockIdx.x] = t;
+  }
+}
+
+// Single block: exclusive scan of the tile partials in place; total -> *total.
+__global__ void k_scan_partials(long long *partial, int64_t ntiles, long long *total) {
+  long long carry = 0;
+  for (int64_t b = 0; b < ntiles; b += blockDim.x) {
+    int64_t i = b + threadIdx.x;
+    long long v = i < ntiles ? partial[i] : 0;
+    long long bt;
+    long long ex = block_excl_scan(v, &bt);
+    if (i < ntiles) partial[i] = ex + carry;
+    carry += bt;
+  }
+  if (threadIdx.x == 0 && total) *total = carry;
+}
+
+__global__ void k_scan_down(const long long *in, long long *out, int64_t n, const long long *partial) {
+  __shared__ long long tile[SCAN_TILE];
+  const int64_t base = (int64_t)blockIdx.x * SCAN_TILE;
+#pragma unroll
+  for (int j = 0; j < SCAN_ITEMS; j++) {
+    int64_t i = base + j * SCAN_THREADS + threadIdx.x;
+    tile[j * SCAN_THREADS + threadIdx.x] = i < n ? in[i] : 0;
+  }
+  __syncthreads();
+  long long loc[SCAN_ITEMS];
+  long long s = 0;
+#pragma unroll
+  for (int j = 0; j < SCAN_ITEMS; j++) {
+    loc[j] = tile[threadIdx.x * SCAN_ITEMS + j];
+    s += loc[j];
+  }
+  long long bt;
+  long long ex = block_excl_scan(s, &bt) + partial[blockIdx.x];
+#pragma unroll
+  for (int j = 0; j < SCAN_ITEMS; j++) {
+    tile[threadIdx.x * SCAN_ITEMS + j] = ex;
+    ex += loc[j];
+  }
+  __syncthreads();
+#pragma unroll
+  for (int j = 0; j < SCAN_ITEMS; j++) {
+    int64_t i = base + j * SCAN_THREADS + threadIdx.x;
+    if (i < n) out[i] = tile[j * SCAN_THREADS + threadIdx.x];
+  }
+}
+
+size_t scan_scratch_bytes(int64_t n) { return arena_bytes(div_up(n, SCAN_TILE) + 1, 8); }
+
+int scan_i64(const long long *in, long long *out, int64_t n, long long *total, Arena &ar, cudaStream_t s) {
+  if (n <= 0) {
+    if (total) DCSR_CUDA(cudaMemsetAsync(total, 0, sizeof(long long), s));
+    return DCSR_OK;
+  }
+  int64_t nt = div_up(n, SCAN_TILE);
+  const size_t mark = ar.used;  // partials are stream-ordered scratch: released on return
+  long long *partial = ar.take<long long>(nt + 1);
+  DCSR_LAUNCH(k_scan_reduce, (unsigned)nt, SCAN_THREADS, 0, s, in, n, partial);
+  DCSR_LAUNCH(k_scan_partials, 1, 1024, 0, s, partial, nt, total);
+  DCSR_LAUNCH(k_scan_down, (unsigned)nt, SCAN_THREADS, 0, s, in, out, n, partial);
+  ar.used = mark;
+  return DCSR_OK;
+}
+
+// ------------------------------------------------------------ radix sort
+//
+// Stable LSD radix sort, 8-bit digits.  Per pass: (1) per-tile digit
+// histograms, (2) exclusive scan over the digit-major histogram table, (3) a
+// stable scatter: each warp ranks its 512 consecutive items with match_any
+// (ties keep input order), warps are ordered by a per-digit prefix across the
+// block, and the block's global digit offsets come from the scanned table.
+
+constexpr int RS_THREADS = 256;
+constexpr int RS_WARPS = RS_THREADS / 32;
+constexpr int RS_ITEMS = 16;  // per lane
+constexpr int RS_TILE = RS_THREADS * RS_ITEMS;
+constexpr int RS_BINS = 256;
+
+__device__ __forceinline__ unsigned lanemask_lt() {
+  unsigned m;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+
+__global__ void __launch_bounds__(RS_THREADS) k_radix_hist(const unsigned long long *keys, int64_t n, int shift,
+                                                            long long *ghist, int64_t ntiles) {
+  __shared__ unsigned h[RS_BINS];
+  h[threadIdx.x] = 0;
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int64_t base = (int64_t)blockIdx.x * RS_TILE + (int64_t)warp * (32 * RS_ITEMS);
+#pragma unroll 4
+  for (int j = 0; j < RS_ITEMS; j++) {
+    int64_t i = base + j * 32 + lane;
+    unsigned d = i < n ? (unsigned)((keys[i] >> shift) & 0xff) : 0x100u;
+    unsigned peers = __match_any_sync(FULL, d);
+    if (d < 0x100u && (__ffs(peers) - 1) == lane) atomicAdd(&h[d], (unsigned)__popc(peers));
+  }
+  __syncthreads();
+  ghist[(int64_t)threadIdx.x * ntiles + blockIdx.x] = h[threadIdx.x];
+}
+
+__global__ void __launch_bounds__(RS_THREADS) k_radix_scatter(const unsigned long long *keys, const unsigned *vals,
+                                                               unsigned long long *keys_out, unsigned *vals_out,
+                                                               int64_t n, int shift, const long long *goff,
+                                                               int64_t ntiles) {
+  __shared__ unsigned wcnt[RS_WARPS][RS_BINS];
+  __shared__ long long boff[RS_BINS];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int w = 0; w < RS_WARPS; w++) wcnt[w][threadIdx.x] = 0;
+  boff[threadIdx.x] = goff[(int64_t)threadIdx.x * ntiles + blockIdx.x];
+  __syncthreads();
+  const int64_t base = (int64_t)blockIdx.x * RS_TILE + (int64_t)warp * (32 * RS_ITEMS);
+  unsigned long long k[RS_ITEMS];
+  unsigned rank[RS_ITEMS];
+  const unsigned lt = lanemask_lt();
+#pragma unroll
+  for (int j = 0; j < RS_ITEMS; j++) {
+    int64_t i = base + j * 32 + lane;
+    k[j] = i < n ? keys[i] : ~0ull;
+    unsigned d = i < n ? (unsigned)((k[j] >> shift) & 0xff) : 0x100u;
+    unsigned peers = __match_any_sync(FULL, d);
+    unsigned pre = d < 0x100u ? wcnt[warp][d] : 0u;
+    rank[j] = pre + __popc(peers & lt);
+    __syncwarp();
+    if (d < 0x100u && (__ffs(peers) - 1) == lane) wcnt[warp][d] = pre + __popc(peers);
+    __syncwarp();
+  }
+  __syncthreads();
+  {  // exclusive prefix across warps per digit
+    unsigned run = 0;
+    for (int w = 0; w < RS_WARPS; w++) {
+      unsigned t = wcnt[w][threadIdx.x];
+      wcnt[w][threadIdx.x] = run;
+      run += t;
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int j = 0; j < RS_ITEMS; j++) {
+    int64_t i = base + j * 32 + lane;
+    if (i < n) {
+      unsigned d = (unsigned)((k[j] >> shift) & 0xff);
+      int64_t pos = boff[d] + wcnt[warp][d] + rank[j];
+      keys_out[pos] = k[j];
+      vals_out[pos] = vals[i];
+    }
+  }
+}
+
+size_t radix_scratch_bytes(int64_t n) {
+  int64_t nt = div_up(n, RS_TILE);
+  return arena_bytes(nt * RS_BINS, 8) + scan_scratch_bytes(nt * RS_BINS);
+}
+
+int radix_sort_pairs(unsigned long long **keys, unsigned **vals, unsigned long long **keys_tmp,
+                     unsigned **vals_tmp, int64_t n, int bits, Arena &ar, cudaStream_t s) {
+  if (n <= 1) return DCSR_OK;
+  int64_t nt = div_up(n, RS_TILE);
+  size_t mark = ar.used;
+  long long *hist = ar.take<long long>(nt * RS_BINS);
+  size_t mark2 = ar.used;
+  for (int shift = 0; shift < bits; shift += 8) {
+    DCSR_LAUNCH(k_radix_hist, (unsigned)nt, RS_THREADS, 0, s, *keys, n, shift, hist, nt);
+    ar.used = mark2;
+    DCSR_TRY(scan_i64(hist, hist, nt * RS_BINS, nullptr, ar, s));
+    DCSR_LAUNCH(k_radix_scatter, (unsigned)nt, RS_THREADS, 0, s, *keys, *vals, *keys_tmp, *vals_tmp, n, shift,
+                hist, nt);
+    unsigned long long *tk = *keys;
+    *keys = *keys_tmp;
+    *keys_tmp = tk;
+    unsigned *tv = *vals;
+    *vals = *vals_tmp;
+    *vals_tmp = tv;
+  }
+  ar.used = mark;
+  return DCSR_OK;
+}
+
+// ------------------------------------------------- public segmented ops
+
+// X[I[n]] += run length, one atomic per run (runs found with warp ballots).
+__global__ void k_count_sorted(const int32_t *I, int64_t n, int32_t *X) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < n; base += stride) {
+    int64_t i = base + threadIdx.x;
+    int32_t key = i < n ? I[i] : INT32_MIN;
+    int32_t prev = __shfl_up_sync(FULL, key, 1);
+    const int lane = threadIdx.x & 31;
+    if (lane == 0) prev = (i > 0 && i < n) ? I[i - 1] : INT32_MIN;
+    bool head = i < n && (key != prev || lane == 0);
+    unsigned hm = __ballot_sync(FULL, head);
+    unsigned valid = __ballot_sync(FULL, i < n);
+    if (head) {
+      unsigned later = hm & ~((2u << lane) - 1u);
+      int end = later ? (__ffs(later) - 1) : (32 - __clz(valid));
+      atomicAdd(&X[key], end - lane);
+    }
+  }
+}
+
+// Reduce-by-key: heads flagged, head positions compacted by scan, then each
+// head sums its run left to right (deterministic order).
+__global__ void k_rbk_flags(const int32_t *keys, int64_t n, long long *flag) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) flag[i] = (i == 0 || keys[i] != keys[i - 1]) ? 1 : 0;
+}
+template <typename V>
+__global__ void k_rbk_emit(const int32_t *keys, const V *vals, int64_t n, const long long *pos,
+                           int32_t *keys_out, V *vals_out) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  if (i > 0 && keys[i] == keys[i - 1]) return;
+  V acc = vals[i];
+  for (int64_t j = i + 1; j < n && keys[j] == keys[i]; j++) acc = acc + vals[j];
+  keys_out[pos[i]] = keys[i];
+  vals_out[pos[i]] = acc;
+}
+
+}  // namespace dcsr
+
+using namespace dcsr;
+
+extern "C" int dcsr_count_sorted_indices(const int32_t *I, int64_t n, int32_t *X, void *stream) {
+  if (n < 0 || (n > 0 && (!I || !X))) return DCSR_BAD_ARG;
+  if (n == 0) return DCSR_OK;
+  cudaStream_t s = (cudaStream_t)stream;
+  int grid = (int)std::min<int64_t>(div_up(n, 256), (int64_t)sm_count() * 8);
+  DCSR_LAUNCH(k_count_sorted, grid, 256, 0, s, I, n, X);
+  return DCSR_OK;
+}
+
+extern "C" int dcsr_reduce_by_key(const int32_t *keys, const void *vals, int64_t n, int32_t dtype, int32_t *keys_out,
+                                  void *vals_out, int64_t *n_out, void *stream) {
+  if (n < 0 || (dtype != DCSR_F32 && dtype != DCSR_F64)) return DCSR_BAD_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  if (n == 0) {
+    if (n_out) DCSR_CUDA(cudaMemsetAsync(n_out, 0, sizeof(int64_t), s));
+    return DCSR_OK;
+  }
+  Arena ar;
+  DCSR_TRY(ar.reserve(arena_bytes(n, 8) + scan_scratch_bytes(n), s));
+  long long *pos = ar.take<long long>(n);
+  unsigned g = (unsigned)div_up(n, 256);
+  DCSR_LAUNCH(k_rbk_flags, g, 256, 0, s, keys, n, pos);
+  DCSR_TRY(scan_i64(pos, pos, n, (long long *)n_out, ar, s));
+  if (dtype == DCSR_F32)
+    DCSR_LAUNCH(k_rbk_emit<float>, g, 256, 0, s, keys, (const float *)vals, n, pos, keys_out, (float *)vals_out);
+  else
+    DCSR_LAUNCH(k_rbk_emit<double>, g, 256, 0, s, keys, (const double *)vals, n, pos, keys_out,
+                (double *)vals_out);
+  ar.release(s);
+  return DCSR_OK;
+}

@@ -1,0 +1,416 @@
+// spgemm.cu -- C = A*B for DCSR matrices (expand - sort - reduce).
+//
+// 1. count   products per row P_i = sum_{k in A_i} |B_k| and a size class
+//            (reference CalcSortSizes_SPMM / SetBins_SPMM include/spmm.inl:951-1061)
+// 2. bucket  rows by class (one radix pass), scan P_i -> per-row staging offsets
+// 3. numeric per row: expand products a_ik*b_kj tagged with their product
+//            index p, sort by (column, p), sum equal columns left to right,
+//            write unique columns to the staging area:
+//              P_i <= 256   warp per row, bitonic sort in shared memory
+//              P_i <= 4096  CTA per row, bitonic sort in shared memory
+//              P_i >  4096  all such rows together: global stable radix sort
+//                           of (row, column) keys (no row is skipped; the
+//                           reference left rows > 2048 products uncomputed,
+//                           include/spmm.h:368-389)
+// 4. layout  C's rows with its own slack policy (CSR load path).
+// Sorting by (column, p) makes every sum run in product order, so values are
+// reproducible and match the CPU oracle bit for bit; explicit zeros are kept
+// (reference include/spmm.inl:215-218).
+#include <algorithm>
+
+#include "internal.cuh"
+
+namespace dcsr {
+
+constexpr int SG_THREADS = 256;
+constexpr int SG_WARP_MAX = 256;   // products per warp-row
+constexpr int SG_CTA_MAX = 4096;   // products per CTA-row
+enum { SG_EMPTY = 0, SG_WARP = 1, SG_CTA = 2, SG_GLOBAL = 3 };
+
+template <typename V>
+__global__ void k_sg_count(Mat<V> A, Mat<V> B, long long *cnt, unsigned long long *cls, unsigned *rows) {
+  const int lane = threadIdx.x & 31;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < A.n_rows; i += nw) {
+    const Chain ch = load_chain(A, (int32_t)i);
+    const int64_t L = A.row_sizes[i];
+    long long s = 0;
+    for (int64_t p = lane; p < L; p += 32) s += B.row_sizes[A.cols[ch.phys(p)]];
+    s = warp_sum(s);
+    if (lane == 0) {
+      cnt[i] = s;
+      cls[i] = s == 0 ? SG_EMPTY : s <= SG_WARP_MAX ? SG_WARP : s <= SG_CTA_MAX ? SG_CTA : SG_GLOBAL;
+      rows[i] = (unsigned)i;
+    }
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) cnt[A.n_rows] = 0;
+}
+
+// class starts [0..4] from the sorted class keys
+__global__ void k_sg_classes(const unsigned long long *keys, int32_t n, long long *starts) {
+  const int c = threadIdx.x;
+  if (c <= 4) {
+    int64_t lo = 0, hi = n;
+    while (lo < hi) {
+      int64_t mid = (lo + hi) >> 1;
+      if (keys[mid] < (unsigned long long)c) lo = mid + 1;
+      else hi = mid;
+    }
+    starts[c] = c == 4 ? n : lo;
+  }
+}
+
+// Expand row i's products into (key = col<<32 | p, prod[p]) over `nthr`
+// cooperating threads (tid in [0, nthr)); returns the product count.
+template <typename V>
+__device__ __forceinline__ int64_t sg_expand(const Mat<V> &A, const Mat<V> &B, int64_t i, int tid, int nthr,
+                                             unsigned long long *key, V *prod) {
+  const Chain ca = load_chain(A, (int32_t)i);
+  const int64_t LA = A.row_sizes[i];
+  int64_t pos = 0;
+  for (int64_t e = 0; e < LA; e++) {
+    const int64_t qa = ca.phys(e);
+    const int32_t k = A.cols[qa];
+    const V a = A.vals[qa];
+    const Chain cb = load_chain(B, k);
+    const int64_t LB = B.row_sizes[k];
+    for (int64_t j = tid; j < LB; j += nthr) {
+      const int64_t qb = cb.phys(j);
+      key[pos + j] = ((unsigned long long)(uint32_t)B.cols[qb] << 32) | (unsigned long long)(pos + j);
+      V pr;
+      if constexpr (sizeof(V) == 4) pr = __fmul_rn(a, B.vals[qb]);
+      else pr = __dmul_rn(a, B.vals[qb]);
+      prod[pos + j] = pr;
+    }
+    pos += LB;
+  }
+  return pos;
+}
+
+__device__ __forceinline__ int next_pow2(int x) {
+  int p = 32;
+  while (p < x) p <<= 1;
+  return p;
+}
+
+// Bitonic sort of n2 (power of two) keys by `nthr` threads; sync() between steps.
+template <typename Sync>
+__device__ __forceinline__ void bitonic(unsigned long long *key, int n2, int tid, int nthr, Sync sync) {
+  for (int k = 2; k <= n2; k <<= 1)
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      for (int t = tid; t < (n2 >> 1); t += nthr) {
+        const int i = ((t & ~(j - 1)) << 1) | (t & (j - 1));
+        const int l = i + j;
+        const bool up = (i & k) == 0;
+        const unsigned long long a = key[i], b = key[l];
+        if ((a > b) == up) {
+          key[i] = b;
+          key[l] = a;
+        }
+      }
+      sync();
+    }
+}
+
+// Warp per row, P_i <= 256.
+template <typename V>
+__global__ void __launch_bounds__(SG_THREADS) k_sg_warp(Mat<V> A, Mat<V> B, const unsigned *rows,
+                                                        const long long *starts, const long long *ub, int32_t *tcol,
+                                                        V *tval, long long *ucnt) {
+  __shared__ unsigned long long skey[SG_THREADS / 32][SG_WARP_MAX];
+  __shared__ V sprod[SG_THREADS / 32][SG_WARP_MAX];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int64_t b = starts[SG_WARP], e = starts[SG_WARP + 1];
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  const unsigned lt = (1u << lane) - 1u;
+  unsigned long long *key = skey[w];
+  V *prod = sprod[w];
+  for (int64_t it = b + (((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5); it < e; it += nw) {
+    const int64_t i = rows[it];
+    const int P = (int)sg_expand(A, B, i, lane, 32, key, prod);
+    const int n2 = next_pow2(P);
+    for (int t = P + lane; t < n2; t += 32) key[t] = ~0ull;
+    __syncwarp();
+    bitonic(key, n2, lane, 32, []() { __syncwarp(); });
+    const int64_t base = ub[i];
+    int heads = 0;
+    for (int c0 = 0; c0 < P; c0 += 32) {
+      const int idx = c0 + lane;
+      const bool valid = idx < P;
+      const unsigned long long k = valid ? key[idx] : 0;
+      const bool head = valid && (idx == 0 || (key[idx - 1] >> 32) != (k >> 32));
+      const unsigned hm = __ballot_sync(FULL, head);
+      if (head) {
+        V v = prod[(uint32_t)k];
+        for (int j = idx + 1; j < P && (key[j] >> 32) == (k >> 32); j++) v = v + prod[(uint32_t)key[j]];
+        const int64_t o = base + heads + __popc(hm & lt);
+        tcol[o] = (int32_t)(k >> 32);
+        tval[o] = v;
+      }
+      heads += __popc(hm);
+    }
+    if (lane == 0) ucnt[i] = heads;
+    __syncwarp();
+  }
+}
+
+// CTA per row, 256 < P_i <= 4096 (dynamic shared memory).
+template <typename V>
+__global__ void __launch_bounds__(SG_THREADS) k_sg_cta(Mat<V> A, Mat<V> B, const unsigned *rows,
+                                                       const long long *starts, const long long *ub, int32_t *tcol,
+                                                       V *tval, long long *ucnt) {
+  extern __shared__ unsigned long long sg_smem[];
+  unsigned long long *key = sg_smem;
+  V *prod = reinterpret_cast<V *>(sg_smem + SG_CTA_MAX);
+  __shared__ int wheads[SG_THREADS / 32 + 1];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int64_t b = starts[SG_CTA], e = starts[SG_CTA + 1];
+  for (int64_t it = b + blockIdx.x; it < e; it += gridDim.x) {
+    const int64_t i = rows[it];
+    const int P = (int)sg_expand(A, B, i, threadIdx.x, SG_THREADS, key, prod);
+    const int n2 = next_pow2(P);
+    for (int t = P + threadIdx.x; t < n2; t += SG_THREADS) key[t] = ~0ull;
+    __syncthreads();
+    bitonic(key, n2, threadIdx.x, SG_THREADS, []() { __syncthreads(); });
+    const int64_t base = ub[i];
+    int heads = 0;  // running total (uniform across the block)
+    for (int c0 = 0; c0 < P; c0 += SG_THREADS) {
+      const int idx = c0 + threadIdx.x;
+      const bool valid = idx < P;
+      const unsigned long long k = valid ? key[idx] : 0;
+      const bool head = valid && (idx == 0 || (key[idx - 1] >> 32) != (k >> 32));
+      const unsigned hm = __ballot_sync(FULL, head);
+      if (lane == 0) wheads[w] = __popc(hm);
+      __syncthreads();
+      int before = 0, total = 0;
+      for (int q = 0; q < SG_THREADS / 32; q++) {
+        if (q < w) before += wheads[q];
+        total += wheads[q];
+      }
+      if (head) {
+        V v = prod[(uint32_t)k];
+        for (int j = idx + 1; j < P && (key[j] >> 32) == (k >> 32); j++) v = v + prod[(uint32_t)key[j]];
+        const int64_t o = base + heads + before + __popc(hm & ((1u << lane) - 1u));
+        tcol[o] = (int32_t)(k >> 32);
+        tval[o] = v;
+      }
+      heads += total;
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) ucnt[i] = heads;
+    __syncthreads();
+  }
+}
+
+// Global path: expand rows with P_i > 4096 into (key = slot<<cb | col, value = global product index).
+template <typename V>
+__global__ void k_sg_global_expand(Mat<V> A, Mat<V> B, const unsigned *rows, const long long *starts,
+                                   const long long *goff, int cb, unsigned long long *gkey, unsigned *gidx,
+                                   V *gprod) {
+  const int lane = threadIdx.x & 31;
+  const int64_t b = starts[SG_GLOBAL], e = starts[SG_GLOBAL + 1];
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t it = b + (((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5); it < e; it += nw) {
+    const int64_t i = rows[it];
+    const int64_t slot = it - b;
+    const int64_t o = goff[slot];
+    const Chain ca = load_chain(A, (int32_t)i);
+    const int64_t LA = A.row_sizes[i];
+    int64_t pos = 0;
+    for (int64_t ea = 0; ea < LA; ea++) {
+      const int64_t qa = ca.phys(ea);
+      const int32_t k = A.cols[qa];
+      const V a = A.vals[qa];
+      const Chain ck = load_chain(B, k);
+      const int64_t LB = B.row_sizes[k];
+      for (int64_t j = lane; j < LB; j += 32) {
+        const int64_t qb = ck.phys(j);
+        gkey[o + pos + j] = ((unsigned long long)slot << cb) | (unsigned long long)(uint32_t)B.cols[qb];
+        gidx[o + pos + j] = (unsigned)(o + pos + j);
+        V pr;
+        if constexpr (sizeof(V) == 4) pr = __fmul_rn(a, B.vals[qb]);
+        else pr = __dmul_rn(a, B.vals[qb]);
+        gprod[o + pos + j] = pr;
+      }
+      pos += LB;
+    }
+  }
+}
+
+// Heads of equal keys after the sort.
+__global__ void k_sg_global_flags(const unsigned long long *gkey, int64_t n, long long *flag) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += stride)
+    flag[q] = (q == 0 || gkey[q] != gkey[q - 1]) ? 1 : 0;
+}
+
+template <typename V>
+__global__ void k_sg_global_emit(const unsigned long long *gkey, const unsigned *gidx, const V *gprod, int64_t n,
+                                 const long long *hpos, const unsigned *rows, const long long *starts,
+                                 const long long *goff, const long long *ub, int cb, int32_t *tcol, V *tval,
+                                 long long *ucnt) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  const unsigned long long cmask = (1ull << cb) - 1;
+  const int64_t b = starts[SG_GLOBAL];
+  for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += stride) {
+    const unsigned long long k = gkey[q];
+    if (q > 0 && gkey[q - 1] == k) continue;
+    const int64_t slot = (int64_t)(k >> cb);
+    const int64_t i = rows[b + slot];
+    V v = gprod[gidx[q]];
+    for (int64_t j = q + 1; j < n && gkey[j] == k; j++) v = v + gprod[gidx[j]];
+    const int64_t first = hpos[goff[slot]];  // head rank of the row's first product
+    const int64_t o = ub[i] + (hpos[q] - first);
+    tcol[o] = (int32_t)(k & cmask);
+    tval[o] = v;
+    atomicAdd((unsigned long long *)&ucnt[i], 1ull);
+  }
+}
+
+template <typename V>
+__global__ void k_sg_compact(int32_t n, const long long *ub, const long long *rp, const int32_t *tcol, const V *tval,
+                             int32_t *ccol, V *cval) {
+  const int lane = threadIdx.x & 31;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += nw) {
+    const int64_t s = ub[i], d = rp[i], L = rp[i + 1] - rp[i];
+    for (int64_t j = lane; j < L; j += 32) {
+      ccol[d + j] = tcol[s + j];
+      cval[d + j] = tval[s + j];
+    }
+  }
+}
+
+// slot products for the global class: goff[slot] = ub-like offsets of the
+// large rows in a dense staging array
+__global__ void k_sg_global_sizes(const unsigned *rows, const long long *starts, const long long *ub,
+                                  long long *gsz) {
+  const int64_t b = starts[SG_GLOBAL], e = starts[SG_GLOBAL + 1];
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t it = b + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; it <= e; it += stride)
+    gsz[it - b] = it < e ? ub[rows[it] + 1] - ub[rows[it]] : 0;
+}
+
+static int grid_for(int64_t n, int block) {
+  int64_t g = div_up(n, block);
+  int64_t cap = (int64_t)sm_count() * 16;
+  return (int)(g < 1 ? 1 : (g > cap ? cap : g));
+}
+
+template <typename V>
+static int spgemm_impl(dcsr_handle hA, dcsr_handle hB, dcsr_handle hC, cudaStream_t s) {
+  const int32_t n = hA->n_rows;
+  Mat<V> A = hA->view<V>(), B = hB->view<V>();
+  Arena ar;
+  DCSR_TRY(ar.reserve(arena_bytes(n + 2, 8) * 3 + arena_bytes(n + 2, 4) * 2 + arena_bytes(8, 8) +
+                          radix_scratch_bytes(n) + scan_scratch_bytes(n + 2), s));
+  long long *cnt = ar.take<long long>(n + 2);
+  unsigned long long *k0 = ar.take<unsigned long long>(n + 2), *k1 = ar.take<unsigned long long>(n + 2);
+  unsigned *r0 = ar.take<unsigned>(n + 2), *r1 = ar.take<unsigned>(n + 2);
+  long long *starts = ar.take<long long>(8);
+  long long *ub = cnt;  // scanned in place
+  if (n > 0) {
+    DCSR_LAUNCH(k_sg_count<V>, grid_for((int64_t)n * 32, SG_THREADS), SG_THREADS, 0, s, A, B, cnt, k0, r0);
+    if (n > 1) DCSR_TRY(radix_sort_pairs(&k0, &r0, &k1, &r1, n, 2, ar, s));
+  }
+  DCSR_LAUNCH(k_sg_classes, 1, 32, 0, s, k0, n, starts);
+  DCSR_TRY(scan_i64(cnt, ub, n + 1, hC->stat + ST_TOTAL, ar, s));
+  long long host[6];
+  DCSR_CUDA(cudaMemcpyAsync(host, starts, sizeof(long long) * 5, cudaMemcpyDeviceToHost, s));
+  DCSR_CUDA(cudaMemcpyAsync(host + 5, hC->stat + ST_TOTAL, sizeof(long long), cudaMemcpyDeviceToHost, s));
+  DCSR_CUDA(cudaStreamSynchronize(s));
+  const int64_t P = host[5];
+  const int64_t n_global = host[SG_GLOBAL + 1] - host[SG_GLOBAL];
+  // staging: unique columns per row at ub[i]
+  int32_t *tcol = nullptr;
+  V *tval = nullptr;
+  long long *ucnt = nullptr;
+  DCSR_CUDA(cudaMallocAsync((void **)&tcol, sizeof(int32_t) * (P + 1), s));
+  DCSR_CUDA(cudaMallocAsync((void **)&tval, sizeof(V) * (P + 1), s));
+  DCSR_CUDA(cudaMallocAsync((void **)&ucnt, sizeof(long long) * (n + 2), s));
+  DCSR_CUDA(cudaMemsetAsync(ucnt, 0, sizeof(long long) * (n + 2), s));
+  static int g_warp = 0, g_cta = 0;
+  const size_t cta_smem = SG_CTA_MAX * (sizeof(unsigned long long) + sizeof(V));
+  if (!g_warp) {
+    g_warp = persistent_grid((const void *)k_sg_warp<double>, SG_THREADS, 0);
+    cudaFuncSetAttribute(k_sg_cta<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)(SG_CTA_MAX * (sizeof(unsigned long long) + sizeof(float))));
+    cudaFuncSetAttribute(k_sg_cta<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)(SG_CTA_MAX * (sizeof(unsigned long long) + sizeof(double))));
+    g_cta = persistent_grid((const void *)k_sg_cta<double>, SG_THREADS,
+                            SG_CTA_MAX * (sizeof(unsigned long long) + sizeof(double)));
+  }
+  if (host[SG_WARP + 1] > host[SG_WARP])
+    DCSR_LAUNCH(k_sg_warp<V>, g_warp, SG_THREADS, 0, s, A, B, r0, starts, ub, tcol, tval, ucnt);
+  if (host[SG_CTA + 1] > host[SG_CTA])
+    DCSR_LAUNCH(k_sg_cta<V>, g_cta, SG_THREADS, cta_smem, s, A, B, r0, starts, ub, tcol, tval, ucnt);
+  if (n_global > 0) {
+    // products of all large rows, laid out densely by slot, then one stable
+    // radix sort by (slot, column) keeps every column's products in p order
+    Arena g;
+    DCSR_TRY(g.reserve(arena_bytes(n_global + 2, 8) + scan_scratch_bytes(n_global + 2), s));
+    long long *goff = g.take<long long>(n_global + 2);
+    DCSR_LAUNCH(k_sg_global_sizes, grid_for(n_global + 1, 256), 256, 0, s, r0, starts, ub, goff);
+    DCSR_TRY(scan_i64(goff, goff, n_global + 1, hC->stat + ST_AUX + 1, g, s));
+    long long Pg = 0;
+    DCSR_CUDA(cudaMemcpyAsync(&Pg, hC->stat + ST_AUX + 1, sizeof(Pg), cudaMemcpyDeviceToHost, s));
+    DCSR_CUDA(cudaStreamSynchronize(s));
+    if (Pg > 0xffffffffLL) return DCSR_NOT_SUPPORTED;
+    Arena gg;
+    DCSR_TRY(gg.reserve(2 * arena_bytes(Pg, 8) + 2 * arena_bytes(Pg, 4) + arena_bytes(Pg, sizeof(V)) +
+                            arena_bytes(Pg + 1, 8) + radix_scratch_bytes(Pg) + scan_scratch_bytes(Pg + 1), s));
+    unsigned long long *gk0 = gg.take<unsigned long long>(Pg), *gk1 = gg.take<unsigned long long>(Pg);
+    unsigned *gi0 = gg.take<unsigned>(Pg), *gi1 = gg.take<unsigned>(Pg);
+    V *gprod = (V *)gg.take<double>(Pg);
+    long long *hpos = gg.take<long long>(Pg + 1);
+    const int cb = bits_for(hB->n_cols);
+    DCSR_LAUNCH(k_sg_global_expand<V>, grid_for(n_global * 32, 256), 256, 0, s, A, B, r0, starts, goff, cb, gk0, gi0,
+                gprod);
+    DCSR_TRY(radix_sort_pairs(&gk0, &gi0, &gk1, &gi1, Pg, bits_for(n_global) + cb, gg, s));
+    DCSR_LAUNCH(k_sg_global_flags, grid_for(Pg, 256), 256, 0, s, gk0, Pg, hpos);
+    DCSR_TRY(scan_i64(hpos, hpos, Pg, nullptr, gg, s));
+    DCSR_LAUNCH(k_sg_global_emit<V>, grid_for(Pg, 256), 256, 0, s, gk0, gi0, gprod, Pg, hpos, r0, starts, goff, ub,
+                cb, tcol, tval, ucnt);
+    gg.release(s);
+    g.release(s);
+  }
+  // compact staging -> CSR, then lay out C with its policy
+  long long *rp = nullptr;
+  int32_t *ccol = nullptr;
+  V *cval = nullptr;
+  Arena c;
+  DCSR_TRY(c.reserve(arena_bytes(n + 2, 8) + scan_scratch_bytes(n + 2), s));
+  rp = c.take<long long>(n + 2);
+  DCSR_TRY(scan_i64(ucnt, rp, n + 1, hC->stat + ST_TOTAL, c, s));
+  long long nnzc = 0;
+  DCSR_CUDA(cudaMemcpyAsync(&nnzc, hC->stat + ST_TOTAL, sizeof(nnzc), cudaMemcpyDeviceToHost, s));
+  DCSR_CUDA(cudaStreamSynchronize(s));
+  DCSR_CUDA(cudaMallocAsync((void **)&ccol, sizeof(int32_t) * (nnzc + 1), s));
+  DCSR_CUDA(cudaMallocAsync((void **)&cval, sizeof(V) * (nnzc + 1), s));
+  if (n > 0)
+    DCSR_LAUNCH(k_sg_compact<V>, grid_for((int64_t)n * 32, 256), 256, 0, s, n, ub, rp, tcol, tval, ccol, cval);
+  DCSR_TRY(hC->scratch.reserve(load_scratch_bytes(hC), s));
+  int st = load_from_csr64(hC, rp, ccol, cval, s);
+  c.release(s);
+  ar.release(s);
+  cudaFreeAsync(tcol, s);
+  cudaFreeAsync(tval, s);
+  cudaFreeAsync(ucnt, s);
+  cudaFreeAsync(ccol, s);
+  cudaFreeAsync(cval, s);
+  return st;
+}
+
+}  // namespace dcsr
+
+using namespace dcsr;
+
+extern "C" int dcsr_spgemm(dcsr_handle A, dcsr_handle B, dcsr_handle C, void *stream) {
+  if (!A || !B || !C) return DCSR_BAD_ARG;
+  if (A->n_cols != B->n_rows || C->n_rows != A->n_rows || C->n_cols != B->n_cols || A->dtype != B->dtype ||
+      C->dtype != A->dtype || C == A || C == B)
+    return DCSR_BAD_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  if (A->dtype == DCSR_F32) return spgemm_impl<float>(A, B, C, s);
+  return spgemm_impl<double>(A, B, C, s);
+}

@@ -1,0 +1,190 @@
+/*
+ * dcsr_b200.h -- C ABI of the B200-native Dynamic-CSR (DCSR) library.
+ *
+ * Every entry point takes plain pointers, sizes and a CUDA stream passed as
+ * `void *` (a cudaStream_t; NULL = the legacy default stream) and returns an
+ * int status (dcsr_status).  Device pointers for inputs/outputs are owned by
+ * the caller; the library owns each matrix's entry pool.  Calls on one handle
+ * must come from one stream at a time; different handles are independent.
+ *
+ * The reference (Vizerai/DCSR) is a header-only C++/CUDA template library in
+ * `namespace device` with no ABI; each function below names the reference
+ * interface it replaces (file:line in the reference tree).
+ *
+ * Layout of a matrix in HBM (reference include/dcsr_matrix.h:9-73):
+ *   row_sizes[n_rows+1]  logical row lengths; row_sizes[n_rows] = pool top
+ *   seg[max_segs*pitch]  (start,end) pool ranges per row and segment layer:
+ *                        seg[l*pitch + 2*r], seg[l*pitch + 2*r + 1];
+ *                        pitch = align_up(2*n_rows, 32); unused = (-1,-1)
+ *   cols[pool_cap] int32, vals[pool_cap] float|double: the entry pool
+ * A row's entries are its segments' contents in layer order, up to its
+ * logical length.  In MERGE mode every row is kept sorted by column with
+ * unique columns; in APPEND mode entries keep insertion order (reference
+ * behaviour).
+ */
+#ifndef DCSR_B200_H
+#define DCSR_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct dcsr_matrix_s *dcsr_handle;
+
+enum { DCSR_F32 = 0, DCSR_F64 = 1 };
+enum { DCSR_MERGE = 0, DCSR_APPEND = 1 };
+
+typedef enum {
+  DCSR_OK = 0,
+  DCSR_POOL_EXHAUSTED = 1, /* update rejected: pool too small (matrix unchanged) */
+  DCSR_LAYER_OVERFLOW = 2, /* update rejected: a row needs > max_segs segments */
+  DCSR_BAD_INDEX = 3,      /* an input row/column index is out of range */
+  DCSR_OOM = 4,            /* device allocation failed */
+  DCSR_BAD_ARG = 5,        /* invalid argument (null handle, size, dtype ...) */
+  DCSR_TIMEOUT = 6,        /* a bounded device wait gave up */
+  DCSR_CUDA_ERROR = 7,     /* a CUDA runtime call failed */
+  DCSR_NOT_SUPPORTED = 8
+} dcsr_status;
+
+/* Row-reduction operators for dcsr_row_reduce. */
+enum { DCSR_REDUCE_SUM = 0, DCSR_REDUCE_MAX = 1, DCSR_REDUCE_MIN = 2, DCSR_REDUCE_COUNT = 3 };
+
+/* Layout policy (all integers so the CPU oracle restates it exactly).
+ * Row capacity on load/compaction: align_up(max(ceil(len*factor_x16/16),
+ * min_cap, len), align).  A MERGE-mode row that outgrows its chain gets a new
+ * segment of policy_cap(new_len) - current_capacity; an APPEND-mode row gets
+ * rlB - free + alpha (reference include/sparse_update.inl:93-105).  The pool
+ * is sized top + max(top*spare_x16/16, min_spare) on load. */
+typedef struct {
+  int32_t max_segs;   /* segment layers per row, 1..8 (reference MAX_OFFSET=4) */
+  int32_t factor_x16; /* per-row slack factor in 1/16 (32 = 2x) */
+  int32_t min_cap;    /* minimum row capacity */
+  int32_t align;      /* capacity alignment in entries (power of two) */
+  int32_t alpha;      /* APPEND-mode extra slack per new segment (reference: 4) */
+  int32_t spare_x16;  /* pool spare capacity in 1/16 of the laid-out size */
+  int32_t min_spare;  /* minimum pool spare, entries */
+  int32_t mode;       /* DCSR_MERGE (canonical) or DCSR_APPEND (reference) */
+  int32_t reloc_min;  /* MERGE: a row whose in-place merge would shift more than
+                         reloc_min entries is instead merged out of place into
+                         one fresh segment of policy_cap(new_len) (chain reset) */
+} dcsr_opts;
+
+/* Snapshot of a matrix's device layout (device pointers). */
+typedef struct {
+  int32_t n_rows, n_cols, dtype, pitch;
+  int64_t pool_cap;
+  int32_t *row_sizes;
+  int32_t *seg;
+  int32_t *cols;
+  void *vals;
+  dcsr_opts opts;
+} dcsr_info_t;
+
+/* ------------------------------------------------------------ lifecycle */
+
+/* Default policy for a mode: MERGE = 2x slack, 16-byte aligned segments;
+ * APPEND = the reference's tight load/compaction with alpha = 4. */
+void dcsr_default_opts(dcsr_opts *opts, int32_t mode);
+
+/* Replaces dcsr_matrix::resize (reference include/dcsr_matrix.h:41-108) and
+ * device::Initialize_Matrix (include/load.h:8-22).  opts may be NULL. */
+int dcsr_create(dcsr_handle *out, int32_t n_rows, int32_t n_cols, int32_t dtype, const dcsr_opts *opts);
+/* Replaces ~dcsr_matrix (include/dcsr_matrix.h:35-39). */
+int dcsr_destroy(dcsr_handle h);
+int dcsr_info(dcsr_handle h, dcsr_info_t *info);
+/* Copy the layout (row_sizes[n_rows+1], seg[max_segs*pitch]) into caller
+ * buffers (host or device; either pointer may be NULL).  Synchronises. */
+int dcsr_get_layout(dcsr_handle h, int32_t *row_sizes, int32_t *seg, void *stream);
+
+/* ----------------------------------------------------------- conversion */
+
+/* CSR -> DCSR.  Replaces device::LoadMatrix(dcsr, csr) (include/load.h:207-227).
+ * In MERGE mode unsorted rows / duplicate columns are canonicalised
+ * (duplicates summed in input order).  Synchronises the stream once. */
+int dcsr_from_csr(dcsr_handle h, const int32_t *row_ptr, const int32_t *cols, const void *vals, int64_t nnz,
+                  void *stream);
+/* COO -> DCSR (any order).  Replaces device::LoadMatrix(dcsr, rows, cols, vals, N)
+ * (include/load.h:27-59, which required row-sorted input).  Synchronises once. */
+int dcsr_from_coo(dcsr_handle h, const int32_t *rows, const int32_t *cols, const void *vals, int64_t nnz,
+                  void *stream);
+/* HYB (ELL column-major with -1 padding + COO overflow) -> DCSR.  Replaces
+ * the reference's HYB -> COO -> DCSR route (include/load.h:61-106,174-205). */
+int dcsr_from_hyb(dcsr_handle h, const int32_t *ell_cols, const void *ell_vals, int32_t ell_width,
+                  int64_t ell_pitch, const int32_t *coo_rows, const int32_t *coo_cols, const void *coo_vals,
+                  int64_t coo_nnz, void *stream);
+
+/* Number of stored entries (synchronises).  Use before dcsr_to_csr. */
+int dcsr_nnz(dcsr_handle h, int64_t *nnz, void *stream);
+/* DCSR -> CSR in row order, any state (chains followed).  Replaces
+ * device::LoadMatrix(csr, dcsr) + DCSRtoCSROffsets (include/load.h:232-253,
+ * include/sparse_update.inl:1101-1116).  Output arrays hold n_rows+1 / nnz. */
+int dcsr_to_csr(dcsr_handle h, int32_t *row_ptr, int32_t *cols, void *vals, void *stream);
+/* DCSR -> COO in row order (rows, cols, vals of length nnz). */
+int dcsr_to_coo(dcsr_handle h, int32_t *rows, int32_t *cols, void *vals, void *stream);
+
+/* -------------------------------------------------------------- updates */
+
+/* In-place batch update with COO triples in any order.  Replaces
+ * device::UpdateMatrix (include/load.h:258-325) + UpdateMatrix_dcsr
+ * (include/sparse_update.inl:16-130).  MERGE: duplicate (row,col) pairs are
+ * summed into the existing entry in batch order; APPEND: reference append.
+ * Asynchronous: all-or-nothing, a rejection (POOL_EXHAUSTED, LAYER_OVERFLOW,
+ * BAD_INDEX) leaves the matrix unchanged and is reported by dcsr_get_status. */
+int dcsr_update(dcsr_handle h, const int32_t *rows, const int32_t *cols, const void *vals, int64_t nnz,
+                void *stream);
+/* dcsr_update plus the repair policy: on rejection compact and retry, then
+ * grow the pool and retry.  Synchronises; returns the final status. */
+int dcsr_update_sync(dcsr_handle h, const int32_t *rows, const int32_t *cols, const void *vals, int64_t nnz,
+                     void *stream);
+/* Read (and clear) the device status of the last asynchronous calls. */
+int dcsr_get_status(dcsr_handle h, void *stream, int32_t *status);
+/* Defragment into a fresh pool, rows in row order with policy capacities.
+ * Replaces device::SortMatrixRow (include/load.h:404-581). */
+int dcsr_compact(dcsr_handle h, void *stream);
+/* Grow the pool to at least pool_cap entries (contents kept). */
+int dcsr_reserve(dcsr_handle h, int64_t pool_cap, void *stream);
+/* Recompute the SpMV row bins.  Replaces device::BinRows (include/load.h:583-610);
+ * bins live in the handle (no process-global __constant__ table). */
+int dcsr_bin_rows(dcsr_handle h, void *stream);
+
+/* ------------------------------------------------------------ operators */
+
+/* Y = alpha*A*X + beta*Y with k (1..8) right-hand sides; X is n_cols x k
+ * row-major with row stride ldx (X[c*ldx + j]), Y is n_rows x k with stride
+ * ldy; values of the matrix dtype.  beta == 0 does not read Y.  Replaces
+ * device::spmv(dcsr, x, y, streams) (include/spmv.h:121-248). */
+int dcsr_spmv(dcsr_handle h, const void *x, int32_t k, int64_t ldx, void *y, int64_t ldy, double alpha,
+              double beta, void *stream);
+/* y[r] = op over row r's entries (sum / max / min / count).  The reference
+ * computes row sums as SpMV with x = 1. */
+int dcsr_row_reduce(dcsr_handle h, int32_t op, void *y, void *stream);
+/* C = A*B.  C must be a handle created with n_rows = A.n_rows, n_cols =
+ * B.n_cols and A's dtype; its content is replaced.  Rows sorted, explicit
+ * zeros kept, all rows computed.  Replaces device::spmm (include/spmm.h:30-391).
+ * Synchronises once (output size). */
+int dcsr_spgemm(dcsr_handle A, dcsr_handle B, dcsr_handle C, void *stream);
+
+/* X[I[n]] += 1 for a sorted index array I.  Replaces
+ * device::count_sorted_indices (include/primitives.h:417-464). */
+int dcsr_count_sorted_indices(const int32_t *I, int64_t n, int32_t *X, void *stream);
+/* Reduce-by-key over sorted int32 keys with left-to-right sums; writes the
+ * unique count to *n_out (device pointer).  Replaces the CTA/global
+ * reduce-by-key of include/reduce.inl:139-308, include/reduce_global.inl. */
+int dcsr_reduce_by_key(const int32_t *keys, const void *vals, int64_t n, int32_t dtype, int32_t *keys_out,
+                       void *vals_out, int64_t *n_out, void *stream);
+
+/* ---------------------------------------------------------------- misc */
+
+const char *dcsr_status_string(int status);
+/* Number of CUDA kernels this library has launched in this process. */
+uint64_t dcsr_launch_count(void);
+/* Library version string. */
+const char *dcsr_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

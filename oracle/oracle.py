@@ -1,0 +1,295 @@
+"""ctypes bindings for the CPU oracle and the reference's cusp host harness.
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and
+bench.py's CPU baseline leg -- never by the dcsr_b200 package.
+
+* ``OracleDcsr`` wraps oracle/dcsr_oracle.c (the CPU restatement of the DCSR
+  operators, see its header for the reference lines each function follows).
+* ``Ref`` wraps oracle/ref_cusp.cpp built against the reference tree
+  (oracle/_ref/libref_cusp_{seq,omp}.so): the reference's own cusp host
+  SpMV / add / SpGEMM / sort_by_row.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+BUILD = os.path.join(HERE, "_build")
+REFDIR = os.path.join(HERE, "_ref")
+
+F32, F64 = 0, 1
+MERGE, APPEND = 0, 1
+STATUS = {0: "OK", 1: "POOL_EXHAUSTED", 2: "LAYER_OVERFLOW", 3: "BAD_INDEX", 5: "BAD_ARG"}
+
+_i32p = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
+_i64p = np.ctypeslib.ndpointer(np.int64, flags="C_CONTIGUOUS")
+_f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+
+
+class OrOpts(C.Structure):
+    _fields_ = [(n, C.c_int32) for n in (
+        "max_segs", "factor_x16", "min_cap", "align", "alpha", "spare_x16", "min_spare", "mode",
+        "reloc_min")]
+
+
+class OrDcsr(C.Structure):
+    _fields_ = [("n_rows", C.c_int32), ("n_cols", C.c_int32), ("dtype", C.c_int32),
+                ("pitch", C.c_int32), ("o", OrOpts), ("pool_cap", C.c_int64),
+                ("row_sizes", C.POINTER(C.c_int32)), ("seg", C.POINTER(C.c_int32)),
+                ("cols", C.POINTER(C.c_int32)), ("vals", C.POINTER(C.c_double))]
+
+
+def build() -> None:
+    """Compile the oracle (and oracle/_ref when the reference tree exists)."""
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        path = os.path.join(BUILD, "liboracle.so")
+        build()  # make: rebuilds only when the oracle sources changed
+        L = C.CDLL(path)
+        P = C.POINTER(OrDcsr)
+        L.or_default_opts.argtypes = [C.POINTER(OrOpts), C.c_int]
+        L.or_create.argtypes = [C.c_int32, C.c_int32, C.c_int32, C.POINTER(OrOpts)]
+        L.or_create.restype = P
+        L.or_destroy.argtypes = [P]
+        L.or_policy_cap.argtypes = [C.POINTER(OrOpts), C.c_int64]
+        L.or_policy_cap.restype = C.c_int64
+        L.or_pool_capacity.argtypes = [C.POINTER(OrOpts), C.c_int64]
+        L.or_pool_capacity.restype = C.c_int64
+        L.or_load_csr.argtypes = [P, _i32p, _i32p, _f64p]
+        L.or_load_coo.argtypes = [P, _i32p, _i32p, _f64p, C.c_int64]
+        L.or_update.argtypes = [P, _i32p, _i32p, _f64p, C.c_int64, C.POINTER(C.c_int64)]
+        L.or_update_auto.argtypes = [P, _i32p, _i32p, _f64p, C.c_int64]
+        L.or_compact.argtypes = [P]
+        L.or_grow.argtypes = [P, C.c_int64]
+        L.or_nnz.argtypes = [P]
+        L.or_nnz.restype = C.c_int64
+        L.or_export_csr.argtypes = [P, _i32p, _i32p, _f64p]
+        L.or_spmv.argtypes = [P, _f64p, C.c_int32, C.c_int64, _f64p, C.c_int64, C.c_double, C.c_double]
+        L.or_row_reduce.argtypes = [P, C.c_int32, _f64p]
+        L.or_spgemm.argtypes = [P, P, C.POINTER(OrOpts), C.POINTER(C.c_int)]
+        L.or_spgemm.restype = P
+        L.or_spgemm_counts.argtypes = [P, P, _i64p]
+        L.or_count_sorted_indices.argtypes = [_i32p, C.c_int64, _i32p]
+        L.or_reduce_by_key.argtypes = [_i32p, _f64p, C.c_int64, C.c_int32, _i32p, _f64p]
+        L.or_reduce_by_key.restype = C.c_int64
+        L.or_bin_counts.argtypes = [P, _i64p]
+        L.or_validate.argtypes = [P]
+        _lib = L
+    return _lib
+
+
+def default_opts(mode: int = MERGE, **kw) -> OrOpts:
+    o = OrOpts()
+    lib().or_default_opts(C.byref(o), mode)
+    for k, v in kw.items():
+        setattr(o, k, int(v))
+    return o
+
+
+def policy_cap(o: OrOpts, n: int) -> int:
+    return lib().or_policy_cap(C.byref(o), n)
+
+
+def pool_capacity(o: OrOpts, top: int) -> int:
+    return lib().or_pool_capacity(C.byref(o), top)
+
+
+def _i32(a):
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+class OracleDcsr:
+    """CPU restatement of one DCSR matrix (see oracle/dcsr_oracle.h)."""
+
+    def __init__(self, n_rows, n_cols, dtype=F32, opts: OrOpts | None = None, _ptr=None):
+        self.opts = opts if opts is not None else default_opts()
+        self.p = _ptr if _ptr is not None else lib().or_create(n_rows, n_cols, dtype, C.byref(self.opts))
+        if not self.p:
+            raise ValueError("or_create failed")
+
+    def __del__(self):
+        if getattr(self, "p", None):
+            lib().or_destroy(self.p)
+            self.p = None
+
+    @property
+    def s(self) -> OrDcsr:
+        return self.p.contents
+
+    n_rows = property(lambda self: self.s.n_rows)
+    n_cols = property(lambda self: self.s.n_cols)
+    dtype = property(lambda self: self.s.dtype)
+    pitch = property(lambda self: self.s.pitch)
+    pool_cap = property(lambda self: self.s.pool_cap)
+
+    def row_sizes(self) -> np.ndarray:
+        return np.ctypeslib.as_array(self.s.row_sizes, (self.n_rows + 1,)).copy()
+
+    def seg(self) -> np.ndarray:
+        return np.ctypeslib.as_array(self.s.seg, (self.s.o.max_segs * self.pitch,)).copy()
+
+    def load_csr(self, row_ptr, cols, vals) -> int:
+        return lib().or_load_csr(self.p, _i32(row_ptr), _i32(cols), _f64(vals))
+
+    def load_coo(self, rows, cols, vals) -> int:
+        return lib().or_load_coo(self.p, _i32(rows), _i32(cols), _f64(vals), len(rows))
+
+    def update(self, rows, cols, vals):
+        need = C.c_int64(0)
+        st = lib().or_update(self.p, _i32(rows), _i32(cols), _f64(vals), len(rows), C.byref(need))
+        return st, need.value
+
+    def update_auto(self, rows, cols, vals) -> int:
+        return lib().or_update_auto(self.p, _i32(rows), _i32(cols), _f64(vals), len(rows))
+
+    def compact(self):
+        lib().or_compact(self.p)
+
+    def grow(self, cap):
+        lib().or_grow(self.p, cap)
+
+    def nnz(self) -> int:
+        return lib().or_nnz(self.p)
+
+    def export_csr(self):
+        nnz = self.nnz()
+        rp = np.zeros(self.n_rows + 1, np.int32)
+        c = np.zeros(max(nnz, 1), np.int32)
+        v = np.zeros(max(nnz, 1), np.float64)
+        lib().or_export_csr(self.p, rp, c, v)
+        return rp, c[:nnz], v[:nnz]
+
+    def spmv(self, x, k=1, alpha=1.0, beta=0.0, y=None):
+        x = _f64(x).reshape(-1)
+        y = np.zeros(self.n_rows * k, np.float64) if y is None else _f64(y).reshape(-1).copy()
+        lib().or_spmv(self.p, x, k, k, y, k, alpha, beta)
+        return y.reshape(self.n_rows, k) if k > 1 else y
+
+    def row_reduce(self, op=0):
+        y = np.zeros(self.n_rows, np.float64)
+        lib().or_row_reduce(self.p, op, y)
+        return y
+
+    def spgemm(self, B: "OracleDcsr", opts: OrOpts | None = None) -> "OracleDcsr":
+        o = opts if opts is not None else default_opts()
+        st = C.c_int(0)
+        p = lib().or_spgemm(self.p, B.p, C.byref(o), C.byref(st))
+        if st.value != 0:
+            raise RuntimeError(f"or_spgemm: {STATUS.get(st.value, st.value)}")
+        return OracleDcsr(0, 0, _ptr=p, opts=o)
+
+    def spgemm_counts(self, B: "OracleDcsr") -> np.ndarray:
+        out = np.zeros(self.n_rows, np.int64)
+        lib().or_spgemm_counts(self.p, B.p, out)
+        return out
+
+    def bin_counts(self) -> np.ndarray:
+        out = np.zeros(7, np.int64)
+        lib().or_bin_counts(self.p, out)
+        return out
+
+    def validate(self) -> int:
+        return lib().or_validate(self.p)
+
+
+def count_sorted_indices(I, X):
+    X = _i32(X).copy()
+    lib().or_count_sorted_indices(_i32(I), len(I), X)
+    return X
+
+
+def reduce_by_key(keys, vals, dtype=F64):
+    keys, vals = _i32(keys), _f64(vals)
+    ok = np.zeros(max(len(keys), 1), np.int32)
+    ov = np.zeros(max(len(keys), 1), np.float64)
+    n = lib().or_reduce_by_key(keys, vals, len(keys), dtype, ok, ov)
+    return ok[:n], ov[:n]
+
+
+# ------------------------------------------------------------ cusp harness
+
+class Ref:
+    """The reference's own cusp host path (oracle/_ref); ``seq`` picks the
+    sequential host system (bit-reproducible), else the OpenMP one."""
+
+    def __init__(self, seq: bool = True):
+        name = "libref_cusp_seq.so" if seq else "libref_cusp_omp.so"
+        path = os.path.join(REFDIR, name)
+        if not os.path.exists(path):
+            raise FileNotFoundError(path)
+        L = C.CDLL(path)
+        L.ref_threads.restype = C.c_int
+        L.ref_spmv.argtypes = [C.c_int32, C.c_int32, C.c_int32, _i32p, _i32p, _f64p, _f64p, _f64p]
+        L.ref_add.argtypes = [C.c_int32, C.c_int32, C.c_int32, _i32p, _i32p, _f64p, _i32p, _i32p, _f64p,
+                              C.c_int64]
+        L.ref_add.restype = C.c_void_p
+        L.ref_spgemm.argtypes = [C.c_int32, C.c_int32, C.c_int32, C.c_int32, _i32p, _i32p, _f64p, _i32p,
+                                 _i32p, _f64p]
+        L.ref_spgemm.restype = C.c_void_p
+        L.ref_sort_by_row.argtypes = [C.c_int32, _i32p, _i32p, _f64p, C.c_int64]
+        L.ref_result_nnz.argtypes = [C.c_void_p]
+        L.ref_result_nnz.restype = C.c_int64
+        L.ref_result_rows_len.argtypes = [C.c_void_p]
+        L.ref_result_rows_len.restype = C.c_int64
+        L.ref_result_get.argtypes = [C.c_void_p, _i32p, _i32p, _f64p]
+        L.ref_result_free.argtypes = [C.c_void_p]
+        L.ref_stream_create.argtypes = [C.c_int32, C.c_int32, _i32p, _i32p, _f64p, _f64p]
+        L.ref_stream_create.restype = C.c_void_p
+        L.ref_stream_step.argtypes = [C.c_void_p, _i32p, _i32p, _f64p, C.c_int64,
+                                      np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS"),
+                                      np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")]
+        L.ref_stream_step.restype = C.c_int64
+        L.ref_stream_free.argtypes = [C.c_void_p]
+        self.L = L
+
+    @staticmethod
+    def available(seq: bool = True) -> bool:
+        return os.path.exists(os.path.join(REFDIR, "libref_cusp_seq.so" if seq else "libref_cusp_omp.so"))
+
+    def threads(self) -> int:
+        return self.L.ref_threads()
+
+    def _take(self, h):
+        nnz = self.L.ref_result_nnz(h)
+        nr = self.L.ref_result_rows_len(h)
+        r = np.zeros(max(nr, 1), np.int32)
+        c = np.zeros(max(nnz, 1), np.int32)
+        v = np.zeros(max(nnz, 1), np.float64)
+        self.L.ref_result_get(h, r, c, v)
+        self.L.ref_result_free(h)
+        return r[:nr], c[:nnz], v[:nnz]
+
+    def spmv(self, dtype, n, m, rp, ci, vv, x):
+        y = np.zeros(n, np.float64)
+        self.L.ref_spmv(dtype, n, m, _i32(rp), _i32(ci), _f64(vv), _f64(x), y)
+        return y
+
+    def add(self, dtype, n, m, rp, ci, vv, br, bc, bv):
+        """cusp::add(A_coo, B_coo): returns COO (rows, cols, vals), zeros dropped."""
+        h = self.L.ref_add(dtype, n, m, _i32(rp), _i32(ci), _f64(vv), _i32(br), _i32(bc), _f64(bv), len(br))
+        return self._take(h)
+
+    def spgemm(self, dtype, n, k, m, arp, aci, av, brp, bci, bv):
+        """cusp::multiply(csr, csr): returns CSR (row_ptr, cols, vals); rows unsorted, zeros dropped."""
+        h = self.L.ref_spgemm(dtype, n, k, m, _i32(arp), _i32(aci), _f64(av), _i32(brp), _i32(bci), _f64(bv))
+        return self._take(h)
+
+    def sort_by_row(self, dtype, rows, cols, vals):
+        r, c, v = _i32(rows).copy(), _i32(cols).copy(), _f64(vals).copy()
+        self.L.ref_sort_by_row(dtype, r, c, v, len(r))
+        return r, c, v
