@@ -132,9 +132,14 @@ struct dcsr_matrix_s {
   int32_t *cols = nullptr;
   void *vals = nullptr;
   long long *stat = nullptr;
-  // SpMV row bins (handle-local; the reference used a global __constant__).
-  int32_t *bin_perm = nullptr;   // [n_rows] row ids grouped by class
-  int32_t *bin_info = nullptr;   // [32]: class offsets [0..8], unit offsets [16..24]
+  // Row-pass schedule (handle-local; the reference used a global __constant__
+  // bin table): rows longer than LONG_ROW and their chunk offsets.
+  int32_t *long_rows = nullptr;  // [n_rows + 1]
+  long long *long_off = nullptr; // [n_rows + 2] chunk offsets of long rows
+  int32_t *long_cnt = nullptr;   // [n_rows + 1] chunk-finisher counters
+  int32_t *sched_info = nullptr; // [32]: [0] long rows, [1] chunks
+  double *part = nullptr;        // chunk partials (reductions)
+  int64_t part_cap = 0;
   bool bins_valid = false;
   dcsr::Arena scratch;
   int device = 0;
@@ -192,18 +197,38 @@ __device__ __forceinline__ T warp_incl_scan(T v) {
 }
 
 // A row's linked segments (at most 8), read from the segment table.
+// st0/cp0 repeat segment 0 in registers for the single-segment fast path.
 struct Chain {
+  int32_t st0, cp0;
   int32_t st[8];
   int32_t cp[8];
   int ns;
   int64_t total;
   __device__ __forceinline__ int64_t phys(int64_t p) const {
+    if (p < cp0) return (int64_t)st0 + p;
+    p -= cp0;
 #pragma unroll 1
-    for (int i = 0; i < ns; i++) {
+    for (int i = 1; i < ns; i++) {
       if (p < cp[i]) return (int64_t)st[i] + p;
       p -= cp[i];
     }
     return -1;
+  }
+  __device__ __forceinline__ void set0(int32_t s, int32_t c) {
+    st0 = st[0] = s;
+    cp0 = cp[0] = c;
+  }
+  // Link a new last segment (layer ns); reset=true replaces the whole chain.
+  __device__ __forceinline__ void append(int32_t s, int32_t c, bool reset) {
+    if (reset) {
+      ns = 0;
+      total = 0;
+    }
+    if (ns == 0) set0(s, c);
+    st[ns] = s;
+    cp[ns] = c;
+    ns++;
+    total += c;
   }
 };
 
@@ -212,10 +237,16 @@ __device__ __forceinline__ Chain load_chain(const Mat<V> &m, int32_t r) {
   Chain c;
   c.ns = 0;
   c.total = 0;
+  c.st0 = 0;
+  c.cp0 = 0;
 #pragma unroll 1
   for (int l = 0; l < m.max_segs; l++) {
     int2 p = *reinterpret_cast<const int2 *>(m.seg + (int64_t)l * m.pitch + 2 * (int64_t)r);
     if (p.x < 0) break;
+    if (l == 0) {
+      c.st0 = p.x;
+      c.cp0 = p.y - p.x;
+    }
     c.st[c.ns] = p.x;
     c.cp[c.ns] = p.y - p.x;
     c.total += p.y - p.x;

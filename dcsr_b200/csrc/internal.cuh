@@ -21,7 +21,13 @@ size_t coo_to_csr_scratch(dcsr_handle h, int64_t nnz);
 int update_async(dcsr_handle h, const int32_t *rows, const int32_t *cols, const void *vals, int64_t nnz,
                  cudaStream_t s);
 int compact(dcsr_handle h, cudaStream_t s);
-int bin_rows(dcsr_handle h, cudaStream_t s);
+int build_schedule(dcsr_handle h, cudaStream_t s);
+int ensure_part(dcsr_handle h, int K, cudaStream_t s);
+// Copy every row's logical entries to dst_off[r] (optionally COO row ids and
+// an int32 row pointer).  Builds the schedule first if needed (so callers
+// must not hold arena memory across this call unless the schedule is valid).
+int copy_rows(dcsr_handle h, const long long *dst_off, int32_t *out_cols, void *out_vals, int32_t *out_rows,
+              int32_t *out_rowptr, cudaStream_t s);
 int reserve(dcsr_handle h, int64_t cap, cudaStream_t s);
 
 }  // namespace dcsr

@@ -93,50 +93,6 @@ __global__ void k_lens(const int32_t *row_sizes, int32_t n, long long *out) {
     out[r] = r < n ? row_sizes[r] : 0;
 }
 
-// Export: warp per row follows the chain; writes row_ptr, (rows), cols, vals.
-template <typename V>
-__global__ void k_export(Mat<V> m, const long long *rp, int32_t *row_ptr, int32_t *rows, int32_t *cols, V *vals) {
-  const int lane = threadIdx.x & 31;
-  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  if (gw == 0 && lane == 0 && row_ptr) row_ptr[m.n_rows] = (int32_t)rp[m.n_rows];
-  for (int64_t r = gw; r < m.n_rows; r += nw) {
-    const Chain ch = load_chain(m, (int32_t)r);
-    const int64_t L = m.row_sizes[r], d = rp[r];
-    if (lane == 0 && row_ptr) row_ptr[r] = (int32_t)d;
-    int64_t p = 0;
-    for (int s = 0; s < ch.ns && p < L; s++) {
-      const int64_t take = ch.cp[s] < L - p ? ch.cp[s] : L - p;
-      for (int64_t j = lane; j < take; j += 32) {
-        cols[d + p + j] = m.cols[ch.st[s] + j];
-        vals[d + p + j] = m.vals[ch.st[s] + j];
-        if (rows) rows[d + p + j] = (int32_t)r;
-      }
-      p += take;
-    }
-  }
-}
-
-// Compaction copy: each row's chain -> contiguous at offs[r] in the new pool.
-template <typename V>
-__global__ void k_compact_copy(Mat<V> m, const long long *offs, int32_t *ncols, V *nvals) {
-  const int lane = threadIdx.x & 31;
-  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  for (int64_t r = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < m.n_rows; r += nw) {
-    const Chain ch = load_chain(m, (int32_t)r);
-    const int64_t L = m.row_sizes[r], d = offs[r];
-    int64_t p = 0;
-    for (int s = 0; s < ch.ns && p < L; s++) {
-      const int64_t take = ch.cp[s] < L - p ? ch.cp[s] : L - p;
-      for (int64_t j = lane; j < take; j += 32) {
-        ncols[d + p + j] = m.cols[ch.st[s] + j];
-        nvals[d + p + j] = m.vals[ch.st[s] + j];
-      }
-      p += take;
-    }
-  }
-}
-
 __global__ void k_sum_lens(const int32_t *row_sizes, int32_t n, long long *out) {
   long long s = 0;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
@@ -167,47 +123,6 @@ __global__ void k_ell_emit(const int32_t *ell_cols, const V *ell_vals, int32_t n
     rows[pos[i]] = (int32_t)r;
     cols[pos[i]] = c;
     vals[pos[i]] = ell_vals[j * pitch + r];
-  }
-}
-
-// Row bins: 7 length classes {<2,<4,<8,<16,<32,<512,>=512} (reference SetBins,
-// include/sparse_update.inl:1121-1150).
-__device__ __forceinline__ int row_class(int32_t len) {
-  return len < 2 ? 0 : len < 4 ? 1 : len < 8 ? 2 : len < 16 ? 3 : len < 32 ? 4 : len < 512 ? 5 : 6;
-}
-__global__ void k_bin_keys(const int32_t *row_sizes, int32_t n, unsigned long long *keys, unsigned *vals) {
-  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += stride) {
-    keys[r] = (unsigned long long)row_class(row_sizes[r]);
-    vals[r] = (unsigned)r;
-  }
-}
-// bin_info: [c] = class start (c = 0..7, [7] = n); [8 + s] = first unit of
-// processing slot s (slot 0 = class 6 ... slot 6 = class 0); [15] = units.
-__global__ void k_bin_info(const unsigned long long *keys, int32_t n, int32_t *info) {
-  __shared__ int32_t start[8];
-  const int c = threadIdx.x;
-  if (c < 8) {
-    int64_t lo = 0, hi = n;
-    while (lo < hi) {
-      int64_t mid = (lo + hi) >> 1;
-      if (keys[mid] < (unsigned long long)c) lo = mid + 1;
-      else hi = mid;
-    }
-    start[c] = c == 7 ? n : (int32_t)lo;
-  }
-  __syncthreads();
-  if (c == 0) {
-    int32_t u = 0;
-    for (int s = 0; s < 7; s++) {
-      const int cls = 6 - s;
-      const int32_t cnt = start[cls + 1] - start[cls];
-      const int32_t rows_per_unit = cls == 6 ? 1 : 256 >> cls;
-      info[8 + s] = u;
-      u += (cnt + rows_per_unit - 1) / rows_per_unit;
-    }
-    info[15] = u;
-    for (int k = 0; k < 8; k++) info[k] = start[k];
   }
 }
 
@@ -289,6 +204,7 @@ int reserve(dcsr_handle h, int64_t cap, cudaStream_t s) {
 int compact(dcsr_handle h, cudaStream_t s) {
   const int32_t n = h->n_rows;
   Arena &ar = h->scratch;
+  if (!h->bins_valid) DCSR_TRY(build_schedule(h, s));  // before taking arena memory
   DCSR_TRY(ar.reserve(arena_bytes(n + 2, 8) + scan_scratch_bytes(n + 1), s));
   long long *caps = ar.take<long long>(n + 2);
   DCSR_LAUNCH(k_caps_from_sizes, grid_for(n + 1, 256), 256, 0, s, h->row_sizes, n, h->o, caps);
@@ -303,39 +219,14 @@ int compact(dcsr_handle h, cudaStream_t s) {
   int32_t *nc;
   void *nv;
   DCSR_TRY(alloc_pool(h, cap, &nc, &nv, s));
-  if (h->dtype == DCSR_F32)
-    DCSR_LAUNCH(k_compact_copy<float>, grid_for((int64_t)n * 32, 256), 256, 0, s, h->view<float>(), caps, nc,
-                (float *)nv);
-  else
-    DCSR_LAUNCH(k_compact_copy<double>, grid_for((int64_t)n * 32, 256), 256, 0, s, h->view<double>(), caps, nc,
-                (double *)nv);
+  // row lengths are unchanged, so the schedule stays valid across compaction
+  DCSR_TRY(copy_rows(h, caps, nc, nv, nullptr, nullptr, s));
   DCSR_LAUNCH(k_layout, grid_for(n + 1, 256), 256, 0, s, h->seg, h->row_sizes, n, h->pitch, h->o.max_segs, caps,
               (const long long *)nullptr);
   free_pool(h, s);
   h->cols = nc;
   h->vals = nv;
   h->pool_cap = cap;
-  h->bins_valid = false;
-  return DCSR_OK;
-}
-
-int bin_rows(dcsr_handle h, cudaStream_t s) {
-  const int32_t n = h->n_rows;
-  Arena &ar = h->scratch;
-  DCSR_TRY(ar.reserve(2 * arena_bytes(n + 1, 8) + arena_bytes(n + 1, 4) + radix_scratch_bytes(n), s));
-  unsigned long long *k0 = ar.take<unsigned long long>(n + 1), *k1 = ar.take<unsigned long long>(n + 1);
-  unsigned *v0 = ar.take<unsigned>(n + 1);
-  unsigned *v1 = (unsigned *)h->bin_perm;
-  if (n > 0) {
-    DCSR_LAUNCH(k_bin_keys, grid_for(n, 256), 256, 0, s, h->row_sizes, n, k0, v0);
-    if (n > 1) {
-      DCSR_TRY(radix_sort_pairs(&k0, &v0, &k1, &v1, n, 3, ar, s));  // one 8-bit pass: result in k1/bin_perm
-    } else {
-      DCSR_CUDA(cudaMemcpyAsync(h->bin_perm, v0, sizeof(unsigned), cudaMemcpyDeviceToDevice, s));
-    }
-  }
-  DCSR_LAUNCH(k_bin_info, 1, 32, 0, s, k0, n, h->bin_info);
-  h->bins_valid = true;
   return DCSR_OK;
 }
 
@@ -384,6 +275,22 @@ int dcsr_create(dcsr_handle *out, int32_t n_rows, int32_t n_cols, int32_t dtype,
   if (o.max_segs < 1 || o.max_segs > 8 || o.factor_x16 < 16 || o.align < 1 || (o.align & (o.align - 1)) ||
       o.min_cap < 0 || o.alpha < 0 || o.spare_x16 < 0 || o.min_spare < 0 || (o.mode != DCSR_MERGE && o.mode != DCSR_APPEND))
     return DCSR_BAD_ARG;
+  {
+    // Pools and scratch use stream-ordered allocation; keep freed blocks in
+    // the device's default pool instead of returning them at every sync, so a
+    // compaction's fresh pool does not re-map memory each time.
+    static bool configured[64] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev >= 0 && dev < 64 && !configured[dev]) {
+      cudaMemPool_t mp;
+      if (cudaDeviceGetDefaultMemPool(&mp, dev) == cudaSuccess) {
+        uint64_t thr = UINT64_MAX;
+        cudaMemPoolSetAttribute(mp, cudaMemPoolAttrReleaseThreshold, &thr);
+      }
+      configured[dev] = true;
+    }
+  }
   dcsr_matrix_s *h = new dcsr_matrix_s;
   h->n_rows = n_rows;
   h->n_cols = n_cols;
@@ -396,14 +303,17 @@ int dcsr_create(dcsr_handle *out, int32_t n_rows, int32_t n_cols, int32_t dtype,
   if (cudaMalloc((void **)&h->row_sizes, sizeof(int32_t) * (n_rows + 1)) != cudaSuccess ||
       cudaMalloc((void **)&h->seg, sizeof(int32_t) * (nseg ? nseg : 1)) != cudaSuccess ||
       cudaMalloc((void **)&h->stat, sizeof(long long) * ST_WORDS) != cudaSuccess ||
-      cudaMalloc((void **)&h->bin_perm, sizeof(int32_t) * (n_rows + 1)) != cudaSuccess ||
-      cudaMalloc((void **)&h->bin_info, sizeof(int32_t) * 32) != cudaSuccess)
+      cudaMalloc((void **)&h->long_rows, sizeof(int32_t) * (n_rows + 1)) != cudaSuccess ||
+      cudaMalloc((void **)&h->long_off, sizeof(long long) * (n_rows + 2)) != cudaSuccess ||
+      cudaMalloc((void **)&h->long_cnt, sizeof(int32_t) * (n_rows + 1)) != cudaSuccess ||
+      cudaMalloc((void **)&h->sched_info, sizeof(int32_t) * 32) != cudaSuccess)
     st = DCSR_OOM;
   if (st == DCSR_OK) {
     cudaMemset(h->row_sizes, 0, sizeof(int32_t) * (n_rows + 1));
     cudaMemset(h->seg, 0xff, sizeof(int32_t) * (nseg ? nseg : 1));
     cudaMemset(h->stat, 0, sizeof(long long) * ST_WORDS);
-    cudaMemset(h->bin_info, 0, sizeof(int32_t) * 32);
+    cudaMemset(h->sched_info, 0, sizeof(int32_t) * 32);
+    cudaMemset(h->long_cnt, 0, sizeof(int32_t) * (n_rows + 1));
     st = reserve(h, pool_capacity(o, 0), 0);
     if (cudaDeviceSynchronize() != cudaSuccess) st = DCSR_CUDA_ERROR;
   }
@@ -423,8 +333,11 @@ int dcsr_destroy(dcsr_handle h) {
   cudaFree(h->row_sizes);
   cudaFree(h->seg);
   cudaFree(h->stat);
-  cudaFree(h->bin_perm);
-  cudaFree(h->bin_info);
+  cudaFree(h->long_rows);
+  cudaFree(h->long_off);
+  cudaFree(h->long_cnt);
+  cudaFree(h->sched_info);
+  if (h->part) cudaFree(h->part);
   cudaDeviceSynchronize();
   delete h;
   return DCSR_OK;
@@ -573,16 +486,12 @@ int dcsr_nnz(dcsr_handle h, int64_t *nnz, void *stream) {
 static int export_impl(dcsr_handle h, int32_t *row_ptr, int32_t *rows, int32_t *cols, void *vals, cudaStream_t s) {
   const int32_t n = h->n_rows;
   Arena &ar = h->scratch;
+  if (!h->bins_valid) DCSR_TRY(build_schedule(h, s));  // before taking arena memory
   DCSR_TRY(ar.reserve(arena_bytes(n + 2, 8) + scan_scratch_bytes(n + 1), s));
   long long *rp = ar.take<long long>(n + 2);
   DCSR_LAUNCH(k_lens, grid_for(n + 1, 256), 256, 0, s, h->row_sizes, n, rp);
   DCSR_TRY(scan_i64(rp, rp, n + 1, nullptr, ar, s));
-  const int g = grid_for((int64_t)(n > 0 ? n : 1) * 32, 256);
-  if (h->dtype == DCSR_F32)
-    DCSR_LAUNCH(k_export<float>, g, 256, 0, s, h->view<float>(), rp, row_ptr, rows, cols, (float *)vals);
-  else
-    DCSR_LAUNCH(k_export<double>, g, 256, 0, s, h->view<double>(), rp, row_ptr, rows, cols, (double *)vals);
-  return DCSR_OK;
+  return copy_rows(h, rp, cols, vals, rows, row_ptr, s);
 }
 
 int dcsr_to_csr(dcsr_handle h, int32_t *row_ptr, int32_t *cols, void *vals, void *stream) {
@@ -648,7 +557,7 @@ int dcsr_reserve(dcsr_handle h, int64_t pool_cap, void *stream) {
 
 int dcsr_bin_rows(dcsr_handle h, void *stream) {
   if (!h) return DCSR_BAD_ARG;
-  return bin_rows(h, (cudaStream_t)stream);
+  return build_schedule(h, (cudaStream_t)stream);
 }
 
 const char *dcsr_status_string(int st) {

@@ -25,7 +25,6 @@
 namespace dcsr {
 
 constexpr int UPD_THREADS = 256;
-constexpr int UPD_WARPS = UPD_THREADS / 32;
 constexpr int RT_TILE = 1024;  // relocation: outputs per tile
 constexpr int RT_THREADS = 256;
 constexpr int RT_ITEMS = RT_TILE / RT_THREADS;
@@ -90,32 +89,66 @@ __global__ void k_touched(const unsigned long long *keys, int64_t n, int cb, int
 
 // --------------------------------------------------------------- planning
 
+// Sub-warp of S lanes (S divides 32): lane-local mask, ballot and helpers.
+template <int S>
+struct Sub {
+  int sl, sw;
+  unsigned mask;
+  __device__ __forceinline__ Sub() {
+    const int lane = lane_id();
+    sl = lane & (S - 1);
+    sw = lane / S;
+    mask = S == 32 ? FULL : (((1u << S) - 1u) << (sw * S));
+  }
+  __device__ __forceinline__ unsigned ballot(bool p) const {
+    const unsigned b = __ballot_sync(mask, p);
+    return S == 32 ? b : (b >> (sw * S)) & ((1u << S) - 1u);
+  }
+  __device__ __forceinline__ unsigned full() const { return S == 32 ? FULL : (1u << S) - 1u; }
+  template <typename T>
+  __device__ __forceinline__ T shfl(T v, int src) const { return __shfl_sync(mask, v, src, S); }
+  __device__ __forceinline__ void sync() const { __syncwarp(mask); }
+  __device__ __forceinline__ int incl_scan(int v) const {
+#pragma unroll
+    for (int o = 1; o < S; o <<= 1) {
+      const int w = __shfl_up_sync(mask, v, o, S);
+      if (sl >= o) v += w;
+    }
+    return v;
+  }
+  // consecutive set bits of a lane-local ballot starting at bit 0
+  __device__ __forceinline__ int leading(unsigned bm) const { return bm == full() ? S : __ffs(~bm) - 1; }
+};
+
+constexpr int PLAN_S = 8;     // lanes per touched row in the plan
+constexpr int SMALL_AFF = 96; // apply: rows shifting <= this many entries use 8-lane sub-warps
+
 template <typename V>
 __global__ void __launch_bounds__(UPD_THREADS) k_plan_merge(Mat<V> m, int64_t T, const int32_t *trow,
                                                             const int32_t *tb0, const int32_t *bcol, const V *bval,
                                                             int32_t *bpos, long long *tcap, long long *ttiles,
                                                             int32_t *tmnew, int32_t *tinfo, int32_t *ncol, V *nval,
                                                             int32_t *nins) {
+  constexpr int S = PLAN_S;
   const int64_t nt = m.stat[ST_TOUCHED];
-  const int lane = lane_id();
   const int64_t gthreads = (int64_t)gridDim.x * blockDim.x;
-  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t <= T; t += gthreads)
+  const int64_t gtid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  for (int64_t t = gtid; t <= T; t += gthreads)
     if (t >= nt) {
       tcap[t] = 0;
       ttiles[t] = 0;
     }
-  const unsigned lt = lanemask_lt_u();
-  const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int64_t nwarps = gthreads >> 5;
-  for (int64_t t = gw; t < nt; t += nwarps) {
+  const Sub<S> sub;
+  const unsigned lt = (1u << sub.sl) - 1u;
+  for (int64_t t = gtid / S; t < nt; t += gthreads / S) {
     const int32_t r = trow[t];
     const int32_t b0 = tb0[t], b1 = tb0[t + 1];
     const int64_t L = m.row_sizes[r];
     const Chain ch = load_chain(m, r);
     int32_t mnew = 0;
     int64_t ins0 = L;
-    for (int32_t base = b0; base < b1; base += 32) {
-      const int32_t i = base + lane;
+    for (int32_t base = b0; base < b1; base += S) {
+      const int32_t i = base + sub.sl;
       const bool valid = i < b1;
       const int32_t c = valid ? bcol[i] : 0;
       const bool head = valid && (i == b0 || bcol[i - 1] != c);
@@ -124,15 +157,15 @@ __global__ void __launch_bounds__(UPD_THREADS) k_plan_merge(Mat<V> m, int64_t T,
       if (head) {
         int64_t lo = 0, hi = L;
         while (lo < hi) {
-          int64_t mid = (lo + hi) >> 1;
-          if (m.cols[ch.phys(mid)] < c) lo = mid + 1;
+          const int64_t mid = (lo + hi) >> 1;
+          if (__ldg(m.cols + ch.phys(mid)) < c) lo = mid + 1;
           else hi = mid;
         }
         pos = lo;
-        isnew = !(lo < L && m.cols[ch.phys(lo)] == c);
+        isnew = !(lo < L && __ldg(m.cols + ch.phys(lo)) == c);
         bpos[i] = isnew ? ~(int32_t)pos : (int32_t)pos;
       }
-      const unsigned nm = __ballot_sync(FULL, isnew);
+      const unsigned nm = sub.ballot(isnew);
       if (nm) {
         if (isnew) {
           const int32_t k = mnew + __popc(nm & lt);
@@ -142,28 +175,32 @@ __global__ void __launch_bounds__(UPD_THREADS) k_plan_merge(Mat<V> m, int64_t T,
           nval[b0 + k] = v;
           nins[b0 + k] = (int32_t)pos;
         }
-        const int64_t p0 = __shfl_sync(FULL, pos, __ffs(nm) - 1);
+        const int64_t p0 = sub.shfl(pos, __ffs(nm) - 1);
         if (mnew == 0) ins0 = p0;
         mnew += __popc(nm);
       }
     }
-    if (lane == 0) {
+    if (sub.sl == 0) {
       const int64_t nl = L + mnew;
       int64_t cap = 0;
-      int layer = -1, reloc = 0;
+      int layer = -1, reloc = 0, big = 0;
       if (mnew > 0 && L - ins0 > m.o.reloc_min) {
         reloc = 1;
         layer = 0;
         cap = policy_cap(m.o, nl);
-      } else if (nl > ch.total) {
-        cap = align_up(policy_cap(m.o, nl) - ch.total, m.o.align);
-        layer = ch.total == 0 ? 0 : ch.ns;
-        if (layer >= m.max_segs) atomicOr((unsigned long long *)&m.stat[ST_AUX], (unsigned long long)AUX_LAYER_OVF);
+      } else {
+        big = mnew > 0 && L - ins0 > SMALL_AFF;
+        if (nl > ch.total) {
+          cap = align_up(policy_cap(m.o, nl) - ch.total, m.o.align);
+          layer = ch.total == 0 ? 0 : ch.ns;
+          if (layer >= m.max_segs)
+            atomicOr((unsigned long long *)&m.stat[ST_AUX], (unsigned long long)AUX_LAYER_OVF);
+        }
       }
       tcap[t] = cap;
       ttiles[t] = reloc ? div_up(nl, RT_TILE) : 0;
       tmnew[t] = mnew;
-      tinfo[t] = (layer & 0xff) | (reloc << 8);
+      tinfo[t] = (layer & 0xff) | (reloc << 8) | (big << 9);
     }
   }
 }
@@ -237,7 +274,9 @@ __global__ void k_check(long long *stat, const int32_t *row_sizes, int32_t n_row
 // Old pool top of the running update (row_sizes[n] is only rewritten by k_finish).
 __device__ __forceinline__ long long old_top(const long long *stat) { return stat[ST_NEED] - stat[ST_TOTAL]; }
 
-template <typename V>
+// Apply for the rows of one width class: S = 8 takes rows shifting at most
+// SMALL_AFF entries (and rows without shifts), S = 32 takes the larger ones.
+template <typename V, int S>
 __global__ void __launch_bounds__(UPD_THREADS) k_apply_merge(Mat<V> m, const int32_t *trow, const int32_t *tb0,
                                                              const int32_t *bcol, const V *bval,
                                                              const int32_t *bpos, const long long *addr,
@@ -245,17 +284,18 @@ __global__ void __launch_bounds__(UPD_THREADS) k_apply_merge(Mat<V> m, const int
                                                              const int32_t *ncol, const V *nval,
                                                              const int32_t *nins) {
   if (!m.stat[ST_GO]) return;
-  __shared__ int hist[UPD_WARPS][32];
+  __shared__ int hist[UPD_THREADS / S][S];
   const int64_t nt = m.stat[ST_TOUCHED];
   const long long top = old_top(m.stat);
-  const int lane = lane_id(), w = threadIdx.x >> 5;
-  const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  for (int64_t t = gw; t < nt; t += nwarps) {
+  const Sub<S> sub;
+  int *h = hist[threadIdx.x / S];
+  const int64_t gthreads = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t t = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / S; t < nt; t += gthreads / S) {
+    const int info = tinfo[t];
+    if (((info >> 9) & 1) != (S == 32 ? 1 : 0)) continue;
     const int32_t r = trow[t];
     const int32_t b0 = tb0[t], b1 = tb0[t + 1];
     const int64_t L = m.row_sizes[r];
-    const int info = tinfo[t];
     const bool reloc = (info >> 8) & 1;
     const int layer = (int8_t)(info & 0xff);
     const int32_t mnew = tmnew[t];
@@ -263,22 +303,14 @@ __global__ void __launch_bounds__(UPD_THREADS) k_apply_merge(Mat<V> m, const int
     Chain ch = load_chain(m, r);
     if (!reloc && cap > 0) {
       const int32_t st = (int32_t)(top + addr[t]);
-      if (layer == 0) {
-        ch.ns = 0;
-        ch.total = 0;
-      }
-      ch.st[ch.ns] = st;
-      ch.cp[ch.ns] = (int32_t)cap;
-      ch.ns++;
-      ch.total += cap;
-      if (lane == 0) {
-        int2 p = make_int2(st, (int32_t)(st + cap));
-        *reinterpret_cast<int2 *>(m.seg + (int64_t)layer * m.pitch + 2 * (int64_t)r) = p;
-      }
+      ch.append(st, (int32_t)cap, layer == 0);
+      if (sub.sl == 0)
+        *reinterpret_cast<int2 *>(m.seg + (int64_t)layer * m.pitch + 2 * (int64_t)r) =
+            make_int2(st, (int32_t)(st + cap));
     }
     // 1. existing columns: value += batch values in batch order
-    for (int32_t base = b0; base < b1; base += 32) {
-      const int32_t i = base + lane;
+    for (int32_t base = b0; base < b1; base += S) {
+      const int32_t i = base + sub.sl;
       if (i < b1) {
         const int32_t c = bcol[i];
         if ((i == b0 || bcol[i - 1] != c) && bpos[i] >= 0) {
@@ -289,37 +321,35 @@ __global__ void __launch_bounds__(UPD_THREADS) k_apply_merge(Mat<V> m, const int
         }
       }
     }
-    __syncwarp();
+    sub.sync();
     if (!reloc && mnew > 0) {
       // 2. shift the entries after the first insertion point, back to front,
-      //    32 per step; shift(i) = #{new k : nins[k] <= i}
+      //    S per step; shift(i) = #{new k : nins[k] <= i}
       const int32_t *ins = nins + b0;
       const int64_t lo_a = ins[0];
       int32_t khi = mnew;
       for (;;) {
-        const int32_t k = khi - 1 - lane;
-        const unsigned bm = __ballot_sync(FULL, k >= 0 && ins[k] >= L);
-        const int cnt = bm == FULL ? 32 : __ffs(~bm) - 1;
+        const int32_t k = khi - 1 - sub.sl;
+        const int cnt = sub.leading(sub.ballot(k >= 0 && ins[k] >= L));
         khi -= cnt;
-        if (cnt < 32) break;
+        if (cnt < S) break;
       }
       int64_t c1 = L;
       while (c1 > lo_a) {
-        const int64_t c0 = c1 - 32 > lo_a ? c1 - 32 : lo_a;
+        const int64_t c0 = c1 - S > lo_a ? c1 - S : lo_a;
         int32_t klo = khi;
         for (;;) {
-          const int32_t k = klo - 1 - lane;
-          const unsigned bm = __ballot_sync(FULL, k >= 0 && ins[k] >= c0);
-          const int cnt = bm == FULL ? 32 : __ffs(~bm) - 1;
+          const int32_t k = klo - 1 - sub.sl;
+          const int cnt = sub.leading(sub.ballot(k >= 0 && ins[k] >= c0));
           klo -= cnt;
-          if (cnt < 32) break;
+          if (cnt < S) break;
         }
-        hist[w][lane] = 0;
-        __syncwarp();
-        for (int32_t k = klo + lane; k < khi; k += 32) atomicAdd(&hist[w][ins[k] - c0], 1);
-        __syncwarp();
-        const int inc = warp_incl_scan(hist[w][lane]);
-        const int64_t i = c0 + lane;
+        h[sub.sl] = 0;
+        sub.sync();
+        for (int32_t k = klo + sub.sl; k < khi; k += S) atomicAdd(&h[ins[k] - c0], 1);
+        sub.sync();
+        const int inc = sub.incl_scan(h[sub.sl]);
+        const int64_t i = c0 + sub.sl;
         const bool act = i < c1;
         int32_t col = 0;
         V val = V(0);
@@ -330,24 +360,24 @@ __global__ void __launch_bounds__(UPD_THREADS) k_apply_merge(Mat<V> m, const int
           val = m.vals[src];
           dst = ch.phys(i + klo + inc);
         }
-        __syncwarp();
+        sub.sync();
         if (act) {
           m.cols[dst] = col;
           m.vals[dst] = val;
         }
-        __syncwarp();
+        sub.sync();
         c1 = c0;
         khi = klo;
       }
       // 3. new columns at nins[k] + k
-      for (int32_t k = lane; k < mnew; k += 32) {
+      for (int32_t k = sub.sl; k < mnew; k += S) {
         const int64_t q = ch.phys((int64_t)ins[k] + k);
         m.cols[q] = ncol[b0 + k];
         m.vals[q] = nval[b0 + k];
       }
     }
-    if (!reloc && lane == 0) m.row_sizes[r] = (int32_t)(L + mnew);
-    __syncwarp();
+    if (!reloc && sub.sl == 0) m.row_sizes[r] = (int32_t)(L + mnew);
+    sub.sync();
   }
 }
 
@@ -451,13 +481,7 @@ __global__ void __launch_bounds__(UPD_THREADS) k_apply_append(Mat<V> m, const in
     Chain ch = load_chain(m, r);
     if (cap > 0) {
       const int32_t st = (int32_t)(top + addr[t]);
-      if (layer == 0) {
-        ch.ns = 0;
-        ch.total = 0;
-      }
-      ch.st[ch.ns] = st;
-      ch.cp[ch.ns] = (int32_t)cap;
-      ch.ns++;
+      ch.append(st, (int32_t)cap, layer == 0);
       if (lane == 0)
         *reinterpret_cast<int2 *>(m.seg + (int64_t)layer * m.pitch + 2 * (int64_t)r) =
             make_int2(st, (int32_t)(st + cap));
@@ -513,11 +537,12 @@ static int update_impl(dcsr_handle h, const int32_t *rows, const int32_t *cols, 
   int32_t *tinfo = (int32_t *)p1;
   int32_t *ncol = (int32_t *)k1;
   int32_t *nins = ncol + T;
-  static int g_plan = 0, g_apply = 0, g_reloc = 0;
+  static int g_plan = 0, g_apply = 0, g_apply8 = 0, g_reloc = 0;
   if (!g_plan) {
-    g_plan = persistent_grid((const void *)k_plan_merge<float>, UPD_THREADS, 0);
-    g_apply = persistent_grid((const void *)k_apply_merge<float>, UPD_THREADS, 0);
-    g_reloc = persistent_grid((const void *)k_relocate<float>, RT_THREADS, 0);
+    g_plan = persistent_grid((const void *)k_plan_merge<double>, UPD_THREADS, 0);
+    g_apply = persistent_grid((const void *)k_apply_merge<double, 32>, UPD_THREADS, 0);
+    g_apply8 = persistent_grid((const void *)k_apply_merge<double, 8>, UPD_THREADS, 0);
+    g_reloc = persistent_grid((const void *)k_relocate<double>, RT_THREADS, 0);
   }
   if (merge) {
     DCSR_LAUNCH(k_plan_merge<V>, g_plan, UPD_THREADS, 0, s, m, T, trow, tb0, bcol, bval, bpos, tcap, ttiles, tmnew,
@@ -529,8 +554,10 @@ static int update_impl(dcsr_handle h, const int32_t *rows, const int32_t *cols, 
   if (merge) DCSR_TRY(scan_i64(ttiles, ttiles, T + 1, h->stat + ST_TILES, ar, s));
   DCSR_LAUNCH(k_check, 1, 1, 0, s, h->stat, h->row_sizes, h->n_rows, h->pool_cap);
   if (merge) {
-    DCSR_LAUNCH(k_apply_merge<V>, g_apply, UPD_THREADS, 0, s, m, trow, tb0, bcol, bval, bpos, tcap, tmnew, tinfo,
-                ncol, nval, nins);
+    DCSR_LAUNCH((k_apply_merge<V, 8>), g_apply8, UPD_THREADS, 0, s, m, trow, tb0, bcol, bval, bpos, tcap, tmnew,
+                tinfo, ncol, nval, nins);
+    DCSR_LAUNCH((k_apply_merge<V, 32>), g_apply, UPD_THREADS, 0, s, m, trow, tb0, bcol, bval, bpos, tcap, tmnew,
+                tinfo, ncol, nval, nins);
     DCSR_LAUNCH(k_relocate<V>, g_reloc, RT_THREADS, 0, s, m, trow, tb0, tcap, ttiles, tmnew, ncol, nval);
   } else {
     DCSR_LAUNCH(k_apply_append<V>, g_apply, UPD_THREADS, 0, s, m, trow, tb0, bcol, bval, tcap, tinfo);

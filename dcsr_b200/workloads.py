@@ -28,7 +28,12 @@ import numpy as np
 
 
 def _csr_from_keys(keys: np.ndarray, n_rows: int, n_cols: int):
-    keys = np.unique(keys)
+    keys = np.sort(keys, kind="stable")
+    if keys.size:
+        keep = np.empty(keys.size, bool)
+        keep[0] = True
+        np.not_equal(keys[1:], keys[:-1], out=keep[1:])
+        keys = keys[keep]
     rows = (keys // n_cols).astype(np.int32)
     cols = (keys % n_cols).astype(np.int32)
     counts = np.bincount(rows, minlength=n_rows)

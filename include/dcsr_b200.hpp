@@ -1,0 +1,181 @@
+// dcsr_b200.hpp -- C++ host mirror of the reference's operator interface.
+//
+// The reference (Vizerai/DCSR) exposes header-only templates in
+// `namespace device` operating on `dcsr_matrix<INDEX_TYPE, VALUE_TYPE,
+// MEM_TYPE, BINS>`.  This header keeps those names and argument meanings on
+// top of the C ABI in dcsr_b200.h, so a caller of the reference can switch by
+// changing the include and the matrix type:
+//
+//   reference (include/...)                      here
+//   dcsr_matrix::resize(rows, cols, bin, factor)  dcsr::dcsr_matrix<V>::resize
+//   device::Initialize_Matrix   load.h:8          device::Initialize_Matrix
+//   device::LoadMatrix(dcsr, rows, cols, vals, N) load.h:27   (COO, any order)
+//   device::LoadMatrix(dcsr, csr)      load.h:207  (row_ptr, cols, vals)
+//   device::LoadMatrix(csr, dcsr)      load.h:232  device::ExportCSR
+//   device::UpdateMatrix(dcsr, r, c, v, permuted) load.h:258
+//   device::SortMatrixRow(dcsr, streams) load.h:404  (compaction)
+//   device::BinRows(dcsr)              load.h:583
+//   device::spmv(dcsr, x, y, streams)  spmv.h:121
+//   device::spmm(A, B, C, streams)     spmm.h:30
+//   device::count_sorted_indices(I, X, n) primitives.h:417
+//
+// Differences, by design: errors are returned as dcsr_status (the reference
+// returned void and wrote out of bounds on overflow); every call takes one
+// stream instead of the reference's eight global streams; bins live in the
+// matrix (no __constant__ table), so several matrices can be used at once.
+#pragma once
+
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+
+#include "dcsr_b200.h"
+
+namespace dcsr {
+
+struct error : std::runtime_error {
+  int status;
+  error(int st, const char *what) : std::runtime_error(std::string(what) + ": " + dcsr_status_string(st)), status(st) {}
+};
+
+inline void check(int st, const char *what) {
+  if (st != DCSR_OK) throw error(st, what);
+}
+
+template <typename V>
+struct dtype_of;
+template <>
+struct dtype_of<float> {
+  static constexpr int32_t value = DCSR_F32;
+};
+template <>
+struct dtype_of<double> {
+  static constexpr int32_t value = DCSR_F64;
+};
+
+// RAII owner of one device-resident DCSR matrix.
+template <typename V>
+class dcsr_matrix {
+ public:
+  dcsr_matrix() = default;
+  dcsr_matrix(int32_t rows, int32_t cols, int32_t mode = DCSR_MERGE) { resize(rows, cols, mode); }
+  ~dcsr_matrix() { reset(); }
+  dcsr_matrix(const dcsr_matrix &) = delete;  // the reference's raw-pointer copy double-freed
+  dcsr_matrix &operator=(const dcsr_matrix &) = delete;
+  dcsr_matrix(dcsr_matrix &&o) noexcept : h_(o.h_), rows_(o.rows_), cols_(o.cols_) { o.h_ = nullptr; }
+
+  // reference dcsr_matrix::resize(n_rows, n_cols, bin_size, factor): here
+  // the per-row slack factor is the policy's factor (x16 fixed point).
+  void resize(int32_t rows, int32_t cols, int32_t mode = DCSR_MERGE, float factor = 0.f, int32_t max_segs = 4) {
+    reset();
+    dcsr_opts o;
+    dcsr_default_opts(&o, mode);
+    if (factor >= 1.f) o.factor_x16 = (int32_t)(factor * 16.f + 0.5f);
+    o.max_segs = max_segs;
+    check(dcsr_create(&h_, rows, cols, dtype_of<V>::value, &o), "dcsr_create");
+    rows_ = rows;
+    cols_ = cols;
+  }
+  void resize(int32_t rows, int32_t cols, const dcsr_opts &o) {
+    reset();
+    check(dcsr_create(&h_, rows, cols, dtype_of<V>::value, &o), "dcsr_create");
+    rows_ = rows;
+    cols_ = cols;
+  }
+  void reset() {
+    if (h_) dcsr_destroy(h_);
+    h_ = nullptr;
+  }
+  dcsr_handle handle() const { return h_; }
+  int32_t num_rows() const { return rows_; }
+  int32_t num_cols() const { return cols_; }
+  int64_t num_entries(void *stream = nullptr) const {
+    int64_t n = 0;
+    check(dcsr_nnz(h_, &n, stream), "dcsr_nnz");
+    return n;
+  }
+  dcsr_info_t info() const {
+    dcsr_info_t i;
+    check(dcsr_info(h_, &i), "dcsr_info");
+    return i;
+  }
+
+ private:
+  dcsr_handle h_ = nullptr;
+  int32_t rows_ = 0, cols_ = 0;
+};
+
+}  // namespace dcsr
+
+// Reference operator names (namespace device, include/load.h etc.).
+namespace device {
+
+// The reference initialised each row with a bin_length chunk that the load
+// then overwrote (include/sparse_update.inl:1158-1176); a fresh handle is
+// already an empty, valid matrix, so this only validates the handle.
+template <typename V>
+inline void Initialize_Matrix(dcsr::dcsr_matrix<V> &mat) {
+  if (!mat.handle()) throw dcsr::error(DCSR_BAD_ARG, "Initialize_Matrix");
+}
+
+// COO -> DCSR (device pointers; any order, duplicates merged in MERGE mode).
+template <typename V>
+inline void LoadMatrix(dcsr::dcsr_matrix<V> &dst, const int32_t *rows, const int32_t *cols, const V *vals, int64_t N,
+                       void *stream = nullptr) {
+  dcsr::check(dcsr_from_coo(dst.handle(), rows, cols, vals, N, stream), "LoadMatrix(coo)");
+}
+
+// CSR -> DCSR (device pointers).
+template <typename V>
+inline void LoadMatrix(dcsr::dcsr_matrix<V> &dst, const int32_t *row_ptr, const int32_t *cols, const V *vals,
+                       int64_t nnz, bool /*csr*/, void *stream = nullptr) {
+  dcsr::check(dcsr_from_csr(dst.handle(), row_ptr, cols, vals, nnz, stream), "LoadMatrix(csr)");
+}
+
+// DCSR -> CSR (device pointers sized n_rows+1 / num_entries()).
+template <typename V>
+inline void ExportCSR(const dcsr::dcsr_matrix<V> &src, int32_t *row_ptr, int32_t *cols, V *vals,
+                      void *stream = nullptr) {
+  dcsr::check(dcsr_to_csr(src.handle(), row_ptr, cols, vals, stream), "LoadMatrix(csr, dcsr)");
+}
+
+// Batch update.  The reference's `permuted` flag chose its thread layout;
+// here the matrix mode (MERGE / APPEND) chooses the semantics and the call
+// applies the repair policy (compact, grow) when the pool or layers run out.
+template <typename V>
+inline int UpdateMatrix(dcsr::dcsr_matrix<V> &mat, const int32_t *rows, const int32_t *cols, const V *vals, int64_t N,
+                        void *stream = nullptr) {
+  int st = dcsr_update_sync(mat.handle(), rows, cols, vals, N, stream);
+  if (st == DCSR_BAD_ARG || st == DCSR_OOM || st == DCSR_CUDA_ERROR) throw dcsr::error(st, "UpdateMatrix");
+  return st;
+}
+
+// Defragmentation (the reference's SortMatrixRow does not sort columns; it
+// copies each row's segment chain contiguously).
+template <typename V>
+inline void SortMatrixRow(dcsr::dcsr_matrix<V> &mat, void *stream = nullptr) {
+  dcsr::check(dcsr_compact(mat.handle(), stream), "SortMatrixRow");
+}
+
+template <typename V>
+inline void BinRows(dcsr::dcsr_matrix<V> &mat, void *stream = nullptr) {
+  dcsr::check(dcsr_bin_rows(mat.handle(), stream), "BinRows");
+}
+
+// y = A x (device pointers); k right-hand sides in row-major [n_cols, k].
+template <typename V>
+inline void spmv(const dcsr::dcsr_matrix<V> &A, const V *x, V *y, void *stream = nullptr, int32_t k = 1) {
+  dcsr::check(dcsr_spmv(A.handle(), x, k, k, y, k, 1.0, 0.0, stream), "spmv");
+}
+
+template <typename V>
+inline void spmm(const dcsr::dcsr_matrix<V> &A, const dcsr::dcsr_matrix<V> &B, dcsr::dcsr_matrix<V> &C,
+                 void *stream = nullptr) {
+  dcsr::check(dcsr_spgemm(A.handle(), B.handle(), C.handle(), stream), "spmm");
+}
+
+inline void count_sorted_indices(const int32_t *I, int32_t *X, int64_t size, void *stream = nullptr) {
+  dcsr::check(dcsr_count_sorted_indices(I, size, X, stream), "count_sorted_indices");
+}
+
+}  // namespace device
