@@ -197,26 +197,32 @@ __device__ __forceinline__ T warp_incl_scan(T v) {
 }
 
 // A row's linked segments (at most 8), read from the segment table.
-// st0/cp0 repeat segment 0 in registers for the single-segment fast path.
+// A row's linked segments.  MAX_SEGS is the compile-time layer limit (the
+// reference's MAX_OFFSET = 4); every loop over layers is fully unrolled so
+// the arrays stay in registers (dynamic indexing would put them in local
+// memory, which measured more traffic than the data itself).
+constexpr int MAX_SEGS = 4;
 struct Chain {
-  int32_t st0, cp0;
-  int32_t st[8];
-  int32_t cp[8];
+  int32_t st[MAX_SEGS];
+  int32_t cp[MAX_SEGS];
   int ns;
   int64_t total;
+  // Physical slot of logical position p (predicated, no early exit: keeps
+  // the arrays in registers in every caller).
   __device__ __forceinline__ int64_t phys(int64_t p) const {
-    if (p < cp0) return (int64_t)st0 + p;
-    p -= cp0;
-#pragma unroll 1
-    for (int i = 1; i < ns; i++) {
-      if (p < cp[i]) return (int64_t)st[i] + p;
-      p -= cp[i];
+    int64_t q = -1;
+    bool done = false;
+#pragma unroll
+    for (int i = 0; i < MAX_SEGS; i++) {
+      const bool live = !done && i < ns;
+      if (live && p < cp[i]) {
+        q = (int64_t)st[i] + p;
+        done = true;
+      } else if (live) {
+        p -= cp[i];
+      }
     }
-    return -1;
-  }
-  __device__ __forceinline__ void set0(int32_t s, int32_t c) {
-    st0 = st[0] = s;
-    cp0 = cp[0] = c;
+    return q;
   }
   // Link a new last segment (layer ns); reset=true replaces the whole chain.
   __device__ __forceinline__ void append(int32_t s, int32_t c, bool reset) {
@@ -224,9 +230,12 @@ struct Chain {
       ns = 0;
       total = 0;
     }
-    if (ns == 0) set0(s, c);
-    st[ns] = s;
-    cp[ns] = c;
+#pragma unroll
+    for (int i = 0; i < MAX_SEGS; i++)
+      if (i == ns) {
+        st[i] = s;
+        cp[i] = c;
+      }
     ns++;
     total += c;
   }
@@ -237,20 +246,24 @@ __device__ __forceinline__ Chain load_chain(const Mat<V> &m, int32_t r) {
   Chain c;
   c.ns = 0;
   c.total = 0;
-  c.st0 = 0;
-  c.cp0 = 0;
-#pragma unroll 1
-  for (int l = 0; l < m.max_segs; l++) {
-    int2 p = *reinterpret_cast<const int2 *>(m.seg + (int64_t)l * m.pitch + 2 * (int64_t)r);
-    if (p.x < 0) break;
-    if (l == 0) {
-      c.st0 = p.x;
-      c.cp0 = p.y - p.x;
+  bool open = true;
+#pragma unroll
+  for (int l = 0; l < MAX_SEGS; l++) {
+    c.st[l] = 0;
+    c.cp[l] = 0;
+    if (open && l < m.max_segs) {
+      const int2 p = __ldg(reinterpret_cast<const int2 *>(m.seg + (int64_t)l * m.pitch + 2 * (int64_t)r));
+      if (p.x < 0) {
+        open = false;
+      } else {
+        c.st[l] = p.x;
+        c.cp[l] = p.y - p.x;
+        c.total += p.y - p.x;
+        c.ns = l + 1;
+      }
+    } else {
+      open = false;
     }
-    c.st[c.ns] = p.x;
-    c.cp[c.ns] = p.y - p.x;
-    c.total += p.y - p.x;
-    c.ns++;
   }
   return c;
 }

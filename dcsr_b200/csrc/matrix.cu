@@ -272,7 +272,7 @@ int dcsr_create(dcsr_handle *out, int32_t n_rows, int32_t n_cols, int32_t dtype,
   dcsr_opts o;
   if (opts) o = *opts;
   else dcsr_default_opts(&o, DCSR_MERGE);
-  if (o.max_segs < 1 || o.max_segs > 8 || o.factor_x16 < 16 || o.align < 1 || (o.align & (o.align - 1)) ||
+  if (o.max_segs < 1 || o.max_segs > MAX_SEGS || o.factor_x16 < 16 || o.align < 1 || (o.align & (o.align - 1)) ||
       o.min_cap < 0 || o.alpha < 0 || o.spare_x16 < 0 || o.min_spare < 0 || (o.mode != DCSR_MERGE && o.mode != DCSR_APPEND))
     return DCSR_BAD_ARG;
   {

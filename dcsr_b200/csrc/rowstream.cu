@@ -228,9 +228,9 @@ __global__ void __launch_bounds__(RS_THREADS_) k_rows_reduce(Mat<V> m, const int
       double acc[K];
 #pragma unroll
       for (int k = 0; k < K; k++) acc[k] = op_init<OP>();
-      const bool fast = ch.cp0 >= c1;  // chunk inside layer 0
-      if (fast && ((ch.st0 + c0) & 3) == 0 && sizeof(V) == 4) {
-        const int64_t base = ch.st0 + c0;
+      const bool fast = ch.cp[0] >= c1;  // chunk inside layer 0
+      if (fast && ((ch.st[0] + c0) & 3) == 0 && sizeof(V) == 4) {
+        const int64_t base = ch.st[0] + c0;
         const int64_t nv = (c1 - c0) >> 2;
         for (int64_t v = threadIdx.x; v < nv; v += RS_THREADS_) {
           const float4 a4 = __ldcs(reinterpret_cast<const float4 *>(m.vals + base) + v);
@@ -252,14 +252,14 @@ __global__ void __launch_bounds__(RS_THREADS_) k_rows_reduce(Mat<V> m, const int
         }
         for (int64_t p = c0 + (nv << 2) + threadIdx.x; p < c1; p += RS_THREADS_) {
           double c[K];
-          contrib<V, K, OP, VEC>(m, ch.st0 + p, x, ldx, c);
+          contrib<V, K, OP, VEC>(m, ch.st[0] + p, x, ldx, c);
 #pragma unroll
           for (int k = 0; k < K; k++) acc[k] = op_comb<OP>(acc[k], c[k]);
         }
       } else {
         for (int64_t p = c0 + threadIdx.x; p < c1; p += RS_THREADS_) {
           double c[K];
-          contrib<V, K, OP, VEC>(m, fast ? ch.st0 + p : ch.phys(p), x, ldx, c);
+          contrib<V, K, OP, VEC>(m, fast ? ch.st[0] + p : ch.phys(p), x, ldx, c);
 #pragma unroll
           for (int k = 0; k < K; k++) acc[k] = op_comb<OP>(acc[k], c[k]);
         }
@@ -386,9 +386,9 @@ __global__ void __launch_bounds__(RS_THREADS_) k_rows_copy(Mat<V> m, const int32
       const int64_t c0 = chunk * CHUNK, c1 = c0 + CHUNK < L ? c0 + CHUNK : L;
       const int64_t d = dst_off[row];
       if (out_rowptr && chunk == 0 && threadIdx.x == 0) out_rowptr[row] = (int32_t)d;
-      const bool fast = ch.cp0 >= c1;
+      const bool fast = ch.cp[0] >= c1;
       for (int64_t p = c0 + threadIdx.x; p < c1; p += RS_THREADS_) {
-        const int64_t q = fast ? (int64_t)ch.st0 + p : ch.phys(p);
+        const int64_t q = fast ? (int64_t)ch.st[0] + p : ch.phys(p);
         out_cols[d + p] = __ldcs(m.cols + q);
         out_vals[d + p] = __ldcs(m.vals + q);
         if (out_rows) out_rows[d + p] = row;

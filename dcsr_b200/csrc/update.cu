@@ -123,6 +123,123 @@ struct Sub {
 constexpr int PLAN_S = 8;     // lanes per touched row in the plan
 constexpr int SMALL_AFF = 96; // apply: rows shifting <= this many entries use 8-lane sub-warps
 
+// MERGE plan, step 1 (thread per batch entry): every (row, col) group head
+// binary-searches its column in the row: bpos = position (existing) or
+// ~insertion point (new); nflag = 1 for new columns.
+template <typename V>
+__global__ void k_head_search(Mat<V> m, const unsigned long long *keys, int64_t T, int cb, const int32_t *bcol,
+                              int32_t *bpos, long long *nflag) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i <= T; i += stride) {
+    if (i == T) {
+      nflag[T] = 0;
+      continue;
+    }
+    const unsigned long long k = keys[i];
+    long long isnew = 0;
+    if (i == 0 || keys[i - 1] != k) {
+      const int32_t r = (int32_t)(k >> cb);
+      const int32_t c = bcol[i];
+      const int64_t L = m.row_sizes[r];
+      const Chain ch = load_chain(m, r);
+      int64_t lo = 0, hi = L;
+      while (lo < hi) {
+        const int64_t mid = (lo + hi) >> 1;
+        if (__ldg(m.cols + ch.phys(mid)) < c) lo = mid + 1;
+        else hi = mid;
+      }
+      isnew = !(lo < L && __ldg(m.cols + ch.phys(lo)) == c);
+      bpos[i] = isnew ? ~(int32_t)lo : (int32_t)lo;
+    }
+    nflag[i] = isnew;
+  }
+}
+
+// MERGE plan, step 2 (thread per batch entry): new groups are written, in
+// column order, to slot b0 + k of their row (k from the scan of nflag), with
+// their batch-order sum.
+template <typename V>
+__global__ void k_new_compact(const unsigned long long *keys, int64_t T, int cb, const int32_t *bcol, const V *bval,
+                              const int32_t *bpos, const long long *nflag_excl, const long long *hpos,
+                              const int32_t *tb0, int32_t *ncol, V *nval, int32_t *nins) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < T; i += stride) {
+    const unsigned long long k = keys[i];
+    if (i > 0 && keys[i - 1] == k) continue;
+    if (bpos[i] >= 0) continue;  // existing column
+    const bool rowhead = i == 0 || (keys[i - 1] >> cb) != (k >> cb);
+    const int64_t t = hpos[i] - (rowhead ? 0 : 1);
+    const int32_t b0 = tb0[t];
+    const int64_t slot = b0 + (nflag_excl[i] - nflag_excl[b0]);
+    V v = bval[i];
+    for (int64_t j = i + 1; j < T && keys[j] == k; j++) v = v + bval[j];
+    ncol[slot] = bcol[i];
+    nval[slot] = v;
+    nins[slot] = ~bpos[i];
+  }
+}
+
+// MERGE plan, step 3 (thread per touched row): new length, capacity, layer,
+// relocation decision and apply width class.
+template <typename V>
+__global__ void k_row_plan(Mat<V> m, int64_t T, const int32_t *trow, const int32_t *tb0, const long long *nflag_excl,
+                           const int32_t *nins, long long *tcap, long long *ttiles, int32_t *tmnew, int32_t *tinfo) {
+  const int64_t nt = m.stat[ST_TOUCHED];
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t <= T; t += stride) {
+    if (t >= nt) {
+      tcap[t] = 0;
+      ttiles[t] = 0;
+      continue;
+    }
+    const int32_t r = trow[t];
+    const int32_t b0 = tb0[t], b1 = tb0[t + 1];
+    const int64_t L = m.row_sizes[r];
+    const int64_t mnew = nflag_excl[b1] - nflag_excl[b0];
+    const int64_t ins0 = mnew > 0 ? nins[b0] : L;
+    const Chain ch = load_chain(m, r);
+    const int64_t nl = L + mnew;
+    int64_t cap = 0;
+    int layer = -1, reloc = 0, big = 0;
+    if (mnew > 0 && L - ins0 > m.o.reloc_min) {
+      reloc = 1;
+      layer = 0;
+      cap = policy_cap(m.o, nl);
+    } else {
+      big = mnew > 0 && L - ins0 > SMALL_AFF;
+      if (nl > ch.total) {
+        cap = align_up(policy_cap(m.o, nl) - ch.total, m.o.align);
+        layer = ch.total == 0 ? 0 : ch.ns;
+        if (layer >= m.max_segs) atomicOr((unsigned long long *)&m.stat[ST_AUX], (unsigned long long)AUX_LAYER_OVF);
+      }
+    }
+    tcap[t] = cap;
+    ttiles[t] = reloc ? div_up(nl, RT_TILE) : 0;
+    tmnew[t] = (int32_t)mnew;
+    tinfo[t] = (layer & 0xff) | (reloc << 8) | (big << 9) | ((mnew > 0 || cap > 0) ? (1 << 10) : 0);
+  }
+}
+
+// Apply, step 1 (thread per batch group): existing columns take their batch
+// values in batch order, in place, before any shift or relocation reads them.
+template <typename V>
+__global__ void k_apply_existing(Mat<V> m, const unsigned long long *keys, int64_t T, int cb, const V *bval,
+                                 const int32_t *bpos) {
+  if (!m.stat[ST_GO]) return;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < T; i += stride) {
+    const unsigned long long k = keys[i];
+    if (i > 0 && keys[i - 1] == k) continue;
+    const int32_t p = bpos[i];
+    if (p < 0) continue;
+    const Chain ch = load_chain(m, (int32_t)(k >> cb));
+    const int64_t q = ch.phys(p);
+    V v = m.vals[q];
+    for (int64_t j = i; j < T && keys[j] == k; j++) v = v + bval[j];
+    m.vals[q] = v;
+  }
+}
+
 template <typename V>
 __global__ void __launch_bounds__(UPD_THREADS) k_plan_merge(Mat<V> m, int64_t T, const int32_t *trow,
                                                             const int32_t *tb0, const int32_t *bcol, const V *bval,
@@ -227,21 +344,22 @@ __global__ void k_plan_append(Mat<V> m, int64_t T, const int32_t *trow, const in
       cap = rlB + m.o.alpha;
       layer = 0;
     } else {
+      // segment holding position rlA (reference walk :77-88): the first
+      // whose cumulative capacity reaches rlA; free = that capacity - rlA
       const Chain ch = load_chain(m, r);
       int off = 0;
-      int64_t nxt;
-      if (rlA > 0) {
-        int64_t a = 0;
-        while (a < rlA && off < ch.ns) {  // bounded by the linked layers
-          a += ch.cp[off];
-          if (a < rlA && off + 1 < ch.ns) off++;
-          else break;
+      int64_t before = 0, after = 0;
+      bool found = false;
+#pragma unroll
+      for (int i = 0; i < MAX_SEGS; i++) {
+        if (!found && i < ch.ns) {
+          after = before + ch.cp[i];
+          off = i;
+          if (after >= rlA || i + 1 >= ch.ns) found = true;
+          else before = after;
         }
-        nxt = (int64_t)ch.st[off] + ch.cp[off] + rlA - a;
-      } else {
-        nxt = ch.st[0];
       }
-      const int64_t fr = (int64_t)ch.st[off] + ch.cp[off] - nxt;
+      const int64_t fr = after - rlA;
       if (fr < rlB) {
         cap = rlB - fr + m.o.alpha;
         layer = off + 1;
@@ -292,7 +410,7 @@ __global__ void __launch_bounds__(UPD_THREADS) k_apply_merge(Mat<V> m, const int
   const int64_t gthreads = (int64_t)gridDim.x * blockDim.x;
   for (int64_t t = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / S; t < nt; t += gthreads / S) {
     const int info = tinfo[t];
-    if (((info >> 9) & 1) != (S == 32 ? 1 : 0)) continue;
+    if (!((info >> 10) & 1) || ((info >> 9) & 1) != (S == 32 ? 1 : 0) || ((info >> 8) & 1)) continue;
     const int32_t r = trow[t];
     const int32_t b0 = tb0[t], b1 = tb0[t + 1];
     const int64_t L = m.row_sizes[r];
@@ -308,20 +426,7 @@ __global__ void __launch_bounds__(UPD_THREADS) k_apply_merge(Mat<V> m, const int
         *reinterpret_cast<int2 *>(m.seg + (int64_t)layer * m.pitch + 2 * (int64_t)r) =
             make_int2(st, (int32_t)(st + cap));
     }
-    // 1. existing columns: value += batch values in batch order
-    for (int32_t base = b0; base < b1; base += S) {
-      const int32_t i = base + sub.sl;
-      if (i < b1) {
-        const int32_t c = bcol[i];
-        if ((i == b0 || bcol[i - 1] != c) && bpos[i] >= 0) {
-          const int64_t q = ch.phys(bpos[i]);
-          V v = m.vals[q];
-          for (int32_t j = i; j < b1 && bcol[j] == c; j++) v = v + bval[j];
-          m.vals[q] = v;
-        }
-      }
-    }
-    sub.sync();
+    // (existing columns were updated by k_apply_existing)
     if (!reloc && mnew > 0) {
       // 2. shift the entries after the first insertion point, back to front,
       //    S per step; shift(i) = #{new k : nins[k] <= i}
@@ -512,7 +617,7 @@ static int update_impl(dcsr_handle h, const int32_t *rows, const int32_t *cols, 
   const int bits = merge ? rb + cb : rb;
   Arena &ar = h->scratch;
   size_t need = 2 * arena_bytes(T, 8) + 2 * arena_bytes(T, 4) + 5 * arena_bytes(T + 2, 4) +
-                2 * arena_bytes(T, sizeof(V)) + 3 * arena_bytes(T + 2, 8) + radix_scratch_bytes(T) +
+                2 * arena_bytes(T, sizeof(V)) + 4 * arena_bytes(T + 2, 8) + radix_scratch_bytes(T) +
                 scan_scratch_bytes(T + 2);
   DCSR_TRY(ar.reserve(need, s));
   unsigned long long *k0 = ar.take<unsigned long long>(T), *k1 = ar.take<unsigned long long>(T);
@@ -522,6 +627,7 @@ static int update_impl(dcsr_handle h, const int32_t *rows, const int32_t *cols, 
   V *bval = ar.take<V>(T), *nval = ar.take<V>(T);
   long long *hflag = ar.take<long long>(T + 2), *tcap = ar.take<long long>(T + 2);
   long long *ttiles = ar.take<long long>(T + 2);
+  long long *nflag = ar.take<long long>(T + 2);
   // tinfo / ncol / nins reuse the sort buffers once the sort is done
   Mat<V> m = h->view<V>();
 
@@ -545,8 +651,11 @@ static int update_impl(dcsr_handle h, const int32_t *rows, const int32_t *cols, 
     g_reloc = persistent_grid((const void *)k_relocate<double>, RT_THREADS, 0);
   }
   if (merge) {
-    DCSR_LAUNCH(k_plan_merge<V>, g_plan, UPD_THREADS, 0, s, m, T, trow, tb0, bcol, bval, bpos, tcap, ttiles, tmnew,
-                tinfo, ncol, nval, nins);
+    const int gT = grid_for(T + 1, 256);
+    DCSR_LAUNCH(k_head_search<V>, gT, 256, 0, s, m, k0, T, cb, bcol, bpos, nflag);
+    DCSR_TRY(scan_i64(nflag, nflag, T + 1, nullptr, ar, s));
+    DCSR_LAUNCH(k_new_compact<V>, gT, 256, 0, s, k0, T, cb, bcol, bval, bpos, nflag, hflag, tb0, ncol, nval, nins);
+    DCSR_LAUNCH(k_row_plan<V>, gT, 256, 0, s, m, T, trow, tb0, nflag, nins, tcap, ttiles, tmnew, tinfo);
   } else {
     DCSR_LAUNCH(k_plan_append<V>, grid_for(T + 1, 256), 256, 0, s, m, T, trow, tb0, tcap, ttiles, tmnew, tinfo);
   }
@@ -554,6 +663,7 @@ static int update_impl(dcsr_handle h, const int32_t *rows, const int32_t *cols, 
   if (merge) DCSR_TRY(scan_i64(ttiles, ttiles, T + 1, h->stat + ST_TILES, ar, s));
   DCSR_LAUNCH(k_check, 1, 1, 0, s, h->stat, h->row_sizes, h->n_rows, h->pool_cap);
   if (merge) {
+    DCSR_LAUNCH(k_apply_existing<V>, grid_for(T, 256), 256, 0, s, m, k0, T, cb, bval, bpos);
     DCSR_LAUNCH((k_apply_merge<V, 8>), g_apply8, UPD_THREADS, 0, s, m, trow, tb0, bcol, bval, bpos, tcap, tmnew,
                 tinfo, ncol, nval, nins);
     DCSR_LAUNCH((k_apply_merge<V, 32>), g_apply, UPD_THREADS, 0, s, m, trow, tb0, bcol, bval, bpos, tcap, tmnew,

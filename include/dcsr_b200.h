@@ -59,7 +59,7 @@ enum { DCSR_REDUCE_SUM = 0, DCSR_REDUCE_MAX = 1, DCSR_REDUCE_MIN = 2, DCSR_REDUC
  * rlB - free + alpha (reference include/sparse_update.inl:93-105).  The pool
  * is sized top + max(top*spare_x16/16, min_spare) on load. */
 typedef struct {
-  int32_t max_segs;   /* segment layers per row, 1..8 (reference MAX_OFFSET=4) */
+  int32_t max_segs;   /* segment layers per row, 1..4 (reference MAX_OFFSET=4) */
   int32_t factor_x16; /* per-row slack factor in 1/16 (32 = 2x) */
   int32_t min_cap;    /* minimum row capacity */
   int32_t align;      /* capacity alignment in entries (power of two) */

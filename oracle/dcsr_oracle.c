@@ -61,7 +61,7 @@ int64_t or_pool_capacity(const or_opts *o, int64_t top) {
 static int64_t seg_index(const or_dcsr *m, int l, int32_t r) { return (int64_t)l * m->pitch + 2 * (int64_t)r; }
 
 or_dcsr *or_create(int32_t n_rows, int32_t n_cols, int32_t dtype, const or_opts *o) {
-  if (n_rows < 0 || n_cols < 0 || o->max_segs < 1 || o->max_segs > 8) return NULL;
+  if (n_rows < 0 || n_cols < 0 || o->max_segs < 1 || o->max_segs > 4) return NULL;
   or_dcsr *m = (or_dcsr *)calloc(1, sizeof(or_dcsr));
   m->n_rows = n_rows;
   m->n_cols = n_cols;
