@@ -2,6 +2,7 @@
 // (key, value) pairs, and the public segmented primitives
 // (count_sorted_indices, reduce_by_key).  All hand-written for sm_100a.
 #include <algorithm>
+#include <mutex>
 
 #include "common.cuh"
 
@@ -290,9 +291,65 @@ __global__ void k_rbk_emit(const int32_t *keys, const V *vals, int64_t n, const 
   vals_out[pos[i]] = acc;
 }
 
+// ------------------------------------------- allocation-free reduce-by-key
+//
+// Scratch for dcsr_reduce_by_key_noalloc: head positions (one int64 per key)
+// and the scan's tile partials, in one static device array.  Every GPU that
+// loads the library holds it until exit.  Host code must not pass the
+// symbol itself to a kernel (in host code it names a host-side stand-in);
+// the device address is looked up once per device.
+constexpr size_t NOALLOC_POS_BYTES = (size_t)DCSR_NOALLOC_MAX_KEYS * sizeof(long long);
+constexpr size_t NOALLOC_BYTES = NOALLOC_POS_BYTES + 2 * 256 +
+                                 ((DCSR_NOALLOC_MAX_KEYS + SCAN_TILE - 1) / SCAN_TILE + 1) * sizeof(long long);
+static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_BYTES];
+
+static int noalloc_scratch(void **out) {
+  static std::mutex mu;
+  static void *ptr[128] = {};
+  int dev = 0;
+  DCSR_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 128) return DCSR_NOT_SUPPORTED;
+  std::lock_guard<std::mutex> lock(mu);
+  if (!ptr[dev]) {
+    void *p = nullptr;
+    DCSR_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+    ptr[dev] = p;
+  }
+  *out = ptr[dev];
+  return DCSR_OK;
+}
+
 }  // namespace dcsr
 
 using namespace dcsr;
+
+extern "C" int dcsr_reduce_by_key_noalloc(const int32_t *keys, const void *vals, int64_t n, int32_t dtype,
+                                          int32_t *keys_out, void *vals_out, int64_t *n_out, void *stream) {
+  if (n < 0 || n > DCSR_NOALLOC_MAX_KEYS || (dtype != DCSR_F32 && dtype != DCSR_F64) || !n_out ||
+      (n > 0 && (!keys || !vals || !keys_out || !vals_out)))
+    return DCSR_BAD_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  if (n == 0) {
+    DCSR_CUDA(cudaMemsetAsync(n_out, 0, sizeof(int64_t), s));
+    return DCSR_OK;
+  }
+  void *base = nullptr;
+  DCSR_TRY(noalloc_scratch(&base));
+  Arena ar;  // a view over the static array: take() only, never reserve()/release()
+  ar.base = (char *)base;
+  ar.cap = NOALLOC_BYTES;
+  ar.used = 0;
+  long long *pos = ar.take<long long>(n);  // fully rewritten below before any read
+  const unsigned g = (unsigned)div_up(n, 256);
+  DCSR_LAUNCH(k_rbk_flags, g, 256, 0, s, keys, n, pos);
+  DCSR_TRY(scan_i64(pos, pos, n, (long long *)n_out, ar, s));
+  if (dtype == DCSR_F32)
+    DCSR_LAUNCH(k_rbk_emit<float>, g, 256, 0, s, keys, (const float *)vals, n, pos, keys_out, (float *)vals_out);
+  else
+    DCSR_LAUNCH(k_rbk_emit<double>, g, 256, 0, s, keys, (const double *)vals, n, pos, keys_out,
+                (double *)vals_out);
+  return DCSR_OK;
+}
 
 extern "C" int dcsr_count_sorted_indices(const int32_t *I, int64_t n, int32_t *X, void *stream) {
   if (n < 0 || (n > 0 && (!I || !X))) return DCSR_BAD_ARG;

@@ -176,6 +176,23 @@ int dcsr_count_sorted_indices(const int32_t *I, int64_t n, int32_t *X, void *str
 int dcsr_reduce_by_key(const int32_t *keys, const void *vals, int64_t n, int32_t dtype, int32_t *keys_out,
                        void *vals_out, int64_t *n_out, void *stream);
 
+/* Allocation-free reduce-by-key.  No counterpart in the reference: it is
+ * for callers that cannot allocate device memory at call time -- a process
+ * that has carved the GPU's memory into fixed budgets up front, or code whose
+ * allocator is not CUDA's and must not have the CUDA allocator (which can
+ * synchronise the device) run underneath it.  Same result as
+ * dcsr_reduce_by_key; its scratch is a static device array compiled into the
+ * library (about 8 MiB per GPU that loads it, held until process exit), so
+ * n is limited to DCSR_NOALLOC_MAX_KEYS (larger n returns DCSR_BAD_ARG
+ * without touching the GPU).  The first call on a device looks up the
+ * array's device address (cudaGetSymbolAddress) with that device current;
+ * make that first call before any stream capture.  All calls share the one
+ * array: calls that overlap on the GPU (different streams, or threads
+ * without ordering) race and must be serialised by the caller. */
+#define DCSR_NOALLOC_MAX_KEYS (1 << 20)
+int dcsr_reduce_by_key_noalloc(const int32_t *keys, const void *vals, int64_t n, int32_t dtype, int32_t *keys_out,
+                               void *vals_out, int64_t *n_out, void *stream);
+
 /* ---------------------------------------------------------------- misc */
 
 const char *dcsr_status_string(int status);
