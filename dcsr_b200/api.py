@@ -42,6 +42,13 @@ class Opts(C.Structure):
         return {n: getattr(self, n) for n, _ in self._fields_}
 
 
+class BatchItem(C.Structure):
+    """dcsr_batch_item of the C ABI."""
+    _fields_ = [("matrix", C.c_void_p), ("rows", C.c_void_p), ("cols", C.c_void_p), ("vals", C.c_void_p),
+                ("nnz", C.c_int64), ("x", C.c_void_p), ("y", C.c_void_p), ("k", C.c_int32), ("ldx", C.c_int64),
+                ("ldy", C.c_int64), ("alpha", C.c_double), ("beta", C.c_double)]
+
+
 class Info(C.Structure):
     _fields_ = [("n_rows", C.c_int32), ("n_cols", C.c_int32), ("dtype", C.c_int32), ("pitch", C.c_int32),
                 ("pool_cap", C.c_int64), ("row_sizes", C.c_void_p), ("seg", C.c_void_p), ("cols", C.c_void_p),
@@ -74,6 +81,13 @@ _SIGS = {
     "dcsr_spgemm": (_i32, [_vp, _vp, _vp, _vp]),
     "dcsr_count_sorted_indices": (_i32, [_vp, _i64, _vp, _vp]),
     "dcsr_reduce_by_key": (_i32, [_vp, _vp, _i64, _i32, _vp, _vp, _vp, _vp]),
+    "dcsr_batch_create": (_i32, [C.POINTER(_vp), _vp, _i32, _vp]),
+    "dcsr_batch_run": (_i32, [_vp, _vp]),
+    "dcsr_batch_capture": (_i32, [_vp, _vp]),
+    "dcsr_batch_launch": (_i32, [_vp, _vp]),
+    "dcsr_batch_status": (_i32, [_vp, _vp, _vp]),
+    "dcsr_batch_repair": (_i32, [_vp, _vp, C.POINTER(_i32), _vp]),
+    "dcsr_batch_destroy": (_i32, [_vp]),
     "dcsr_status_string": (C.c_char_p, [_i32]),
     "dcsr_launch_count": (C.c_uint64, []),
     "dcsr_version": (C.c_char_p, []),
@@ -315,3 +329,67 @@ def reduce_by_key(keys: torch.Tensor, vals: torch.Tensor, stream=None):
                                     _ptr(cnt), _stream(stream)), "dcsr_reduce_by_key")
     m = int(cnt.item())
     return ko[:m], vo[:m]
+
+
+class DcsrBatch:
+    """Batched update + SpMV over many matrices (dcsr_batch_* of the C ABI).
+
+    ``work`` is a list of dicts with keys ``matrix`` (DcsrMatrix), optional
+    ``rows``/``cols``/``vals`` (the update triples, device tensors) and optional
+    ``x``/``y`` ([n_cols, k] / [n_rows, k] or 1-D device tensors), ``alpha``,
+    ``beta``.  The tensors are referenced for the batch's lifetime: write new
+    triples or right-hand sides into them in place between runs.
+    """
+
+    def __init__(self, work, stream=None):
+        items = (BatchItem * len(work))()
+        self._keep = []
+        for i, w in enumerate(work):
+            m = w["matrix"]
+            it = items[i]
+            it.matrix = m.h.value
+            r, c, v = w.get("rows"), w.get("cols"), w.get("vals")
+            if r is not None and r.numel() > 0:
+                it.rows, it.cols, it.vals = _ptr(r).value, _ptr(c).value, _ptr(v).value
+                it.nnz = r.numel()
+            x, y = w.get("x"), w.get("y")
+            if x is not None:
+                k = 1 if x.dim() == 1 else x.shape[1]
+                it.x, it.y, it.k, it.ldx, it.ldy = _ptr(x).value, _ptr(y).value, k, k, k
+                it.alpha, it.beta = float(w.get("alpha", 1.0)), float(w.get("beta", 0.0))
+            self._keep += [m, r, c, v, x, y]
+        self.count = len(work)
+        self.h = C.c_void_p()
+        _check(lib().dcsr_batch_create(C.byref(self.h), items, len(work), _stream(stream)), "dcsr_batch_create")
+
+    def run(self, stream=None):
+        _check(lib().dcsr_batch_run(self.h, _stream(stream)), "dcsr_batch_run")
+
+    def capture(self, stream=None):
+        _check(lib().dcsr_batch_capture(self.h, _stream(stream)), "dcsr_batch_capture")
+
+    def launch(self, stream=None):
+        _check(lib().dcsr_batch_launch(self.h, _stream(stream)), "dcsr_batch_launch")
+
+    def status(self, stream=None) -> np.ndarray:
+        st = np.zeros(self.count, dtype=np.int32)
+        _check(lib().dcsr_batch_status(self.h, st.ctypes.data_as(C.c_void_p), _stream(stream)), "dcsr_batch_status")
+        return st
+
+    def repair(self, statuses: np.ndarray, stream=None) -> int:
+        st = np.ascontiguousarray(statuses, dtype=np.int32)
+        n = _i32(0)
+        _check(lib().dcsr_batch_repair(self.h, st.ctypes.data_as(C.c_void_p), C.byref(n), _stream(stream)),
+               "dcsr_batch_repair")
+        return int(n.value)
+
+    def close(self):
+        if self.h:
+            lib().dcsr_batch_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

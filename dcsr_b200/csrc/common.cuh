@@ -9,6 +9,7 @@
 #include <atomic>
 #include <cstdio>
 #include <cstdlib>
+#include <cstring>
 
 #include "../../include/dcsr_b200.h"
 
@@ -65,11 +66,15 @@ enum StatWord {
   ST_STATUS = 0,   // dcsr_status of the last rejected operation (sticky until read)
   ST_GO = 1,       // 1 when the current update plan was accepted
   ST_NEED = 2,     // pool top the current update requires
-  ST_TOUCHED = 3,  // touched rows of the current batch
-  ST_TILES = 4,    // relocation tiles of the current batch
+  ST_TOUCHED = 3,  // touched rows of the current batch (batch-global word)
+  ST_TILES = 4,    // relocation tiles of the current batch (batch-global word)
   ST_TOTAL = 5,    // scratch total (scan results)
-  ST_AUX = 6,
-  ST_WORDS = 8
+  ST_AUX = 6,      // per-update flags (bad index, layer overflow)
+  ST_SCRATCH = 7,  // one-off device-side result words
+  ST_TOP = 8,      // pool top before the current update
+  ST_T0 = 9,       // this matrix's touched-row range [T0, T1) in the batch
+  ST_T1 = 10,
+  ST_WORDS = 16
 };
 
 // Device view of a matrix passed by value to kernels.
@@ -133,13 +138,19 @@ struct dcsr_matrix_s {
   void *vals = nullptr;
   long long *stat = nullptr;
   // Row-pass schedule (handle-local; the reference used a global __constant__
-  // bin table): rows longer than LONG_ROW and their chunk offsets.
+  // bin table): long rows with their chunk offsets, medium rows.
   int32_t *long_rows = nullptr;  // [n_rows + 1]
   long long *long_off = nullptr; // [n_rows + 2] chunk offsets of long rows
   int32_t *long_cnt = nullptr;   // [n_rows + 1] chunk-finisher counters
-  int32_t *sched_info = nullptr; // [32]: [0] long rows, [1] chunks
+  int32_t *sched_info = nullptr; // [32]: [0] long rows, [1] chunks, [2] medium rows
   double *part = nullptr;        // chunk partials (reductions)
   int64_t part_cap = 0;
+  int32_t *chunk_li = nullptr;   // long-row index of every chunk
+  int64_t chunk_cap = 0;
+  int32_t *med_rows = nullptr;   // [n_rows + 1] medium-length rows
+  // Row-class thresholds of the row passes (rows of at most short_max
+  // entries are streamed by row blocks, rows above long_min are chunked).
+  int32_t short_max = 64, long_min = 4096;
   bool bins_valid = false;
   dcsr::Arena scratch;
   int device = 0;
@@ -147,6 +158,7 @@ struct dcsr_matrix_s {
   template <typename V>
   dcsr::Mat<V> view() const {
     dcsr::Mat<V> m;
+    std::memset(&m, 0, sizeof(m));  // deterministic padding (descriptor images are compared bytewise)
     m.n_rows = n_rows;
     m.n_cols = n_cols;
     m.max_segs = o.max_segs;
@@ -196,7 +208,6 @@ __device__ __forceinline__ T warp_incl_scan(T v) {
   return v;
 }
 
-// A row's linked segments (at most 8), read from the segment table.
 // A row's linked segments.  MAX_SEGS is the compile-time layer limit (the
 // reference's MAX_OFFSET = 4); every loop over layers is fully unrolled so
 // the arrays stay in registers (dynamic indexing would put them in local
@@ -241,28 +252,27 @@ struct Chain {
   }
 };
 
+// All layer pairs are loaded independently (no dependent load chain), then
+// the chain is the leading run of linked layers.
 template <typename V>
 __device__ __forceinline__ Chain load_chain(const Mat<V> &m, int32_t r) {
   Chain c;
+  int2 p[MAX_SEGS];
+#pragma unroll
+  for (int l = 0; l < MAX_SEGS; l++)
+    p[l] = l < m.max_segs ? __ldg(reinterpret_cast<const int2 *>(m.seg + (int64_t)l * m.pitch + 2 * (int64_t)r))
+                          : make_int2(-1, -1);
   c.ns = 0;
   c.total = 0;
   bool open = true;
 #pragma unroll
   for (int l = 0; l < MAX_SEGS; l++) {
-    c.st[l] = 0;
-    c.cp[l] = 0;
-    if (open && l < m.max_segs) {
-      const int2 p = __ldg(reinterpret_cast<const int2 *>(m.seg + (int64_t)l * m.pitch + 2 * (int64_t)r));
-      if (p.x < 0) {
-        open = false;
-      } else {
-        c.st[l] = p.x;
-        c.cp[l] = p.y - p.x;
-        c.total += p.y - p.x;
-        c.ns = l + 1;
-      }
-    } else {
-      open = false;
+    open = open && p[l].x >= 0;
+    c.st[l] = open ? p[l].x : 0;
+    c.cp[l] = open ? p[l].y - p[l].x : 0;
+    if (open) {
+      c.total += p[l].y - p[l].x;
+      c.ns = l + 1;
     }
   }
   return c;

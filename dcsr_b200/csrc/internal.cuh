@@ -20,8 +20,54 @@ size_t coo_to_csr_scratch(dcsr_handle h, int64_t nnz);
 
 int update_async(dcsr_handle h, const int32_t *rows, const int32_t *cols, const void *vals, int64_t nnz,
                  cudaStream_t s);
+
+// One matrix of a batched update (device-resident array element).
+template <typename V>
+struct BatchItem {
+  Mat<V> m;
+  const int32_t *rows, *cols;
+  const V *vals;
+  long long toff;  // first index of this matrix's triples in the batch
+  long long T;     // its triple count
+};
+// Update `count` matrices at once (items_dev: device BatchItem<V>[count],
+// toff prefix over T); gstat: batch-global status words.
+int update_many(const void *items_dev, int dtype, int count, int64_t T, bool merge, int rb, int cb, long long *gstat,
+                Arena &ar, cudaStream_t s);
+size_t update_scratch_bytes(int64_t T, size_t vsize);
 int compact(dcsr_handle h, cudaStream_t s);
 int build_schedule(dcsr_handle h, cudaStream_t s);
+
+// One matrix of a row pass (SpMV / reduction) over a set of matrices.
+template <typename V>
+struct RowItem {
+  Mat<V> m;
+  const int32_t *long_rows;
+  const long long *long_off;
+  const int32_t *chunk_li;
+  const int32_t *med_rows;
+  int32_t *info;  // [0] long rows, [1] chunks, [2] medium rows
+  int32_t *long_cnt;
+  double *part;
+  const V *x;
+  V *y;
+  int64_t ldx, ldy;
+  double alpha, beta;
+  long long row0;             // first row of this matrix in the batch's row space
+  int32_t short_max, long_min; // row classes: short <= short_max < medium <= long_min < long
+  const int32_t *skip;        // batch: nonzero -> this matrix's pass is skipped (may be null)
+};
+// Rebuild the schedules of `count` matrices at once (items: device
+// RowItem<V>[count] in row-space order; R = total rows).  Needs
+// schedule_scratch_bytes(R) free in the arena.
+int schedule_many(const void *items_dev, int dtype, int count, int64_t R, Arena &ar, cudaStream_t s);
+size_t schedule_scratch_bytes(int64_t R);
+// y = A x for `count` matrices that share k (items: device RowItem<V>[count]);
+// pref: device scratch of 3*(count+1) long longs.
+int spmv_many(const void *items_dev, int dtype, int count, int k, bool vec, long long *pref, cudaStream_t s);
+template <typename V>
+RowItem<V> row_item(dcsr_handle h, const void *x, void *y, int64_t ldx, int64_t ldy, double alpha, double beta);
+// Size the handle's chunk table and chunk partials (K results per chunk).
 int ensure_part(dcsr_handle h, int K, cudaStream_t s);
 // Copy every row's logical entries to dst_off[r] (optionally COO row ids and
 // an int32 row pointer).  Builds the schedule first if needed (so callers

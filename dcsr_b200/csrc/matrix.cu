@@ -306,6 +306,7 @@ int dcsr_create(dcsr_handle *out, int32_t n_rows, int32_t n_cols, int32_t dtype,
       cudaMalloc((void **)&h->long_rows, sizeof(int32_t) * (n_rows + 1)) != cudaSuccess ||
       cudaMalloc((void **)&h->long_off, sizeof(long long) * (n_rows + 2)) != cudaSuccess ||
       cudaMalloc((void **)&h->long_cnt, sizeof(int32_t) * (n_rows + 1)) != cudaSuccess ||
+      cudaMalloc((void **)&h->med_rows, sizeof(int32_t) * (n_rows + 1)) != cudaSuccess ||
       cudaMalloc((void **)&h->sched_info, sizeof(int32_t) * 32) != cudaSuccess)
     st = DCSR_OOM;
   if (st == DCSR_OK) {
@@ -336,8 +337,10 @@ int dcsr_destroy(dcsr_handle h) {
   cudaFree(h->long_rows);
   cudaFree(h->long_off);
   cudaFree(h->long_cnt);
+  cudaFree(h->med_rows);
   cudaFree(h->sched_info);
   if (h->part) cudaFree(h->part);
+  if (h->chunk_li) cudaFree(h->chunk_li);
   cudaDeviceSynchronize();
   delete h;
   return DCSR_OK;

@@ -1,112 +1,310 @@
-// rowstream.cu -- row-parallel passes over a DCSR matrix: SpMV (1..8 RHS),
-// row reductions, DCSR -> CSR/COO export and the compaction copy.
+// rowstream.cu -- row-parallel passes over one DCSR matrix or a set of them:
+// SpMV (1..8 RHS), row reductions, DCSR -> CSR/COO export, compaction copy.
 //
-// Work decomposition (one persistent launch per pass):
-//   long rows   (length > LONG_ROW) are cut into CHUNK-entry chunks, one CTA
-//               per chunk (128-bit loads when the segment is 16-byte aligned);
-//               reductions combine chunk partials in chunk order (the CTA that
-//               finishes a row's last chunk sums them), so results do not
-//               depend on scheduling.
-//   other rows  a warp takes 32 consecutive rows and streams their layer-0
-//               entries across its lanes (row found by a shuffle search over
-//               the lanes' prefix sums), so consecutive rows' contiguous pool
-//               ranges are read coalesced; reductions use a segmented warp
-//               scan; entries in further chained segments are done row by row
-//               by the whole warp.
-// Long-row chunks come first in the unit order so they start early.
+// Rows are split into three classes by the schedule (rebuilt lazily after
+// any change of row lengths), each with its own launch so each has its own
+// register budget and its units carry bounded work:
+//   short  (<= short_max entries)  a warp takes 32 consecutive rows and
+//          streams each segment layer's entries across its lanes, U windows
+//          of 32 entries at a time with every window's loads issued first;
+//          a lane's row comes from ballots over the window's row starts
+//          (__fns), reductions use a segmented scan whose segment tests are
+//          bit operations on that start mask.
+//   medium (<= long_min)          one warp per row, lanes strided, U loads in
+//          flight per lane, one warp reduction per row.
+//   long                          CHUNK-entry chunks, one CTA per chunk,
+//          STEP entries in flight per CTA step (128-bit loads when aligned);
+//          multi-chunk rows combine their partials in chunk order (the CTA
+//          that finishes the last chunk sums them).
+// Every row's result is therefore independent of scheduling.  Products
+// accumulate in FP64 per lane; the short class's per-window partials use the
+// matrix type (FP32 partials of at most 32 products, then FP64).
 //
-// The schedule (long-row list + chunk offsets) is rebuilt lazily after any
-// change of row lengths.  Reference: spmv_dcsr_bin* include/spmv.inl:364-622
-// (seven bin kernels on seven streams, rows read with stale Prow_sizes),
-// CompactIndices include/sparse_update.inl:916-1007, DCSRtoCSROffsets :1101.
+// Reference: spmv_dcsr_bin* include/spmv.inl:364-622 (seven bin kernels on
+// seven streams, rows read with stale Prow_sizes), CompactIndices
+// include/sparse_update.inl:916-1007, DCSRtoCSROffsets :1101-1116.
+#include <algorithm>
+#include <cstring>
+#include <type_traits>
+
 #include "internal.cuh"
 
 namespace dcsr {
 
 constexpr int RS_THREADS_ = 256;
-constexpr int LONG_ROW = 512;
-constexpr int CHUNK = 4096;
+constexpr int RS_WARPS = RS_THREADS_ / 32;
+constexpr int CHUNK = 65536;  // long-row entries per CTA unit
+constexpr int STEP = 4096;    // entries a CTA has in flight per step
+enum { P_BLOCKS = 0, P_CHUNKS = 1, P_MED = 2 };
+
+// ------------------------------------------------------------- sources
+// A row pass runs over one matrix (RowOne, descriptor passed by value) or a
+// set of matrices laid end to end in one row space (RowMany, descriptors in
+// device memory, per-class unit prefixes computed on the device).
+
+template <typename V>
+struct RowOne {
+  RowItem<V> it;
+  __device__ __forceinline__ int n_items() const { return 1; }
+  __device__ __forceinline__ const RowItem<V> &item(int) const { return it; }
+  __device__ __forceinline__ int find_row(int64_t) const { return 0; }
+  __device__ __forceinline__ int64_t units(int part) const {
+    if (part == P_CHUNKS) return it.info[1];
+    if (part == P_MED) return div_up(it.info[2], RS_WARPS);
+    return div_up(div_up(it.m.n_rows, 32), RS_WARPS);
+  }
+  __device__ __forceinline__ int locate(int, int64_t u, int64_t &lu) const {
+    lu = u;
+    return 0;
+  }
+};
+
+template <typename V>
+struct RowMany {
+  const RowItem<V> *its;
+  int count;
+  const long long *pref;  // [3][count+1] unit prefixes per class
+  __device__ __forceinline__ int n_items() const { return count; }
+  __device__ __forceinline__ const RowItem<V> &item(int i) const { return its[i]; }
+  __device__ __forceinline__ int find_row(int64_t g) const {  // matrix holding global row g
+    int lo = 0, hi = count;
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) >> 1;
+      if (its[mid].row0 <= g) lo = mid;
+      else hi = mid;
+    }
+    return lo;
+  }
+  __device__ __forceinline__ int64_t units(int part) const { return pref[part * (count + 1) + count]; }
+  __device__ __forceinline__ int locate(int part, int64_t u, int64_t &lu) const {
+    const long long *p = pref + part * (count + 1);
+    int lo = 0, hi = count;
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) >> 1;
+      if (p[mid] <= u) lo = mid;
+      else hi = mid;
+    }
+    lu = u - p[lo];
+    return lo;
+  }
+};
 
 // ---------------------------------------------------------------- schedule
+// Per row: lflag = (is_long << 32) | chunks, mflag = is_medium; two scans
+// give every long row its index and first chunk and every medium row its
+// slot, per matrix (differences of the scans at the matrix's first row).
 
-// packed[r] = (is_long << 32) | chunks  (r < n), packed[n] = 0
-__global__ void k_sched_flags(const int32_t *row_sizes, int32_t n, long long *packed) {
-  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r <= n; r += stride) {
-    long long v = 0;
-    if (r < n) {
-      const int32_t L = row_sizes[r];
-      if (L > LONG_ROW) v = (1ll << 32) | (long long)((L + CHUNK - 1) / CHUNK);
-    }
-    packed[r] = v;
-  }
+__device__ __forceinline__ void sched_flags_row(int32_t L, int32_t smax, int32_t lmin, long long &lf,
+                                                long long &mf) {
+  lf = L > lmin ? ((1ll << 32) | (long long)((L + CHUNK - 1) / CHUNK)) : 0;
+  mf = (L > smax && L <= lmin) ? 1 : 0;
 }
-__global__ void k_sched_emit(const int32_t *row_sizes, int32_t n, const long long *scanned, int32_t *long_rows,
-                             long long *long_off, int32_t *info) {
+
+template <typename V, typename Src>
+__global__ void k_sched_flags(Src src, int64_t R, long long *lflag, long long *mflag) {
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r <= n; r += stride) {
-    const long long s = scanned[r];
-    if (r == n) {
-      info[0] = (int32_t)(s >> 32);          // long rows
-      info[1] = (int32_t)(s & 0xffffffff);   // chunks
-      long_off[s >> 32] = s & 0xffffffff;
-      continue;
+  for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g <= R; g += stride) {
+    long long lf = 0, mf = 0;
+    if (g < R) {
+      const RowItem<V> &it = src.item(src.find_row(g));
+      sched_flags_row(it.m.row_sizes[g - it.row0], it.short_max, it.long_min, lf, mf);
     }
-    if (row_sizes[r] > LONG_ROW) {
-      long_rows[s >> 32] = (int32_t)r;
-      long_off[s >> 32] = s & 0xffffffff;
-    }
+    lflag[g] = lf;
+    mflag[g] = mf;
   }
 }
 
-int build_schedule(dcsr_handle h, cudaStream_t s) {
-  const int32_t n = h->n_rows;
-  Arena &ar = h->scratch;
-  DCSR_TRY(ar.reserve(arena_bytes(n + 2, 8) + scan_scratch_bytes(n + 1), s));
-  long long *packed = ar.take<long long>(n + 2);
-  const int g = (int)std::min<int64_t>(div_up(n + 1, 256), (int64_t)sm_count() * 16);
-  DCSR_LAUNCH(k_sched_flags, g, 256, 0, s, h->row_sizes, n, packed);
-  DCSR_TRY(scan_i64(packed, packed, n + 1, nullptr, ar, s));
-  DCSR_LAUNCH(k_sched_emit, g, 256, 0, s, h->row_sizes, n, packed, h->long_rows, h->long_off, h->sched_info);
-  // finisher counters start at zero; finishers reset their own counter
-  DCSR_CUDA(cudaMemsetAsync(h->long_cnt, 0, sizeof(int32_t) * (n + 1), s));
+template <typename V, typename Src>
+__global__ void k_sched_emit(Src src, int64_t R, const long long *lscan, const long long *mscan) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < R; g += stride) {
+    const RowItem<V> &it = src.item(src.find_row(g));
+    const int64_t r = g - it.row0;
+    const int32_t L = it.m.row_sizes[r];
+    if (L > it.long_min) {
+      const long long s = lscan[g] - lscan[it.row0];
+      const_cast<int32_t *>(it.long_rows)[s >> 32] = (int32_t)r;
+      const_cast<long long *>(it.long_off)[s >> 32] = s & 0xffffffff;
+      it.long_cnt[s >> 32] = 0;
+    } else if (L > it.short_max) {
+      const_cast<int32_t *>(it.med_rows)[mscan[g] - mscan[it.row0]] = (int32_t)r;
+    }
+  }
+}
+
+// Per matrix (one warp each): class counts, the long-row offset sentinel and
+// the chunk -> long-row table.
+template <typename V, typename Src>
+__global__ void k_sched_info(Src src, const long long *lscan, const long long *mscan) {
+  const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  for (int i = w; i < src.n_items(); i += nw) {
+    const RowItem<V> &it = src.item(i);
+    const int64_t a = it.row0, b = it.row0 + it.m.n_rows;
+    const long long ls = lscan[b] - lscan[a];
+    const int32_t n_long = (int32_t)(ls >> 32), n_chunks = (int32_t)(ls & 0xffffffff);
+    if (lane == 0) {
+      it.info[0] = n_long;
+      it.info[1] = n_chunks;
+      it.info[2] = (int32_t)(mscan[b] - mscan[a]);
+      const_cast<long long *>(it.long_off)[n_long] = n_chunks;
+    }
+    __syncwarp();
+    for (int32_t li = lane; li < n_long; li += 32) {
+      const long long c0 = it.long_off[li];
+      const long long c1 = li + 1 < n_long ? it.long_off[li + 1] : n_chunks;
+      for (long long c = c0; c < c1; c++) const_cast<int32_t *>(it.chunk_li)[c] = li;
+    }
+  }
+}
+
+static int64_t max_chunks(dcsr_handle h) { return h->pool_cap / CHUNK + h->pool_cap / h->long_min + 2; }
+
+int ensure_part(dcsr_handle h, int K, cudaStream_t s) {
+  if (max_chunks(h) > h->chunk_cap) {
+    if (h->chunk_li) DCSR_CUDA(cudaFreeAsync(h->chunk_li, s));
+    h->chunk_li = nullptr;
+    DCSR_CUDA(cudaMallocAsync((void **)&h->chunk_li, sizeof(int32_t) * max_chunks(h), s));
+    h->chunk_cap = max_chunks(h);
+    h->bins_valid = false;  // the chunk table is gone
+  }
+  const int64_t need = max_chunks(h) * K;
+  if (need <= h->part_cap) return DCSR_OK;
+  if (h->part) DCSR_CUDA(cudaFreeAsync(h->part, s));
+  h->part = nullptr;
+  DCSR_CUDA(cudaMallocAsync((void **)&h->part, sizeof(double) * need, s));
+  h->part_cap = need;
+  return DCSR_OK;
+}
+
+template <typename V>
+RowItem<V> row_item(dcsr_handle h, const void *x, void *y, int64_t ldx, int64_t ldy, double alpha, double beta) {
+  RowItem<V> it;
+  std::memset(&it, 0, sizeof(it));  // padding too: batch descriptor images are compared bytewise
+  it.m = h->view<V>();
+  it.long_rows = h->long_rows;
+  it.long_off = h->long_off;
+  it.chunk_li = h->chunk_li;
+  it.med_rows = h->med_rows;
+  it.info = h->sched_info;
+  it.long_cnt = h->long_cnt;
+  it.part = h->part;
+  it.x = (const V *)x;
+  it.y = (V *)y;
+  it.ldx = ldx;
+  it.ldy = ldy;
+  it.alpha = alpha;
+  it.beta = beta;
+  it.row0 = 0;
+  it.short_max = h->short_max;
+  it.long_min = h->long_min;
+  it.skip = nullptr;
+  return it;
+}
+template RowItem<float> row_item<float>(dcsr_handle, const void *, void *, int64_t, int64_t, double, double);
+template RowItem<double> row_item<double>(dcsr_handle, const void *, void *, int64_t, int64_t, double, double);
+
+static int grid_for(int64_t n, int block) {
+  int64_t g = div_up(n, block);
+  int64_t cap = (int64_t)sm_count() * 16;
+  return (int)(g < 1 ? 1 : (g > cap ? cap : g));
+}
+
+size_t schedule_scratch_bytes(int64_t R) { return 2 * arena_bytes(R + 2, 8) + scan_scratch_bytes(R + 1); }
+
+// Needs schedule_scratch_bytes(R) free in the arena (reserved by the caller).
+template <typename V, typename Src>
+static int schedule_src(const Src &src, int count, int64_t R, Arena &ar, cudaStream_t s) {
+  long long *lf = ar.take<long long>(R + 2), *mf = ar.take<long long>(R + 2);
+  const int g = grid_for(R + 1, 256);
+  DCSR_LAUNCH((k_sched_flags<V, Src>), g, 256, 0, s, src, R, lf, mf);
+  DCSR_TRY(scan_i64(lf, lf, R + 1, nullptr, ar, s));
+  DCSR_TRY(scan_i64(mf, mf, R + 1, nullptr, ar, s));
+  DCSR_LAUNCH((k_sched_emit<V, Src>), g, 256, 0, s, src, R, lf, mf);
+  DCSR_LAUNCH((k_sched_info<V, Src>), grid_for((int64_t)count * 32, 256), 256, 0, s, src, lf, mf);
+  return DCSR_OK;
+}
+
+int schedule_many(const void *items_dev, int dtype, int count, int64_t R, Arena &ar, cudaStream_t s) {
+  if (count == 0) return DCSR_OK;
+  if (dtype == DCSR_F32)
+    return schedule_src<float>(RowMany<float>{(const RowItem<float> *)items_dev, count, nullptr}, count, R, ar, s);
+  return schedule_src<double>(RowMany<double>{(const RowItem<double> *)items_dev, count, nullptr}, count, R, ar, s);
+}
+
+template <typename V>
+static int build_schedule_t(dcsr_handle h, cudaStream_t s) {
+  DCSR_TRY(ensure_part(h, 1, s));
+  DCSR_TRY(h->scratch.reserve(schedule_scratch_bytes(h->n_rows), s));
+  RowOne<V> src{row_item<V>(h, nullptr, nullptr, 0, 0, 0.0, 0.0)};
+  DCSR_TRY(schedule_src<V>(src, 1, h->n_rows, h->scratch, s));
   h->bins_valid = true;
   return DCSR_OK;
 }
 
-// ------------------------------------------------------------- helpers
-
-// Row containing stream position e: largest lane j with excl_j <= e.
-__device__ __forceinline__ int find_row(int64_t e, int64_t excl) {
-  int j = 0;
-#pragma unroll
-  for (int step = 16; step > 0; step >>= 1) {
-    const int cand = j + step;
-    const int64_t v = __shfl_sync(FULL, excl, cand & 31);
-    if (cand < 32 && v <= e) j = cand;
-  }
-  return j;
+int build_schedule(dcsr_handle h, cudaStream_t s) {
+  if (h->dtype == DCSR_F32) return build_schedule_t<float>(h, s);
+  return build_schedule_t<double>(h, s);
 }
 
-// Per-lane row of the warp's row block [r0, r0+32).
+// Exclusive prefix over the matrices of each class's unit count (one block
+// of 1024 threads, 1024 matrices per round).
+template <typename V>
+__global__ void __launch_bounds__(1024) k_unit_prefix(const RowItem<V> *its, int count, long long *pref) {
+  __shared__ long long wsum[3][32];
+  __shared__ long long carry[3];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (threadIdx.x < 3) carry[threadIdx.x] = 0;
+  __syncthreads();
+  for (int b = 0; b < count; b += 1024) {
+    const int i = b + threadIdx.x;
+    long long u[3] = {0, 0, 0}, inc[3];
+    if (i < count) {
+      u[P_BLOCKS] = div_up(div_up(its[i].m.n_rows, 32), RS_WARPS);
+      u[P_CHUNKS] = its[i].info[1];
+      u[P_MED] = div_up(its[i].info[2], RS_WARPS);
+    }
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      inc[c] = warp_incl_scan(u[c]);
+      if (lane == 31) wsum[c][w] = inc[c];
+    }
+    __syncthreads();
+    if (w == 0) {
+#pragma unroll
+      for (int c = 0; c < 3; c++) wsum[c][lane] = warp_incl_scan(wsum[c][lane]);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int c = 0; c < 3; c++)
+      if (i < count) pref[c * (count + 1) + i] = carry[c] + (w ? wsum[c][w - 1] : 0) + inc[c] - u[c];
+    __syncthreads();
+    if (threadIdx.x < 3) carry[threadIdx.x] += wsum[threadIdx.x][31];
+    __syncthreads();
+  }
+  if (threadIdx.x < 3) pref[threadIdx.x * (count + 1) + count] = carry[threadIdx.x];
+}
+
+// ------------------------------------------------------------- helpers
+
 struct RowBlock {
-  int32_t row;   // global row id (or -1)
-  int32_t len;   // logical length
-  bool stream;   // streamed by the block (non-empty and not long)
+  int32_t row;  // row id within its matrix (or -1)
+  int32_t len;  // logical length
+  bool stream;  // streamed by the block (non-empty and short)
 };
 
 template <typename V>
-__device__ __forceinline__ RowBlock load_block(const Mat<V> &m, int64_t r0, int lane) {
+__device__ __forceinline__ RowBlock load_block(const Mat<V> &m, int64_t r0, int lane, int32_t smax) {
   RowBlock b;
   const int64_t r = r0 + lane;
   b.row = r < m.n_rows ? (int32_t)r : -1;
   b.len = b.row >= 0 ? __ldg(m.row_sizes + r) : 0;
-  b.stream = b.len > 0 && b.len <= LONG_ROW;
+  b.stream = b.len > 0 && b.len <= smax;
   return b;
 }
 
-// Entries of the lane's row that live in segment layer l (coalesced pair
-// loads across the block); cum accumulates the capacity of layers < l.
+// Entries of the lane's row in segment layer l (coalesced pair loads across
+// the block); cum accumulates the capacity of layers < l.
 template <typename V>
 __device__ __forceinline__ void next_layer(const Mat<V> &m, const RowBlock &b, int l, int64_t &cum, int32_t &len_l,
                                            int32_t &st_l) {
@@ -125,8 +323,29 @@ __device__ __forceinline__ void next_layer(const Mat<V> &m, const RowBlock &b, i
   }
 }
 
-template <typename V, int K, bool VEC>
-__device__ __forceinline__ void load_xk(const V *__restrict__ x, int64_t c, int64_t ldx, double (&xv)[K]) {
+// Row of each lane's entry in the window [w0, w0+32): M has bit p set where a
+// row starts at w0+p; the lane's row is the k-th starting row (k = starts at
+// positions <= lane) or, before the first start, the row running into the
+// window.  Lanes past the stream's end get the last row (callers mask them).
+struct WinMap {
+  int j;
+  unsigned M;
+};
+__device__ __forceinline__ WinMap window_map(int32_t w0, int32_t excl, int32_t incl, int32_t len, int lane) {
+  const bool starts = len > 0 && excl >= w0 && excl < w0 + 32;
+  const bool runs_in = len > 0 && excl < w0 && incl > w0;
+  const unsigned O = __ballot_sync(FULL, starts);
+  const unsigned M = __reduce_or_sync(FULL, starts ? (1u << (excl - w0)) : 0u);
+  const unsigned C = __ballot_sync(FULL, runs_in);
+  const int k = __popc(M & (0xffffffffu >> (31 - lane)));
+  WinMap r;
+  r.j = k == 0 ? (C ? __ffs(C) - 1 : 0) : (int)__fns(O, 0, k);
+  r.M = M;
+  return r;
+}
+
+template <typename T, typename V, int K, bool VEC>
+__device__ __forceinline__ void load_xk(const V *__restrict__ x, int64_t c, int64_t ldx, T (&xv)[K]) {
   if constexpr (VEC && sizeof(V) == 4 && K == 4) {
     const float4 t = __ldg(reinterpret_cast<const float4 *>(x + c * 4));
     xv[0] = t.x; xv[1] = t.y; xv[2] = t.z; xv[3] = t.w;
@@ -142,39 +361,46 @@ __device__ __forceinline__ void load_xk(const V *__restrict__ x, int64_t c, int6
 #pragma unroll
     for (int k = 0; k < K; k += 2) {
       const double2 t = __ldg(reinterpret_cast<const double2 *>(x + c * K + k));
-      xv[k] = t.x; xv[k + 1] = t.y;
+      xv[k] = (T)t.x; xv[k + 1] = (T)t.y;
     }
   } else {
 #pragma unroll
-    for (int k = 0; k < K; k++) xv[k] = (double)__ldg(x + c * ldx + k);
+    for (int k = 0; k < K; k++) xv[k] = (T)__ldg(x + c * ldx + k);
   }
 }
 
 enum { OP_SPMV = 0, OP_SUM = 1, OP_MAX = 2, OP_MIN = 3, OP_COUNT = 4 };
 
-template <int OP>
-__device__ __forceinline__ double op_init() {
-  return OP == OP_MAX ? -INFINITY : OP == OP_MIN ? INFINITY : 0.0;
+template <typename T, int OP>
+__device__ __forceinline__ T op_init() {
+  return OP == OP_MAX ? (T)-INFINITY : OP == OP_MIN ? (T)INFINITY : (T)0;
 }
-template <int OP>
-__device__ __forceinline__ double op_comb(double a, double b) {
+// Every rounding step is an explicit round-to-nearest intrinsic: the
+// compiler may not contract a product into a later sum (it could choose
+// differently in different instantiations, and the batched and per-call
+// passes must agree bit for bit).
+__device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+
+template <typename T, int OP>
+__device__ __forceinline__ T op_comb(T a, T b) {
   if (OP == OP_MAX) return a > b ? a : b;
   if (OP == OP_MIN) return a < b ? a : b;
-  return a + b;
+  return add_rn(a, b);
 }
 
-// Contribution of one entry to the K accumulators.
+// acc (op) a*x for one entry with value a and column c (FP64 accumulators)
 template <typename V, int K, int OP, bool VEC>
-__device__ __forceinline__ void contrib(const Mat<V> &m, int64_t q, const V *x, int64_t ldx, double (&c)[K]) {
-  const double a = (double)__ldcs(m.vals + q);
+__device__ __forceinline__ void accum_entry(double a, int32_t c, const V *x, int64_t ldx, double (&acc)[K]) {
   if constexpr (OP == OP_SPMV) {
-    const int32_t col = __ldcs(m.cols + q);
     double xv[K];
-    load_xk<V, K, VEC>(x, col, ldx, xv);
+    load_xk<double, V, K, VEC>(x, c, ldx, xv);
 #pragma unroll
-    for (int k = 0; k < K; k++) c[k] = a * xv[k];
+    for (int k = 0; k < K; k++) acc[k] = __fma_rn(a, xv[k], acc[k]);
   } else {
-    c[0] = OP == OP_COUNT ? 1.0 : a;
+    acc[0] = op_comb<double, OP>(acc[0], OP == OP_COUNT ? 1.0 : a);
   }
 }
 
@@ -186,89 +412,89 @@ __device__ __forceinline__ void write_y(V *y, int64_t ldy, int32_t row, const do
     double v = acc[k];
     if ((OP == OP_MAX || OP == OP_MIN) && len == 0) v = 0.0;
     if (OP == OP_SPMV) {
-      v *= alpha;
-      if (beta != 0.0) v += beta * (double)y[(int64_t)row * ldy + k];
+      v = mul_rn(v, alpha);
+      if (beta != 0.0) v = __fma_rn(beta, (double)y[(int64_t)row * ldy + k], v);
     }
     y[(int64_t)row * ldy + k] = (V)v;
   }
 }
 
+template <int K>
+struct Windows {
+  static constexpr int U = K <= 2 ? 4 : (K <= 4 ? 2 : 1);
+};
+
 // --------------------------------------------------------- reduction pass
 
-template <typename V, int K, int OP, bool VEC>
-__global__ void __launch_bounds__(RS_THREADS_) k_rows_reduce(Mat<V> m, const int32_t *__restrict__ long_rows,
-                                                             const long long *__restrict__ long_off,
-                                                             const int32_t *__restrict__ info, int32_t *long_cnt,
-                                                             double *part, const V *__restrict__ x, int64_t ldx,
-                                                             V *__restrict__ y, int64_t ldy, double alpha,
-                                                             double beta) {
-  __shared__ double red[RS_THREADS_ / 32][K];
+template <typename V, int K, int OP, bool VEC, int PART, typename Src>
+__global__ void __launch_bounds__(RS_THREADS_) k_rows_reduce(Src src) {
+  using P = typename std::conditional<sizeof(V) == 4, float, double>::type;  // window partials
+  constexpr int U = Windows<K>::U;
+  __shared__ double red[RS_WARPS][K];
   __shared__ int last_flag;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const int32_t n_long = info[0];
-  const int64_t n_chunks = info[1];
-  const int64_t n_blocks = div_up(m.n_rows, 32);
-  const int64_t units = n_chunks + div_up(n_blocks, RS_THREADS_ / 32);
+  const int64_t units = src.units(PART);
   for (int64_t u = blockIdx.x; u < units; u += gridDim.x) {
-    if (u < n_chunks) {
+    int64_t lu;
+    const RowItem<V> &it = src.item(src.locate(PART, u, lu));
+    if (it.skip && *it.skip) continue;  // a batch matrix whose update was rejected: y untouched
+    const Mat<V> &m = it.m;
+    const V *__restrict__ x = it.x;
+    const int64_t ldx = it.ldx;
+    if constexpr (PART == P_CHUNKS) {
       // ---- one chunk of a long row, whole CTA
-      int64_t lo = 0, hi = n_long;
-      while (lo < hi) {
-        const int64_t mid = (lo + hi) >> 1;
-        if (long_off[mid] <= u) lo = mid + 1;
-        else hi = mid;
-      }
-      const int64_t li = lo - 1;
-      const int32_t row = long_rows[li];
-      const int64_t chunk = u - long_off[li];
-      const int64_t nch = long_off[li + 1] - long_off[li];
+      const int64_t li = it.chunk_li[lu];
+      const int32_t row = it.long_rows[li];
+      const int64_t chunk = lu - it.long_off[li];
+      const int64_t nch = it.long_off[li + 1] - it.long_off[li];
       const int64_t L = m.row_sizes[row];
       const Chain ch = load_chain(m, row);
       const int64_t c0 = chunk * CHUNK, c1 = c0 + CHUNK < L ? c0 + CHUNK : L;
       double acc[K];
 #pragma unroll
-      for (int k = 0; k < K; k++) acc[k] = op_init<OP>();
+      for (int k = 0; k < K; k++) acc[k] = op_init<double, OP>();
       const bool fast = ch.cp[0] >= c1;  // chunk inside layer 0
-      if (fast && ((ch.st[0] + c0) & 3) == 0 && sizeof(V) == 4) {
-        const int64_t base = ch.st[0] + c0;
-        const int64_t nv = (c1 - c0) >> 2;
-        for (int64_t v = threadIdx.x; v < nv; v += RS_THREADS_) {
-          const float4 a4 = __ldcs(reinterpret_cast<const float4 *>(m.vals + base) + v);
-          const float av[4] = {a4.x, a4.y, a4.z, a4.w};
-          if constexpr (OP == OP_SPMV) {
-            const int4 c4 = __ldcs(reinterpret_cast<const int4 *>(m.cols + base) + v);
-            const int32_t cv[4] = {c4.x, c4.y, c4.z, c4.w};
+      if (fast && sizeof(V) == 4 && ((ch.st[0] + c0) & 3) == 0) {
+        constexpr int G = STEP / 4 / RS_THREADS_;
+        for (int64_t s0 = c0; s0 < c1; s0 += STEP) {
+          const int64_t s1 = s0 + STEP < c1 ? s0 + STEP : c1;
+          const int64_t base = ch.st[0] + s0;
+          const int nv = (int)((s1 - s0) >> 2);
+          float4 a4[G];
+          int4 c4[G] = {};
 #pragma unroll
-            for (int e = 0; e < 4; e++) {
-              double xv[K];
-              load_xk<V, K, VEC>(x, cv[e], ldx, xv);
-#pragma unroll
-              for (int k = 0; k < K; k++) acc[k] = fma((double)av[e], xv[k], acc[k]);
+          for (int g = 0; g < G; g++) {
+            const int v = threadIdx.x + g * RS_THREADS_;
+            if (v < nv) {
+              a4[g] = __ldcs(reinterpret_cast<const float4 *>(m.vals + base) + v);
+              if (OP == OP_SPMV) c4[g] = __ldcs(reinterpret_cast<const int4 *>(m.cols + base) + v);
             }
-          } else {
-#pragma unroll
-            for (int e = 0; e < 4; e++) acc[0] = op_comb<OP>(acc[0], OP == OP_COUNT ? 1.0 : (double)av[e]);
           }
-        }
-        for (int64_t p = c0 + (nv << 2) + threadIdx.x; p < c1; p += RS_THREADS_) {
-          double c[K];
-          contrib<V, K, OP, VEC>(m, ch.st[0] + p, x, ldx, c);
 #pragma unroll
-          for (int k = 0; k < K; k++) acc[k] = op_comb<OP>(acc[k], c[k]);
+          for (int g = 0; g < G; g++) {
+            if (threadIdx.x + g * RS_THREADS_ < nv) {
+              accum_entry<V, K, OP, VEC>(a4[g].x, c4[g].x, x, ldx, acc);
+              accum_entry<V, K, OP, VEC>(a4[g].y, c4[g].y, x, ldx, acc);
+              accum_entry<V, K, OP, VEC>(a4[g].z, c4[g].z, x, ldx, acc);
+              accum_entry<V, K, OP, VEC>(a4[g].w, c4[g].w, x, ldx, acc);
+            }
+          }
+          for (int64_t p = s0 + ((int64_t)nv << 2) + threadIdx.x; p < s1; p += RS_THREADS_)
+            accum_entry<V, K, OP, VEC>((double)__ldcs(m.vals + ch.st[0] + p),
+                                       OP == OP_SPMV ? __ldcs(m.cols + ch.st[0] + p) : 0, x, ldx, acc);
         }
       } else {
         for (int64_t p = c0 + threadIdx.x; p < c1; p += RS_THREADS_) {
-          double c[K];
-          contrib<V, K, OP, VEC>(m, fast ? ch.st[0] + p : ch.phys(p), x, ldx, c);
-#pragma unroll
-          for (int k = 0; k < K; k++) acc[k] = op_comb<OP>(acc[k], c[k]);
+          const int64_t q = fast ? (int64_t)ch.st[0] + p : ch.phys(p);
+          accum_entry<V, K, OP, VEC>((double)__ldcs(m.vals + q), OP == OP_SPMV ? __ldcs(m.cols + q) : 0, x, ldx,
+                                     acc);
         }
       }
 #pragma unroll
       for (int k = 0; k < K; k++) {
         double v = acc[k];
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) v = op_comb<OP>(v, __shfl_xor_sync(FULL, v, o));
+        for (int o = 16; o > 0; o >>= 1) v = op_comb<double, OP>(v, __shfl_xor_sync(FULL, v, o));
         if (lane == 0) red[w][k] = v;
       }
       __syncthreads();
@@ -277,180 +503,293 @@ __global__ void __launch_bounds__(RS_THREADS_) k_rows_reduce(Mat<V> m, const int
 #pragma unroll
         for (int k = 0; k < K; k++) {
           t[k] = red[0][k];
-          for (int q = 1; q < RS_THREADS_ / 32; q++) t[k] = op_comb<OP>(t[k], red[q][k]);
-          part[(long_off[li] + chunk) * K + k] = t[k];
+          for (int q = 1; q < RS_WARPS; q++) t[k] = op_comb<double, OP>(t[k], red[q][k]);
         }
-        __threadfence();
-        const int done = atomicAdd(&long_cnt[li], 1);
-        last_flag = done == nch - 1;
+        if (nch == 1) {  // the whole row in one unit: no partials
+          write_y<V, K, OP>(it.y, it.ldy, row, t, it.alpha, it.beta, (int32_t)L);
+          last_flag = 0;
+        } else {
+#pragma unroll
+          for (int k = 0; k < K; k++) it.part[(it.long_off[li] + chunk) * K + k] = t[k];
+          __threadfence();
+          last_flag = atomicAdd(&it.long_cnt[li], 1) == nch - 1;
+        }
       }
       __syncthreads();
       if (last_flag && threadIdx.x == 0) {
         __threadfence();
         double out[K];
 #pragma unroll
-        for (int k = 0; k < K; k++) out[k] = op_init<OP>();
+        for (int k = 0; k < K; k++) out[k] = op_init<double, OP>();
         for (int64_t q = 0; q < nch; q++)
 #pragma unroll
-          for (int k = 0; k < K; k++) out[k] = op_comb<OP>(out[k], __ldcg(part + (long_off[li] + q) * K + k));
-        write_y<V, K, OP>(y, ldy, row, out, alpha, beta, (int32_t)L);
-        long_cnt[li] = 0;
+          for (int k = 0; k < K; k++)
+            out[k] = op_comb<double, OP>(out[k], __ldcg(it.part + (it.long_off[li] + q) * K + k));
+        write_y<V, K, OP>(it.y, it.ldy, row, out, it.alpha, it.beta, (int32_t)L);
+        it.long_cnt[li] = 0;
       }
       __syncthreads();
-      continue;
-    }
-    // ---- row blocks: one warp per 32 consecutive rows
-    const int64_t blk = (u - n_chunks) * (RS_THREADS_ / 32) + w;
-    if (blk >= n_blocks) continue;
-    const int64_t r0 = blk * 32;
-    const RowBlock rb = load_block(m, r0, lane);
-    double acc[K];
+    } else if constexpr (PART == P_MED) {
+      // ---- one medium row per warp
+      const int64_t mi = lu * RS_WARPS + w;
+      if (mi >= it.info[2]) continue;
+      const int32_t row = it.med_rows[mi];
+      const int64_t L = m.row_sizes[row];
+      const Chain ch = load_chain(m, row);
+      double acc[K];
 #pragma unroll
-    for (int k = 0; k < K; k++) acc[k] = op_init<OP>();
-    int64_t cum = 0;  // capacity of this lane's row in the layers before l
-    for (int l = 0; l < m.max_segs; l++) {
-      int32_t len_l, st_l;
-      next_layer(m, rb, l, cum, len_l, st_l);
-      if (!__any_sync(FULL, len_l > 0)) break;
-      const int64_t incl = warp_incl_scan((int64_t)len_l);
-      const int64_t excl = incl - len_l;
-      const int64_t E = __shfl_sync(FULL, incl, 31);
-      for (int64_t base = 0; base < E; base += 32) {
-        const int64_t e = base + lane;
-        const int j = find_row(e < E ? e : E - 1, excl);
-        const int64_t ej = __shfl_sync(FULL, excl, j);
-        const int32_t sj = __shfl_sync(FULL, st_l, j);
-        double c[K];
-        if (e < E) {
-          contrib<V, K, OP, VEC>(m, (int64_t)sj + (e - ej), x, ldx, c);
-        } else {
+      for (int k = 0; k < K; k++) acc[k] = op_init<double, OP>();
+      int64_t before = 0;
 #pragma unroll
-          for (int k = 0; k < K; k++) c[k] = op_init<OP>();
-        }
-        // segmented inclusive scan by row j (rows are non-decreasing over lanes)
-        const int jj = e < E ? j : 32;
+      for (int l = 0; l < MAX_SEGS; l++) {
+        if (l < ch.ns && before < L) {
+          const int64_t take = (int64_t)ch.cp[l] < L - before ? (int64_t)ch.cp[l] : L - before;
+          const int64_t st = ch.st[l];
+          for (int64_t b0 = 0; b0 < take; b0 += 32 * 4) {
+            double a[4];
+            int32_t col[4];
 #pragma unroll
-        for (int d = 1; d < 32; d <<= 1) {
-          const int jo = __shfl_up_sync(FULL, jj, d);
+            for (int i = 0; i < 4; i++) {
+              const int64_t p = b0 + 32 * i + lane;
+              const int64_t q = st + (p < take ? p : 0);
+              a[i] = (double)__ldcs(m.vals + q);
+              col[i] = OP == OP_SPMV ? __ldcs(m.cols + q) : 0;
+            }
 #pragma unroll
-          for (int k = 0; k < K; k++) {
-            const double co = __shfl_up_sync(FULL, c[k], d);
-            if (lane >= d && jo == jj) c[k] = op_comb<OP>(c[k], co);
+            for (int i = 0; i < 4; i++)
+              if (b0 + 32 * i + lane < take) accum_entry<V, K, OP, VEC>(a[i], col[i], x, ldx, acc);
           }
-        }
-        // lane j collects the tail of its row's run in this 32-entry window
-        const bool hit = len_l > 0 && excl < base + 32 && incl > base;
-        const int tail = (int)((incl < base + 32 ? incl : base + 32) - 1 - base);
-#pragma unroll
-        for (int k = 0; k < K; k++) {
-          const double got = __shfl_sync(FULL, c[k], hit ? tail : 0);
-          if (hit) acc[k] = op_comb<OP>(acc[k], got);
+          before += ch.cp[l];
         }
       }
+#pragma unroll
+      for (int k = 0; k < K; k++) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) acc[k] = op_comb<double, OP>(acc[k], __shfl_xor_sync(FULL, acc[k], o));
+      }
+      if (lane == 0) write_y<V, K, OP>(it.y, it.ldy, row, acc, it.alpha, it.beta, (int32_t)L);
+    } else {
+      // ---- short rows: one warp per 32 consecutive rows
+      const int64_t blk = lu * RS_WARPS + w;
+      if (blk * 32 >= m.n_rows) continue;
+      const RowBlock rb = load_block(m, blk * 32, lane, it.short_max);
+      double acc[K];
+#pragma unroll
+      for (int k = 0; k < K; k++) acc[k] = op_init<double, OP>();
+      int64_t cum = 0;  // capacity of this lane's row in the layers before l
+      for (int l = 0; l < m.max_segs; l++) {
+        int32_t len_l, st_l;
+        next_layer(m, rb, l, cum, len_l, st_l);
+        if (!__any_sync(FULL, len_l > 0)) break;
+        const int32_t incl = warp_incl_scan(len_l);  // block-local (<= 32 * short_max)
+        const int32_t excl = incl - len_l;
+        const int32_t E = __shfl_sync(FULL, incl, 31);
+        for (int32_t base = 0; base < E; base += 32 * U) {
+          int32_t q[U];
+          unsigned Mw[U];
+          bool ok[U];
+#pragma unroll
+          for (int i = 0; i < U; i++) {
+            const int32_t w0 = base + 32 * i;
+            const WinMap wm = window_map(w0, excl, incl, len_l, lane);
+            const int32_t ej = __shfl_sync(FULL, excl, wm.j);
+            const int32_t sj = __shfl_sync(FULL, st_l, wm.j);
+            ok[i] = w0 + lane < E;
+            Mw[i] = wm.M;
+            q[i] = sj + (ok[i] ? w0 + lane - ej : 0);
+          }
+          V a[U];
+          int32_t col[U];
+#pragma unroll
+          for (int i = 0; i < U; i++) {
+            a[i] = __ldcs(m.vals + q[i]);
+            col[i] = OP == OP_SPMV ? __ldcs(m.cols + q[i]) : 0;
+          }
+#pragma unroll
+          for (int i = 0; i < U; i++) {
+            P c[K];
+#pragma unroll
+            for (int k = 0; k < K; k++) c[k] = op_init<P, OP>();
+            if (ok[i]) {
+              if constexpr (OP == OP_SPMV) {
+                P xv[K];
+                load_xk<P, V, K, VEC>(x, col[i], ldx, xv);
+#pragma unroll
+                for (int k = 0; k < K; k++) c[k] = mul_rn((P)a[i], xv[k]);
+              } else {
+                c[0] = OP == OP_COUNT ? (P)1 : (P)a[i];
+              }
+            }
+            // segmented inclusive scan: lanes p-d and p share a row unless a
+            // row starts in (p-d, p] (bit test on the window's start mask)
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+              const bool same = lane >= d && ((Mw[i] >> (lane - d + 1)) & ((1u << d) - 1u)) == 0;
+#pragma unroll
+              for (int k = 0; k < K; k++) {
+                const P co = __shfl_up_sync(FULL, c[k], d);
+                if (same) c[k] = op_comb<P, OP>(c[k], co);
+              }
+            }
+            // lane j collects the tail of its row's run in this window
+            const int32_t w0 = base + 32 * i;
+            const bool hit = len_l > 0 && excl < w0 + 32 && incl > w0;
+            const int tail = (incl < w0 + 32 ? incl : w0 + 32) - 1 - w0;
+#pragma unroll
+            for (int k = 0; k < K; k++) {
+              const P got = __shfl_sync(FULL, c[k], hit ? tail : 0);
+              if (hit) acc[k] = op_comb<double, OP>(acc[k], (double)got);
+            }
+          }
+        }
+      }
+      if (rb.row >= 0 && rb.len <= it.short_max) write_y<V, K, OP>(it.y, it.ldy, rb.row, acc, it.alpha, it.beta, rb.len);
     }
-    if (rb.row >= 0 && rb.len <= LONG_ROW) write_y<V, K, OP>(y, ldy, rb.row, acc, alpha, beta, rb.len);
   }
 }
 
 // -------------------------------------------------------------- copy pass
 // Copies each row's logical entries to dst_off[r] in (out_cols, out_vals),
-// optionally writing COO row ids and an int32 row pointer.
+// optionally writing COO row ids and an int32 row pointer (one matrix).
 
-template <typename V>
-__global__ void __launch_bounds__(RS_THREADS_) k_rows_copy(Mat<V> m, const int32_t *__restrict__ long_rows,
-                                                           const long long *__restrict__ long_off,
-                                                           const int32_t *__restrict__ info,
-                                                           const long long *__restrict__ dst_off,
+template <typename V, int PART>
+__global__ void __launch_bounds__(RS_THREADS_) k_rows_copy(RowItem<V> it, const long long *__restrict__ dst_off,
                                                            int32_t *__restrict__ out_cols, V *__restrict__ out_vals,
                                                            int32_t *__restrict__ out_rows,
                                                            int32_t *__restrict__ out_rowptr) {
+  constexpr int U = 4;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const int32_t n_long = info[0];
-  const int64_t n_chunks = info[1];
-  const int64_t n_blocks = div_up(m.n_rows, 32);
-  const int64_t units = n_chunks + div_up(n_blocks, RS_THREADS_ / 32);
-  if (out_rowptr && blockIdx.x == 0 && threadIdx.x == 0) out_rowptr[m.n_rows] = (int32_t)dst_off[m.n_rows];
+  const Mat<V> &m = it.m;
+  RowOne<V> src{it};
+  const int64_t units = src.units(PART);
+  if (PART == P_BLOCKS && out_rowptr && blockIdx.x == 0 && threadIdx.x == 0)
+    out_rowptr[m.n_rows] = (int32_t)dst_off[m.n_rows];
   for (int64_t u = blockIdx.x; u < units; u += gridDim.x) {
-    if (u < n_chunks) {
-      int64_t lo = 0, hi = n_long;
-      while (lo < hi) {
-        const int64_t mid = (lo + hi) >> 1;
-        if (long_off[mid] <= u) lo = mid + 1;
-        else hi = mid;
+    if constexpr (PART == P_CHUNKS || PART == P_MED) {
+      // long-row chunk (whole CTA) or medium row (one warp)
+      int32_t row;
+      int64_t c0, c1, L;
+      int tid, nthr;
+      if (PART == P_CHUNKS) {
+        const int64_t li = it.chunk_li[u];
+        row = it.long_rows[li];
+        const int64_t chunk = u - it.long_off[li];
+        L = m.row_sizes[row];
+        c0 = chunk * CHUNK;
+        c1 = c0 + CHUNK < L ? c0 + CHUNK : L;
+        tid = threadIdx.x;
+        nthr = RS_THREADS_;
+      } else {
+        const int64_t mi = u * RS_WARPS + w;
+        if (mi >= it.info[2]) continue;
+        row = it.med_rows[mi];
+        L = m.row_sizes[row];
+        c0 = 0;
+        c1 = L;
+        tid = lane;
+        nthr = 32;
       }
-      const int64_t li = lo - 1;
-      const int32_t row = long_rows[li];
-      const int64_t chunk = u - long_off[li];
-      const int64_t L = m.row_sizes[row];
       const Chain ch = load_chain(m, row);
-      const int64_t c0 = chunk * CHUNK, c1 = c0 + CHUNK < L ? c0 + CHUNK : L;
       const int64_t d = dst_off[row];
-      if (out_rowptr && chunk == 0 && threadIdx.x == 0) out_rowptr[row] = (int32_t)d;
+      if (out_rowptr && c0 == 0 && tid == 0) out_rowptr[row] = (int32_t)d;
       const bool fast = ch.cp[0] >= c1;
-      for (int64_t p = c0 + threadIdx.x; p < c1; p += RS_THREADS_) {
-        const int64_t q = fast ? (int64_t)ch.st[0] + p : ch.phys(p);
-        out_cols[d + p] = __ldcs(m.cols + q);
-        out_vals[d + p] = __ldcs(m.vals + q);
-        if (out_rows) out_rows[d + p] = row;
+      constexpr int G = 16;
+      for (int64_t s0 = c0; s0 < c1; s0 += (int64_t)G * nthr) {
+        int32_t cv[G];
+        V vv[G];
+#pragma unroll
+        for (int g = 0; g < G; g++) {
+          const int64_t p = s0 + tid + (int64_t)g * nthr;
+          if (p < c1) {
+            const int64_t q = fast ? (int64_t)ch.st[0] + p : ch.phys(p);
+            cv[g] = __ldcs(m.cols + q);
+            vv[g] = __ldcs(m.vals + q);
+          }
+        }
+#pragma unroll
+        for (int g = 0; g < G; g++) {
+          const int64_t p = s0 + tid + (int64_t)g * nthr;
+          if (p < c1) {
+            out_cols[d + p] = cv[g];
+            out_vals[d + p] = vv[g];
+            if (out_rows) out_rows[d + p] = row;
+          }
+        }
       }
-      continue;
-    }
-    const int64_t blk = (u - n_chunks) * (RS_THREADS_ / 32) + w;
-    if (blk >= n_blocks) continue;
-    const int64_t r0 = blk * 32;
-    const RowBlock rb = load_block(m, r0, lane);
-    const int64_t dme = rb.row >= 0 ? dst_off[rb.row] : 0;
-    if (out_rowptr && rb.row >= 0) out_rowptr[rb.row] = (int32_t)dme;
-    int64_t cum = 0;
-    for (int l = 0; l < m.max_segs; l++) {
-      const int64_t dl = dme + cum;  // destination of this layer's part
-      int32_t len_l, st_l;
-      next_layer(m, rb, l, cum, len_l, st_l);
-      if (!__any_sync(FULL, len_l > 0)) break;
-      const int64_t incl = warp_incl_scan((int64_t)len_l);
-      const int64_t excl = incl - len_l;
-      const int64_t E = __shfl_sync(FULL, incl, 31);
-      for (int64_t base = 0; base < E; base += 32) {
-        const int64_t e = base + lane;
-        const int j = find_row(e < E ? e : E - 1, excl);
-        const int64_t ej = __shfl_sync(FULL, excl, j);
-        const int32_t sj = __shfl_sync(FULL, st_l, j);
-        const int64_t dj = __shfl_sync(FULL, dl, j);
-        if (e < E) {
-          const int64_t q = (int64_t)sj + (e - ej);
-          out_cols[dj + (e - ej)] = __ldcs(m.cols + q);
-          out_vals[dj + (e - ej)] = __ldcs(m.vals + q);
-          if (out_rows) out_rows[dj + (e - ej)] = (int32_t)(r0 + j);
+    } else {
+      const int64_t blk = u * RS_WARPS + w;
+      if (blk * 32 >= m.n_rows) continue;
+      const int64_t r0 = blk * 32;
+      const RowBlock rb = load_block(m, r0, lane, it.short_max);
+      const int64_t dme = rb.row >= 0 ? dst_off[rb.row] : 0;
+      if (out_rowptr && rb.row >= 0 && rb.len <= it.short_max) out_rowptr[rb.row] = (int32_t)dme;
+      int64_t cum = 0;
+      for (int l = 0; l < m.max_segs; l++) {
+        const int64_t dl = dme + cum;  // destination of this layer's part
+        int32_t len_l, st_l;
+        next_layer(m, rb, l, cum, len_l, st_l);
+        if (!__any_sync(FULL, len_l > 0)) break;
+        const int32_t incl = warp_incl_scan(len_l);
+        const int32_t excl = incl - len_l;
+        const int32_t E = __shfl_sync(FULL, incl, 31);
+        for (int32_t base = 0; base < E; base += 32 * U) {
+          int64_t q[U], dst[U];
+          int jw[U];
+#pragma unroll
+          for (int i = 0; i < U; i++) {
+            const int32_t w0 = base + 32 * i;
+            const WinMap wm = window_map(w0, excl, incl, len_l, lane);
+            const int32_t ej = __shfl_sync(FULL, excl, wm.j);
+            const int32_t sj = __shfl_sync(FULL, st_l, wm.j);
+            const int64_t dj = __shfl_sync(FULL, dl, wm.j);
+            const bool ok = w0 + lane < E;
+            const int32_t off = ok ? w0 + lane - ej : 0;
+            jw[i] = ok ? wm.j : -1;
+            q[i] = (int64_t)sj + off;
+            dst[i] = dj + off;
+          }
+          int32_t cv[U];
+          V vv[U];
+#pragma unroll
+          for (int i = 0; i < U; i++) {
+            cv[i] = __ldcs(m.cols + q[i]);
+            vv[i] = __ldcs(m.vals + q[i]);
+          }
+#pragma unroll
+          for (int i = 0; i < U; i++) {
+            if (jw[i] >= 0) {
+              out_cols[dst[i]] = cv[i];
+              out_vals[dst[i]] = vv[i];
+              if (out_rows) out_rows[dst[i]] = (int32_t)(r0 + jw[i]);
+            }
+          }
         }
       }
     }
   }
 }
 
-static int grid_of(const void *k) {
-  return persistent_grid(k, RS_THREADS_, 0);
+static int grid_of(const void *k) { return persistent_grid(k, RS_THREADS_, 0); }
+
+template <typename V, int K, int OP, bool VEC, typename Src>
+static int launch_reduce_src(const Src &src, cudaStream_t s) {
+  static int g0 = 0, g1 = 0, g2 = 0;
+  if (!g0) {
+    g0 = grid_of((const void *)k_rows_reduce<V, K, OP, VEC, P_BLOCKS, Src>);
+    g1 = grid_of((const void *)k_rows_reduce<V, K, OP, VEC, P_CHUNKS, Src>);
+    g2 = grid_of((const void *)k_rows_reduce<V, K, OP, VEC, P_MED, Src>);
+  }
+  DCSR_LAUNCH((k_rows_reduce<V, K, OP, VEC, P_CHUNKS, Src>), g1, RS_THREADS_, 0, s, src);
+  DCSR_LAUNCH((k_rows_reduce<V, K, OP, VEC, P_MED, Src>), g2, RS_THREADS_, 0, s, src);
+  DCSR_LAUNCH((k_rows_reduce<V, K, OP, VEC, P_BLOCKS, Src>), g0, RS_THREADS_, 0, s, src);
+  return DCSR_OK;
 }
 
 template <typename V, int K, int OP, bool VEC>
 static int launch_reduce(dcsr_handle h, const V *x, int64_t ldx, V *y, int64_t ldy, double alpha, double beta,
                          cudaStream_t s) {
-  static int grid = 0;
-  if (!grid) grid = grid_of((const void *)k_rows_reduce<V, K, OP, VEC>);
-  DCSR_TRY(ensure_part(h, K, s));
-  DCSR_LAUNCH((k_rows_reduce<V, K, OP, VEC>), grid, RS_THREADS_, 0, s, h->view<V>(), h->long_rows, h->long_off,
-              h->sched_info, h->long_cnt, h->part, x, ldx, y, ldy, alpha, beta);
-  return DCSR_OK;
-}
-
-int ensure_part(dcsr_handle h, int K, cudaStream_t s) {
-  // chunks <= nnz / CHUNK + long rows <= pool / CHUNK + n_rows
-  const int64_t need = (h->pool_cap / CHUNK + h->pool_cap / LONG_ROW + 2) * K;
-  if (need <= h->part_cap) return DCSR_OK;
-  if (h->part) DCSR_CUDA(cudaFreeAsync(h->part, s));
-  h->part = nullptr;
-  DCSR_CUDA(cudaMallocAsync((void **)&h->part, sizeof(double) * need, s));
-  h->part_cap = need;
-  return DCSR_OK;
+  RowOne<V> src{row_item<V>(h, x, y, ldx, ldy, alpha, beta)};
+  return launch_reduce_src<V, K, OP, VEC>(src, s);
 }
 
 template <typename V, int K>
@@ -489,20 +828,56 @@ static int reduce_dispatch(dcsr_handle h, int32_t op, V *y, cudaStream_t s) {
   return DCSR_BAD_ARG;
 }
 
+// Batched SpMV over matrices that share k.
+template <typename V, int K, bool VEC>
+static int spmv_many_k(const RowItem<V> *its, int count, long long *pref, cudaStream_t s) {
+  DCSR_LAUNCH(k_unit_prefix<V>, 1, 1024, 0, s, its, count, pref);
+  RowMany<V> src{its, count, pref};
+  return launch_reduce_src<V, K, OP_SPMV, VEC>(src, s);
+}
+
+template <typename V>
+static int spmv_many_t(const RowItem<V> *its, int count, int k, bool vec, long long *pref, cudaStream_t s) {
+  switch (k) {
+    case 1: return spmv_many_k<V, 1, false>(its, count, pref, s);
+    case 2: return vec ? spmv_many_k<V, 2, true>(its, count, pref, s) : spmv_many_k<V, 2, false>(its, count, pref, s);
+    case 3: return spmv_many_k<V, 3, false>(its, count, pref, s);
+    case 4: return vec ? spmv_many_k<V, 4, true>(its, count, pref, s) : spmv_many_k<V, 4, false>(its, count, pref, s);
+    case 5: return spmv_many_k<V, 5, false>(its, count, pref, s);
+    case 6: return vec ? spmv_many_k<V, 6, true>(its, count, pref, s) : spmv_many_k<V, 6, false>(its, count, pref, s);
+    case 7: return spmv_many_k<V, 7, false>(its, count, pref, s);
+    case 8: return vec ? spmv_many_k<V, 8, true>(its, count, pref, s) : spmv_many_k<V, 8, false>(its, count, pref, s);
+  }
+  return DCSR_BAD_ARG;
+}
+
+int spmv_many(const void *items_dev, int dtype, int count, int k, bool vec, long long *pref, cudaStream_t s) {
+  if (count == 0) return DCSR_OK;
+  if (dtype == DCSR_F32) return spmv_many_t<float>((const RowItem<float> *)items_dev, count, k, vec, pref, s);
+  return spmv_many_t<double>((const RowItem<double> *)items_dev, count, k, vec, pref, s);
+}
+
+template <typename V>
+static int launch_copy(dcsr_handle h, const long long *dst_off, int32_t *out_cols, V *out_vals, int32_t *out_rows,
+                       int32_t *out_rowptr, cudaStream_t s) {
+  static int g0 = 0, g1 = 0, g2 = 0;
+  if (!g0) {
+    g0 = grid_of((const void *)k_rows_copy<V, P_BLOCKS>);
+    g1 = grid_of((const void *)k_rows_copy<V, P_CHUNKS>);
+    g2 = grid_of((const void *)k_rows_copy<V, P_MED>);
+  }
+  const RowItem<V> it = row_item<V>(h, nullptr, nullptr, 0, 0, 0.0, 0.0);
+  DCSR_LAUNCH((k_rows_copy<V, P_CHUNKS>), g1, RS_THREADS_, 0, s, it, dst_off, out_cols, out_vals, out_rows, out_rowptr);
+  DCSR_LAUNCH((k_rows_copy<V, P_MED>), g2, RS_THREADS_, 0, s, it, dst_off, out_cols, out_vals, out_rows, out_rowptr);
+  DCSR_LAUNCH((k_rows_copy<V, P_BLOCKS>), g0, RS_THREADS_, 0, s, it, dst_off, out_cols, out_vals, out_rows, out_rowptr);
+  return DCSR_OK;
+}
+
 int copy_rows(dcsr_handle h, const long long *dst_off, int32_t *out_cols, void *out_vals, int32_t *out_rows,
               int32_t *out_rowptr, cudaStream_t s) {
   if (!h->bins_valid) DCSR_TRY(build_schedule(h, s));
-  static int gf = 0, gd = 0;
-  if (h->dtype == DCSR_F32) {
-    if (!gf) gf = grid_of((const void *)k_rows_copy<float>);
-    DCSR_LAUNCH(k_rows_copy<float>, gf, RS_THREADS_, 0, s, h->view<float>(), h->long_rows, h->long_off,
-                h->sched_info, dst_off, out_cols, (float *)out_vals, out_rows, out_rowptr);
-  } else {
-    if (!gd) gd = grid_of((const void *)k_rows_copy<double>);
-    DCSR_LAUNCH(k_rows_copy<double>, gd, RS_THREADS_, 0, s, h->view<double>(), h->long_rows, h->long_off,
-                h->sched_info, dst_off, out_cols, (double *)out_vals, out_rows, out_rowptr);
-  }
-  return DCSR_OK;
+  if (h->dtype == DCSR_F32) return launch_copy<float>(h, dst_off, out_cols, (float *)out_vals, out_rows, out_rowptr, s);
+  return launch_copy<double>(h, dst_off, out_cols, (double *)out_vals, out_rows, out_rowptr, s);
 }
 
 }  // namespace dcsr
@@ -515,6 +890,7 @@ extern "C" int dcsr_spmv(dcsr_handle h, const void *x, int32_t k, int64_t ldx, v
     return DCSR_BAD_ARG;
   cudaStream_t s = (cudaStream_t)stream;
   if (h->n_rows == 0) return DCSR_OK;
+  DCSR_TRY(ensure_part(h, k, s));
   if (!h->bins_valid) DCSR_TRY(build_schedule(h, s));
   if (h->dtype == DCSR_F32)
     return spmv_dispatch<float>(h, (const float *)x, k, ldx, (float *)y, ldy, alpha, beta, s);
@@ -525,6 +901,7 @@ extern "C" int dcsr_row_reduce(dcsr_handle h, int32_t op, void *y, void *stream)
   if (!h || (h->n_rows > 0 && !y) || op < 0 || op > 3) return DCSR_BAD_ARG;
   cudaStream_t s = (cudaStream_t)stream;
   if (h->n_rows == 0) return DCSR_OK;
+  DCSR_TRY(ensure_part(h, 1, s));
   if (!h->bins_valid) DCSR_TRY(build_schedule(h, s));
   if (h->dtype == DCSR_F32) return reduce_dispatch<float>(h, op, (float *)y, s);
   return reduce_dispatch<double>(h, op, (double *)y, s);

@@ -1,25 +1,31 @@
-// update.cu -- in-place batch updates of a DCSR matrix and COO grouping.
+// update.cu -- in-place batch updates of one DCSR matrix or of a set of
+// matrices at once, and COO grouping for loads.
 //
-// Pipeline (all on the caller's stream, no host synchronisation):
-//   keys     (row,col) keys with an index check            k_make_keys
-//   sort     stable LSD radix sort of (key, batch index)    radix_sort_pairs
-//   bucket   sorted columns/values + per-row batch ranges   k_gather_sorted, scan, k_touched
-//   plan     per touched row: duplicate search, new length, capacity, new
-//            segment size and layer (no mutation)           k_plan_merge / k_plan_append
-//   alloc    exclusive scan of new segment sizes (deterministic, row order)
-//   check    pool / layer / index verdict -> go flag         k_check
-//   apply    warp per row: merge in place (or append)       k_apply_merge / k_apply_append
-//   relocate rows whose in-place shift would exceed reloc_min are merged out
-//            of place into a fresh segment, tile-parallel   k_relocate
-//   finish   chain reset of relocated rows, new pool top    k_finish
-// A rejected batch (status != OK) leaves the matrix untouched.
+// Pipeline (all on the caller's stream, no host synchronisation); every
+// kernel runs over the union of all matrices' triples / touched rows:
+//   keys     (matrix, row, col) keys with an index check        k_make_keys
+//   sort     stable LSD radix sort of (key, global triple index) radix_sort_pairs
+//   bucket   sorted columns/values + per-row batch ranges        k_gather_sorted, scan, k_touched
+//   plan     MERGE: each (row, col) group binary-searches its row
+//            (thread per group), new groups are placed by a scan, then
+//            per touched row: new length, capacity, layer, relocation
+//            APPEND: the reference's segment walk per touched row
+//   alloc    exclusive scan of new segment sizes (row order, per matrix
+//            offsets taken relative to its first touched row)
+//   check    per matrix: pool / layer / index verdict -> go flag  k_check
+//   apply    existing columns in place (thread per group), then per row
+//            the in-place shift + inserts (8- or 32-lane sub-warps)
+//   relocate rows whose in-place shift would exceed reloc_min are merged
+//            out of place into a fresh segment, tile-parallel      k_relocate
+//   finish   chain reset of relocated rows, new pool tops          k_finish
+// A rejected matrix (status != OK) is left untouched; the others proceed.
 //
 // Reference: device::UpdateMatrix include/load.h:258-325 and UpdateMatrix_dcsr
 // include/sparse_update.inl:16-130 (segment walk, bump allocation, layer
 // linking).  The reference appends without merging and allocates with
 // atomicAdd; here MERGE mode keeps rows sorted and unique (duplicates summed
 // in batch order) and the allocation is a row-ordered scan, so layouts are
-// reproducible bit for bit.
+// reproducible bit for bit, alone or in a batch.
 #include "internal.cuh"
 
 namespace dcsr {
@@ -28,62 +34,134 @@ constexpr int UPD_THREADS = 256;
 constexpr int RT_TILE = 1024;  // relocation: outputs per tile
 constexpr int RT_THREADS = 256;
 constexpr int RT_ITEMS = RT_TILE / RT_THREADS;
+constexpr int SMALL_AFF = 96;  // apply: rows shifting <= this many entries use 8-lane sub-warps
 
 enum { AUX_BAD_INDEX = 1, AUX_LAYER_OVF = 2 };
 
-__device__ __forceinline__ unsigned lanemask_lt_u() {
-  unsigned m;
-  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
-  return m;
+// Key layout: [matrix | row | col] (MERGE) or [matrix | row] (APPEND).
+struct KeyFmt {
+  int cb, rb, merge;
+  __device__ __forceinline__ int32_t row(unsigned long long k) const {
+    const unsigned long long rk = merge ? (k >> cb) : k;
+    return (int32_t)(rk & ((1ull << rb) - 1));
+  }
+  __device__ __forceinline__ int item(unsigned long long k) const { return (int)(k >> (rb + (merge ? cb : 0))); }
+  __device__ __forceinline__ unsigned long long rowkey(unsigned long long k) const { return merge ? (k >> cb) : k; }
+  __device__ __forceinline__ int32_t col(unsigned long long k) const { return (int32_t)(k & ((1ull << cb) - 1)); }
+};
+
+// ------------------------------------------------------------ matrix sources
+
+// One matrix, passed by value.
+template <typename V>
+struct UpdOne {
+  Mat<V> m;
+  const int32_t *rows, *cols;
+  const V *vals;
+  __device__ __forceinline__ const Mat<V> &mat(int) const { return m; }
+  __device__ __forceinline__ long long *st(int) const { return m.stat; }
+  __device__ __forceinline__ int item_of_g(int64_t) const { return 0; }
+  __device__ __forceinline__ int64_t local(int, int64_t g) const { return g; }
+  __device__ __forceinline__ const int32_t *urows(int) const { return rows; }
+  __device__ __forceinline__ const int32_t *ucols(int) const { return cols; }
+  __device__ __forceinline__ const V *uvals(int) const { return vals; }
+};
+
+// A set of matrices: device array of batch items.
+template <typename V>
+struct UpdMany {
+  const BatchItem<V> *it;
+  int count;
+  __device__ __forceinline__ const Mat<V> &mat(int i) const { return it[i].m; }
+  __device__ __forceinline__ long long *st(int i) const { return it[i].m.stat; }
+  __device__ __forceinline__ int item_of_g(int64_t g) const {
+    int lo = 0, hi = count;  // largest i with toff <= g
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) >> 1;
+      if (it[mid].toff <= g) lo = mid;
+      else hi = mid;
+    }
+    return lo;
+  }
+  __device__ __forceinline__ int64_t local(int i, int64_t g) const { return g - it[i].toff; }
+  __device__ __forceinline__ const int32_t *urows(int i) const { return it[i].rows; }
+  __device__ __forceinline__ const int32_t *ucols(int i) const { return it[i].cols; }
+  __device__ __forceinline__ const V *uvals(int i) const { return (const V *)it[i].vals; }
+};
+
+// ------------------------------------------------------------------ keys
+
+template <typename V, typename Src>
+__global__ void k_item_init(Src src, int count) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+    long long *st = src.st(i);
+    st[ST_AUX] = 0;
+    st[ST_T0] = 0;
+    st[ST_T1] = 0;
+    st[ST_GO] = 0;
+  }
 }
 
-__device__ __forceinline__ int32_t key_row(unsigned long long k, int cb, int merge) {
-  return merge ? (int32_t)(k >> cb) : (int32_t)k;
-}
-
-__global__ void k_make_keys(const int32_t *rows, const int32_t *cols, int64_t n, int32_t n_rows, int32_t n_cols,
-                            int cb, int merge, unsigned long long *keys, unsigned *perm, long long *stat) {
+template <typename V, typename Src>
+__global__ void k_make_keys(Src src, int64_t n, KeyFmt f, unsigned long long *keys, unsigned *perm) {
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
-    int32_t r = rows[i], c = cols[i];
-    if (r < 0 || r >= n_rows || c < 0 || c >= n_cols) {
-      atomicOr((unsigned long long *)&stat[ST_AUX], (unsigned long long)AUX_BAD_INDEX);
+  for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < n; g += stride) {
+    const int i = src.item_of_g(g);
+    const int64_t l = src.local(i, g);
+    const Mat<V> &m = src.mat(i);
+    int32_t r = src.urows(i)[l], c = src.ucols(i)[l];
+    if (r < 0 || r >= m.n_rows || c < 0 || c >= m.n_cols) {
+      atomicOr((unsigned long long *)&src.st(i)[ST_AUX], (unsigned long long)AUX_BAD_INDEX);
       r = 0;
       c = 0;
     }
-    keys[i] = merge ? (((unsigned long long)r << cb) | (unsigned long long)c) : (unsigned long long)r;
-    perm[i] = (unsigned)i;
+    const unsigned long long it = (unsigned long long)i << (f.rb + (f.merge ? f.cb : 0));
+    keys[g] = f.merge ? (it | ((unsigned long long)r << f.cb) | (unsigned long long)c) : (it | (unsigned long long)r);
+    perm[g] = (unsigned)g;
   }
 }
 
-template <typename V>
-__global__ void k_gather_sorted(const unsigned long long *keys, const unsigned *perm, const int32_t *cols,
-                                const V *vals, int64_t n, int cb, int merge, int32_t n_cols, int32_t *bcol,
-                                V *bval, long long *hflag) {
+template <typename V, typename Src>
+__global__ void k_gather_sorted(Src src, const unsigned long long *keys, const unsigned *perm, int64_t n, KeyFmt f,
+                                int32_t *bcol, V *bval, long long *hflag) {
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  const unsigned long long cmask = (1ull << cb) - 1;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
-    unsigned long long k = keys[i];
-    unsigned p = perm[i];
-    int32_t c = merge ? (int32_t)(k & cmask) : cols[p];
-    if (c < 0 || c >= n_cols) c = 0;  // rejected batch; keeps later reads in range
-    bcol[i] = c;
-    bval[i] = vals[p];
-    hflag[i] = (i == 0 || key_row(keys[i - 1], cb, merge) != key_row(k, cb, merge)) ? 1 : 0;
+  for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < n; g += stride) {
+    const unsigned long long k = keys[g];
+    const unsigned p = perm[g];
+    const int i = f.item(k);
+    const int64_t l = src.local(i, p);
+    int32_t c = f.merge ? f.col(k) : src.ucols(i)[l];
+    if (c < 0 || c >= src.mat(i).n_cols) c = 0;  // rejected matrix; keeps later reads in range
+    bcol[g] = c;
+    bval[g] = src.uvals(i)[l];
+    hflag[g] = (g == 0 || f.rowkey(keys[g - 1]) != f.rowkey(k)) ? 1 : 0;
   }
 }
 
-__global__ void k_touched(const unsigned long long *keys, int64_t n, int cb, int merge, const long long *hpos,
-                          int32_t *trow, int32_t *tb0) {
+template <typename V, typename Src>
+__global__ void k_touched(Src src, const unsigned long long *keys, int64_t n, KeyFmt f, const long long *hpos,
+                          const long long *gstat, int32_t *trow, int32_t *tb0, int32_t *tmat) {
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
-    int32_t r = key_row(keys[i], cb, merge);
-    bool head = i == 0 || key_row(keys[i - 1], cb, merge) != r;
+  for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < n; g += stride) {
+    const unsigned long long k = keys[g];
+    const bool head = g == 0 || f.rowkey(keys[g - 1]) != f.rowkey(k);
     if (head) {
-      trow[hpos[i]] = r;
-      tb0[hpos[i]] = (int32_t)i;
+      const int64_t t = hpos[g];
+      const int i = f.item(k);
+      trow[t] = f.row(k);
+      tb0[t] = (int32_t)g;
+      tmat[t] = i;
+      const int prev = g == 0 ? -1 : f.item(keys[g - 1]);
+      if (prev != i) {
+        src.st(i)[ST_T0] = t;
+        if (prev >= 0) src.st(prev)[ST_T1] = t;
+      }
     }
-    if (i == n - 1) tb0[hpos[i] + (head ? 1 : 0)] = (int32_t)n;
+    if (g == n - 1) {
+      const int64_t nt = hpos[g] + (head ? 1 : 0);
+      tb0[nt] = (int32_t)n;
+      src.st(f.item(k))[ST_T1] = nt;
+    }
   }
 }
 
@@ -105,8 +183,6 @@ struct Sub {
     return S == 32 ? b : (b >> (sw * S)) & ((1u << S) - 1u);
   }
   __device__ __forceinline__ unsigned full() const { return S == 32 ? FULL : (1u << S) - 1u; }
-  template <typename T>
-  __device__ __forceinline__ T shfl(T v, int src) const { return __shfl_sync(mask, v, src, S); }
   __device__ __forceinline__ void sync() const { __syncwarp(mask); }
   __device__ __forceinline__ int incl_scan(int v) const {
 #pragma unroll
@@ -120,26 +196,24 @@ struct Sub {
   __device__ __forceinline__ int leading(unsigned bm) const { return bm == full() ? S : __ffs(~bm) - 1; }
 };
 
-constexpr int PLAN_S = 8;     // lanes per touched row in the plan
-constexpr int SMALL_AFF = 96; // apply: rows shifting <= this many entries use 8-lane sub-warps
-
 // MERGE plan, step 1 (thread per batch entry): every (row, col) group head
 // binary-searches its column in the row: bpos = position (existing) or
 // ~insertion point (new); nflag = 1 for new columns.
-template <typename V>
-__global__ void k_head_search(Mat<V> m, const unsigned long long *keys, int64_t T, int cb, const int32_t *bcol,
+template <typename V, typename Src>
+__global__ void k_head_search(Src src, const unsigned long long *keys, int64_t T, KeyFmt f, const int32_t *bcol,
                               int32_t *bpos, long long *nflag) {
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i <= T; i += stride) {
-    if (i == T) {
+  for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g <= T; g += stride) {
+    if (g == T) {
       nflag[T] = 0;
       continue;
     }
-    const unsigned long long k = keys[i];
+    const unsigned long long k = keys[g];
     long long isnew = 0;
-    if (i == 0 || keys[i - 1] != k) {
-      const int32_t r = (int32_t)(k >> cb);
-      const int32_t c = bcol[i];
+    if (g == 0 || keys[g - 1] != k) {
+      const Mat<V> &m = src.mat(f.item(k));
+      const int32_t r = f.row(k);
+      const int32_t c = bcol[g];
       const int64_t L = m.row_sizes[r];
       const Chain ch = load_chain(m, r);
       int64_t lo = 0, hi = L;
@@ -149,9 +223,9 @@ __global__ void k_head_search(Mat<V> m, const unsigned long long *keys, int64_t 
         else hi = mid;
       }
       isnew = !(lo < L && __ldg(m.cols + ch.phys(lo)) == c);
-      bpos[i] = isnew ? ~(int32_t)lo : (int32_t)lo;
+      bpos[g] = isnew ? ~(int32_t)lo : (int32_t)lo;
     }
-    nflag[i] = isnew;
+    nflag[g] = isnew;
   }
 }
 
@@ -159,32 +233,33 @@ __global__ void k_head_search(Mat<V> m, const unsigned long long *keys, int64_t 
 // column order, to slot b0 + k of their row (k from the scan of nflag), with
 // their batch-order sum.
 template <typename V>
-__global__ void k_new_compact(const unsigned long long *keys, int64_t T, int cb, const int32_t *bcol, const V *bval,
-                              const int32_t *bpos, const long long *nflag_excl, const long long *hpos,
+__global__ void k_new_compact(const unsigned long long *keys, int64_t T, KeyFmt f, const int32_t *bcol,
+                              const V *bval, const int32_t *bpos, const long long *nflag_excl, const long long *hpos,
                               const int32_t *tb0, int32_t *ncol, V *nval, int32_t *nins) {
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < T; i += stride) {
-    const unsigned long long k = keys[i];
-    if (i > 0 && keys[i - 1] == k) continue;
-    if (bpos[i] >= 0) continue;  // existing column
-    const bool rowhead = i == 0 || (keys[i - 1] >> cb) != (k >> cb);
-    const int64_t t = hpos[i] - (rowhead ? 0 : 1);
+  for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < T; g += stride) {
+    const unsigned long long k = keys[g];
+    if (g > 0 && keys[g - 1] == k) continue;
+    if (bpos[g] >= 0) continue;  // existing column
+    const bool rowhead = g == 0 || f.rowkey(keys[g - 1]) != f.rowkey(k);
+    const int64_t t = hpos[g] - (rowhead ? 0 : 1);
     const int32_t b0 = tb0[t];
-    const int64_t slot = b0 + (nflag_excl[i] - nflag_excl[b0]);
-    V v = bval[i];
-    for (int64_t j = i + 1; j < T && keys[j] == k; j++) v = v + bval[j];
-    ncol[slot] = bcol[i];
+    const int64_t slot = b0 + (nflag_excl[g] - nflag_excl[b0]);
+    V v = bval[g];
+    for (int64_t j = g + 1; j < T && keys[j] == k; j++) v = v + bval[j];
+    ncol[slot] = bcol[g];
     nval[slot] = v;
-    nins[slot] = ~bpos[i];
+    nins[slot] = ~bpos[g];
   }
 }
 
 // MERGE plan, step 3 (thread per touched row): new length, capacity, layer,
 // relocation decision and apply width class.
-template <typename V>
-__global__ void k_row_plan(Mat<V> m, int64_t T, const int32_t *trow, const int32_t *tb0, const long long *nflag_excl,
-                           const int32_t *nins, long long *tcap, long long *ttiles, int32_t *tmnew, int32_t *tinfo) {
-  const int64_t nt = m.stat[ST_TOUCHED];
+template <typename V, typename Src>
+__global__ void k_row_plan(Src src, int64_t T, const long long *gstat, const int32_t *trow, const int32_t *tb0,
+                           const int32_t *tmat, const long long *nflag_excl, const int32_t *nins, long long *tcap,
+                           long long *ttiles, int32_t *tmnew, int32_t *tinfo) {
+  const int64_t nt = gstat[ST_TOUCHED];
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
   for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t <= T; t += stride) {
     if (t >= nt) {
@@ -192,6 +267,8 @@ __global__ void k_row_plan(Mat<V> m, int64_t T, const int32_t *trow, const int32
       ttiles[t] = 0;
       continue;
     }
+    const int i = tmat[t];
+    const Mat<V> &m = src.mat(i);
     const int32_t r = trow[t];
     const int32_t b0 = tb0[t], b1 = tb0[t + 1];
     const int64_t L = m.row_sizes[r];
@@ -210,7 +287,8 @@ __global__ void k_row_plan(Mat<V> m, int64_t T, const int32_t *trow, const int32
       if (nl > ch.total) {
         cap = align_up(policy_cap(m.o, nl) - ch.total, m.o.align);
         layer = ch.total == 0 ? 0 : ch.ns;
-        if (layer >= m.max_segs) atomicOr((unsigned long long *)&m.stat[ST_AUX], (unsigned long long)AUX_LAYER_OVF);
+        if (layer >= m.max_segs)
+          atomicOr((unsigned long long *)&src.st(i)[ST_AUX], (unsigned long long)AUX_LAYER_OVF);
       }
     }
     tcap[t] = cap;
@@ -220,113 +298,12 @@ __global__ void k_row_plan(Mat<V> m, int64_t T, const int32_t *trow, const int32
   }
 }
 
-// Apply, step 1 (thread per batch group): existing columns take their batch
-// values in batch order, in place, before any shift or relocation reads them.
-template <typename V>
-__global__ void k_apply_existing(Mat<V> m, const unsigned long long *keys, int64_t T, int cb, const V *bval,
-                                 const int32_t *bpos) {
-  if (!m.stat[ST_GO]) return;
-  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < T; i += stride) {
-    const unsigned long long k = keys[i];
-    if (i > 0 && keys[i - 1] == k) continue;
-    const int32_t p = bpos[i];
-    if (p < 0) continue;
-    const Chain ch = load_chain(m, (int32_t)(k >> cb));
-    const int64_t q = ch.phys(p);
-    V v = m.vals[q];
-    for (int64_t j = i; j < T && keys[j] == k; j++) v = v + bval[j];
-    m.vals[q] = v;
-  }
-}
-
-template <typename V>
-__global__ void __launch_bounds__(UPD_THREADS) k_plan_merge(Mat<V> m, int64_t T, const int32_t *trow,
-                                                            const int32_t *tb0, const int32_t *bcol, const V *bval,
-                                                            int32_t *bpos, long long *tcap, long long *ttiles,
-                                                            int32_t *tmnew, int32_t *tinfo, int32_t *ncol, V *nval,
-                                                            int32_t *nins) {
-  constexpr int S = PLAN_S;
-  const int64_t nt = m.stat[ST_TOUCHED];
-  const int64_t gthreads = (int64_t)gridDim.x * blockDim.x;
-  const int64_t gtid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  for (int64_t t = gtid; t <= T; t += gthreads)
-    if (t >= nt) {
-      tcap[t] = 0;
-      ttiles[t] = 0;
-    }
-  const Sub<S> sub;
-  const unsigned lt = (1u << sub.sl) - 1u;
-  for (int64_t t = gtid / S; t < nt; t += gthreads / S) {
-    const int32_t r = trow[t];
-    const int32_t b0 = tb0[t], b1 = tb0[t + 1];
-    const int64_t L = m.row_sizes[r];
-    const Chain ch = load_chain(m, r);
-    int32_t mnew = 0;
-    int64_t ins0 = L;
-    for (int32_t base = b0; base < b1; base += S) {
-      const int32_t i = base + sub.sl;
-      const bool valid = i < b1;
-      const int32_t c = valid ? bcol[i] : 0;
-      const bool head = valid && (i == b0 || bcol[i - 1] != c);
-      int64_t pos = 0;
-      bool isnew = false;
-      if (head) {
-        int64_t lo = 0, hi = L;
-        while (lo < hi) {
-          const int64_t mid = (lo + hi) >> 1;
-          if (__ldg(m.cols + ch.phys(mid)) < c) lo = mid + 1;
-          else hi = mid;
-        }
-        pos = lo;
-        isnew = !(lo < L && __ldg(m.cols + ch.phys(lo)) == c);
-        bpos[i] = isnew ? ~(int32_t)pos : (int32_t)pos;
-      }
-      const unsigned nm = sub.ballot(isnew);
-      if (nm) {
-        if (isnew) {
-          const int32_t k = mnew + __popc(nm & lt);
-          V v = bval[i];
-          for (int32_t j = i + 1; j < b1 && bcol[j] == c; j++) v = v + bval[j];
-          ncol[b0 + k] = c;
-          nval[b0 + k] = v;
-          nins[b0 + k] = (int32_t)pos;
-        }
-        const int64_t p0 = sub.shfl(pos, __ffs(nm) - 1);
-        if (mnew == 0) ins0 = p0;
-        mnew += __popc(nm);
-      }
-    }
-    if (sub.sl == 0) {
-      const int64_t nl = L + mnew;
-      int64_t cap = 0;
-      int layer = -1, reloc = 0, big = 0;
-      if (mnew > 0 && L - ins0 > m.o.reloc_min) {
-        reloc = 1;
-        layer = 0;
-        cap = policy_cap(m.o, nl);
-      } else {
-        big = mnew > 0 && L - ins0 > SMALL_AFF;
-        if (nl > ch.total) {
-          cap = align_up(policy_cap(m.o, nl) - ch.total, m.o.align);
-          layer = ch.total == 0 ? 0 : ch.ns;
-          if (layer >= m.max_segs)
-            atomicOr((unsigned long long *)&m.stat[ST_AUX], (unsigned long long)AUX_LAYER_OVF);
-        }
-      }
-      tcap[t] = cap;
-      ttiles[t] = reloc ? div_up(nl, RT_TILE) : 0;
-      tmnew[t] = mnew;
-      tinfo[t] = (layer & 0xff) | (reloc << 8) | (big << 9);
-    }
-  }
-}
-
 // APPEND mode: the reference's segment walk and allocation size.
-template <typename V>
-__global__ void k_plan_append(Mat<V> m, int64_t T, const int32_t *trow, const int32_t *tb0, long long *tcap,
-                              long long *ttiles, int32_t *tmnew, int32_t *tinfo) {
-  const int64_t nt = m.stat[ST_TOUCHED];
+template <typename V, typename Src>
+__global__ void k_plan_append(Src src, int64_t T, const long long *gstat, const int32_t *trow, const int32_t *tb0,
+                              const int32_t *tmat, long long *tcap, long long *ttiles, int32_t *tmnew,
+                              int32_t *tinfo) {
+  const int64_t nt = gstat[ST_TOUCHED];
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
   for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t <= T; t += stride) {
     if (t >= nt) {
@@ -334,6 +311,8 @@ __global__ void k_plan_append(Mat<V> m, int64_t T, const int32_t *trow, const in
       ttiles[t] = 0;
       continue;
     }
+    const int i = tmat[t];
+    const Mat<V> &m = src.mat(i);
     const int32_t r = trow[t];
     const int64_t rlB = tb0[t + 1] - tb0[t];
     const int64_t rlA = m.row_sizes[r];
@@ -351,11 +330,11 @@ __global__ void k_plan_append(Mat<V> m, int64_t T, const int32_t *trow, const in
       int64_t before = 0, after = 0;
       bool found = false;
 #pragma unroll
-      for (int i = 0; i < MAX_SEGS; i++) {
-        if (!found && i < ch.ns) {
-          after = before + ch.cp[i];
-          off = i;
-          if (after >= rlA || i + 1 >= ch.ns) found = true;
+      for (int q = 0; q < MAX_SEGS; q++) {
+        if (!found && q < ch.ns) {
+          after = before + ch.cp[q];
+          off = q;
+          if (after >= rlA || q + 1 >= ch.ns) found = true;
           else before = after;
         }
       }
@@ -363,73 +342,100 @@ __global__ void k_plan_append(Mat<V> m, int64_t T, const int32_t *trow, const in
       if (fr < rlB) {
         cap = rlB - fr + m.o.alpha;
         layer = off + 1;
-        if (layer >= m.max_segs) atomicOr((unsigned long long *)&m.stat[ST_AUX], (unsigned long long)AUX_LAYER_OVF);
+        if (layer >= m.max_segs)
+          atomicOr((unsigned long long *)&src.st(i)[ST_AUX], (unsigned long long)AUX_LAYER_OVF);
       }
     }
     tcap[t] = cap;
     ttiles[t] = 0;
     tmnew[t] = (int32_t)rlB;
-    tinfo[t] = layer & 0xff;
+    tinfo[t] = (layer & 0xff) | (1 << 10);
   }
 }
 
-__global__ void k_check(long long *stat, const int32_t *row_sizes, int32_t n_rows, int64_t pool_cap) {
-  const long long aux = stat[ST_AUX];
-  const long long top = row_sizes[n_rows];
-  const long long need = top + stat[ST_TOTAL];
-  stat[ST_NEED] = need;
-  int st = DCSR_OK;
-  if (aux & AUX_BAD_INDEX) st = DCSR_BAD_INDEX;
-  else if (aux & AUX_LAYER_OVF) st = DCSR_LAYER_OVERFLOW;
-  else if (need > pool_cap || need > 0x7fffffffLL) st = DCSR_POOL_EXHAUSTED;
-  stat[ST_GO] = st == DCSR_OK ? 1 : 0;
-  if (st != DCSR_OK && stat[ST_STATUS] == 0) stat[ST_STATUS] = st;
-  stat[ST_AUX] = 0;
+// Per matrix: requirement from the scanned capacities, verdict and go flag.
+template <typename V, typename Src>
+__global__ void k_check(Src src, int count, const long long *addr) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+    long long *st = src.st(i);
+    const Mat<V> &m = src.mat(i);
+    const long long aux = st[ST_AUX];
+    const long long top = m.row_sizes[m.n_rows];
+    const long long need = top + (addr[st[ST_T1]] - addr[st[ST_T0]]);
+    st[ST_TOP] = top;
+    st[ST_NEED] = need;
+    int s = DCSR_OK;
+    if (aux & AUX_BAD_INDEX) s = DCSR_BAD_INDEX;
+    else if (aux & AUX_LAYER_OVF) s = DCSR_LAYER_OVERFLOW;
+    else if (need > m.pool_cap || need > 0x7fffffffLL) s = DCSR_POOL_EXHAUSTED;
+    st[ST_GO] = s == DCSR_OK ? 1 : 0;
+    if (s != DCSR_OK && st[ST_STATUS] == 0) st[ST_STATUS] = s;
+    st[ST_AUX] = 0;
+  }
 }
 
 // --------------------------------------------------------------- applying
 
-// Old pool top of the running update (row_sizes[n] is only rewritten by k_finish).
-__device__ __forceinline__ long long old_top(const long long *stat) { return stat[ST_NEED] - stat[ST_TOTAL]; }
+// Apply, step 1 (thread per batch group): existing columns take their batch
+// values in batch order, in place, before any shift or relocation reads them.
+template <typename V, typename Src>
+__global__ void k_apply_existing(Src src, const unsigned long long *keys, int64_t T, KeyFmt f, const V *bval,
+                                 const int32_t *bpos) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < T; g += stride) {
+    const unsigned long long k = keys[g];
+    if (g > 0 && keys[g - 1] == k) continue;
+    const int32_t p = bpos[g];
+    if (p < 0) continue;
+    const int i = f.item(k);
+    if (!src.st(i)[ST_GO]) continue;
+    const Mat<V> &m = src.mat(i);
+    const Chain ch = load_chain(m, f.row(k));
+    const int64_t q = ch.phys(p);
+    V v = m.vals[q];
+    for (int64_t j = g; j < T && keys[j] == k; j++) v = v + bval[j];
+    m.vals[q] = v;
+  }
+}
 
-// Apply for the rows of one width class: S = 8 takes rows shifting at most
-// SMALL_AFF entries (and rows without shifts), S = 32 takes the larger ones.
-template <typename V, int S>
-__global__ void __launch_bounds__(UPD_THREADS) k_apply_merge(Mat<V> m, const int32_t *trow, const int32_t *tb0,
-                                                             const int32_t *bcol, const V *bval,
-                                                             const int32_t *bpos, const long long *addr,
-                                                             const int32_t *tmnew, const int32_t *tinfo,
-                                                             const int32_t *ncol, const V *nval,
-                                                             const int32_t *nins) {
-  if (!m.stat[ST_GO]) return;
+// Apply, step 2, for the rows of one width class: S = 8 takes rows shifting
+// at most SMALL_AFF entries (and rows without shifts), S = 32 the larger ones.
+// Links a new segment when planned, shifts entries after the first insertion
+// point back to front (S per step; shift(i) = #{new k : nins[k] <= i}, from a
+// histogram of the insertion points in the window), then writes new columns.
+template <typename V, typename Src, int S>
+__global__ void __launch_bounds__(UPD_THREADS) k_apply_merge(Src src, const long long *gstat, const int32_t *trow,
+                                                             const int32_t *tb0, const int32_t *tmat,
+                                                             const long long *addr, const int32_t *tmnew,
+                                                             const int32_t *tinfo, const int32_t *ncol,
+                                                             const V *nval, const int32_t *nins) {
   __shared__ int hist[UPD_THREADS / S][S];
-  const int64_t nt = m.stat[ST_TOUCHED];
-  const long long top = old_top(m.stat);
+  const int64_t nt = gstat[ST_TOUCHED];
   const Sub<S> sub;
   int *h = hist[threadIdx.x / S];
   const int64_t gthreads = (int64_t)gridDim.x * blockDim.x;
   for (int64_t t = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / S; t < nt; t += gthreads / S) {
     const int info = tinfo[t];
     if (!((info >> 10) & 1) || ((info >> 9) & 1) != (S == 32 ? 1 : 0) || ((info >> 8) & 1)) continue;
+    const int i = tmat[t];
+    const long long *st = src.st(i);
+    if (!st[ST_GO]) continue;
+    const Mat<V> &m = src.mat(i);
     const int32_t r = trow[t];
-    const int32_t b0 = tb0[t], b1 = tb0[t + 1];
+    const int32_t b0 = tb0[t];
     const int64_t L = m.row_sizes[r];
-    const bool reloc = (info >> 8) & 1;
     const int layer = (int8_t)(info & 0xff);
     const int32_t mnew = tmnew[t];
     const long long cap = addr[t + 1] - addr[t];
     Chain ch = load_chain(m, r);
-    if (!reloc && cap > 0) {
-      const int32_t st = (int32_t)(top + addr[t]);
-      ch.append(st, (int32_t)cap, layer == 0);
+    if (cap > 0) {
+      const int32_t stp = (int32_t)(st[ST_TOP] + (addr[t] - addr[st[ST_T0]]));
+      ch.append(stp, (int32_t)cap, layer == 0);
       if (sub.sl == 0)
         *reinterpret_cast<int2 *>(m.seg + (int64_t)layer * m.pitch + 2 * (int64_t)r) =
-            make_int2(st, (int32_t)(st + cap));
+            make_int2(stp, (int32_t)(stp + cap));
     }
-    // (existing columns were updated by k_apply_existing)
-    if (!reloc && mnew > 0) {
-      // 2. shift the entries after the first insertion point, back to front,
-      //    S per step; shift(i) = #{new k : nins[k] <= i}
+    if (mnew > 0) {
       const int32_t *ins = nins + b0;
       const int64_t lo_a = ins[0];
       int32_t khi = mnew;
@@ -454,16 +460,16 @@ __global__ void __launch_bounds__(UPD_THREADS) k_apply_merge(Mat<V> m, const int
         for (int32_t k = klo + sub.sl; k < khi; k += S) atomicAdd(&h[ins[k] - c0], 1);
         sub.sync();
         const int inc = sub.incl_scan(h[sub.sl]);
-        const int64_t i = c0 + sub.sl;
-        const bool act = i < c1;
+        const int64_t e = c0 + sub.sl;
+        const bool act = e < c1;
         int32_t col = 0;
         V val = V(0);
         int64_t dst = 0;
         if (act) {
-          const int64_t src = ch.phys(i);
-          col = m.cols[src];
-          val = m.vals[src];
-          dst = ch.phys(i + klo + inc);
+          const int64_t srcq = ch.phys(e);
+          col = m.cols[srcq];
+          val = m.vals[srcq];
+          dst = ch.phys(e + klo + inc);
         }
         sub.sync();
         if (act) {
@@ -474,36 +480,38 @@ __global__ void __launch_bounds__(UPD_THREADS) k_apply_merge(Mat<V> m, const int
         c1 = c0;
         khi = klo;
       }
-      // 3. new columns at nins[k] + k
       for (int32_t k = sub.sl; k < mnew; k += S) {
         const int64_t q = ch.phys((int64_t)ins[k] + k);
         m.cols[q] = ncol[b0 + k];
         m.vals[q] = nval[b0 + k];
       }
     }
-    if (!reloc && sub.sl == 0) m.row_sizes[r] = (int32_t)(L + mnew);
+    if (sub.sl == 0) m.row_sizes[r] = (int32_t)(L + mnew);
     sub.sync();
   }
 }
 
 // Relocation: merge-path over (old row, new columns) into a fresh segment.
-template <typename V>
-__global__ void __launch_bounds__(RT_THREADS) k_relocate(Mat<V> m, const int32_t *trow, const int32_t *tb0,
+template <typename V, typename Src>
+__global__ void __launch_bounds__(RT_THREADS) k_relocate(Src src, const long long *gstat, const int32_t *trow,
+                                                         const int32_t *tb0, const int32_t *tmat,
                                                          const long long *addr, const long long *toff,
                                                          const int32_t *tmnew, const int32_t *ncol,
                                                          const V *nval) {
-  if (!m.stat[ST_GO]) return;
-  const int64_t nt = m.stat[ST_TOUCHED];
-  const int64_t ntiles = m.stat[ST_TILES];
-  const long long top = old_top(m.stat);
+  const int64_t nt = gstat[ST_TOUCHED];
+  const int64_t ntiles = gstat[ST_TILES];
   for (int64_t q = blockIdx.x; q < ntiles; q += gridDim.x) {
     int64_t lo = 0, hi = nt;
     while (lo < hi) {
-      int64_t mid = (lo + hi) >> 1;
+      const int64_t mid = (lo + hi) >> 1;
       if (toff[mid] <= q) lo = mid + 1;
       else hi = mid;
     }
     const int64_t t = lo - 1;
+    const int i = tmat[t];
+    const long long *st = src.st(i);
+    if (!st[ST_GO]) continue;
+    const Mat<V> &m = src.mat(i);
     const int64_t j = q - toff[t];
     const int32_t r = trow[t];
     const int32_t b0 = tb0[t];
@@ -511,7 +519,7 @@ __global__ void __launch_bounds__(RT_THREADS) k_relocate(Mat<V> m, const int32_t
     const int64_t L = m.row_sizes[r];
     const Chain ch = load_chain(m, r);
     const int64_t nl = L + mn;
-    const int64_t start = top + addr[t];
+    const int64_t start = st[ST_TOP] + (addr[t] - addr[st[ST_T0]]);
     const int64_t o1 = (j + 1) * RT_TILE < nl ? (j + 1) * RT_TILE : nl;
     const int64_t o = j * RT_TILE + (int64_t)threadIdx.x * RT_ITEMS;
     if (o >= o1) continue;
@@ -519,7 +527,7 @@ __global__ void __launch_bounds__(RT_THREADS) k_relocate(Mat<V> m, const int32_t
     const V *BV = nval + b0;
     int64_t a = o - mn > 0 ? o - mn : 0, b = o < L ? o : L;
     while (a < b) {
-      int64_t mid = (a + b) >> 1;
+      const int64_t mid = (a + b) >> 1;
       if (m.cols[ch.phys(mid)] < B[o - mid - 1]) a = mid + 1;
       else b = mid;
     }
@@ -546,38 +554,49 @@ __global__ void __launch_bounds__(RT_THREADS) k_relocate(Mat<V> m, const int32_t
   }
 }
 
-template <typename V>
-__global__ void k_finish(Mat<V> m, const int32_t *trow, const long long *addr, const int32_t *tmnew,
-                         const int32_t *tinfo) {
-  if (!m.stat[ST_GO]) return;
-  const int64_t nt = m.stat[ST_TOUCHED];
-  const long long top = old_top(m.stat);
+template <typename V, typename Src>
+__global__ void k_finish(Src src, int count, const long long *gstat, const int32_t *trow, const int32_t *tmat,
+                         const long long *addr, const int32_t *tmnew, const int32_t *tinfo) {
+  const int64_t nt = gstat[ST_TOUCHED];
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
   const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   for (int64_t t = tid; t < nt; t += stride) {
     if (!((tinfo[t] >> 8) & 1)) continue;
+    const int i = tmat[t];
+    const long long *st = src.st(i);
+    if (!st[ST_GO]) continue;
+    const Mat<V> &m = src.mat(i);
     const int32_t r = trow[t];
-    const int32_t st = (int32_t)(top + addr[t]);
+    const int32_t stp = (int32_t)(st[ST_TOP] + (addr[t] - addr[st[ST_T0]]));
     const int32_t cap = (int32_t)(addr[t + 1] - addr[t]);
     for (int l = 1; l < m.max_segs; l++)
       *reinterpret_cast<int2 *>(m.seg + (int64_t)l * m.pitch + 2 * (int64_t)r) = make_int2(-1, -1);
-    *reinterpret_cast<int2 *>(m.seg + 2 * (int64_t)r) = make_int2(st, st + cap);
+    *reinterpret_cast<int2 *>(m.seg + 2 * (int64_t)r) = make_int2(stp, stp + cap);
     m.row_sizes[r] = m.row_sizes[r] + tmnew[t];
   }
-  if (tid == 0) m.row_sizes[m.n_rows] = (int32_t)m.stat[ST_NEED];
+  for (int64_t i = tid; i < count; i += stride) {
+    const long long *st = src.st((int)i);
+    if (st[ST_GO]) {
+      const Mat<V> &m = src.mat((int)i);
+      m.row_sizes[m.n_rows] = (int32_t)st[ST_NEED];
+    }
+  }
 }
 
-template <typename V>
-__global__ void __launch_bounds__(UPD_THREADS) k_apply_append(Mat<V> m, const int32_t *trow, const int32_t *tb0,
+template <typename V, typename Src>
+__global__ void __launch_bounds__(UPD_THREADS) k_apply_append(Src src, const long long *gstat, const int32_t *trow,
+                                                              const int32_t *tb0, const int32_t *tmat,
                                                               const int32_t *bcol, const V *bval,
                                                               const long long *addr, const int32_t *tinfo) {
-  if (!m.stat[ST_GO]) return;
-  const int64_t nt = m.stat[ST_TOUCHED];
-  const long long top = old_top(m.stat);
+  const int64_t nt = gstat[ST_TOUCHED];
   const int lane = lane_id();
   const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
   for (int64_t t = gw; t < nt; t += nwarps) {
+    const int i = tmat[t];
+    const long long *st = src.st(i);
+    if (!st[ST_GO]) continue;
+    const Mat<V> &m = src.mat(i);
     const int32_t r = trow[t];
     const int32_t b0 = tb0[t], b1 = tb0[t + 1];
     const int64_t L = m.row_sizes[r];
@@ -585,11 +604,11 @@ __global__ void __launch_bounds__(UPD_THREADS) k_apply_append(Mat<V> m, const in
     const long long cap = addr[t + 1] - addr[t];
     Chain ch = load_chain(m, r);
     if (cap > 0) {
-      const int32_t st = (int32_t)(top + addr[t]);
-      ch.append(st, (int32_t)cap, layer == 0);
+      const int32_t stp = (int32_t)(st[ST_TOP] + (addr[t] - addr[st[ST_T0]]));
+      ch.append(stp, (int32_t)cap, layer == 0);
       if (lane == 0)
         *reinterpret_cast<int2 *>(m.seg + (int64_t)layer * m.pitch + 2 * (int64_t)r) =
-            make_int2(st, (int32_t)(st + cap));
+            make_int2(stp, (int32_t)(stp + cap));
     }
     for (int32_t j = lane; j < b1 - b0; j += 32) {
       const int64_t q = ch.phys(L + j);
@@ -609,70 +628,81 @@ static int grid_for(int64_t n, int block) {
   return (int)(g < 1 ? 1 : (g > cap ? cap : g));
 }
 
-template <typename V>
-static int update_impl(dcsr_handle h, const int32_t *rows, const int32_t *cols, const V *vals, int64_t T,
-                       cudaStream_t s) {
-  const bool merge = h->o.mode == DCSR_MERGE;
-  const int cb = bits_for(h->n_cols), rb = bits_for(h->n_rows);
-  const int bits = merge ? rb + cb : rb;
-  Arena &ar = h->scratch;
-  size_t need = 2 * arena_bytes(T, 8) + 2 * arena_bytes(T, 4) + 5 * arena_bytes(T + 2, 4) +
-                2 * arena_bytes(T, sizeof(V)) + 4 * arena_bytes(T + 2, 8) + radix_scratch_bytes(T) +
-                scan_scratch_bytes(T + 2);
-  DCSR_TRY(ar.reserve(need, s));
+size_t update_scratch_bytes(int64_t T, size_t vsize) {
+  return 2 * arena_bytes(T, 8) + 2 * arena_bytes(T, 4) + 6 * arena_bytes(T + 2, 4) + 2 * arena_bytes(T, vsize) +
+         4 * arena_bytes(T + 2, 8) + radix_scratch_bytes(T) + scan_scratch_bytes(T + 2);
+}
+
+// The update of `count` matrices (one Src) with T triples in total.
+// gstat: batch-global status words (ST_TOUCHED, ST_TILES, ST_TOTAL).
+template <typename V, typename Src>
+static int update_pipeline(const Src &src, int count, int64_t T, bool merge, int rb, int cb, long long *gstat,
+                           Arena &ar, cudaStream_t s) {
+  const int ib = count > 1 ? bits_for(count) : 0;
+  const KeyFmt f{cb, rb, merge ? 1 : 0};
+  const int bits = ib + rb + (merge ? cb : 0);
+  if (bits > 63) return DCSR_NOT_SUPPORTED;
+  DCSR_TRY(ar.reserve(update_scratch_bytes(T, sizeof(V)), s));
   unsigned long long *k0 = ar.take<unsigned long long>(T), *k1 = ar.take<unsigned long long>(T);
   unsigned *p0 = ar.take<unsigned>(T), *p1 = ar.take<unsigned>(T);
   int32_t *bcol = ar.take<int32_t>(T + 2), *bpos = ar.take<int32_t>(T + 2), *trow = ar.take<int32_t>(T + 2);
-  int32_t *tb0 = ar.take<int32_t>(T + 2), *tmnew = ar.take<int32_t>(T + 2);
+  int32_t *tb0 = ar.take<int32_t>(T + 2), *tmnew = ar.take<int32_t>(T + 2), *tmat = ar.take<int32_t>(T + 2);
   V *bval = ar.take<V>(T), *nval = ar.take<V>(T);
   long long *hflag = ar.take<long long>(T + 2), *tcap = ar.take<long long>(T + 2);
-  long long *ttiles = ar.take<long long>(T + 2);
-  long long *nflag = ar.take<long long>(T + 2);
-  // tinfo / ncol / nins reuse the sort buffers once the sort is done
-  Mat<V> m = h->view<V>();
+  long long *ttiles = ar.take<long long>(T + 2), *nflag = ar.take<long long>(T + 2);
+  const int gT = grid_for(T + 1, 256);
+  const int gI = grid_for(count, 256);
 
-  DCSR_CUDA(cudaMemsetAsync(h->stat + ST_AUX, 0, sizeof(long long), s));
-  DCSR_LAUNCH(k_make_keys, grid_for(T, 256), 256, 0, s, rows, cols, T, h->n_rows, h->n_cols, cb, merge ? 1 : 0, k0,
-              p0, h->stat);
+  DCSR_LAUNCH((k_item_init<V, Src>), gI, 256, 0, s, src, count);
+  DCSR_LAUNCH((k_make_keys<V, Src>), gT, 256, 0, s, src, T, f, k0, p0);
   DCSR_TRY(radix_sort_pairs(&k0, &p0, &k1, &p1, T, bits, ar, s));
-  DCSR_LAUNCH(k_gather_sorted<V>, grid_for(T, 256), 256, 0, s, k0, p0, cols, vals, T, cb, merge ? 1 : 0, h->n_cols,
-              bcol, bval, hflag);
-  DCSR_TRY(scan_i64(hflag, hflag, T, h->stat + ST_TOUCHED, ar, s));
-  DCSR_LAUNCH(k_touched, grid_for(T, 256), 256, 0, s, k0, T, cb, merge ? 1 : 0, hflag, trow, tb0);
+  DCSR_LAUNCH((k_gather_sorted<V, Src>), gT, 256, 0, s, src, k0, p0, T, f, bcol, bval, hflag);
+  DCSR_TRY(scan_i64(hflag, hflag, T, gstat + ST_TOUCHED, ar, s));
+  DCSR_LAUNCH((k_touched<V, Src>), gT, 256, 0, s, src, k0, T, f, hflag, gstat, trow, tb0, tmat);
   // k1 / p1 are free after the sort: carve tinfo, ncol, nins from them
   int32_t *tinfo = (int32_t *)p1;
   int32_t *ncol = (int32_t *)k1;
   int32_t *nins = ncol + T;
-  static int g_plan = 0, g_apply = 0, g_apply8 = 0, g_reloc = 0;
-  if (!g_plan) {
-    g_plan = persistent_grid((const void *)k_plan_merge<double>, UPD_THREADS, 0);
-    g_apply = persistent_grid((const void *)k_apply_merge<double, 32>, UPD_THREADS, 0);
-    g_apply8 = persistent_grid((const void *)k_apply_merge<double, 8>, UPD_THREADS, 0);
-    g_reloc = persistent_grid((const void *)k_relocate<double>, RT_THREADS, 0);
+  static int g_apply = 0, g_apply8 = 0, g_reloc = 0;
+  if (!g_apply) {
+    g_apply = persistent_grid((const void *)k_apply_merge<double, UpdOne<double>, 32>, UPD_THREADS, 0);
+    g_apply8 = persistent_grid((const void *)k_apply_merge<double, UpdOne<double>, 8>, UPD_THREADS, 0);
+    g_reloc = persistent_grid((const void *)k_relocate<double, UpdOne<double>>, RT_THREADS, 0);
   }
   if (merge) {
-    const int gT = grid_for(T + 1, 256);
-    DCSR_LAUNCH(k_head_search<V>, gT, 256, 0, s, m, k0, T, cb, bcol, bpos, nflag);
+    DCSR_LAUNCH((k_head_search<V, Src>), gT, 256, 0, s, src, k0, T, f, bcol, bpos, nflag);
     DCSR_TRY(scan_i64(nflag, nflag, T + 1, nullptr, ar, s));
-    DCSR_LAUNCH(k_new_compact<V>, gT, 256, 0, s, k0, T, cb, bcol, bval, bpos, nflag, hflag, tb0, ncol, nval, nins);
-    DCSR_LAUNCH(k_row_plan<V>, gT, 256, 0, s, m, T, trow, tb0, nflag, nins, tcap, ttiles, tmnew, tinfo);
+    DCSR_LAUNCH(k_new_compact<V>, gT, 256, 0, s, k0, T, f, bcol, bval, bpos, nflag, hflag, tb0, ncol, nval, nins);
+    DCSR_LAUNCH((k_row_plan<V, Src>), gT, 256, 0, s, src, T, gstat, trow, tb0, tmat, nflag, nins, tcap, ttiles,
+                tmnew, tinfo);
   } else {
-    DCSR_LAUNCH(k_plan_append<V>, grid_for(T + 1, 256), 256, 0, s, m, T, trow, tb0, tcap, ttiles, tmnew, tinfo);
+    DCSR_LAUNCH((k_plan_append<V, Src>), gT, 256, 0, s, src, T, gstat, trow, tb0, tmat, tcap, ttiles, tmnew, tinfo);
   }
-  DCSR_TRY(scan_i64(tcap, tcap, T + 1, h->stat + ST_TOTAL, ar, s));
-  if (merge) DCSR_TRY(scan_i64(ttiles, ttiles, T + 1, h->stat + ST_TILES, ar, s));
-  DCSR_LAUNCH(k_check, 1, 1, 0, s, h->stat, h->row_sizes, h->n_rows, h->pool_cap);
+  DCSR_TRY(scan_i64(tcap, tcap, T + 1, gstat + ST_TOTAL, ar, s));
+  if (merge) DCSR_TRY(scan_i64(ttiles, ttiles, T + 1, gstat + ST_TILES, ar, s));
+  DCSR_LAUNCH((k_check<V, Src>), gI, 256, 0, s, src, count, tcap);
   if (merge) {
-    DCSR_LAUNCH(k_apply_existing<V>, grid_for(T, 256), 256, 0, s, m, k0, T, cb, bval, bpos);
-    DCSR_LAUNCH((k_apply_merge<V, 8>), g_apply8, UPD_THREADS, 0, s, m, trow, tb0, bcol, bval, bpos, tcap, tmnew,
+    DCSR_LAUNCH((k_apply_existing<V, Src>), gT, 256, 0, s, src, k0, T, f, bval, bpos);
+    DCSR_LAUNCH((k_apply_merge<V, Src, 8>), g_apply8, UPD_THREADS, 0, s, src, gstat, trow, tb0, tmat, tcap, tmnew,
                 tinfo, ncol, nval, nins);
-    DCSR_LAUNCH((k_apply_merge<V, 32>), g_apply, UPD_THREADS, 0, s, m, trow, tb0, bcol, bval, bpos, tcap, tmnew,
+    DCSR_LAUNCH((k_apply_merge<V, Src, 32>), g_apply, UPD_THREADS, 0, s, src, gstat, trow, tb0, tmat, tcap, tmnew,
                 tinfo, ncol, nval, nins);
-    DCSR_LAUNCH(k_relocate<V>, g_reloc, RT_THREADS, 0, s, m, trow, tb0, tcap, ttiles, tmnew, ncol, nval);
+    DCSR_LAUNCH((k_relocate<V, Src>), g_reloc, RT_THREADS, 0, s, src, gstat, trow, tb0, tmat, tcap, ttiles, tmnew,
+                ncol, nval);
   } else {
-    DCSR_LAUNCH(k_apply_append<V>, g_apply, UPD_THREADS, 0, s, m, trow, tb0, bcol, bval, tcap, tinfo);
+    DCSR_LAUNCH((k_apply_append<V, Src>), g_apply, UPD_THREADS, 0, s, src, gstat, trow, tb0, tmat, bcol, bval, tcap,
+                tinfo);
   }
-  DCSR_LAUNCH(k_finish<V>, grid_for(T, 256), 256, 0, s, m, trow, tcap, tmnew, tinfo);
+  DCSR_LAUNCH((k_finish<V, Src>), gT, 256, 0, s, src, count, gstat, trow, tmat, tcap, tmnew, tinfo);
+  return DCSR_OK;
+}
+
+template <typename V>
+static int update_one(dcsr_handle h, const int32_t *rows, const int32_t *cols, const V *vals, int64_t T,
+                      cudaStream_t s) {
+  UpdOne<V> src{h->view<V>(), rows, cols, vals};
+  DCSR_TRY(update_pipeline<V>(src, 1, T, h->o.mode == DCSR_MERGE, bits_for(h->n_rows), bits_for(h->n_cols), h->stat,
+                              h->scratch, s));
   h->bins_valid = false;
   return DCSR_OK;
 }
@@ -681,16 +711,43 @@ int update_async(dcsr_handle h, const int32_t *rows, const int32_t *cols, const 
                  cudaStream_t s) {
   if (nnz == 0) return DCSR_OK;
   if (nnz > 0x7ffffff0LL) return DCSR_BAD_ARG;
-  if (!h->vals) DCSR_TRY(reserve(h, 0, s));
-  if (h->dtype == DCSR_F32) return update_impl<float>(h, rows, cols, (const float *)vals, nnz, s);
-  return update_impl<double>(h, rows, cols, (const double *)vals, nnz, s);
+  if (h->dtype == DCSR_F32) return update_one<float>(h, rows, cols, (const float *)vals, nnz, s);
+  return update_one<double>(h, rows, cols, (const double *)vals, nnz, s);
+}
+
+template <typename V>
+static int update_many_t(const BatchItem<V> *items_dev, int count, int64_t T, bool merge, int rb, int cb,
+                         long long *gstat, Arena &ar, cudaStream_t s) {
+  UpdMany<V> src{items_dev, count};
+  return update_pipeline<V>(src, count, T, merge, rb, cb, gstat, ar, s);
+}
+
+int update_many(const void *items_dev, int dtype, int count, int64_t T, bool merge, int rb, int cb, long long *gstat,
+                Arena &ar, cudaStream_t s) {
+  if (T == 0 || count == 0) return DCSR_OK;
+  if (dtype == DCSR_F32)
+    return update_many_t<float>((const BatchItem<float> *)items_dev, count, T, merge, rb, cb, gstat, ar, s);
+  return update_many_t<double>((const BatchItem<double> *)items_dev, count, T, merge, rb, cb, gstat, ar, s);
 }
 
 // ------------------------------------------------------------- COO -> CSR
 
-template <typename V>
-__global__ void k_group(const unsigned long long *keys, const unsigned *perm, const int32_t *cols, const V *vals,
-                        int64_t n, int cb, int merge, int32_t n_cols, long long *flag) {
+__global__ void k_coo_keys(const int32_t *rows, const int32_t *cols, int64_t n, int32_t n_rows, int32_t n_cols,
+                           int cb, int merge, unsigned long long *keys, unsigned *perm, long long *stat) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    int32_t r = rows[i], c = cols[i];
+    if (r < 0 || r >= n_rows || c < 0 || c >= n_cols) {
+      atomicOr((unsigned long long *)&stat[ST_AUX], (unsigned long long)AUX_BAD_INDEX);
+      r = 0;
+      c = 0;
+    }
+    keys[i] = merge ? (((unsigned long long)r << cb) | (unsigned long long)c) : (unsigned long long)r;
+    perm[i] = (unsigned)i;
+  }
+}
+
+__global__ void k_group(const unsigned long long *keys, int64_t n, int merge, long long *flag) {
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
     flag[i] = (!merge || i == 0 || keys[i] != keys[i - 1]) ? 1 : 0;
@@ -712,7 +769,8 @@ __global__ void k_group_emit(const unsigned long long *keys, const unsigned *per
     if (c < 0 || c >= n_cols) c = 0;
     ocols[pos[i]] = c;
     ovals[pos[i]] = v;
-    atomicAdd((unsigned long long *)&rowcnt[key_row(k, cb, merge)], 1ull);
+    const int32_t r = merge ? (int32_t)(k >> cb) : (int32_t)k;
+    atomicAdd((unsigned long long *)&rowcnt[r], 1ull);
   }
 }
 
@@ -734,10 +792,10 @@ static int coo_impl(dcsr_handle h, const int32_t *rows, const int32_t *cols, con
   long long *cnt = ar.take<long long>(h->n_rows + 2);
   DCSR_CUDA(cudaMemsetAsync(cnt, 0, sizeof(long long) * (h->n_rows + 2), s));
   if (T > 0) {
-    DCSR_LAUNCH(k_make_keys, grid_for(T, 256), 256, 0, s, rows, cols, T, h->n_rows, h->n_cols, cb, merge ? 1 : 0,
-                k0, p0, h->stat);
+    DCSR_LAUNCH(k_coo_keys, grid_for(T, 256), 256, 0, s, rows, cols, T, h->n_rows, h->n_cols, cb, merge ? 1 : 0, k0,
+                p0, h->stat);
     DCSR_TRY(radix_sort_pairs(&k0, &p0, &k1, &p1, T, merge ? rb + cb : rb, ar, s));
-    DCSR_LAUNCH(k_group<V>, grid_for(T, 256), 256, 0, s, k0, p0, cols, vals, T, cb, merge ? 1 : 0, h->n_cols, flag);
+    DCSR_LAUNCH(k_group, grid_for(T, 256), 256, 0, s, k0, T, merge ? 1 : 0, flag);
     DCSR_TRY(scan_i64(flag, flag, T, nullptr, ar, s));
     DCSR_LAUNCH(k_group_emit<V>, grid_for(T, 256), 256, 0, s, k0, p0, cols, vals, T, cb, merge ? 1 : 0, h->n_cols,
                 flag, oc, ov, cnt);

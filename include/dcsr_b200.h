@@ -176,6 +176,47 @@ int dcsr_count_sorted_indices(const int32_t *I, int64_t n, int32_t *X, void *str
 int dcsr_reduce_by_key(const int32_t *keys, const void *vals, int64_t n, int32_t dtype, int32_t *keys_out,
                        void *vals_out, int64_t *n_out, void *stream);
 
+/* ------------------------------------------------------- batched form */
+
+/* One matrix's work in a batch: an update batch (nnz may be 0) followed by
+ * Y = alpha*A*X + beta*Y (x == NULL: no SpMV).  Pointers are device pointers
+ * that stay valid for the batch's lifetime (a captured graph replays them). */
+typedef struct {
+  dcsr_handle matrix;
+  const int32_t *rows;
+  const int32_t *cols;
+  const void *vals;
+  int64_t nnz;
+  const void *x;
+  void *y;
+  int32_t k;
+  int64_t ldx, ldy;
+  double alpha, beta;
+} dcsr_batch_item;
+
+typedef struct dcsr_batch_s *dcsr_batch;
+
+/* A batch over `count` matrices of one dtype and mode (each matrix at most
+ * once).  The reference has no batched form; it would run count separate
+ * UpdateMatrix + spmv sequences (include/load.h:258, include/spmv.h:121). */
+int dcsr_batch_create(dcsr_batch *out, const dcsr_batch_item *items, int32_t count, void *stream);
+/* Enqueue the batch: one merged update over all matrices (one sort, one
+ * plan, one apply for the union of their triples) then one SpMV pass per
+ * distinct k.  Asynchronous; per-matrix rejections are read with
+ * dcsr_batch_status.  Results equal the per-call operators bit for bit. */
+int dcsr_batch_run(dcsr_batch b, void *stream);
+/* Capture dcsr_batch_run into a CUDA graph (instantiated once). */
+int dcsr_batch_capture(dcsr_batch b, void *stream);
+/* Launch the captured graph (one launch for the whole batch). */
+int dcsr_batch_launch(dcsr_batch b, void *stream);
+/* Per-matrix statuses of the last run (synchronises, clears them). */
+int dcsr_batch_status(dcsr_batch b, int32_t *statuses, void *stream);
+/* For matrices whose update was rejected: apply the repair policy
+ * (compact, grow) and redo their update and SpMV per call.  Returns the
+ * number of matrices repaired in *repaired (may be NULL). */
+int dcsr_batch_repair(dcsr_batch b, const int32_t *statuses, int32_t *repaired, void *stream);
+int dcsr_batch_destroy(dcsr_batch b);
+
 /* Allocation-free reduce-by-key.  No counterpart in the reference: it is
  * for callers that cannot allocate device memory at call time -- a process
  * that has carved the GPU's memory into fixed budgets up front, or code whose

@@ -86,8 +86,9 @@ def test_rows_in_every_bin(dcsr):
     """Rows whose lengths hit every bin boundary 0,1,2,3,4,7,8,15,16,31,32,
     511,512,2000 plus chained rows after updates."""
     rng = np.random.default_rng(3)
-    lens = [0, 1, 2, 3, 4, 7, 8, 15, 16, 31, 32, 511, 512, 513, 2000, 0, 5, 4096, 4097, 9000] + [3] * 40
-    n, m = len(lens), 20000
+    lens = [0, 1, 2, 3, 4, 7, 8, 15, 16, 31, 32, 511, 512, 513, 2000, 0, 5, 4096, 4097, 9000, 65536, 65537,
+            140000] + [3] * 40
+    n, m = len(lens), 200000
     rp = np.concatenate([[0], np.cumsum(lens)]).astype(np.int32)
     cols = np.concatenate([np.sort(rng.choice(m, L, replace=False)) for L in lens]).astype(np.int32)
     vals = rng.uniform(-1, 1, cols.size).astype(np.float32)
