@@ -49,6 +49,29 @@ class BatchItem(C.Structure):
                 ("ldy", C.c_int64), ("alpha", C.c_double), ("beta", C.c_double)]
 
 
+class ServerOpts(C.Structure):
+    """dcsr_server_opts of the C ABI."""
+    _fields_ = [("max_batch", C.c_int32), ("depth", C.c_int32), ("mem_budget", C.c_int64),
+                ("mem_reserve", C.c_int64), ("plain", C.c_int32)]
+
+
+class Request(C.Structure):
+    """dcsr_request of the C ABI."""
+    _fields_ = [("kind", C.c_int32), ("matrix", C.c_int32), ("rows", C.c_void_p), ("cols", C.c_void_p),
+                ("vals", C.c_void_p), ("nnz", C.c_int64), ("x", C.c_void_p), ("y", C.c_void_p), ("k", C.c_int32),
+                ("alpha", C.c_double), ("beta", C.c_double), ("row_ptr", C.c_void_p), ("out_cols", C.c_void_p),
+                ("out_vals", C.c_void_p), ("cap", C.c_int64)]
+
+
+class Result(C.Structure):
+    """dcsr_result of the C ABI."""
+    _fields_ = [("status", C.c_int32), ("batch_size", C.c_int32), ("nnz", C.c_int64), ("queue_us", C.c_double),
+                ("latency_us", C.c_double)]
+
+
+REQ_UPDATE, REQ_SPMV, REQ_EXPORT = range(3)
+
+
 class Info(C.Structure):
     _fields_ = [("n_rows", C.c_int32), ("n_cols", C.c_int32), ("dtype", C.c_int32), ("pitch", C.c_int32),
                 ("pool_cap", C.c_int64), ("row_sizes", C.c_void_p), ("seg", C.c_void_p), ("cols", C.c_void_p),
@@ -88,6 +111,12 @@ _SIGS = {
     "dcsr_batch_status": (_i32, [_vp, _vp, _vp]),
     "dcsr_batch_repair": (_i32, [_vp, _vp, C.POINTER(_i32), _vp]),
     "dcsr_batch_destroy": (_i32, [_vp]),
+    "dcsr_server_default_opts": (None, [_vp]),
+    "dcsr_server_create": (_i32, [C.POINTER(_vp), _vp, _i32, _vp]),
+    "dcsr_server_submit": (_i32, [_vp, _vp, C.POINTER(C.c_uint64)]),
+    "dcsr_server_wait": (_i32, [_vp, C.c_uint64, _i64, _vp]),
+    "dcsr_server_stats": (_i32, [_vp, C.POINTER(_i64), C.POINTER(_i64), C.POINTER(_i64)]),
+    "dcsr_server_destroy": (_i32, [_vp]),
     "dcsr_status_string": (C.c_char_p, [_i32]),
     "dcsr_launch_count": (C.c_uint64, []),
     "dcsr_version": (C.c_char_p, []),
@@ -387,6 +416,79 @@ class DcsrBatch:
         if self.h:
             lib().dcsr_batch_destroy(self.h)
             self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _host(t):
+    """Pointer of a contiguous CPU tensor (pinned memory keeps the server's copies asynchronous)."""
+    if t.is_cuda or not t.is_contiguous():
+        raise ValueError("contiguous host tensor expected")
+    return t.data_ptr()
+
+
+class DcsrServer:
+    """Request server over resident matrices (dcsr_server_* of the C ABI).
+
+    Requests carry host tensors (allocate them with ``pin_memory()``); they are
+    referenced until their result is taken with ``wait``.
+    """
+
+    def __init__(self, matrices, max_batch=256, depth=2, mem_budget=0, mem_reserve=1 << 30, plain=False):
+        o = ServerOpts()
+        lib().dcsr_server_default_opts(C.byref(o))
+        o.max_batch, o.depth, o.mem_budget, o.mem_reserve, o.plain = max_batch, depth, mem_budget, mem_reserve, int(plain)
+        self.matrices = list(matrices)
+        arr = (C.c_void_p * len(self.matrices))(*[m.h.value for m in self.matrices])
+        self.h = C.c_void_p()
+        _check(lib().dcsr_server_create(C.byref(self.h), arr, len(self.matrices), C.byref(o)), "dcsr_server_create")
+        self._keep = {}
+
+    def _submit(self, req, keep):
+        t = C.c_uint64()
+        _check(lib().dcsr_server_submit(self.h, C.byref(req), C.byref(t)), "dcsr_server_submit")
+        self._keep[t.value] = keep
+        return t.value
+
+    def submit_update(self, i, rows, cols, vals):
+        r = Request(kind=REQ_UPDATE, matrix=i, nnz=rows.numel())
+        if rows.numel():
+            r.rows, r.cols, r.vals = _host(rows), _host(cols), _host(vals)
+        return self._submit(r, (rows, cols, vals))
+
+    def submit_spmv(self, i, x, y, alpha=1.0, beta=0.0):
+        """y (host, [n_rows] or [n_rows, k]) = alpha*A@x + beta*y."""
+        k = 1 if x.dim() == 1 else x.shape[1]
+        r = Request(kind=REQ_SPMV, matrix=i, x=_host(x), y=_host(y), k=k, alpha=alpha, beta=beta)
+        return self._submit(r, (x, y))
+
+    def submit_export(self, i, row_ptr, cols, vals):
+        r = Request(kind=REQ_EXPORT, matrix=i, row_ptr=_host(row_ptr), cap=cols.numel())
+        if cols.numel():
+            r.out_cols, r.out_vals = _host(cols), _host(vals)
+        return self._submit(r, (row_ptr, cols, vals))
+
+    def wait(self, ticket, timeout_us=-1) -> dict:
+        res = Result()
+        _check(lib().dcsr_server_wait(self.h, ticket, timeout_us, C.byref(res)), "dcsr_server_wait")
+        self._keep.pop(ticket, None)
+        return {"status": res.status, "batch_size": res.batch_size, "nnz": res.nnz, "queue_us": res.queue_us,
+                "latency_us": res.latency_us}
+
+    def stats(self):
+        c, b, m = _i64(), _i64(), _i64()
+        _check(lib().dcsr_server_stats(self.h, C.byref(c), C.byref(b), C.byref(m)), "dcsr_server_stats")
+        return {"completed": c.value, "batches": b.value, "mem_in_use": m.value}
+
+    def close(self):
+        if self.h:
+            lib().dcsr_server_destroy(self.h)
+            self.h = C.c_void_p()
+            self._keep.clear()
 
     def __del__(self):
         try:

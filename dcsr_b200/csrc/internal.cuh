@@ -1,5 +1,7 @@
 // internal.cuh -- cross-file internal API of the DCSR library.
 #pragma once
+#include <vector>
+
 #include "common.cuh"
 
 namespace dcsr {
@@ -75,5 +77,54 @@ int ensure_part(dcsr_handle h, int K, cudaStream_t s);
 int copy_rows(dcsr_handle h, const long long *dst_off, int32_t *out_cols, void *out_vals, int32_t *out_rows,
               int32_t *out_rowptr, cudaStream_t s);
 int reserve(dcsr_handle h, int64_t cap, cudaStream_t s);
+
+// The device side of a batch (batch.cu): a plan over a set of
+// dcsr_batch_items, their descriptor image, and the enqueue of the merged
+// update + schedule rebuild + grouped SpMV.  Buffers grow, never shrink, so
+// one core can serve many batches (the server re-plans one per slot).
+struct BatchCore {
+  struct Group {
+    int k = 1;
+    bool vec = false;
+    std::vector<int> idx;  // items of this group, in item order
+    size_t off = 0;        // descriptor offset in the image
+    size_t pref_off = 0;   // unit-prefix offset in pref
+  };
+  int count = 0, dtype = 0, mode = 0;
+  std::vector<dcsr_batch_item> items;
+  int64_t T = 0, R = 0;
+  int rb = 1, cb = 1;
+  std::vector<Group> groups;
+  // image: BatchItem[count] | RowItem[count] (row space) | group RowItems
+  size_t off_row = 0, img_bytes = 0, img_cap = 0;
+  unsigned char *img_dev = nullptr;
+  unsigned char *img_host = nullptr;  // pinned copy of the last upload
+  std::vector<unsigned char> img_new;
+  int cnt_cap = 0;
+  int32_t *skip = nullptr;        // [count] 1: the matrix's update was rejected this run
+  long long *status_dev = nullptr;  // [2*count] (status, pool top needed) per matrix
+  size_t pref_cap = 0;
+  long long *pref = nullptr;
+  long long *gstat = nullptr;
+  Arena ar;
+
+  // Validate and plan `items` (one dtype and mode, each matrix once); grows
+  // buffers with stream-ordered allocation on s.
+  int plan(const dcsr_batch_item *items, int count, cudaStream_t s);
+  // Rebuild the descriptor image from the handles (sizing their schedule
+  // buffers first) and upload it if it changed.  sync=true waits for the
+  // upload; otherwise the caller guarantees the previous upload of this core
+  // has completed before the next call (the pinned image is reused).
+  int upload(cudaStream_t s, bool sync, bool force = false);
+  // Reserve the arena for this plan (before a capture: runs must not allocate).
+  int reserve_scratch(cudaStream_t s);
+  // Merged update, skip flags, schedule rebuild, grouped SpMV (capturable).
+  int enqueue(cudaStream_t s);
+  // (status, needed pool top) of every matrix into host memory (async);
+  // clears the device statuses.
+  int status_async(long long *host, cudaStream_t s);
+  void mark_scheduled();
+  void release();
+};
 
 }  // namespace dcsr

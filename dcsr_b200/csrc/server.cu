@@ -1,0 +1,565 @@
+// server.cu -- the serving form: a request loop over resident matrices with
+// admission by device memory and continuous batching through BatchCore.
+//
+// One worker thread owns the device side.  Each turn it
+//   1. retires every in-flight batch whose completion event has fired:
+//      repairs rejected updates (compact / grow / retry, then the skipped
+//      SpMV), grows pools that are nearly full, frees the batch's staging,
+//      releases its matrices and memory, publishes the results;
+//   2. if a slot is free, forms a batch from the queue in arrival order:
+//      a request joins unless its matrix is in flight or already blocked in
+//      this batch, or it would break the per-matrix order (within a batch a
+//      matrix takes at most an update, then an SpMV, or an export alone);
+//      admission stops at the first request whose device bytes exceed what
+//      is left of the budget;
+//   3. launches it on the slot's stream: host -> device copies of the
+//      requests' inputs, the merged update + grouped SpMV of BatchCore, the
+//      exports, device -> host copies of the results, a completion event.
+// Up to `depth` batches are in flight on different streams, so copies and
+// kernels of consecutive batches overlap on the device.  Results do not
+// depend on how requests were batched: each matrix sees the same sequence of
+// operations, and every kernel's result for a matrix is independent of the
+// other matrices in its launch.
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <mutex>
+#include <thread>
+#include <unordered_map>
+
+#include "internal.cuh"
+
+namespace dcsr {
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+struct Req {
+  dcsr_request r;
+  uint64_t ticket = 0;
+  Clock::time_point t_submit, t_launch;
+  int64_t cost = 0;
+  size_t off[3] = {0, 0, 0};  // staging offsets: update rows/cols/vals | spmv x/y | export rp/cols/vals
+  int item = -1;              // batch item of its matrix (update / SpMV)
+  int32_t status = DCSR_OK;
+  int64_t nnz = 0;
+};
+
+struct Slot {
+  cudaStream_t s = nullptr;
+  cudaEvent_t done = nullptr;
+  BatchCore core;
+  bool busy = false;
+  std::vector<Req> reqs;
+  std::vector<int> mats;
+  std::vector<dcsr_batch_item> items;
+  std::vector<int> item_upd, item_spmv;  // request index per item (-1: none)
+  unsigned char *stage = nullptr;
+  long long *status_host = nullptr;
+  int status_cap = 0;
+  int64_t cost = 0;
+  bool statuses = false;
+};
+
+}  // namespace
+}  // namespace dcsr
+
+using namespace dcsr;
+
+struct dcsr_server_s {
+  std::vector<dcsr_handle> mats;
+  std::vector<char> busy;
+  std::vector<uint32_t> stamp;  // per matrix: batch-formation generation
+  std::vector<int> state;       // per matrix in the forming batch: 0 none, 1 update, 2 spmv, 3 export, -1 blocked
+  uint32_t gen = 0;
+  dcsr_server_opts o{};
+  int64_t budget = 0, in_use = 0;
+  std::mutex mu;
+  std::condition_variable cv_submit, cv_done;
+  std::deque<Req> queue;
+  std::unordered_map<uint64_t, dcsr_result> done;
+  uint64_t next_ticket = 1;
+  std::vector<Slot> slots;
+  std::thread worker;
+  bool stop = false;
+  int64_t completed = 0, batches = 0;
+  int device = 0;
+  int fatal = DCSR_OK;
+};
+
+namespace {
+
+size_t vs_of(dcsr_handle h) { return h->vsize(); }
+size_t al256(size_t x) { return (x + 255) & ~size_t(255); }
+
+int64_t req_cost(dcsr_handle h, const dcsr_request &r) {
+  const int64_t vs = (int64_t)vs_of(h), n = h->n_rows, m = h->n_cols;
+  switch (r.kind) {
+    case DCSR_REQ_UPDATE: return r.nnz * (8 + vs) + (int64_t)update_scratch_bytes(r.nnz, vs) + 16 * n + 4096;
+    case DCSR_REQ_SPMV: return (int64_t)r.k * vs * (m + n) + 16 * n + 4096;
+    default: return 4 * (n + 1) + h->pool_cap * (4 + vs) + 8 * (n + 2) + 4096;
+  }
+}
+
+int check_req(dcsr_server s, const dcsr_request &r) {
+  if (r.matrix < 0 || r.matrix >= (int)s->mats.size()) return DCSR_BAD_ARG;
+  dcsr_handle h = s->mats[r.matrix];
+  switch (r.kind) {
+    case DCSR_REQ_UPDATE: return r.nnz < 0 || (r.nnz > 0 && (!r.rows || !r.cols || !r.vals)) ? DCSR_BAD_ARG : DCSR_OK;
+    case DCSR_REQ_SPMV:
+      return r.k < 1 || r.k > 8 || (h->n_cols > 0 && !r.x) || (h->n_rows > 0 && !r.y) ? DCSR_BAD_ARG : DCSR_OK;
+    case DCSR_REQ_EXPORT: return !r.row_ptr || r.cap < 0 || (r.cap > 0 && (!r.out_cols || !r.out_vals)) ? DCSR_BAD_ARG
+                                                                                                         : DCSR_OK;
+  }
+  return DCSR_BAD_ARG;
+}
+
+void publish(dcsr_server s, std::vector<Req> &reqs, int batch_size) {
+  const auto now = Clock::now();
+  std::lock_guard<std::mutex> lk(s->mu);
+  for (auto &q : reqs) {
+    dcsr_result res;
+    res.status = q.status;
+    res.batch_size = batch_size;
+    res.nnz = q.nnz;
+    res.queue_us = std::chrono::duration<double, std::micro>(q.t_launch - q.t_submit).count();
+    res.latency_us = std::chrono::duration<double, std::micro>(now - q.t_submit).count();
+    s->done[q.ticket] = res;
+    s->completed++;
+  }
+  s->cv_done.notify_all();
+}
+
+// Form a batch from the queue (caller holds the lock).
+void form(dcsr_server s, std::vector<Req> &take) {
+  const int maxb = s->o.plain ? 1 : s->o.max_batch;
+  s->gen++;
+  int64_t room = s->budget - s->in_use;
+  std::deque<Req> rest;
+  bool full = false;
+  while (!s->queue.empty()) {
+    Req q = std::move(s->queue.front());
+    s->queue.pop_front();
+    const int m = q.r.matrix;
+    if (full) {
+      rest.push_back(std::move(q));
+      continue;
+    }
+    if (s->stamp[m] != s->gen) {
+      s->stamp[m] = s->gen;
+      s->state[m] = s->busy[m] ? -1 : 0;
+    }
+    const int kind = q.r.kind == DCSR_REQ_UPDATE ? 1 : q.r.kind == DCSR_REQ_SPMV ? 2 : 3;
+    int &st = s->state[m];
+    // order within a batch: update < SpMV; an export only alone
+    const bool fits_order = st >= 0 && kind > st && !(kind == 3 && st != 0) && !(st == 3);
+    if (!fits_order) {
+      st = -1;  // every later request of this matrix waits too
+      rest.push_back(std::move(q));
+      continue;
+    }
+    if (q.cost > room) {
+      if (take.empty() && s->in_use == 0 && q.cost > s->budget) {
+        q.status = DCSR_OOM;  // can never be admitted: fail it rather than block the queue
+        q.t_launch = Clock::now();
+        std::vector<Req> one(1, q);
+        s->mu.unlock();
+        publish(s, one, 0);
+        s->mu.lock();
+        continue;
+      }
+      full = true;  // FIFO admission: later requests wait for memory too
+      rest.push_back(std::move(q));
+      continue;
+    }
+    st = kind;
+    room -= q.cost;
+    take.push_back(std::move(q));
+    if ((int)take.size() >= maxb) full = true;
+  }
+  s->queue.swap(rest);
+}
+
+int launch(dcsr_server s, Slot &sl, std::vector<Req> &take) {
+  cudaStream_t st = sl.s;
+  const auto now = Clock::now();
+  sl.reqs.swap(take);
+  sl.mats.clear();
+  sl.items.clear();
+  sl.item_upd.clear();
+  sl.item_spmv.clear();
+  sl.cost = 0;
+  sl.statuses = false;
+  // staging layout
+  size_t bytes = 0;
+  std::unordered_map<int, int> item_of;
+  for (size_t i = 0; i < sl.reqs.size(); i++) {
+    Req &q = sl.reqs[i];
+    q.t_launch = now;
+    sl.cost += q.cost;
+    dcsr_handle h = s->mats[q.r.matrix];
+    const size_t vs = vs_of(h);
+    if (q.r.kind == DCSR_REQ_UPDATE) {
+      q.off[0] = bytes;
+      bytes = al256(bytes + 4 * q.r.nnz);
+      q.off[1] = bytes;
+      bytes = al256(bytes + 4 * q.r.nnz);
+      q.off[2] = bytes;
+      bytes = al256(bytes + vs * q.r.nnz);
+    } else if (q.r.kind == DCSR_REQ_SPMV) {
+      q.off[0] = bytes;
+      bytes = al256(bytes + vs * q.r.k * h->n_cols);
+      q.off[1] = bytes;
+      bytes = al256(bytes + vs * q.r.k * h->n_rows);
+    } else {
+      q.off[0] = bytes;
+      bytes = al256(bytes + 4 * ((size_t)h->n_rows + 1));
+      q.off[1] = bytes;
+      bytes = al256(bytes + 4 * (size_t)h->pool_cap);
+      q.off[2] = bytes;
+      bytes = al256(bytes + vs * (size_t)h->pool_cap);
+    }
+    if (!item_of.count(q.r.matrix)) sl.mats.push_back(q.r.matrix);
+    if (q.r.kind != DCSR_REQ_EXPORT) {
+      auto it = item_of.find(q.r.matrix);
+      if (it == item_of.end()) {
+        dcsr_batch_item bi;
+        std::memset(&bi, 0, sizeof(bi));
+        bi.matrix = h;
+        item_of[q.r.matrix] = (int)sl.items.size();
+        sl.items.push_back(bi);
+        sl.item_upd.push_back(-1);
+        sl.item_spmv.push_back(-1);
+        it = item_of.find(q.r.matrix);
+      }
+      q.item = it->second;
+      (q.r.kind == DCSR_REQ_UPDATE ? sl.item_upd : sl.item_spmv)[q.item] = (int)i;
+    } else {
+      item_of.emplace(q.r.matrix, -1);
+    }
+  }
+  sl.busy = true;  // from here on the slot owns its requests, matrices and memory
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->in_use += sl.cost;
+    for (int m : sl.mats) s->busy[m] = 1;
+    s->batches++;
+  }
+  sl.stage = nullptr;
+  if (bytes) DCSR_CUDA(cudaMallocAsync((void **)&sl.stage, bytes, st));
+  // inputs host -> device, batch items over the staged buffers
+  for (auto &q : sl.reqs) {
+    dcsr_handle h = s->mats[q.r.matrix];
+    const size_t vs = vs_of(h);
+    unsigned char *b = sl.stage;
+    if (q.r.kind == DCSR_REQ_UPDATE && q.r.nnz > 0) {
+      DCSR_CUDA(cudaMemcpyAsync(b + q.off[0], q.r.rows, 4 * q.r.nnz, cudaMemcpyHostToDevice, st));
+      DCSR_CUDA(cudaMemcpyAsync(b + q.off[1], q.r.cols, 4 * q.r.nnz, cudaMemcpyHostToDevice, st));
+      DCSR_CUDA(cudaMemcpyAsync(b + q.off[2], q.r.vals, vs * q.r.nnz, cudaMemcpyHostToDevice, st));
+      dcsr_batch_item &bi = sl.items[q.item];
+      bi.rows = (const int32_t *)(b + q.off[0]);
+      bi.cols = (const int32_t *)(b + q.off[1]);
+      bi.vals = b + q.off[2];
+      bi.nnz = q.r.nnz;
+    } else if (q.r.kind == DCSR_REQ_SPMV) {
+      DCSR_CUDA(cudaMemcpyAsync(b + q.off[0], q.r.x, vs * q.r.k * h->n_cols, cudaMemcpyHostToDevice, st));
+      if (q.r.beta != 0.0)
+        DCSR_CUDA(cudaMemcpyAsync(b + q.off[1], q.r.y, vs * q.r.k * h->n_rows, cudaMemcpyHostToDevice, st));
+      dcsr_batch_item &bi = sl.items[q.item];
+      bi.x = b + q.off[0];
+      bi.y = b + q.off[1];
+      bi.k = q.r.k;
+      bi.ldx = bi.ldy = q.r.k;
+      bi.alpha = q.r.alpha;
+      bi.beta = q.r.beta;
+    }
+  }
+  if (s->o.plain) {
+    // the per-call path: one request, its operator, synchronously
+    Req &q = sl.reqs[0];
+    dcsr_handle h = s->mats[q.r.matrix];
+    unsigned char *b = sl.stage;
+    if (q.r.kind == DCSR_REQ_UPDATE) {
+      q.status = dcsr_update_sync(h, (const int32_t *)(b + q.off[0]), (const int32_t *)(b + q.off[1]), b + q.off[2],
+                                  q.r.nnz, st);
+    } else if (q.r.kind == DCSR_REQ_SPMV) {
+      DCSR_TRY(dcsr_spmv(h, b + q.off[0], q.r.k, q.r.k, b + q.off[1], q.r.k, q.r.alpha, q.r.beta, st));
+    }
+  } else if (!sl.items.empty()) {
+    DCSR_TRY(sl.core.plan(sl.items.data(), (int)sl.items.size(), st));
+    DCSR_TRY(sl.core.upload(st, false, true));
+    DCSR_TRY(sl.core.reserve_scratch(st));
+    DCSR_TRY(sl.core.enqueue(st));
+    bool any_upd = false;
+    for (int v : sl.item_upd) any_upd |= v >= 0;
+    if (any_upd) {
+      if (sl.status_cap < (int)sl.items.size()) {
+        if (sl.status_host) DCSR_CUDA(cudaFreeHost(sl.status_host));
+        sl.status_host = nullptr;
+        DCSR_CUDA(cudaMallocHost((void **)&sl.status_host, sizeof(long long) * 2 * sl.items.size()));
+        sl.status_cap = (int)sl.items.size();
+      }
+      DCSR_TRY(sl.core.status_async(sl.status_host, st));
+      sl.statuses = true;
+    }
+    sl.core.mark_scheduled();
+  }
+  // exports, then results device -> host
+  for (auto &q : sl.reqs) {
+    dcsr_handle h = s->mats[q.r.matrix];
+    const size_t vs = vs_of(h);
+    unsigned char *b = sl.stage;
+    if (q.r.kind == DCSR_REQ_SPMV) {
+      DCSR_CUDA(cudaMemcpyAsync(q.r.y, b + q.off[1], vs * q.r.k * h->n_rows, cudaMemcpyDeviceToHost, st));
+    } else if (q.r.kind == DCSR_REQ_EXPORT) {
+      DCSR_TRY(dcsr_to_csr(h, (int32_t *)(b + q.off[0]), (int32_t *)(b + q.off[1]), b + q.off[2], st));
+      const int64_t n_copy = q.r.cap < h->pool_cap ? q.r.cap : h->pool_cap;
+      DCSR_CUDA(cudaMemcpyAsync(q.r.row_ptr, b + q.off[0], 4 * ((size_t)h->n_rows + 1), cudaMemcpyDeviceToHost, st));
+      if (n_copy > 0) {
+        DCSR_CUDA(cudaMemcpyAsync(q.r.out_cols, b + q.off[1], 4 * n_copy, cudaMemcpyDeviceToHost, st));
+        DCSR_CUDA(cudaMemcpyAsync(q.r.out_vals, b + q.off[2], vs * n_copy, cudaMemcpyDeviceToHost, st));
+      }
+    }
+  }
+  DCSR_CUDA(cudaEventRecord(sl.done, st));
+  return DCSR_OK;
+}
+
+int retire(dcsr_server s, Slot &sl) {
+  cudaStream_t st = sl.s;
+  if (sl.statuses) {
+    for (size_t i = 0; i < sl.items.size(); i++) {
+      const int ui = sl.item_upd[i];
+      if (ui < 0) continue;
+      Req &q = sl.reqs[ui];
+      dcsr_handle h = s->mats[q.r.matrix];
+      int status = (int)sl.status_host[2 * i];
+      const long long need = sl.status_host[2 * i + 1];
+      if (status != DCSR_OK) {
+        if (status == DCSR_POOL_EXHAUSTED || status == DCSR_LAYER_OVERFLOW)
+          status = dcsr_update_sync(h, sl.items[i].rows, sl.items[i].cols, sl.items[i].vals, sl.items[i].nnz, st);
+        const int si = sl.item_spmv[i];
+        if (si >= 0) {  // its SpMV was skipped in the batch
+          // (the skipped pass left the staged y as it was copied in)
+          Req &p = sl.reqs[si];
+          const size_t vs = vs_of(h);
+          DCSR_TRY(dcsr_spmv(h, sl.items[i].x, p.r.k, p.r.k, sl.items[i].y, p.r.k, p.r.alpha, p.r.beta, st));
+          DCSR_CUDA(cudaMemcpyAsync(p.r.y, sl.items[i].y, vs * p.r.k * h->n_rows, cudaMemcpyDeviceToHost, st));
+        }
+        DCSR_CUDA(cudaStreamSynchronize(st));
+      } else if (h->pool_cap - need < h->pool_cap / 8) {
+        // nearly full: grow ahead of the next update (stream-ordered, no sync)
+        DCSR_TRY(reserve(h, pool_capacity(h->o, need), st));
+      }
+      q.status = status;
+    }
+  }
+  for (auto &q : sl.reqs) {
+    if (q.r.kind != DCSR_REQ_EXPORT) continue;
+    dcsr_handle h = s->mats[q.r.matrix];
+    q.nnz = q.r.row_ptr[h->n_rows];
+    if (q.nnz > q.r.cap) q.status = DCSR_BAD_ARG;
+  }
+  if (sl.stage) DCSR_CUDA(cudaFreeAsync(sl.stage, st));
+  sl.stage = nullptr;
+  sl.busy = false;
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->in_use -= sl.cost;
+    for (int m : sl.mats) s->busy[m] = 0;
+  }
+  publish(s, sl.reqs, (int)sl.reqs.size());
+  sl.reqs.clear();
+  return DCSR_OK;
+}
+
+// A batch that could not be launched or retired: its requests fail with
+// `status`.  A CUDA error is sticky (the context may be unusable): every
+// later request fails with it too.
+void fail_slot(dcsr_server s, Slot &sl, int status) {
+  for (auto &q : sl.reqs) q.status = status;
+  if (sl.busy) {
+    if (sl.stage) cudaFreeAsync(sl.stage, sl.s);
+    sl.stage = nullptr;
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->in_use -= sl.cost;
+    for (int m : sl.mats) s->busy[m] = 0;
+  }
+  sl.busy = false;
+  if (status == DCSR_CUDA_ERROR) {
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->fatal = status;
+  }
+  publish(s, sl.reqs, (int)sl.reqs.size());
+  sl.reqs.clear();
+}
+
+void worker_main(dcsr_server s) {
+  cudaSetDevice(s->device);
+  for (;;) {
+    bool progressed = false;
+    for (auto &sl : s->slots) {
+      if (!sl.busy) continue;
+      const cudaError_t e = cudaEventQuery(sl.done);
+      if (e == cudaErrorNotReady) continue;
+      const int st = e == cudaSuccess ? retire(s, sl) : DCSR_CUDA_ERROR;
+      if (st != DCSR_OK) fail_slot(s, sl, st);
+      progressed = true;
+    }
+    Slot *free_slot = nullptr;
+    for (auto &sl : s->slots)
+      if (!sl.busy) {
+        free_slot = &sl;
+        break;
+      }
+    if (free_slot) {
+      std::vector<Req> take;
+      {
+        std::lock_guard<std::mutex> lk(s->mu);
+        if (s->fatal != DCSR_OK) {  // a CUDA error: fail everything queued
+          std::vector<Req> all(s->queue.begin(), s->queue.end());
+          s->queue.clear();
+          for (auto &q : all) {
+            q.status = s->fatal;
+            q.t_launch = Clock::now();
+          }
+          s->mu.unlock();
+          publish(s, all, 0);
+          s->mu.lock();
+        } else {
+          form(s, take);
+        }
+      }
+      if (!take.empty()) {
+        const int st = launch(s, *free_slot, take);
+        if (st != DCSR_OK) {
+          if (free_slot->reqs.empty()) free_slot->reqs.swap(take);
+          fail_slot(s, *free_slot, st);
+        }
+        progressed = true;
+      }
+    }
+    if (!progressed) {
+      std::unique_lock<std::mutex> lk(s->mu);
+      bool inflight = false;
+      for (auto &sl : s->slots) inflight |= sl.busy;
+      if (s->stop && s->queue.empty() && !inflight) break;
+      if (!inflight) {
+        s->cv_submit.wait_for(lk, std::chrono::milliseconds(2));
+      } else {
+        lk.unlock();
+        std::this_thread::yield();
+      }
+    }
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+void dcsr_server_default_opts(dcsr_server_opts *o) {
+  if (!o) return;
+  o->max_batch = 256;
+  o->depth = 2;
+  o->mem_budget = 0;
+  o->mem_reserve = 1ll << 30;
+  o->plain = 0;
+}
+
+int dcsr_server_create(dcsr_server *out, const dcsr_handle *matrices, int32_t count, const dcsr_server_opts *opts) {
+  if (!out || !matrices || count < 1) return DCSR_BAD_ARG;
+  dcsr_server_opts o;
+  dcsr_server_default_opts(&o);
+  if (opts) o = *opts;
+  if (o.max_batch < 1 || o.depth < 1 || o.depth > 16 || o.mem_budget < 0 || o.mem_reserve < 0) return DCSR_BAD_ARG;
+  for (int i = 0; i < count; i++)
+    if (!matrices[i]) return DCSR_BAD_ARG;
+  dcsr_server s = new dcsr_server_s;
+  s->o = o;
+  s->mats.assign(matrices, matrices + count);
+  s->busy.assign(count, 0);
+  s->stamp.assign(count, 0);
+  s->state.assign(count, 0);
+  cudaGetDevice(&s->device);
+  if (o.mem_budget > 0) {
+    s->budget = o.mem_budget;
+  } else {
+    size_t fr = 0, tot = 0;
+    DCSR_CUDA(cudaMemGetInfo(&fr, &tot));
+    s->budget = (int64_t)fr - o.mem_reserve;
+    if (s->budget < (64ll << 20)) s->budget = 64ll << 20;
+  }
+  const int depth = o.plain ? 1 : o.depth;
+  s->slots.resize(depth);
+  for (auto &sl : s->slots) {
+    if (cudaStreamCreateWithFlags(&sl.s, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming) != cudaSuccess) {
+      delete s;
+      return DCSR_CUDA_ERROR;
+    }
+  }
+  s->worker = std::thread(worker_main, s);
+  *out = s;
+  return DCSR_OK;
+}
+
+int dcsr_server_submit(dcsr_server s, const dcsr_request *req, uint64_t *ticket) {
+  if (!s || !req || !ticket) return DCSR_BAD_ARG;
+  DCSR_TRY(check_req(s, *req));
+  Req q;
+  q.r = *req;
+  q.t_submit = Clock::now();
+  q.cost = req_cost(s->mats[req->matrix], *req);
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (s->stop) return DCSR_BAD_ARG;
+    q.ticket = s->next_ticket++;
+    *ticket = q.ticket;
+    s->queue.push_back(std::move(q));
+  }
+  s->cv_submit.notify_one();
+  return DCSR_OK;
+}
+
+int dcsr_server_wait(dcsr_server s, uint64_t ticket, int64_t timeout_us, dcsr_result *out) {
+  if (!s || !out) return DCSR_BAD_ARG;
+  std::unique_lock<std::mutex> lk(s->mu);
+  if (ticket == 0 || ticket >= s->next_ticket) return DCSR_BAD_ARG;
+  auto ready = [&] { return s->done.count(ticket) > 0; };
+  if (timeout_us < 0) s->cv_done.wait(lk, ready);
+  else if (!s->cv_done.wait_for(lk, std::chrono::microseconds(timeout_us), ready)) return DCSR_TIMEOUT;
+  *out = s->done[ticket];
+  s->done.erase(ticket);
+  return DCSR_OK;
+}
+
+int dcsr_server_stats(dcsr_server s, int64_t *completed, int64_t *batches, int64_t *mem_in_use) {
+  if (!s) return DCSR_BAD_ARG;
+  std::lock_guard<std::mutex> lk(s->mu);
+  if (completed) *completed = s->completed;
+  if (batches) *batches = s->batches;
+  if (mem_in_use) *mem_in_use = s->in_use;
+  return DCSR_OK;
+}
+
+int dcsr_server_destroy(dcsr_server s) {
+  if (!s) return DCSR_BAD_ARG;
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->stop = true;
+  }
+  s->cv_submit.notify_all();
+  if (s->worker.joinable()) s->worker.join();
+  for (auto &sl : s->slots) {
+    if (sl.s) cudaStreamSynchronize(sl.s);
+    sl.core.release();
+    if (sl.status_host) cudaFreeHost(sl.status_host);
+    if (sl.done) cudaEventDestroy(sl.done);
+    if (sl.s) cudaStreamDestroy(sl.s);
+  }
+  delete s;
+  return DCSR_OK;
+}
+
+}  // extern "C"

@@ -217,6 +217,74 @@ int dcsr_batch_status(dcsr_batch b, int32_t *statuses, void *stream);
 int dcsr_batch_repair(dcsr_batch b, const int32_t *statuses, int32_t *repaired, void *stream);
 int dcsr_batch_destroy(dcsr_batch b);
 
+/* ------------------------------------------------------------ serving */
+
+/* A request server over a table of resident matrices.  Requests (update,
+ * SpMV, export) carry HOST buffers; a worker thread admits queued requests
+ * while their device memory fits the budget, coalesces them into batches
+ * (merged update + grouped SpMV through the batched kernels, then exports),
+ * keeps up to `depth` batches in flight on separate streams, and refills
+ * slots as batches retire (continuous batching).  Per matrix, requests take
+ * effect in submission order: a matrix is in at most one in-flight batch, and
+ * within a batch its update precedes its SpMV.  A rejected update is repaired
+ * (compact, grow, retry) before its result is reported, and pools nearing
+ * full are grown ahead of the next update.  The reference has no serving
+ * layer; its callers loop over UpdateMatrix / spmv (src/Fill_Test.inl). */
+typedef struct dcsr_server_s *dcsr_server;
+
+typedef struct {
+  int32_t max_batch;   /* requests coalesced into one batch (default 256) */
+  int32_t depth;       /* batches in flight, one stream each (default 2) */
+  int64_t mem_budget;  /* device bytes in-flight requests may hold; 0: free memory at creation - mem_reserve */
+  int64_t mem_reserve; /* default 1 GiB */
+  int32_t plain;       /* 1: no coalescing -- each request alone through the per-call operators */
+} dcsr_server_opts;
+
+enum { DCSR_REQ_UPDATE = 0, DCSR_REQ_SPMV = 1, DCSR_REQ_EXPORT = 2 };
+
+typedef struct {
+  int32_t kind;   /* DCSR_REQ_* */
+  int32_t matrix; /* index into the server's matrix table */
+  /* UPDATE: nnz host triples (merged / appended by the matrix's mode) */
+  const int32_t *rows;
+  const int32_t *cols;
+  const void *vals;
+  int64_t nnz;
+  /* SPMV: y = alpha*A*x + beta*y, host x [n_cols x k], y [n_rows x k] row-major */
+  const void *x;
+  void *y;
+  int32_t k;
+  double alpha, beta;
+  /* EXPORT: host CSR of the matrix: row_ptr [n_rows+1], cols/vals with room for cap entries */
+  int32_t *row_ptr;
+  int32_t *out_cols;
+  void *out_vals;
+  int64_t cap;
+} dcsr_request;
+
+typedef struct {
+  int32_t status;     /* DCSR_OK, the update's final status, BAD_ARG if cap < nnz */
+  int32_t batch_size; /* requests in the batch that served it */
+  int64_t nnz;        /* EXPORT: entries of the matrix */
+  double queue_us;    /* submit -> launch */
+  double latency_us;  /* submit -> result in host memory */
+} dcsr_result;
+
+void dcsr_server_default_opts(dcsr_server_opts *o);
+/* Host buffers of a request must stay valid (and unread / unwritten by the
+ * caller) until its result is taken with dcsr_server_wait.  The matrices must
+ * not be used outside the server while it runs. */
+int dcsr_server_create(dcsr_server *out, const dcsr_handle *matrices, int32_t count, const dcsr_server_opts *opts);
+/* Thread-safe, non-blocking: queue a request, return its ticket. */
+int dcsr_server_submit(dcsr_server s, const dcsr_request *req, uint64_t *ticket);
+/* Wait (at most timeout_us; < 0: forever) for a ticket's result and forget
+ * the ticket.  DCSR_TIMEOUT if it has not completed. */
+int dcsr_server_wait(dcsr_server s, uint64_t ticket, int64_t timeout_us, dcsr_result *out);
+/* Counters: completed requests, batches launched, budget bytes in use. */
+int dcsr_server_stats(dcsr_server s, int64_t *completed, int64_t *batches, int64_t *mem_in_use);
+/* Drain the queue, stop the worker, release the server (not the matrices). */
+int dcsr_server_destroy(dcsr_server s);
+
 /* Allocation-free reduce-by-key.  No counterpart in the reference: it is
  * for callers that cannot allocate device memory at call time -- a process
  * that has carved the GPU's memory into fixed budgets up front, or code whose
