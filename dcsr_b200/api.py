@@ -60,7 +60,7 @@ class Request(C.Structure):
     _fields_ = [("kind", C.c_int32), ("matrix", C.c_int32), ("rows", C.c_void_p), ("cols", C.c_void_p),
                 ("vals", C.c_void_p), ("nnz", C.c_int64), ("x", C.c_void_p), ("y", C.c_void_p), ("k", C.c_int32),
                 ("alpha", C.c_double), ("beta", C.c_double), ("row_ptr", C.c_void_p), ("out_cols", C.c_void_p),
-                ("out_vals", C.c_void_p), ("cap", C.c_int64)]
+                ("out_vals", C.c_void_p), ("cap", C.c_int64), ("on_device", C.c_int32)]
 
 
 class Result(C.Structure):
@@ -117,6 +117,7 @@ _SIGS = {
     "dcsr_server_wait": (_i32, [_vp, C.c_uint64, _i64, _vp]),
     "dcsr_server_stats": (_i32, [_vp, C.POINTER(_i64), C.POINTER(_i64), C.POINTER(_i64)]),
     "dcsr_server_destroy": (_i32, [_vp]),
+    "dcsr_server_replay": (_i32, [_vp, _vp, _vp, _i64, _vp, C.POINTER(_dbl)]),
     "dcsr_status_string": (C.c_char_p, [_i32]),
     "dcsr_launch_count": (C.c_uint64, []),
     "dcsr_version": (C.c_char_p, []),
@@ -424,11 +425,18 @@ class DcsrBatch:
             pass
 
 
-def _host(t):
-    """Pointer of a contiguous CPU tensor (pinned memory keeps the server's copies asynchronous)."""
-    if t.is_cuda or not t.is_contiguous():
-        raise ValueError("contiguous host tensor expected")
-    return t.data_ptr()
+def _buf(*ts):
+    """Pointers of a request's tensors and whether they are device memory
+    (all of a request's tensors must be on the same side; host tensors
+    should be pinned so the server's copies stay asynchronous)."""
+    ts = [t for t in ts if t is not None]
+    dev = {t.is_cuda for t in ts}
+    if len(dev) > 1:
+        raise ValueError("a request's tensors must all be host or all be device tensors")
+    for t in ts:
+        if not t.is_contiguous():
+            raise ValueError("contiguous tensor expected")
+    return dev == {True}
 
 
 class DcsrServer:
@@ -455,21 +463,24 @@ class DcsrServer:
         return t.value
 
     def submit_update(self, i, rows, cols, vals):
-        r = Request(kind=REQ_UPDATE, matrix=i, nnz=rows.numel())
+        r = Request(kind=REQ_UPDATE, matrix=i, nnz=rows.numel(), on_device=int(_buf(rows, cols, vals)))
         if rows.numel():
-            r.rows, r.cols, r.vals = _host(rows), _host(cols), _host(vals)
+            r.rows, r.cols, r.vals = rows.data_ptr(), cols.data_ptr(), vals.data_ptr()
         return self._submit(r, (rows, cols, vals))
 
     def submit_spmv(self, i, x, y, alpha=1.0, beta=0.0):
-        """y (host, [n_rows] or [n_rows, k]) = alpha*A@x + beta*y."""
+        """y ([n_rows] or [n_rows, k]) = alpha*A@x + beta*y."""
         k = 1 if x.dim() == 1 else x.shape[1]
-        r = Request(kind=REQ_SPMV, matrix=i, x=_host(x), y=_host(y), k=k, alpha=alpha, beta=beta)
+        r = Request(kind=REQ_SPMV, matrix=i, x=x.data_ptr(), y=y.data_ptr(), k=k, alpha=alpha, beta=beta,
+                    on_device=int(_buf(x, y)))
         return self._submit(r, (x, y))
 
     def submit_export(self, i, row_ptr, cols, vals):
-        r = Request(kind=REQ_EXPORT, matrix=i, row_ptr=_host(row_ptr), cap=cols.numel())
+        """CSR of the matrix into row_ptr [n_rows+1] and cols/vals (capacity = their length)."""
+        r = Request(kind=REQ_EXPORT, matrix=i, row_ptr=row_ptr.data_ptr(), cap=cols.numel(),
+                    on_device=int(_buf(row_ptr, cols, vals)))
         if cols.numel():
-            r.out_cols, r.out_vals = _host(cols), _host(vals)
+            r.out_cols, r.out_vals = cols.data_ptr(), vals.data_ptr()
         return self._submit(r, (row_ptr, cols, vals))
 
     def wait(self, ticket, timeout_us=-1) -> dict:

@@ -61,10 +61,13 @@ void fill_image(const BatchCore &b, unsigned char *img) {
     u.T = it.nnz;
     up[i] = u;
     toff += it.nnz;
+  }
+  for (size_t q = 0; q < b.sched.size(); q++) {
+    dcsr_handle h = b.items[b.sched[q]].matrix;
     RowItem<V> r = row_item<V>(h, nullptr, nullptr, 0, 0, 0.0, 0.0);
     r.row0 = row0;
     row0 += h->n_rows;
-    rows[i] = r;
+    rows[q] = r;
   }
   for (auto &g : b.groups) {
     RowItem<V> *gi = (RowItem<V> *)(img + g.off);
@@ -91,7 +94,7 @@ int grow_dev(T **p, size_t n, size_t &cap, cudaStream_t s) {
 
 }  // namespace
 
-int BatchCore::plan(const dcsr_batch_item *its, int n, cudaStream_t s) {
+int BatchCore::plan(const dcsr_batch_item *its, int n, cudaStream_t s, bool all_schedules) {
   if (n < 1 || !its || !its[0].matrix) return DCSR_BAD_ARG;
   const int dt = its[0].matrix->dtype, md = its[0].matrix->o.mode;
   int32_t max_rows = 1, max_cols = 1;
@@ -119,7 +122,6 @@ int BatchCore::plan(const dcsr_batch_item *its, int n, cudaStream_t s) {
   mode = md;
   items.assign(its, its + n);
   T = t;
-  R = r;
   rb = bits_for((int64_t)max_rows);
   cb = bits_for((int64_t)max_cols);
   // SpMV groups by (k, vectorisable x)
@@ -141,9 +143,20 @@ int BatchCore::plan(const dcsr_batch_item *its, int n, cudaStream_t s) {
     }
     groups[gi].idx.push_back(i);
   }
+  // schedules to rebuild: every matrix, or the updated ones and those whose
+  // schedule is stale (after sizing their schedule buffers, which can
+  // invalidate a schedule)
+  DCSR_TRY(ensure_buffers(s));
+  sched.clear();
+  R = 0;
+  for (int i = 0; i < n; i++)
+    if (all_schedules || its[i].nnz > 0 || !its[i].matrix->bins_valid) {
+      sched.push_back(i);
+      R += its[i].matrix->n_rows;
+    }
   size_t off = align_up((int64_t)(n * desc_size(dtype, false)), 256);
   off_row = off;
-  off = align_up((int64_t)(off + n * desc_size(dtype, true)), 256);
+  off = align_up((int64_t)(off + sched.size() * desc_size(dtype, true)), 256);
   size_t poff = 0;
   for (auto &g : groups) {
     g.off = off;
@@ -172,10 +185,14 @@ int BatchCore::plan(const dcsr_batch_item *its, int n, cudaStream_t s) {
   return DCSR_OK;
 }
 
-int BatchCore::upload(cudaStream_t s, bool sync, bool force) {
+int BatchCore::ensure_buffers(cudaStream_t s) {
   for (auto &g : groups)
     for (int i : g.idx) DCSR_TRY(ensure_part(items[i].matrix, g.k, s));
   for (int i = 0; i < count; i++) DCSR_TRY(ensure_part(items[i].matrix, 1, s));
+  return DCSR_OK;
+}
+
+int BatchCore::upload(cudaStream_t s, bool sync, bool force) {
   img_new.assign(img_bytes, 0);
   if (dtype == DCSR_F32) fill_image<float>(*this, img_new.data());
   else fill_image<double>(*this, img_new.data());
@@ -205,8 +222,10 @@ int BatchCore::enqueue(cudaStream_t s) {
   } else {
     DCSR_CUDA(cudaMemsetAsync(skip, 0, sizeof(int32_t) * count, s));
   }
-  DCSR_TRY(ar.reserve(schedule_scratch_bytes(R), s));
-  DCSR_TRY(schedule_many(img_dev + off_row, dtype, count, R, ar, s));
+  if (!sched.empty()) {
+    DCSR_TRY(ar.reserve(schedule_scratch_bytes(R), s));
+    DCSR_TRY(schedule_many(img_dev + off_row, dtype, (int)sched.size(), R, ar, s));
+  }
   for (auto &g : groups)
     DCSR_TRY(spmv_many(img_dev + g.off, dtype, (int)g.idx.size(), g.k, g.vec, pref + g.pref_off, s));
   return DCSR_OK;
@@ -271,7 +290,7 @@ int dcsr_batch_create(dcsr_batch *out, const dcsr_batch_item *items, int32_t cou
   if (!out || count < 1 || !items) return DCSR_BAD_ARG;
   cudaStream_t s = (cudaStream_t)stream;
   dcsr_batch b = new dcsr_batch_s;
-  int st = b->core.plan(items, count, s);
+  int st = b->core.plan(items, count, s, true);
   // scratch for the largest phase, reserved now so runs (and captures) never allocate
   if (st == DCSR_OK) st = b->core.reserve_scratch(s);
   if (st == DCSR_OK && cudaMallocHost((void **)&b->status_host, sizeof(long long) * 2 * count) != cudaSuccess)
@@ -289,6 +308,7 @@ int dcsr_batch_create(dcsr_batch *out, const dcsr_batch_item *items, int32_t cou
 int dcsr_batch_run(dcsr_batch b, void *stream) {
   if (!b) return DCSR_BAD_ARG;
   cudaStream_t s = (cudaStream_t)stream;
+  DCSR_TRY(b->core.ensure_buffers(s));
   DCSR_TRY(b->core.upload(s, true));
   DCSR_TRY(b->core.reserve_scratch(s));
   DCSR_TRY(b->core.enqueue(s));
@@ -299,6 +319,7 @@ int dcsr_batch_run(dcsr_batch b, void *stream) {
 int dcsr_batch_capture(dcsr_batch b, void *stream) {
   if (!b || !stream) return DCSR_BAD_ARG;  // the legacy default stream cannot be captured
   cudaStream_t s = (cudaStream_t)stream;
+  DCSR_TRY(b->core.ensure_buffers(s));
   DCSR_TRY(b->core.upload(s, true));
   DCSR_TRY(b->core.reserve_scratch(s));
   DCSR_CUDA(cudaStreamSynchronize(s));
@@ -333,6 +354,7 @@ int dcsr_batch_capture(dcsr_batch b, void *stream) {
 int dcsr_batch_launch(dcsr_batch b, void *stream) {
   if (!b || !b->exec) return DCSR_BAD_ARG;
   cudaStream_t s = (cudaStream_t)stream;
+  DCSR_TRY(b->core.ensure_buffers(s));
   DCSR_TRY(b->core.upload(s, true));
   DCSR_CUDA(cudaGraphLaunch(b->exec, s));
   count_launch(b->graph_kernels);

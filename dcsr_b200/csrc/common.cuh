@@ -278,6 +278,34 @@ __device__ __forceinline__ Chain load_chain(const Mat<V> &m, int32_t r) {
   return c;
 }
 
+// The leading layers of row r that hold its first len entries, for passes
+// that only read a row: layer 0 is loaded at once (independent of len, so
+// its load overlaps the caller's load of the row length); layer l+1 only
+// when layers 0..l hold fewer than len entries (most rows need layer 0
+// alone, so the other layers' table entries are not read at all).
+template <typename V>
+__device__ __forceinline__ Chain load_chain_used(const Mat<V> &m, int32_t r, int32_t len) {
+  Chain c;
+  c.ns = 0;
+  int64_t covered = 0;
+#pragma unroll
+  for (int l = 0; l < MAX_SEGS; l++) {
+    c.st[l] = 0;
+    c.cp[l] = 0;
+    if (l < m.max_segs && c.ns == l && (l == 0 || covered < len)) {
+      const int2 p = __ldg(reinterpret_cast<const int2 *>(m.seg + (int64_t)l * m.pitch + 2 * (int64_t)r));
+      if (p.x >= 0) {
+        c.st[l] = p.x;
+        c.cp[l] = p.y - p.x;
+        covered += p.y - p.x;
+        c.ns = l + 1;
+      }
+    }
+  }
+  c.total = covered;
+  return c;
+}
+
 // Persistent-grid size for a kernel: blocks resident across all SMs.
 int persistent_grid(const void *kernel, int block, size_t smem);
 int sm_count();

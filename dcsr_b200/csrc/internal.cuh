@@ -72,10 +72,13 @@ RowItem<V> row_item(dcsr_handle h, const void *x, void *y, int64_t ldx, int64_t 
 // Size the handle's chunk table and chunk partials (K results per chunk).
 int ensure_part(dcsr_handle h, int K, cudaStream_t s);
 // Copy every row's logical entries to dst_off[r] (optionally COO row ids and
-// an int32 row pointer).  Builds the schedule first if needed (so callers
-// must not hold arena memory across this call unless the schedule is valid).
+// an int32 row pointer); entries at positions >= limit are not written.
+// Builds the schedule first if needed (so callers must not hold arena memory
+// across this call unless the schedule is valid).
 int copy_rows(dcsr_handle h, const long long *dst_off, int32_t *out_cols, void *out_vals, int32_t *out_rows,
-              int32_t *out_rowptr, cudaStream_t s);
+              int32_t *out_rowptr, cudaStream_t s, int64_t limit = INT64_MAX);
+// DCSR -> CSR writing at most `limit` entries (the row pointer is complete).
+int export_csr(dcsr_handle h, int32_t *row_ptr, int32_t *cols, void *vals, int64_t limit, cudaStream_t s);
 int reserve(dcsr_handle h, int64_t cap, cudaStream_t s);
 
 // The device side of a batch (batch.cu): a plan over a set of
@@ -95,7 +98,8 @@ struct BatchCore {
   int64_t T = 0, R = 0;
   int rb = 1, cb = 1;
   std::vector<Group> groups;
-  // image: BatchItem[count] | RowItem[count] (row space) | group RowItems
+  std::vector<int> sched;  // items whose schedules the run rebuilds
+  // image: BatchItem[count] | RowItem[sched] (row space) | group RowItems
   size_t off_row = 0, img_bytes = 0, img_cap = 0;
   unsigned char *img_dev = nullptr;
   unsigned char *img_host = nullptr;  // pinned copy of the last upload
@@ -109,10 +113,13 @@ struct BatchCore {
   Arena ar;
 
   // Validate and plan `items` (one dtype and mode, each matrix once); grows
-  // buffers with stream-ordered allocation on s.
-  int plan(const dcsr_batch_item *items, int count, cudaStream_t s);
-  // Rebuild the descriptor image from the handles (sizing their schedule
-  // buffers first) and upload it if it changed.  sync=true waits for the
+  // buffers with stream-ordered allocation on s.  all_schedules: every run
+  // rebuilds every matrix's schedule (a captured graph must not depend on
+  // host state); else only updated matrices and stale schedules.
+  int plan(const dcsr_batch_item *items, int count, cudaStream_t s, bool all_schedules);
+  // Size every matrix's schedule buffers for its pool (before an upload).
+  int ensure_buffers(cudaStream_t s);
+  // Rebuild the descriptor image from the handles and upload it if it changed.  sync=true waits for the
   // upload; otherwise the caller guarantees the previous upload of this core
   // has completed before the next call (the pinned image is reused).
   int upload(cudaStream_t s, bool sync, bool force = false);

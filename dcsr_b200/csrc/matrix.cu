@@ -181,6 +181,9 @@ int load_from_csr64(dcsr_handle h, const long long *rp, const int32_t *cols, con
     DCSR_LAUNCH(k_copy_csr<double>, grid_for((int64_t)n * 32, 256), 256, 0, s, n, caps, rp, cols,
                 (const double *)vals, h->cols, (double *)h->vals);
   h->bins_valid = false;
+  // A load is a one-off: a resident matrix keeps no load-sized scratch (the
+  // stream-ordered pool keeps the memory for the next allocation).
+  h->scratch.release(s);
   return DCSR_OK;
 }
 
@@ -227,6 +230,7 @@ int compact(dcsr_handle h, cudaStream_t s) {
   h->cols = nc;
   h->vals = nv;
   h->pool_cap = cap;
+  h->scratch.release(s);
   return DCSR_OK;
 }
 
@@ -486,7 +490,8 @@ int dcsr_nnz(dcsr_handle h, int64_t *nnz, void *stream) {
   return DCSR_OK;
 }
 
-static int export_impl(dcsr_handle h, int32_t *row_ptr, int32_t *rows, int32_t *cols, void *vals, cudaStream_t s) {
+static int export_impl(dcsr_handle h, int32_t *row_ptr, int32_t *rows, int32_t *cols, void *vals, cudaStream_t s,
+                       int64_t limit = INT64_MAX) {
   const int32_t n = h->n_rows;
   Arena &ar = h->scratch;
   if (!h->bins_valid) DCSR_TRY(build_schedule(h, s));  // before taking arena memory
@@ -494,8 +499,9 @@ static int export_impl(dcsr_handle h, int32_t *row_ptr, int32_t *rows, int32_t *
   long long *rp = ar.take<long long>(n + 2);
   DCSR_LAUNCH(k_lens, grid_for(n + 1, 256), 256, 0, s, h->row_sizes, n, rp);
   DCSR_TRY(scan_i64(rp, rp, n + 1, nullptr, ar, s));
-  return copy_rows(h, rp, cols, vals, rows, row_ptr, s);
+  return copy_rows(h, rp, cols, vals, rows, row_ptr, s, limit);
 }
+
 
 int dcsr_to_csr(dcsr_handle h, int32_t *row_ptr, int32_t *cols, void *vals, void *stream) {
   if (!h || !row_ptr) return DCSR_BAD_ARG;
@@ -582,3 +588,9 @@ uint64_t dcsr_launch_count(void) { return g_launches.load(); }
 const char *dcsr_version(void) { return "dcsr_b200 0.1 (sm_100a)"; }
 
 }  // extern "C"
+
+namespace dcsr {
+int export_csr(dcsr_handle h, int32_t *row_ptr, int32_t *cols, void *vals, int64_t limit, cudaStream_t s) {
+  return export_impl(h, row_ptr, nullptr, cols, vals, s, limit);
+}
+}  // namespace dcsr

@@ -4,21 +4,30 @@
 // Rows are split into three classes by the schedule (rebuilt lazily after
 // any change of row lengths), each with its own launch so each has its own
 // register budget and its units carry bounded work:
-//   short  (<= short_max entries)  a warp takes 32 consecutive rows and
+//   short  (<= short_max entries)  a warp takes 32 consecutive rows.  With
+//          one value per entry (SpMV k=1, row reductions, the copy pass) it
 //          streams each segment layer's entries across its lanes, U windows
-//          of 32 entries at a time with every window's loads issued first;
-//          a lane's row comes from ballots over the window's row starts
-//          (__fns), reductions use a segmented scan whose segment tests are
-//          bit operations on that start mask.
+//          of 32 entries at a time with every window's loads issued first; a
+//          lane's row comes from ballots over the window's row starts
+//          (__fns) and sums use a segmented scan whose segment tests are bit
+//          operations on that start mask -- uneven rows cost nothing extra.
+//          With k >= 2 values per entry (where the scan's k shuffles per
+//          step would dominate) the warp splits into groups of G lanes, G in
+//          {1..16} from the block's mean row length; a group walks one row
+//          with four loads in flight per lane and reduces over its lanes with
+//          log2(G) shuffles.
 //   medium (<= long_min)          one warp per row, lanes strided, U loads in
 //          flight per lane, one warp reduction per row.
 //   long                          CHUNK-entry chunks, one CTA per chunk,
 //          STEP entries in flight per CTA step (128-bit loads when aligned);
 //          multi-chunk rows combine their partials in chunk order (the CTA
 //          that finishes the last chunk sums them).
-// Every row's result is therefore independent of scheduling.  Products
-// accumulate in FP64 per lane; the short class's per-window partials use the
-// matrix type (FP32 partials of at most 32 products, then FP64).
+// A row's result depends only on the row (its length picks its class, the
+// block's lengths pick G), never on which launch or batch it runs in.
+// Products accumulate in FP64 per lane (fused multiply-add); the k=1
+// stream's per-window partials use the matrix type (FP32 partials of at
+// most 32 products, then FP64); every rounding step is an explicit
+// round-to-nearest intrinsic.
 //
 // Reference: spmv_dcsr_bin* include/spmv.inl:364-622 (seven bin kernels on
 // seven streams, rows read with stale Prow_sizes), CompactIndices
@@ -344,6 +353,46 @@ __device__ __forceinline__ WinMap window_map(int32_t w0, int32_t excl, int32_t i
   return r;
 }
 
+// Lanes per row for a block of 32 short rows: the largest power of two
+// G <= mean length / 4 (1..16), so a lane has about four or more entries of
+// its row in flight and a block takes G passes of 32/G rows.
+__device__ __forceinline__ int group_width(int32_t total) {
+  const int32_t mean = total >> 5;
+  return mean < 8 ? 1 : mean < 16 ? 2 : mean < 32 ? 4 : mean < 64 ? 8 : 16;
+}
+
+// The chain of the row owned by lane `owner` (every lane loaded its own row's
+// chain at the block's start; a pass hands it to the row's group).
+__device__ __forceinline__ Chain shfl_chain(const Chain &own, int owner) {
+  Chain c;
+#pragma unroll
+  for (int l = 0; l < MAX_SEGS; l++) {
+    c.st[l] = __shfl_sync(FULL, own.st[l], owner);
+    c.cp[l] = __shfl_sync(FULL, own.cp[l], owner);
+  }
+  c.ns = __shfl_sync(FULL, own.ns, owner);
+  c.total = 0;
+  return c;
+}
+
+// Visit the logical entries [0, len) of a row: lane j of a G-lane group takes
+// entries j, j+G, ...; f(st, p0, take, before) handles the UN entries
+// p0 + i*G (< take) of the layer starting at pool slot st, whose first entry
+// is logical position `before`.
+template <int UN, typename F>
+__device__ __forceinline__ void for_row_entries(const Chain &ch, int32_t len, int j, int G, F &&f) {
+  int32_t before = 0;
+#pragma unroll
+  for (int l = 0; l < MAX_SEGS; l++) {
+    if (l < ch.ns && before < len) {
+      const int32_t take = ch.cp[l] < len - before ? ch.cp[l] : len - before;
+      const int64_t st = ch.st[l];
+      for (int32_t p0 = j; p0 < take; p0 += UN * G) f(st, p0, take, before);
+      before += ch.cp[l];
+    }
+  }
+}
+
 template <typename T, typename V, int K, bool VEC>
 __device__ __forceinline__ void load_xk(const V *__restrict__ x, int64_t c, int64_t ldx, T (&xv)[K]) {
   if constexpr (VEC && sizeof(V) == 4 && K == 4) {
@@ -419,17 +468,10 @@ __device__ __forceinline__ void write_y(V *y, int64_t ldy, int32_t row, const do
   }
 }
 
-template <int K>
-struct Windows {
-  static constexpr int U = K <= 2 ? 4 : (K <= 4 ? 2 : 1);
-};
-
 // --------------------------------------------------------- reduction pass
 
 template <typename V, int K, int OP, bool VEC, int PART, typename Src>
 __global__ void __launch_bounds__(RS_THREADS_) k_rows_reduce(Src src) {
-  using P = typename std::conditional<sizeof(V) == 4, float, double>::type;  // window partials
-  constexpr int U = Windows<K>::U;
   __shared__ double red[RS_WARPS][K];
   __shared__ int last_flag;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -569,81 +611,122 @@ __global__ void __launch_bounds__(RS_THREADS_) k_rows_reduce(Src src) {
       }
       if (lane == 0) write_y<V, K, OP>(it.y, it.ldy, row, acc, it.alpha, it.beta, (int32_t)L);
     } else {
-      // ---- short rows: one warp per 32 consecutive rows
+      // ---- short rows: a warp takes 32 consecutive rows
       const int64_t blk = lu * RS_WARPS + w;
       if (blk * 32 >= m.n_rows) continue;
-      const RowBlock rb = load_block(m, blk * 32, lane, it.short_max);
-      double acc[K];
+      if constexpr (K == 1) {
+        // one value per entry: stream the block's entries across the lanes
+        using P = typename std::conditional<sizeof(V) == 4, float, double>::type;  // window partials
+        constexpr int U = 4;
+        const RowBlock rb = load_block(m, blk * 32, lane, it.short_max);
+        double acc[K];
 #pragma unroll
-      for (int k = 0; k < K; k++) acc[k] = op_init<double, OP>();
-      int64_t cum = 0;  // capacity of this lane's row in the layers before l
-      for (int l = 0; l < m.max_segs; l++) {
-        int32_t len_l, st_l;
-        next_layer(m, rb, l, cum, len_l, st_l);
-        if (!__any_sync(FULL, len_l > 0)) break;
-        const int32_t incl = warp_incl_scan(len_l);  // block-local (<= 32 * short_max)
-        const int32_t excl = incl - len_l;
-        const int32_t E = __shfl_sync(FULL, incl, 31);
-        for (int32_t base = 0; base < E; base += 32 * U) {
-          int32_t q[U];
-          unsigned Mw[U];
-          bool ok[U];
+        for (int k = 0; k < K; k++) acc[k] = op_init<double, OP>();
+        int64_t cum = 0;  // capacity of this lane's row in the layers before l
+        for (int l = 0; l < m.max_segs; l++) {
+          int32_t len_l, st_l;
+          next_layer(m, rb, l, cum, len_l, st_l);
+          if (!__any_sync(FULL, len_l > 0)) break;
+          const int32_t incl = warp_incl_scan(len_l);  // block-local (<= 32 * short_max)
+          const int32_t excl = incl - len_l;
+          const int32_t E = __shfl_sync(FULL, incl, 31);
+          for (int32_t base = 0; base < E; base += 32 * U) {
+            int32_t q[U];
+            unsigned Mw[U];
+            bool ok[U];
 #pragma unroll
-          for (int i = 0; i < U; i++) {
-            const int32_t w0 = base + 32 * i;
-            const WinMap wm = window_map(w0, excl, incl, len_l, lane);
-            const int32_t ej = __shfl_sync(FULL, excl, wm.j);
-            const int32_t sj = __shfl_sync(FULL, st_l, wm.j);
-            ok[i] = w0 + lane < E;
-            Mw[i] = wm.M;
-            q[i] = sj + (ok[i] ? w0 + lane - ej : 0);
-          }
-          V a[U];
-          int32_t col[U];
-#pragma unroll
-          for (int i = 0; i < U; i++) {
-            a[i] = __ldcs(m.vals + q[i]);
-            col[i] = OP == OP_SPMV ? __ldcs(m.cols + q[i]) : 0;
-          }
-#pragma unroll
-          for (int i = 0; i < U; i++) {
-            P c[K];
-#pragma unroll
-            for (int k = 0; k < K; k++) c[k] = op_init<P, OP>();
-            if (ok[i]) {
-              if constexpr (OP == OP_SPMV) {
-                P xv[K];
-                load_xk<P, V, K, VEC>(x, col[i], ldx, xv);
-#pragma unroll
-                for (int k = 0; k < K; k++) c[k] = mul_rn((P)a[i], xv[k]);
-              } else {
-                c[0] = OP == OP_COUNT ? (P)1 : (P)a[i];
-              }
+            for (int i = 0; i < U; i++) {
+              const int32_t w0 = base + 32 * i;
+              const WinMap wm = window_map(w0, excl, incl, len_l, lane);
+              const int32_t ej = __shfl_sync(FULL, excl, wm.j);
+              const int32_t sj = __shfl_sync(FULL, st_l, wm.j);
+              ok[i] = w0 + lane < E;
+              Mw[i] = wm.M;
+              q[i] = sj + (ok[i] ? w0 + lane - ej : 0);
             }
-            // segmented inclusive scan: lanes p-d and p share a row unless a
-            // row starts in (p-d, p] (bit test on the window's start mask)
+            V a[U];
+            int32_t col[U];
 #pragma unroll
-            for (int d = 1; d < 32; d <<= 1) {
-              const bool same = lane >= d && ((Mw[i] >> (lane - d + 1)) & ((1u << d) - 1u)) == 0;
+            for (int i = 0; i < U; i++) {
+              a[i] = __ldcs(m.vals + q[i]);
+              col[i] = OP == OP_SPMV ? __ldcs(m.cols + q[i]) : 0;
+            }
+#pragma unroll
+            for (int i = 0; i < U; i++) {
+              P c[K];
+#pragma unroll
+              for (int k = 0; k < K; k++) c[k] = op_init<P, OP>();
+              if (ok[i]) {
+                if constexpr (OP == OP_SPMV) {
+                  P xv[K];
+                  load_xk<P, V, K, VEC>(x, col[i], ldx, xv);
+#pragma unroll
+                  for (int k = 0; k < K; k++) c[k] = mul_rn((P)a[i], xv[k]);
+                } else {
+                  c[0] = OP == OP_COUNT ? (P)1 : (P)a[i];
+                }
+              }
+              // segmented inclusive scan: lanes p-d and p share a row unless a
+              // row starts in (p-d, p] (bit test on the window's start mask)
+#pragma unroll
+              for (int d = 1; d < 32; d <<= 1) {
+                const bool same = lane >= d && ((Mw[i] >> (lane - d + 1)) & ((1u << d) - 1u)) == 0;
+#pragma unroll
+                for (int k = 0; k < K; k++) {
+                  const P co = __shfl_up_sync(FULL, c[k], d);
+                  if (same) c[k] = op_comb<P, OP>(c[k], co);
+                }
+              }
+              // lane j collects the tail of its row's run in this window
+              const int32_t w0 = base + 32 * i;
+              const bool hit = len_l > 0 && excl < w0 + 32 && incl > w0;
+              const int tail = (incl < w0 + 32 ? incl : w0 + 32) - 1 - w0;
 #pragma unroll
               for (int k = 0; k < K; k++) {
-                const P co = __shfl_up_sync(FULL, c[k], d);
-                if (same) c[k] = op_comb<P, OP>(c[k], co);
+                const P got = __shfl_sync(FULL, c[k], hit ? tail : 0);
+                if (hit) acc[k] = op_comb<double, OP>(acc[k], (double)got);
               }
-            }
-            // lane j collects the tail of its row's run in this window
-            const int32_t w0 = base + 32 * i;
-            const bool hit = len_l > 0 && excl < w0 + 32 && incl > w0;
-            const int tail = (incl < w0 + 32 ? incl : w0 + 32) - 1 - w0;
-#pragma unroll
-            for (int k = 0; k < K; k++) {
-              const P got = __shfl_sync(FULL, c[k], hit ? tail : 0);
-              if (hit) acc[k] = op_comb<double, OP>(acc[k], (double)got);
             }
           }
         }
+        if (rb.row >= 0 && rb.len <= it.short_max) write_y<V, K, OP>(it.y, it.ldy, rb.row, acc, it.alpha, it.beta, rb.len);
+      } else {
+        // K values per entry: G lanes per row
+        const RowBlock rb = load_block(m, blk * 32, lane, it.short_max);
+        const Chain own = load_chain_used(m, rb.row >= 0 ? rb.row : 0, rb.stream ? rb.len : 0);
+        const int G = group_width(warp_sum(rb.stream ? rb.len : 0));
+        const int per = 32 / G, j = lane & (G - 1), g = lane / G;
+        for (int pass = 0; pass < G; pass++) {
+          const int owner = pass * per + g;
+          const int32_t row = __shfl_sync(FULL, rb.row, owner);
+          const int32_t len = __shfl_sync(FULL, rb.len, owner);
+          const Chain ch = shfl_chain(own, owner);
+          double acc[K];
+#pragma unroll
+          for (int k = 0; k < K; k++) acc[k] = op_init<double, OP>();
+          if (row >= 0 && len > 0 && len <= it.short_max) {
+            constexpr int UN = K <= 2 ? 8 : 4;  // entries in flight per lane
+            for_row_entries<UN>(ch, len, j, G, [&](int64_t st, int32_t p0, int32_t take, int32_t) {
+              V a[UN];
+              int32_t col[UN];
+#pragma unroll
+              for (int i = 0; i < UN; i++) {
+                const int32_t p = p0 + i * G;
+                const int64_t q = st + (p < take ? p : 0);
+                a[i] = __ldcs(m.vals + q);
+                col[i] = OP == OP_SPMV ? __ldcs(m.cols + q) : 0;
+              }
+#pragma unroll
+              for (int i = 0; i < UN; i++)
+                if (p0 + i * G < take) accum_entry<V, K, OP, VEC>((double)a[i], col[i], x, ldx, acc);
+            });
+          }
+#pragma unroll
+          for (int k = 0; k < K; k++)
+            for (int o = G >> 1; o > 0; o >>= 1) acc[k] = op_comb<double, OP>(acc[k], __shfl_xor_sync(FULL, acc[k], o));
+          if (j == 0 && row >= 0 && len <= it.short_max) write_y<V, K, OP>(it.y, it.ldy, row, acc, it.alpha, it.beta, len);
+        }
       }
-      if (rb.row >= 0 && rb.len <= it.short_max) write_y<V, K, OP>(it.y, it.ldy, rb.row, acc, it.alpha, it.beta, rb.len);
     }
   }
 }
@@ -656,7 +739,7 @@ template <typename V, int PART>
 __global__ void __launch_bounds__(RS_THREADS_) k_rows_copy(RowItem<V> it, const long long *__restrict__ dst_off,
                                                            int32_t *__restrict__ out_cols, V *__restrict__ out_vals,
                                                            int32_t *__restrict__ out_rows,
-                                                           int32_t *__restrict__ out_rowptr) {
+                                                           int32_t *__restrict__ out_rowptr, int64_t limit) {
   constexpr int U = 4;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const Mat<V> &m = it.m;
@@ -709,7 +792,7 @@ __global__ void __launch_bounds__(RS_THREADS_) k_rows_copy(RowItem<V> it, const 
 #pragma unroll
         for (int g = 0; g < G; g++) {
           const int64_t p = s0 + tid + (int64_t)g * nthr;
-          if (p < c1) {
+          if (p < c1 && d + p < limit) {
             out_cols[d + p] = cv[g];
             out_vals[d + p] = vv[g];
             if (out_rows) out_rows[d + p] = row;
@@ -757,7 +840,7 @@ __global__ void __launch_bounds__(RS_THREADS_) k_rows_copy(RowItem<V> it, const 
           }
 #pragma unroll
           for (int i = 0; i < U; i++) {
-            if (jw[i] >= 0) {
+            if (jw[i] >= 0 && dst[i] < limit) {
               out_cols[dst[i]] = cv[i];
               out_vals[dst[i]] = vv[i];
               if (out_rows) out_rows[dst[i]] = (int32_t)(r0 + jw[i]);
@@ -859,7 +942,7 @@ int spmv_many(const void *items_dev, int dtype, int count, int k, bool vec, long
 
 template <typename V>
 static int launch_copy(dcsr_handle h, const long long *dst_off, int32_t *out_cols, V *out_vals, int32_t *out_rows,
-                       int32_t *out_rowptr, cudaStream_t s) {
+                       int32_t *out_rowptr, int64_t limit, cudaStream_t s) {
   static int g0 = 0, g1 = 0, g2 = 0;
   if (!g0) {
     g0 = grid_of((const void *)k_rows_copy<V, P_BLOCKS>);
@@ -867,17 +950,21 @@ static int launch_copy(dcsr_handle h, const long long *dst_off, int32_t *out_col
     g2 = grid_of((const void *)k_rows_copy<V, P_MED>);
   }
   const RowItem<V> it = row_item<V>(h, nullptr, nullptr, 0, 0, 0.0, 0.0);
-  DCSR_LAUNCH((k_rows_copy<V, P_CHUNKS>), g1, RS_THREADS_, 0, s, it, dst_off, out_cols, out_vals, out_rows, out_rowptr);
-  DCSR_LAUNCH((k_rows_copy<V, P_MED>), g2, RS_THREADS_, 0, s, it, dst_off, out_cols, out_vals, out_rows, out_rowptr);
-  DCSR_LAUNCH((k_rows_copy<V, P_BLOCKS>), g0, RS_THREADS_, 0, s, it, dst_off, out_cols, out_vals, out_rows, out_rowptr);
+  DCSR_LAUNCH((k_rows_copy<V, P_CHUNKS>), g1, RS_THREADS_, 0, s, it, dst_off, out_cols, out_vals, out_rows, out_rowptr,
+              limit);
+  DCSR_LAUNCH((k_rows_copy<V, P_MED>), g2, RS_THREADS_, 0, s, it, dst_off, out_cols, out_vals, out_rows, out_rowptr,
+              limit);
+  DCSR_LAUNCH((k_rows_copy<V, P_BLOCKS>), g0, RS_THREADS_, 0, s, it, dst_off, out_cols, out_vals, out_rows,
+              out_rowptr, limit);
   return DCSR_OK;
 }
 
 int copy_rows(dcsr_handle h, const long long *dst_off, int32_t *out_cols, void *out_vals, int32_t *out_rows,
-              int32_t *out_rowptr, cudaStream_t s) {
+              int32_t *out_rowptr, cudaStream_t s, int64_t limit) {
   if (!h->bins_valid) DCSR_TRY(build_schedule(h, s));
-  if (h->dtype == DCSR_F32) return launch_copy<float>(h, dst_off, out_cols, (float *)out_vals, out_rows, out_rowptr, s);
-  return launch_copy<double>(h, dst_off, out_cols, (double *)out_vals, out_rows, out_rowptr, s);
+  if (h->dtype == DCSR_F32)
+    return launch_copy<float>(h, dst_off, out_cols, (float *)out_vals, out_rows, out_rowptr, limit, s);
+  return launch_copy<double>(h, dst_off, out_cols, (double *)out_vals, out_rows, out_rowptr, limit, s);
 }
 
 }  // namespace dcsr

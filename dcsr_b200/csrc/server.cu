@@ -40,7 +40,8 @@ struct Req {
   Clock::time_point t_submit, t_launch;
   int64_t cost = 0;
   size_t off[3] = {0, 0, 0};  // staging offsets: update rows/cols/vals | spmv x/y | export rp/cols/vals
-  int item = -1;              // batch item of its matrix (update / SpMV)
+  int item = -1;              // batch item of its matrix (update / SpMV), export number (export)
+  bool direct = false;        // export written straight into the caller's device buffers
   int32_t status = DCSR_OK;
   int64_t nnz = 0;
 };
@@ -57,8 +58,11 @@ struct Slot {
   unsigned char *stage = nullptr;
   long long *status_host = nullptr;
   int status_cap = 0;
+  int32_t *nnz_host = nullptr;  // pinned: entry count of each export
+  int nnz_cap = 0;
   int64_t cost = 0;
   bool statuses = false;
+  int phase = 0;  // 1: batch in flight; 2: exports' entries being copied out
 };
 
 }  // namespace
@@ -130,21 +134,20 @@ void publish(dcsr_server s, std::vector<Req> &reqs, int batch_size) {
   s->cv_done.notify_all();
 }
 
-// Form a batch from the queue (caller holds the lock).
+// Form a batch from the queue (caller holds the lock).  Requests are taken
+// in arrival order; the scan stops when the batch is full, at the first
+// request that does not fit the memory budget, or after a bounded number of
+// skipped requests; skipped ones go back to the front in their order.
 void form(dcsr_server s, std::vector<Req> &take) {
   const int maxb = s->o.plain ? 1 : s->o.max_batch;
+  const size_t max_skip = 4 * (size_t)maxb + 1024;
   s->gen++;
   int64_t room = s->budget - s->in_use;
-  std::deque<Req> rest;
-  bool full = false;
-  while (!s->queue.empty()) {
+  std::vector<Req> skipped;
+  while (!s->queue.empty() && (int)take.size() < maxb && skipped.size() < max_skip) {
     Req q = std::move(s->queue.front());
     s->queue.pop_front();
     const int m = q.r.matrix;
-    if (full) {
-      rest.push_back(std::move(q));
-      continue;
-    }
     if (s->stamp[m] != s->gen) {
       s->stamp[m] = s->gen;
       s->state[m] = s->busy[m] ? -1 : 0;
@@ -155,7 +158,7 @@ void form(dcsr_server s, std::vector<Req> &take) {
     const bool fits_order = st >= 0 && kind > st && !(kind == 3 && st != 0) && !(st == 3);
     if (!fits_order) {
       st = -1;  // every later request of this matrix waits too
-      rest.push_back(std::move(q));
+      skipped.push_back(std::move(q));
       continue;
     }
     if (q.cost > room) {
@@ -168,16 +171,14 @@ void form(dcsr_server s, std::vector<Req> &take) {
         s->mu.lock();
         continue;
       }
-      full = true;  // FIFO admission: later requests wait for memory too
-      rest.push_back(std::move(q));
-      continue;
+      skipped.push_back(std::move(q));  // FIFO admission: later requests wait for memory too
+      break;
     }
     st = kind;
     room -= q.cost;
     take.push_back(std::move(q));
-    if ((int)take.size() >= maxb) full = true;
   }
-  s->queue.swap(rest);
+  for (auto it = skipped.rbegin(); it != skipped.rend(); ++it) s->queue.push_front(std::move(*it));
 }
 
 int launch(dcsr_server s, Slot &sl, std::vector<Req> &take) {
@@ -190,8 +191,11 @@ int launch(dcsr_server s, Slot &sl, std::vector<Req> &take) {
   sl.item_spmv.clear();
   sl.cost = 0;
   sl.statuses = false;
-  // staging layout
+  // staging layout: host inputs of updates and SpMVs, every export's output
+  // (exports are staged even to device buffers: the entry count is only
+  // known on the device, so the caller's buffer is filled by a bounded copy)
   size_t bytes = 0;
+  int n_exp = 0;
   std::unordered_map<int, int> item_of;
   for (size_t i = 0; i < sl.reqs.size(); i++) {
     Req &q = sl.reqs[i];
@@ -199,25 +203,30 @@ int launch(dcsr_server s, Slot &sl, std::vector<Req> &take) {
     sl.cost += q.cost;
     dcsr_handle h = s->mats[q.r.matrix];
     const size_t vs = vs_of(h);
-    if (q.r.kind == DCSR_REQ_UPDATE) {
+    if (q.r.kind == DCSR_REQ_UPDATE && !q.r.on_device) {
       q.off[0] = bytes;
       bytes = al256(bytes + 4 * q.r.nnz);
       q.off[1] = bytes;
       bytes = al256(bytes + 4 * q.r.nnz);
       q.off[2] = bytes;
       bytes = al256(bytes + vs * q.r.nnz);
-    } else if (q.r.kind == DCSR_REQ_SPMV) {
+    } else if (q.r.kind == DCSR_REQ_SPMV && !q.r.on_device) {
       q.off[0] = bytes;
       bytes = al256(bytes + vs * q.r.k * h->n_cols);
       q.off[1] = bytes;
       bytes = al256(bytes + vs * q.r.k * h->n_rows);
-    } else {
-      q.off[0] = bytes;
-      bytes = al256(bytes + 4 * ((size_t)h->n_rows + 1));
-      q.off[1] = bytes;
-      bytes = al256(bytes + 4 * (size_t)h->pool_cap);
-      q.off[2] = bytes;
-      bytes = al256(bytes + vs * (size_t)h->pool_cap);
+    } else if (q.r.kind == DCSR_REQ_EXPORT) {
+      // device buffers take the export directly (bounded by cap on the device)
+      q.direct = q.r.on_device;
+      if (!q.direct) {
+        q.off[0] = bytes;
+        bytes = al256(bytes + 4 * ((size_t)h->n_rows + 1));
+        q.off[1] = bytes;
+        bytes = al256(bytes + 4 * (size_t)h->pool_cap);
+        q.off[2] = bytes;
+        bytes = al256(bytes + vs * (size_t)h->pool_cap);
+      }
+      q.item = n_exp++;
     }
     if (!item_of.count(q.r.matrix)) sl.mats.push_back(q.r.matrix);
     if (q.r.kind != DCSR_REQ_EXPORT) {
@@ -245,29 +254,46 @@ int launch(dcsr_server s, Slot &sl, std::vector<Req> &take) {
     for (int m : sl.mats) s->busy[m] = 1;
     s->batches++;
   }
+  if (n_exp > sl.nnz_cap) {
+    if (sl.nnz_host) DCSR_CUDA(cudaFreeHost(sl.nnz_host));
+    sl.nnz_host = nullptr;
+    DCSR_CUDA(cudaMallocHost((void **)&sl.nnz_host, sizeof(int32_t) * n_exp));
+    sl.nnz_cap = n_exp;
+  }
   sl.stage = nullptr;
   if (bytes) DCSR_CUDA(cudaMallocAsync((void **)&sl.stage, bytes, st));
-  // inputs host -> device, batch items over the staged buffers
+  // inputs host -> device; batch items over the staged (or the caller's device) buffers
   for (auto &q : sl.reqs) {
     dcsr_handle h = s->mats[q.r.matrix];
     const size_t vs = vs_of(h);
     unsigned char *b = sl.stage;
     if (q.r.kind == DCSR_REQ_UPDATE && q.r.nnz > 0) {
-      DCSR_CUDA(cudaMemcpyAsync(b + q.off[0], q.r.rows, 4 * q.r.nnz, cudaMemcpyHostToDevice, st));
-      DCSR_CUDA(cudaMemcpyAsync(b + q.off[1], q.r.cols, 4 * q.r.nnz, cudaMemcpyHostToDevice, st));
-      DCSR_CUDA(cudaMemcpyAsync(b + q.off[2], q.r.vals, vs * q.r.nnz, cudaMemcpyHostToDevice, st));
       dcsr_batch_item &bi = sl.items[q.item];
-      bi.rows = (const int32_t *)(b + q.off[0]);
-      bi.cols = (const int32_t *)(b + q.off[1]);
-      bi.vals = b + q.off[2];
+      if (q.r.on_device) {
+        bi.rows = q.r.rows;
+        bi.cols = q.r.cols;
+        bi.vals = q.r.vals;
+      } else {
+        DCSR_CUDA(cudaMemcpyAsync(b + q.off[0], q.r.rows, 4 * q.r.nnz, cudaMemcpyHostToDevice, st));
+        DCSR_CUDA(cudaMemcpyAsync(b + q.off[1], q.r.cols, 4 * q.r.nnz, cudaMemcpyHostToDevice, st));
+        DCSR_CUDA(cudaMemcpyAsync(b + q.off[2], q.r.vals, vs * q.r.nnz, cudaMemcpyHostToDevice, st));
+        bi.rows = (const int32_t *)(b + q.off[0]);
+        bi.cols = (const int32_t *)(b + q.off[1]);
+        bi.vals = b + q.off[2];
+      }
       bi.nnz = q.r.nnz;
     } else if (q.r.kind == DCSR_REQ_SPMV) {
-      DCSR_CUDA(cudaMemcpyAsync(b + q.off[0], q.r.x, vs * q.r.k * h->n_cols, cudaMemcpyHostToDevice, st));
-      if (q.r.beta != 0.0)
-        DCSR_CUDA(cudaMemcpyAsync(b + q.off[1], q.r.y, vs * q.r.k * h->n_rows, cudaMemcpyHostToDevice, st));
       dcsr_batch_item &bi = sl.items[q.item];
-      bi.x = b + q.off[0];
-      bi.y = b + q.off[1];
+      if (q.r.on_device) {
+        bi.x = q.r.x;
+        bi.y = q.r.y;
+      } else {
+        DCSR_CUDA(cudaMemcpyAsync(b + q.off[0], q.r.x, vs * q.r.k * h->n_cols, cudaMemcpyHostToDevice, st));
+        if (q.r.beta != 0.0)
+          DCSR_CUDA(cudaMemcpyAsync(b + q.off[1], q.r.y, vs * q.r.k * h->n_rows, cudaMemcpyHostToDevice, st));
+        bi.x = b + q.off[0];
+        bi.y = b + q.off[1];
+      }
       bi.k = q.r.k;
       bi.ldx = bi.ldy = q.r.k;
       bi.alpha = q.r.alpha;
@@ -278,15 +304,15 @@ int launch(dcsr_server s, Slot &sl, std::vector<Req> &take) {
     // the per-call path: one request, its operator, synchronously
     Req &q = sl.reqs[0];
     dcsr_handle h = s->mats[q.r.matrix];
-    unsigned char *b = sl.stage;
     if (q.r.kind == DCSR_REQ_UPDATE) {
-      q.status = dcsr_update_sync(h, (const int32_t *)(b + q.off[0]), (const int32_t *)(b + q.off[1]), b + q.off[2],
-                                  q.r.nnz, st);
+      const dcsr_batch_item &bi = sl.items[q.item];
+      q.status = dcsr_update_sync(h, bi.rows, bi.cols, bi.vals, q.r.nnz, st);
     } else if (q.r.kind == DCSR_REQ_SPMV) {
-      DCSR_TRY(dcsr_spmv(h, b + q.off[0], q.r.k, q.r.k, b + q.off[1], q.r.k, q.r.alpha, q.r.beta, st));
+      const dcsr_batch_item &bi = sl.items[q.item];
+      DCSR_TRY(dcsr_spmv(h, bi.x, q.r.k, q.r.k, bi.y, q.r.k, q.r.alpha, q.r.beta, st));
     }
   } else if (!sl.items.empty()) {
-    DCSR_TRY(sl.core.plan(sl.items.data(), (int)sl.items.size(), st));
+    DCSR_TRY(sl.core.plan(sl.items.data(), (int)sl.items.size(), st, false));
     DCSR_TRY(sl.core.upload(st, false, true));
     DCSR_TRY(sl.core.reserve_scratch(st));
     DCSR_TRY(sl.core.enqueue(st));
@@ -304,29 +330,51 @@ int launch(dcsr_server s, Slot &sl, std::vector<Req> &take) {
     }
     sl.core.mark_scheduled();
   }
-  // exports, then results device -> host
+  // exports, then results to the caller
   for (auto &q : sl.reqs) {
     dcsr_handle h = s->mats[q.r.matrix];
     const size_t vs = vs_of(h);
     unsigned char *b = sl.stage;
-    if (q.r.kind == DCSR_REQ_SPMV) {
+    if (q.r.kind == DCSR_REQ_SPMV && !q.r.on_device) {
       DCSR_CUDA(cudaMemcpyAsync(q.r.y, b + q.off[1], vs * q.r.k * h->n_rows, cudaMemcpyDeviceToHost, st));
     } else if (q.r.kind == DCSR_REQ_EXPORT) {
-      DCSR_TRY(dcsr_to_csr(h, (int32_t *)(b + q.off[0]), (int32_t *)(b + q.off[1]), b + q.off[2], st));
-      const int64_t n_copy = q.r.cap < h->pool_cap ? q.r.cap : h->pool_cap;
-      DCSR_CUDA(cudaMemcpyAsync(q.r.row_ptr, b + q.off[0], 4 * ((size_t)h->n_rows + 1), cudaMemcpyDeviceToHost, st));
-      if (n_copy > 0) {
-        DCSR_CUDA(cudaMemcpyAsync(q.r.out_cols, b + q.off[1], 4 * n_copy, cudaMemcpyDeviceToHost, st));
-        DCSR_CUDA(cudaMemcpyAsync(q.r.out_vals, b + q.off[2], vs * n_copy, cudaMemcpyDeviceToHost, st));
-      }
+      int32_t *rp = q.direct ? q.r.row_ptr : (int32_t *)(b + q.off[0]);
+      int32_t *oc = q.direct ? q.r.out_cols : (int32_t *)(b + q.off[1]);
+      void *ov = q.direct ? q.r.out_vals : b + q.off[2];
+      DCSR_TRY(export_csr(h, rp, oc, ov, q.direct ? q.r.cap : INT64_MAX, st));
+      DCSR_CUDA(cudaMemcpyAsync(sl.nnz_host + q.item, rp + h->n_rows, 4, cudaMemcpyDeviceToHost, st));
+      // a staged export's row pointer now; its entries once their count is known
+      if (!q.direct)
+        DCSR_CUDA(cudaMemcpyAsync(q.r.row_ptr, rp, 4 * ((size_t)h->n_rows + 1), cudaMemcpyDefault, st));
     }
   }
   DCSR_CUDA(cudaEventRecord(sl.done, st));
+  sl.phase = 1;
   return DCSR_OK;
 }
 
+// Release a finished batch and publish its results.
+int finish(dcsr_server s, Slot &sl) {
+  if (sl.stage) DCSR_CUDA(cudaFreeAsync(sl.stage, sl.s));
+  sl.stage = nullptr;
+  sl.busy = false;
+  sl.phase = 0;
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->in_use -= sl.cost;
+    for (int m : sl.mats) s->busy[m] = 0;
+  }
+  publish(s, sl.reqs, (int)sl.reqs.size());
+  sl.reqs.clear();
+  return DCSR_OK;
+}
+
+// The batch's event fired.  Phase 1: repairs, pool pre-growth, export sizes;
+// staged exports then copy exactly their entries out (phase 2) before the
+// batch finishes.
 int retire(dcsr_server s, Slot &sl) {
   cudaStream_t st = sl.s;
+  if (sl.phase == 2) return finish(s, sl);
   if (sl.statuses) {
     for (size_t i = 0; i < sl.items.size(); i++) {
       const int ui = sl.item_upd[i];
@@ -344,7 +392,8 @@ int retire(dcsr_server s, Slot &sl) {
           Req &p = sl.reqs[si];
           const size_t vs = vs_of(h);
           DCSR_TRY(dcsr_spmv(h, sl.items[i].x, p.r.k, p.r.k, sl.items[i].y, p.r.k, p.r.alpha, p.r.beta, st));
-          DCSR_CUDA(cudaMemcpyAsync(p.r.y, sl.items[i].y, vs * p.r.k * h->n_rows, cudaMemcpyDeviceToHost, st));
+          if (!p.r.on_device)
+            DCSR_CUDA(cudaMemcpyAsync(p.r.y, sl.items[i].y, vs * p.r.k * h->n_rows, cudaMemcpyDeviceToHost, st));
         }
         DCSR_CUDA(cudaStreamSynchronize(st));
       } else if (h->pool_cap - need < h->pool_cap / 8) {
@@ -354,23 +403,25 @@ int retire(dcsr_server s, Slot &sl) {
       q.status = status;
     }
   }
+  bool copies = false;
   for (auto &q : sl.reqs) {
     if (q.r.kind != DCSR_REQ_EXPORT) continue;
-    dcsr_handle h = s->mats[q.r.matrix];
-    q.nnz = q.r.row_ptr[h->n_rows];
+    q.nnz = sl.nnz_host[q.item];
     if (q.nnz > q.r.cap) q.status = DCSR_BAD_ARG;
+    const int64_t n_copy = q.nnz < q.r.cap ? q.nnz : q.r.cap;
+    if (!q.direct && n_copy > 0) {
+      const size_t vs = vs_of(s->mats[q.r.matrix]);
+      DCSR_CUDA(cudaMemcpyAsync(q.r.out_cols, sl.stage + q.off[1], 4 * n_copy, cudaMemcpyDefault, st));
+      DCSR_CUDA(cudaMemcpyAsync(q.r.out_vals, sl.stage + q.off[2], vs * n_copy, cudaMemcpyDefault, st));
+      copies = true;
+    }
   }
-  if (sl.stage) DCSR_CUDA(cudaFreeAsync(sl.stage, st));
-  sl.stage = nullptr;
-  sl.busy = false;
-  {
-    std::lock_guard<std::mutex> lk(s->mu);
-    s->in_use -= sl.cost;
-    for (int m : sl.mats) s->busy[m] = 0;
+  if (copies) {
+    DCSR_CUDA(cudaEventRecord(sl.done, st));
+    sl.phase = 2;
+    return DCSR_OK;
   }
-  publish(s, sl.reqs, (int)sl.reqs.size());
-  sl.reqs.clear();
-  return DCSR_OK;
+  return finish(s, sl);
 }
 
 // A batch that could not be launched or retired: its requests fail with
@@ -378,6 +429,7 @@ int retire(dcsr_server s, Slot &sl) {
 // later request fails with it too.
 void fail_slot(dcsr_server s, Slot &sl, int status) {
   for (auto &q : sl.reqs) q.status = status;
+  sl.phase = 0;
   if (sl.busy) {
     if (sl.stage) cudaFreeAsync(sl.stage, sl.s);
     sl.stage = nullptr;
@@ -555,10 +607,38 @@ int dcsr_server_destroy(dcsr_server s) {
     if (sl.s) cudaStreamSynchronize(sl.s);
     sl.core.release();
     if (sl.status_host) cudaFreeHost(sl.status_host);
+    if (sl.nnz_host) cudaFreeHost(sl.nnz_host);
     if (sl.done) cudaEventDestroy(sl.done);
     if (sl.s) cudaStreamDestroy(sl.s);
   }
   delete s;
+  return DCSR_OK;
+}
+
+int dcsr_server_replay(dcsr_server s, const dcsr_request *requests, const double *arrival_us, int64_t count,
+                       dcsr_result *results, double *wall_us) {
+  if (!s || (count > 0 && (!requests || !arrival_us || !results))) return DCSR_BAD_ARG;
+  std::vector<uint64_t> tickets(count);
+  std::vector<double> late(count);
+  const auto t0 = Clock::now();
+  for (int64_t i = 0; i < count; i++) {
+    const auto due = t0 + std::chrono::duration_cast<Clock::duration>(std::chrono::duration<double, std::micro>(
+                              arrival_us[i]));
+    for (auto now = Clock::now(); now < due; now = Clock::now()) {
+      if (due - now > std::chrono::microseconds(200)) std::this_thread::sleep_for(due - now - std::chrono::microseconds(100));
+    }
+    late[i] = std::chrono::duration<double, std::micro>(Clock::now() - due).count();
+    DCSR_TRY(dcsr_server_submit(s, &requests[i], &tickets[i]));
+  }
+  double last = 0;
+  for (int64_t i = 0; i < count; i++) {
+    DCSR_TRY(dcsr_server_wait(s, tickets[i], -1, &results[i]));
+    results[i].queue_us += late[i];
+    results[i].latency_us += late[i];
+    const double done = arrival_us[i] + results[i].latency_us;
+    last = done > last ? done : last;
+  }
+  if (wall_us) *wall_us = last;
   return DCSR_OK;
 }
 

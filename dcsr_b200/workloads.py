@@ -170,3 +170,49 @@ def batched_matrix(spec):
     uv = rng.uniform(-1.0, 1.0, T).astype(np.float32)
     x = rng.uniform(-1.0, 1.0, (n, spec["k"])).astype(np.float32)
     return row_ptr, cols, vals, (ur, uc, uv), x
+
+
+def device_matrix(spec, dev, dtype=None):
+    """One batched/served matrix generated on the device (seeded torch
+    generator): COO (rows, cols, vals) with Poisson(degree) entries per row,
+    uniform columns (duplicate pairs are summed by a MERGE-mode load) and
+    U(-1,1) values."""
+    import torch
+    dtype = dtype or torch.float32
+    g = torch.Generator(device=dev)
+    g.manual_seed(spec["seed"])
+    n = spec["n"]
+    lens = torch.poisson(torch.full((n,), float(spec["degree"]), device=dev), generator=g).to(torch.int64)
+    lens.clamp_(max=n)
+    rows = torch.repeat_interleave(torch.arange(n, device=dev, dtype=torch.int32), lens)
+    cols = torch.randint(0, n, (rows.numel(),), device=dev, dtype=torch.int32, generator=g)
+    vals = torch.rand(rows.numel(), device=dev, dtype=dtype, generator=g) * 2 - 1
+    return rows, cols, vals
+
+
+def device_updates(spec, dev, rnd=0, dtype=None):
+    """Update batch `rnd` of a batched/served spec, on the device: uniform
+    rows and columns, U(-1,1) values."""
+    import torch
+    dtype = dtype or torch.float32
+    g = torch.Generator(device=dev)
+    g.manual_seed(spec["seed"] * 7919 + 1 + rnd)
+    n, T = spec["n"], spec["updates"]
+    r = torch.randint(0, n, (T,), device=dev, dtype=torch.int32, generator=g)
+    c = torch.randint(0, n, (T,), device=dev, dtype=torch.int32, generator=g)
+    v = torch.rand(T, device=dev, dtype=dtype, generator=g) * 2 - 1
+    return r, c, v
+
+
+def served_trace(seed: int, n_mats: int, count: int, min_upd: int = 10, max_upd: int = 100_000):
+    """Request mix of the served workload: (kind, matrix, size) with kind 0 =
+    update (40%, log-uniform [10, 100k] triples), 1 = SpMV (50%, k uniform in
+    1..8), 2 = export (10%); matrices uniform."""
+    rng = np.random.default_rng(seed)
+    u = rng.random(count)
+    kind = np.where(u < 0.4, 0, np.where(u < 0.9, 1, 2)).astype(np.int32)
+    mat = rng.integers(0, n_mats, count).astype(np.int32)
+    upd = np.exp(rng.uniform(np.log(min_upd), np.log(max_upd), count)).astype(np.int64)
+    k = rng.integers(1, 9, count).astype(np.int32)
+    size = np.where(kind == 0, upd, np.where(kind == 1, k, 0))
+    return kind, mat, size

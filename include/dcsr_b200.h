@@ -260,6 +260,8 @@ typedef struct {
   int32_t *out_cols;
   void *out_vals;
   int64_t cap;
+  /* 1: every buffer of this request is device memory (no host staging) */
+  int32_t on_device;
 } dcsr_request;
 
 typedef struct {
@@ -284,6 +286,13 @@ int dcsr_server_wait(dcsr_server s, uint64_t ticket, int64_t timeout_us, dcsr_re
 int dcsr_server_stats(dcsr_server s, int64_t *completed, int64_t *batches, int64_t *mem_in_use);
 /* Drain the queue, stop the worker, release the server (not the matrices). */
 int dcsr_server_destroy(dcsr_server s);
+/* Load generator for measurements: submit requests[i] at arrival_us[i]
+ * microseconds after the call starts (non-decreasing), then wait for all;
+ * results[i] receives each result with its latency counted from the
+ * scheduled arrival (a late submission is not forgiven); *wall_us = the time
+ * from the start to the last completion. */
+int dcsr_server_replay(dcsr_server s, const dcsr_request *requests, const double *arrival_us, int64_t count,
+                       dcsr_result *results, double *wall_us);
 
 /* Allocation-free reduce-by-key.  No counterpart in the reference: it is
  * for callers that cannot allocate device memory at call time -- a process

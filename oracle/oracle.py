@@ -255,6 +255,15 @@ class Ref:
                                       np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")]
         L.ref_stream_step.restype = C.c_int64
         L.ref_stream_free.argtypes = [C.c_void_p]
+        f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
+        L.ref_res_create.argtypes = [C.c_int32, C.c_int32, _i32p, _i32p, f32p]
+        L.ref_res_create.restype = C.c_void_p
+        L.ref_res_update.argtypes = [C.c_void_p, _i32p, _i32p, f32p, C.c_int64]
+        L.ref_res_update.restype = C.c_int64
+        L.ref_res_spmv.argtypes = [C.c_void_p, f32p, C.c_int32, f32p]
+        L.ref_res_export.argtypes = [C.c_void_p, _i32p, _i32p, f32p]
+        L.ref_res_export.restype = C.c_int64
+        L.ref_res_free.argtypes = [C.c_void_p]
         self.L = L
 
     @staticmethod

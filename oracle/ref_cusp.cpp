@@ -226,4 +226,69 @@ int64_t ref_stream_step(void *h, const int32_t *br, const int32_t *bc, const dou
 
 void ref_stream_free(void *h) { delete (Stream<float> *)h; }
 
+// Resident FP32 CSR matrices for the served-workload baseline: each request
+// is one stock cusp operation on one matrix -- an update is cusp::add of the
+// batch (src/Fill_Test.inl:243-245), an SpMV is one cusp::multiply per
+// right-hand side (cusp's CSR SpMV takes one vector), an export is a copy of
+// the CSR arrays out of the matrix.
+void *ref_res_create(int32_t n, int32_t m, const int32_t *rp, const int32_t *ci, const float *vv) {
+  Stream<float> *s = new Stream<float>;
+  int64_t nnz = rp[n];
+  cusp::csr_matrix<int, float, HM> A(n, m, nnz);
+  for (int32_t i = 0; i <= n; i++) A.row_offsets[i] = rp[i];
+  for (int64_t j = 0; j < nnz; j++) {
+    A.column_indices[j] = ci[j];
+    A.values[j] = vv[j];
+  }
+  s->A = A;
+  s->x = cusp::array1d<float, DM>(m, 0.0f);
+  s->y = cusp::array1d<float, DM>(n, 0.0f);
+  return s;
+}
+
+int64_t ref_res_update(void *h, const int32_t *br, const int32_t *bc, const float *bv, int64_t bn) {
+  Stream<float> *s = (Stream<float> *)h;
+  int32_t n = (int32_t)s->A.num_rows, m = (int32_t)s->A.num_cols;
+  cusp::coo_matrix<int, float, HM> Bh(n, m, bn);
+  for (int64_t j = 0; j < bn; j++) {
+    Bh.row_indices[j] = br[j];
+    Bh.column_indices[j] = bc[j];
+    Bh.values[j] = bv[j];
+  }
+  cusp::coo_matrix<int, float, DM> B = Bh, Acoo = s->A, C;
+  cusp::add(Acoo, B, C);
+  s->A = C;
+  return (int64_t)s->A.num_entries;
+}
+
+// y[:, j] = A x[:, j] for j < k; x is [m x k], y is [n x k] row-major.
+void ref_res_spmv(void *h, const float *x, int32_t k, float *y) {
+  Stream<float> *s = (Stream<float> *)h;
+  int32_t n = (int32_t)s->A.num_rows, m = (int32_t)s->A.num_cols;
+  cusp::array1d<float, HM> xh(m), yh(n);
+  for (int32_t j = 0; j < k; j++) {
+    for (int32_t i = 0; i < m; i++) xh[i] = x[(int64_t)i * k + j];
+    s->x = xh;
+    cusp::multiply(s->A, s->x, s->y);
+    yh = s->y;
+    for (int32_t i = 0; i < n; i++) y[(int64_t)i * k + j] = yh[i];
+  }
+}
+
+int64_t ref_res_export(void *h, int32_t *rp, int32_t *ci, float *vv) {
+  Stream<float> *s = (Stream<float> *)h;
+  cusp::csr_matrix<int, float, HM> Ch = s->A;
+  const int64_t nnz = (int64_t)Ch.num_entries;
+  if (rp)
+    for (size_t i = 0; i < Ch.row_offsets.size(); i++) rp[i] = Ch.row_offsets[i];
+  if (ci)
+    for (int64_t j = 0; j < nnz; j++) {
+      ci[j] = Ch.column_indices[j];
+      vv[j] = Ch.values[j];
+    }
+  return nnz;
+}
+
+void ref_res_free(void *h) { delete (Stream<float> *)h; }
+
 }  // extern "C"

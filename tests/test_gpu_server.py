@@ -198,3 +198,67 @@ def test_admission_by_memory(dcsr):
     t = srv.submit_spmv(5, pinned(np.ones((64, 1), np.float32)), torch.zeros(64, 1).pin_memory())
     assert srv.wait(t, 30_000_000)["status"] == 0
     srv.close()
+
+
+def test_export_capacity_bound(dcsr):
+    """An export whose buffers are too small reports BAD_ARG with the entry
+    count and writes nothing past its capacity (device buffers are written
+    directly with a device-side bound; host buffers get exactly min(nnz, cap)
+    entries); full-size exports equal the per-call export."""
+    mats = make_mats(dcsr, 8)
+    A = mats[0]
+    rp_ref, c_ref, v_ref = A.to_csr()
+    nnz = c_ref.numel()
+    cap, guard = nnz // 2, 1000
+    srv = dcsr.DcsrServer(mats)
+    rp = torch.empty(A.n_rows + 1, dtype=torch.int32, device="cuda")
+    c = torch.full((cap + guard,), -7, dtype=torch.int32, device="cuda")
+    v = torch.full((cap + guard,), -7.0, device="cuda")
+    res = srv.wait(srv.submit_export(0, rp, c[:cap], v[:cap]))
+    assert res["status"] == dcsr.BAD_ARG and res["nnz"] == nnz
+    assert torch.equal(rp, rp_ref)
+    assert torch.equal(c[:cap], c_ref[:cap]) and torch.equal(v[:cap], v_ref[:cap])
+    assert bool((c[cap:] == -7).all()) and bool((v[cap:] == -7.0).all())
+    rph = torch.empty(A.n_rows + 1, dtype=torch.int32).pin_memory()
+    ch = torch.full((cap + guard,), -7, dtype=torch.int32).pin_memory()
+    vh = torch.full((cap + guard,), -7.0).pin_memory()
+    res = srv.wait(srv.submit_export(0, rph, ch[:cap], vh[:cap]))
+    assert res["status"] == dcsr.BAD_ARG and res["nnz"] == nnz
+    assert torch.equal(ch[:cap], c_ref[:cap].cpu()) and bool((ch[cap:] == -7).all())
+    c2 = torch.empty(nnz, dtype=torch.int32, device="cuda")
+    v2 = torch.empty(nnz, device="cuda")
+    res = srv.wait(srv.submit_export(0, rp, c2, v2))
+    assert res["status"] == 0 and torch.equal(c2, c_ref) and torch.equal(v2, v_ref)
+    srv.close()
+
+
+def test_device_requests_match_host_requests(dcsr):
+    """The same requests with device buffers and with pinned host buffers
+    give identical results."""
+    mats_h = make_mats(dcsr, 9)
+    mats_d = make_mats(dcsr, 9)
+    reqs = make_requests(10, mats_h, count=60)
+    host, _, _ = serve(dcsr, mats_h, reqs, "mix", max_batch=16)
+    srv = dcsr.DcsrServer(mats_d, max_batch=16)
+    pend = []
+    for kind, i, p in reqs:
+        A = mats_d[i]
+        if kind == "update":
+            bufs = tuple(torch.from_numpy(a).cuda() for a in p)
+            pend.append((srv.submit_update(i, *bufs), bufs))
+        elif kind == "spmv":
+            bufs = (torch.from_numpy(p[0]).cuda(), torch.from_numpy(p[1]).cuda())
+            pend.append((srv.submit_spmv(i, bufs[0], bufs[1], p[2], p[3]), bufs))
+        else:
+            bufs = (torch.empty(A.n_rows + 1, dtype=torch.int32, device="cuda"),
+                    torch.empty(p, dtype=torch.int32, device="cuda"), torch.empty(p, device="cuda"))
+            pend.append((srv.submit_export(i, *bufs), bufs))
+    for j, ((t, b), r) in enumerate(zip(pend, reqs)):
+        res = srv.wait(t)
+        out = outputs(res, tuple(x.cpu() for x in b), r)
+        for x, y in zip(out, host[j]):
+            if isinstance(x, torch.Tensor):
+                assert torch.equal(x, y), f"request {j} ({r[0]}) differs"
+            else:
+                assert x == y
+    srv.close()
