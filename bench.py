@@ -642,8 +642,8 @@ def main():
     ap.add_argument("--served-requests", type=int, default=20000)
     ap.add_argument("--plain-requests", type=int, default=3000)
     ap.add_argument("--max-batch", type=int, default=256)
-    ap.add_argument("--depth", type=int, default=2)
-    ap.add_argument("--load-fracs", type=float, nargs="+", default=[0.5, 0.7, 0.85, 0.95])
+    ap.add_argument("--depth", type=int, default=6)
+    ap.add_argument("--load-fracs", type=float, nargs="+", default=[0.3, 0.5, 0.7, 0.85, 0.95])
     ap.add_argument("--plain-fracs", type=float, nargs="+", default=[0.5, 0.7, 0.9])
     ap.add_argument("--batched-mats", type=int, default=512)
     ap.add_argument("--batched-reps", type=int, default=5)

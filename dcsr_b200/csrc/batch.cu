@@ -76,6 +76,10 @@ void fill_image(const BatchCore &b, unsigned char *img) {
       const dcsr_batch_item &it = b.items[i];
       RowItem<V> r = row_item<V>(it.matrix, it.x, it.y, it.ldx, it.ldy, it.alpha, it.beta);
       r.skip = b.skip + i;
+      r.k = it.k;
+      // x rows as 8/16-byte vectors: even k, packed rows, aligned base
+      const size_t al = it.k * sizeof(V) >= 16 ? 16 : it.k * sizeof(V);
+      r.vec = it.k > 1 && it.k % 2 == 0 && it.ldx == it.k && ((uintptr_t)it.x % al) == 0;
       gi[j] = r;
     }
   }
@@ -124,22 +128,21 @@ int BatchCore::plan(const dcsr_batch_item *its, int n, cudaStream_t s, bool all_
   T = t;
   rb = bits_for((int64_t)max_rows);
   cb = bits_for((int64_t)max_cols);
-  // SpMV groups by (k, vectorisable x)
+  // SpMV groups by k family: 1, 2, 4 (k = 3, 4) and 8 (k = 5..8); the kernel
+  // reads each item's k, so a run has at most four SpMV passes whatever the
+  // mix of k
   groups.clear();
   for (int i = 0; i < n; i++) {
     const dcsr_batch_item &it = its[i];
     if (!it.x || it.matrix->n_rows == 0) continue;
-    const size_t vs = it.matrix->vsize();
-    const size_t al = it.k * vs >= 16 ? 16 : it.k * vs;
-    const bool vec = it.k > 1 && it.k % 2 == 0 && it.ldx == it.k && ((uintptr_t)it.x % al) == 0;
+    const int gk = it.k <= 2 ? it.k : it.k <= 4 ? 4 : 8;
     int gi = -1;
     for (size_t q = 0; q < groups.size(); q++)
-      if (groups[q].k == it.k && groups[q].vec == vec) gi = (int)q;
+      if (groups[q].k == gk) gi = (int)q;
     if (gi < 0) {
       groups.emplace_back();
       gi = (int)groups.size() - 1;
-      groups[gi].k = it.k;
-      groups[gi].vec = vec;
+      groups[gi].k = gk;
     }
     groups[gi].idx.push_back(i);
   }
@@ -227,7 +230,7 @@ int BatchCore::enqueue(cudaStream_t s) {
     DCSR_TRY(schedule_many(img_dev + off_row, dtype, (int)sched.size(), R, ar, s));
   }
   for (auto &g : groups)
-    DCSR_TRY(spmv_many(img_dev + g.off, dtype, (int)g.idx.size(), g.k, g.vec, pref + g.pref_off, s));
+    DCSR_TRY(spmv_many(img_dev + g.off, dtype, (int)g.idx.size(), g.k, pref + g.pref_off, s));
   return DCSR_OK;
 }
 

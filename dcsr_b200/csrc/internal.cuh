@@ -58,15 +58,17 @@ struct RowItem {
   long long row0;             // first row of this matrix in the batch's row space
   int32_t short_max, long_min; // row classes: short <= short_max < medium <= long_min < long
   const int32_t *skip;        // batch: nonzero -> this matrix's pass is skipped (may be null)
+  int32_t k, vec;             // runtime-k passes: right-hand sides, x rows loadable as vectors
 };
 // Rebuild the schedules of `count` matrices at once (items: device
 // RowItem<V>[count] in row-space order; R = total rows).  Needs
 // schedule_scratch_bytes(R) free in the arena.
 int schedule_many(const void *items_dev, int dtype, int count, int64_t R, Arena &ar, cudaStream_t s);
 size_t schedule_scratch_bytes(int64_t R);
-// y = A x for `count` matrices that share k (items: device RowItem<V>[count]);
-// pref: device scratch of 3*(count+1) long longs.
-int spmv_many(const void *items_dev, int dtype, int count, int k, bool vec, long long *pref, cudaStream_t s);
+// y = A x for `count` matrices (items: device RowItem<V>[count]) of one k
+// family: kf = 1, 2, 4 or 8, every item's k <= kf (each item's own k / vec
+// are read by the kernel); pref: device scratch of 3*(count+1) long longs.
+int spmv_many(const void *items_dev, int dtype, int count, int k, long long *pref, cudaStream_t s);
 template <typename V>
 RowItem<V> row_item(dcsr_handle h, const void *x, void *y, int64_t ldx, int64_t ldy, double alpha, double beta);
 // Size the handle's chunk table and chunk partials (K results per chunk).
@@ -87,8 +89,7 @@ int reserve(dcsr_handle h, int64_t cap, cudaStream_t s);
 // one core can serve many batches (the server re-plans one per slot).
 struct BatchCore {
   struct Group {
-    int k = 1;
-    bool vec = false;
+    int k = 1;  // k family: 1, 2, 4 (k 3..4) or 8 (k 5..8)
     std::vector<int> idx;  // items of this group, in item order
     size_t off = 0;        // descriptor offset in the image
     size_t pref_off = 0;   // unit-prefix offset in pref

@@ -119,11 +119,41 @@ __global__ void k_scan_down(const long long *in, long long *out, int64_t n, cons
   }
 }
 
+// Small inputs: one block; coalesced loads into shared memory, each thread
+// scans 4 consecutive values, one block scan, coalesced stores.
+constexpr int SCAN_SMALL = 1024 * 4;
+__global__ void __launch_bounds__(1024) k_scan_small(const long long *in, long long *out, int64_t n,
+                                                      long long *total) {
+  __shared__ long long tile[SCAN_SMALL];
+  for (int i = threadIdx.x; i < SCAN_SMALL; i += 1024) tile[i] = i < n ? in[i] : 0;
+  __syncthreads();
+  long long loc[4], sum = 0;
+#pragma unroll
+  for (int j = 0; j < 4; j++) {
+    loc[j] = tile[threadIdx.x * 4 + j];
+    sum += loc[j];
+  }
+  long long bt;
+  long long ex = block_excl_scan(sum, &bt);
+#pragma unroll
+  for (int j = 0; j < 4; j++) {
+    tile[threadIdx.x * 4 + j] = ex;
+    ex += loc[j];
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < n; i += 1024) out[i] = tile[i];
+  if (threadIdx.x == 0 && total) *total = bt;
+}
+
 size_t scan_scratch_bytes(int64_t n) { return arena_bytes(div_up(n, SCAN_TILE) + 1, 8); }
 
 int scan_i64(const long long *in, long long *out, int64_t n, long long *total, Arena &ar, cudaStream_t s) {
   if (n <= 0) {
     if (total) DCSR_CUDA(cudaMemsetAsync(total, 0, sizeof(long long), s));
+    return DCSR_OK;
+  }
+  if (n <= SCAN_SMALL) {
+    DCSR_LAUNCH(k_scan_small, 1, 1024, 0, s, in, out, n, total);
     return DCSR_OK;
   }
   int64_t nt = div_up(n, SCAN_TILE);
@@ -146,9 +176,9 @@ int scan_i64(const long long *in, long long *out, int64_t n, long long *total, A
 
 constexpr int RS_THREADS = 256;
 constexpr int RS_WARPS = RS_THREADS / 32;
-constexpr int RS_ITEMS = 16;  // per lane
-constexpr int RS_TILE = RS_THREADS * RS_ITEMS;
 constexpr int RS_BINS = 256;
+// items per lane: 16 for large inputs, 4 below RS_MID items (more, shorter tiles)
+constexpr int64_t RS_MID = 1 << 18;
 
 __device__ __forceinline__ unsigned lanemask_lt() {
   unsigned m;
@@ -156,8 +186,10 @@ __device__ __forceinline__ unsigned lanemask_lt() {
   return m;
 }
 
+template <int RS_ITEMS>
 __global__ void __launch_bounds__(RS_THREADS) k_radix_hist(const unsigned long long *keys, int64_t n, int shift,
                                                             long long *ghist, int64_t ntiles) {
+  constexpr int RS_TILE = RS_THREADS * RS_ITEMS;
   __shared__ unsigned h[RS_BINS];
   h[threadIdx.x] = 0;
   __syncthreads();
@@ -174,10 +206,12 @@ __global__ void __launch_bounds__(RS_THREADS) k_radix_hist(const unsigned long l
   ghist[(int64_t)threadIdx.x * ntiles + blockIdx.x] = h[threadIdx.x];
 }
 
+template <int RS_ITEMS>
 __global__ void __launch_bounds__(RS_THREADS) k_radix_scatter(const unsigned long long *keys, const unsigned *vals,
                                                                unsigned long long *keys_out, unsigned *vals_out,
                                                                int64_t n, int shift, const long long *goff,
                                                                int64_t ntiles) {
+  constexpr int RS_TILE = RS_THREADS * RS_ITEMS;
   __shared__ unsigned wcnt[RS_WARPS][RS_BINS];
   __shared__ long long boff[RS_BINS];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -222,24 +256,111 @@ __global__ void __launch_bounds__(RS_THREADS) k_radix_scatter(const unsigned lon
   }
 }
 
+// Small inputs (n <= RS_SMALL): one 1024-thread block runs every pass in
+// shared memory on (key, 16-bit input index) pairs -- per pass a digit
+// histogram, its scan, and a stable scatter in rounds of 1024 consecutive
+// items (warp ranks from match_any, warps ordered by a per-digit prefix) --
+// then gathers the values by index.  Same order as the multi-block sort.
+constexpr int RS_SMALL = 8192;
+constexpr size_t RS_SMALL_SMEM = (size_t)RS_SMALL * (2 * 8 + 2 * 2) + 32 * RS_BINS * 4 + 2 * RS_BINS * 4;
+
+__global__ void __launch_bounds__(1024) k_radix_small(const unsigned long long *keys, const unsigned *vals,
+                                                       unsigned long long *keys_out, unsigned *vals_out, int n,
+                                                       int bits) {
+  extern __shared__ __align__(16) unsigned char sm[];
+  unsigned long long *ka = (unsigned long long *)sm;
+  unsigned long long *kb = ka + RS_SMALL;
+  unsigned short *ia = (unsigned short *)(kb + RS_SMALL);
+  unsigned short *ib = ia + RS_SMALL;
+  unsigned *wc = (unsigned *)(ib + RS_SMALL);  // [32][256]
+  unsigned *base = wc + 32 * RS_BINS;          // running digit offsets
+  unsigned *rtot = base + RS_BINS;             // this round's digit totals
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const unsigned lt = lanemask_lt();
+  for (int i = tid; i < n; i += 1024) {
+    ka[i] = keys[i];
+    ia[i] = (unsigned short)i;
+  }
+  for (int shift = 0; shift < bits; shift += 8) {
+    if (tid < RS_BINS) base[tid] = 0;
+    __syncthreads();
+    for (int i = tid; i < n; i += 1024) atomicAdd(&base[(unsigned)(ka[i] >> shift) & 0xff], 1u);
+    __syncthreads();
+    if (warp == 0) {  // exclusive scan of the 256 digit counts (8 per lane)
+      unsigned v[8], t = 0;
+#pragma unroll
+      for (int j = 0; j < 8; j++) {
+        v[j] = base[lane * 8 + j];
+        t += v[j];
+      }
+      unsigned ex = warp_incl_scan(t) - t;
+#pragma unroll
+      for (int j = 0; j < 8; j++) {
+        base[lane * 8 + j] = ex;
+        ex += v[j];
+      }
+    }
+    __syncthreads();
+    for (int r0 = 0; r0 < n; r0 += 1024) {
+      const int i = r0 + tid;
+      for (int q = tid; q < 32 * RS_BINS; q += 1024) wc[q] = 0;
+      __syncthreads();
+      const unsigned long long k = i < n ? ka[i] : 0ull;
+      const unsigned d = i < n ? (unsigned)(k >> shift) & 0xff : 0x100u;
+      const unsigned peers = __match_any_sync(FULL, d);
+      const unsigned rank = __popc(peers & lt);
+      if (d < 0x100u && (__ffs(peers) - 1) == lane) wc[warp * RS_BINS + d] = __popc(peers);
+      __syncthreads();
+      if (tid < RS_BINS) {  // prefix across warps for digit tid
+        unsigned run = 0;
+        for (int w = 0; w < 32; w++) {
+          const unsigned c = wc[w * RS_BINS + tid];
+          wc[w * RS_BINS + tid] = run;
+          run += c;
+        }
+        rtot[tid] = run;
+      }
+      __syncthreads();
+      if (d < 0x100u) {
+        const unsigned pos = base[d] + wc[warp * RS_BINS + d] + rank;
+        kb[pos] = k;
+        ib[pos] = ia[i];
+      }
+      __syncthreads();
+      if (tid < RS_BINS) base[tid] += rtot[tid];
+      __syncthreads();
+    }
+    unsigned long long *tk = ka;
+    ka = kb;
+    kb = tk;
+    unsigned short *ti = ia;
+    ia = ib;
+    ib = ti;
+  }
+  for (int i = tid; i < n; i += 1024) {
+    keys_out[i] = ka[i];
+    vals_out[i] = vals[ia[i]];
+  }
+}
+
 size_t radix_scratch_bytes(int64_t n) {
-  int64_t nt = div_up(n, RS_TILE);
+  int64_t nt = div_up(n, RS_THREADS * 4);
   return arena_bytes(nt * RS_BINS, 8) + scan_scratch_bytes(nt * RS_BINS);
 }
 
-int radix_sort_pairs(unsigned long long **keys, unsigned **vals, unsigned long long **keys_tmp,
-                     unsigned **vals_tmp, int64_t n, int bits, Arena &ar, cudaStream_t s) {
-  if (n <= 1) return DCSR_OK;
-  int64_t nt = div_up(n, RS_TILE);
+template <int ITEMS>
+static int radix_passes(unsigned long long **keys, unsigned **vals, unsigned long long **keys_tmp,
+                        unsigned **vals_tmp, int64_t n, int bits, Arena &ar, cudaStream_t s) {
+  const int64_t nt = div_up(n, RS_THREADS * ITEMS);
   size_t mark = ar.used;
   long long *hist = ar.take<long long>(nt * RS_BINS);
   size_t mark2 = ar.used;
   for (int shift = 0; shift < bits; shift += 8) {
-    DCSR_LAUNCH(k_radix_hist, (unsigned)nt, RS_THREADS, 0, s, *keys, n, shift, hist, nt);
+    DCSR_LAUNCH(k_radix_hist<ITEMS>, (unsigned)nt, RS_THREADS, 0, s, *keys, n, shift, hist, nt);
     ar.used = mark2;
     DCSR_TRY(scan_i64(hist, hist, nt * RS_BINS, nullptr, ar, s));
-    DCSR_LAUNCH(k_radix_scatter, (unsigned)nt, RS_THREADS, 0, s, *keys, *vals, *keys_tmp, *vals_tmp, n, shift,
-                hist, nt);
+    DCSR_LAUNCH(k_radix_scatter<ITEMS>, (unsigned)nt, RS_THREADS, 0, s, *keys, *vals, *keys_tmp, *vals_tmp, n,
+                shift, hist, nt);
     unsigned long long *tk = *keys;
     *keys = *keys_tmp;
     *keys_tmp = tk;
@@ -249,6 +370,28 @@ int radix_sort_pairs(unsigned long long **keys, unsigned **vals, unsigned long l
   }
   ar.used = mark;
   return DCSR_OK;
+}
+
+int radix_sort_pairs(unsigned long long **keys, unsigned **vals, unsigned long long **keys_tmp,
+                     unsigned **vals_tmp, int64_t n, int bits, Arena &ar, cudaStream_t s) {
+  if (n <= 1) return DCSR_OK;
+  if (n <= RS_SMALL) {
+    static bool attr = false;
+    if (!attr) {
+      DCSR_CUDA(cudaFuncSetAttribute(k_radix_small, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)RS_SMALL_SMEM));
+      attr = true;
+    }
+    DCSR_LAUNCH(k_radix_small, 1, 1024, RS_SMALL_SMEM, s, *keys, *vals, *keys_tmp, *vals_tmp, (int)n, bits);
+    unsigned long long *tk = *keys;
+    *keys = *keys_tmp;
+    *keys_tmp = tk;
+    unsigned *tv = *vals;
+    *vals = *vals_tmp;
+    *vals_tmp = tv;
+    return DCSR_OK;
+  }
+  if (n <= RS_MID) return radix_passes<4>(keys, vals, keys_tmp, vals_tmp, n, bits, ar, s);
+  return radix_passes<16>(keys, vals, keys_tmp, vals_tmp, n, bits, ar, s);
 }
 
 // ------------------------------------------------- public segmented ops

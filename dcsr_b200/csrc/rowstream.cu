@@ -208,6 +208,8 @@ RowItem<V> row_item(dcsr_handle h, const void *x, void *y, int64_t ldx, int64_t 
   it.short_max = h->short_max;
   it.long_min = h->long_min;
   it.skip = nullptr;
+  it.k = 1;
+  it.vec = 0;
   return it;
 }
 template RowItem<float> row_item<float>(dcsr_handle, const void *, void *, int64_t, int64_t, double, double);
@@ -453,11 +455,65 @@ __device__ __forceinline__ void accum_entry(double a, int32_t c, const V *x, int
   }
 }
 
-template <typename V, int K, int OP>
-__device__ __forceinline__ void write_y(V *y, int64_t ldy, int32_t row, const double (&acc)[K], double alpha,
-                                        double beta, int32_t len) {
+// K < 0: the number of right-hand sides is a runtime value kr <= -K (one
+// launch serves matrices with different k); accumulators are sized for -K.
+template <int K>
+struct KArr {
+  static constexpr int N = K < 0 ? -K : K;
+};
+
+// acc (op) a*x for one entry, k from the template (K > 0) or the item (K < 0).
+template <typename V, int K, int OP, bool VEC>
+__device__ __forceinline__ void accum_k(double a, int32_t c, const V *x, int64_t ldx, int kr, bool vec,
+                                        double (&acc)[KArr<K>::N]) {
+  constexpr int N = KArr<K>::N;
+  if constexpr (K > 0) {
+    accum_entry<V, K, OP, VEC>(a, c, x, ldx, acc);
+  } else if constexpr (OP == OP_SPMV) {
+    const V *xr = x + (int64_t)c * ldx;
+    double xv[N];
+    if (vec && kr == N && N % (16 / (int)sizeof(V)) == 0) {  // whole 16-byte vectors
 #pragma unroll
-  for (int k = 0; k < K; k++) {
+      for (int q = 0; q < N; q += 16 / (int)sizeof(V)) {
+        if constexpr (sizeof(V) == 4) {
+          const float4 t = __ldg(reinterpret_cast<const float4 *>(xr) + q / 4);
+          xv[q] = t.x; xv[q + 1] = t.y; xv[q + 2] = t.z; xv[q + 3] = t.w;
+        } else {
+          const double2 t = __ldg(reinterpret_cast<const double2 *>(xr) + q / 2);
+          xv[q] = t.x; xv[q + 1] = t.y;
+        }
+      }
+    } else if (vec) {  // even kr: pairs
+#pragma unroll
+      for (int q = 0; q < N; q += 2)
+        if (q < kr) {
+          if constexpr (sizeof(V) == 4) {
+            const float2 t = __ldg(reinterpret_cast<const float2 *>(xr) + q / 2);
+            xv[q] = t.x; xv[q + 1] = t.y;
+          } else {
+            const double2 t = __ldg(reinterpret_cast<const double2 *>(xr) + q / 2);
+            xv[q] = t.x; xv[q + 1] = t.y;
+          }
+        }
+    } else {
+#pragma unroll
+      for (int q = 0; q < N; q++)
+        if (q < kr) xv[q] = __ldg(xr + q);
+    }
+#pragma unroll
+    for (int q = 0; q < N; q++)
+      if (q < kr) acc[q] = __fma_rn(a, xv[q], acc[q]);
+  } else {
+    acc[0] = op_comb<double, OP>(acc[0], OP == OP_COUNT ? 1.0 : a);
+  }
+}
+
+template <typename V, int K, int OP>
+__device__ __forceinline__ void write_y(V *y, int64_t ldy, int32_t row, const double (&acc)[KArr<K>::N],
+                                        double alpha, double beta, int32_t len, int kr) {
+#pragma unroll
+  for (int k = 0; k < KArr<K>::N; k++) {
+    if (K < 0 && k >= kr) break;
     double v = acc[k];
     if ((OP == OP_MAX || OP == OP_MIN) && len == 0) v = 0.0;
     if (OP == OP_SPMV) {
@@ -472,7 +528,8 @@ __device__ __forceinline__ void write_y(V *y, int64_t ldy, int32_t row, const do
 
 template <typename V, int K, int OP, bool VEC, int PART, typename Src>
 __global__ void __launch_bounds__(RS_THREADS_) k_rows_reduce(Src src) {
-  __shared__ double red[RS_WARPS][K];
+  constexpr int KA = KArr<K>::N;
+  __shared__ double red[RS_WARPS][KA];
   __shared__ int last_flag;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int64_t units = src.units(PART);
@@ -483,6 +540,8 @@ __global__ void __launch_bounds__(RS_THREADS_) k_rows_reduce(Src src) {
     const Mat<V> &m = it.m;
     const V *__restrict__ x = it.x;
     const int64_t ldx = it.ldx;
+    const int kr = K < 0 ? it.k : K;
+    const bool vec = K < 0 ? it.vec != 0 : VEC;
     if constexpr (PART == P_CHUNKS) {
       // ---- one chunk of a long row, whole CTA
       const int64_t li = it.chunk_li[lu];
@@ -492,11 +551,11 @@ __global__ void __launch_bounds__(RS_THREADS_) k_rows_reduce(Src src) {
       const int64_t L = m.row_sizes[row];
       const Chain ch = load_chain(m, row);
       const int64_t c0 = chunk * CHUNK, c1 = c0 + CHUNK < L ? c0 + CHUNK : L;
-      double acc[K];
+      double acc[KA];
 #pragma unroll
-      for (int k = 0; k < K; k++) acc[k] = op_init<double, OP>();
+      for (int k = 0; k < KA; k++) acc[k] = op_init<double, OP>();
       const bool fast = ch.cp[0] >= c1;  // chunk inside layer 0
-      if (fast && sizeof(V) == 4 && ((ch.st[0] + c0) & 3) == 0) {
+      if (K > 0 && fast && sizeof(V) == 4 && ((ch.st[0] + c0) & 3) == 0) {
         constexpr int G = STEP / 4 / RS_THREADS_;
         for (int64_t s0 = c0; s0 < c1; s0 += STEP) {
           const int64_t s1 = s0 + STEP < c1 ? s0 + STEP : c1;
@@ -515,25 +574,26 @@ __global__ void __launch_bounds__(RS_THREADS_) k_rows_reduce(Src src) {
 #pragma unroll
           for (int g = 0; g < G; g++) {
             if (threadIdx.x + g * RS_THREADS_ < nv) {
-              accum_entry<V, K, OP, VEC>(a4[g].x, c4[g].x, x, ldx, acc);
-              accum_entry<V, K, OP, VEC>(a4[g].y, c4[g].y, x, ldx, acc);
-              accum_entry<V, K, OP, VEC>(a4[g].z, c4[g].z, x, ldx, acc);
-              accum_entry<V, K, OP, VEC>(a4[g].w, c4[g].w, x, ldx, acc);
+              accum_k<V, K, OP, VEC>(a4[g].x, c4[g].x, x, ldx, kr, vec, acc);
+              accum_k<V, K, OP, VEC>(a4[g].y, c4[g].y, x, ldx, kr, vec, acc);
+              accum_k<V, K, OP, VEC>(a4[g].z, c4[g].z, x, ldx, kr, vec, acc);
+              accum_k<V, K, OP, VEC>(a4[g].w, c4[g].w, x, ldx, kr, vec, acc);
             }
           }
           for (int64_t p = s0 + ((int64_t)nv << 2) + threadIdx.x; p < s1; p += RS_THREADS_)
-            accum_entry<V, K, OP, VEC>((double)__ldcs(m.vals + ch.st[0] + p),
-                                       OP == OP_SPMV ? __ldcs(m.cols + ch.st[0] + p) : 0, x, ldx, acc);
+            accum_k<V, K, OP, VEC>((double)__ldcs(m.vals + ch.st[0] + p),
+                                       OP == OP_SPMV ? __ldcs(m.cols + ch.st[0] + p) : 0, x, ldx, kr, vec, acc);
         }
       } else {
         for (int64_t p = c0 + threadIdx.x; p < c1; p += RS_THREADS_) {
           const int64_t q = fast ? (int64_t)ch.st[0] + p : ch.phys(p);
-          accum_entry<V, K, OP, VEC>((double)__ldcs(m.vals + q), OP == OP_SPMV ? __ldcs(m.cols + q) : 0, x, ldx,
+          accum_k<V, K, OP, VEC>((double)__ldcs(m.vals + q), OP == OP_SPMV ? __ldcs(m.cols + q) : 0, x, ldx, kr, vec,
                                      acc);
         }
       }
 #pragma unroll
-      for (int k = 0; k < K; k++) {
+      for (int k = 0; k < KA; k++) {
+        if (K < 0 && k >= kr) break;
         double v = acc[k];
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) v = op_comb<double, OP>(v, __shfl_xor_sync(FULL, v, o));
@@ -541,18 +601,19 @@ __global__ void __launch_bounds__(RS_THREADS_) k_rows_reduce(Src src) {
       }
       __syncthreads();
       if (threadIdx.x == 0) {
-        double t[K];
+        double t[KA];
 #pragma unroll
-        for (int k = 0; k < K; k++) {
+        for (int k = 0; k < KA; k++) {
+        if (K < 0 && k >= kr) break;
           t[k] = red[0][k];
           for (int q = 1; q < RS_WARPS; q++) t[k] = op_comb<double, OP>(t[k], red[q][k]);
         }
         if (nch == 1) {  // the whole row in one unit: no partials
-          write_y<V, K, OP>(it.y, it.ldy, row, t, it.alpha, it.beta, (int32_t)L);
+          write_y<V, K, OP>(it.y, it.ldy, row, t, it.alpha, it.beta, (int32_t)L, kr);
           last_flag = 0;
         } else {
 #pragma unroll
-          for (int k = 0; k < K; k++) it.part[(it.long_off[li] + chunk) * K + k] = t[k];
+          for (int k = 0; k < KA; k++) it.part[(it.long_off[li] + chunk) * KA + k] = t[k];
           __threadfence();
           last_flag = atomicAdd(&it.long_cnt[li], 1) == nch - 1;
         }
@@ -560,14 +621,14 @@ __global__ void __launch_bounds__(RS_THREADS_) k_rows_reduce(Src src) {
       __syncthreads();
       if (last_flag && threadIdx.x == 0) {
         __threadfence();
-        double out[K];
+        double out[KA];
 #pragma unroll
-        for (int k = 0; k < K; k++) out[k] = op_init<double, OP>();
+        for (int k = 0; k < KA; k++) out[k] = op_init<double, OP>();
         for (int64_t q = 0; q < nch; q++)
 #pragma unroll
-          for (int k = 0; k < K; k++)
-            out[k] = op_comb<double, OP>(out[k], __ldcg(it.part + (it.long_off[li] + q) * K + k));
-        write_y<V, K, OP>(it.y, it.ldy, row, out, it.alpha, it.beta, (int32_t)L);
+          for (int k = 0; k < KA; k++)
+            out[k] = op_comb<double, OP>(out[k], __ldcg(it.part + (it.long_off[li] + q) * KA + k));
+        write_y<V, K, OP>(it.y, it.ldy, row, out, it.alpha, it.beta, (int32_t)L, kr);
         it.long_cnt[li] = 0;
       }
       __syncthreads();
@@ -578,9 +639,9 @@ __global__ void __launch_bounds__(RS_THREADS_) k_rows_reduce(Src src) {
       const int32_t row = it.med_rows[mi];
       const int64_t L = m.row_sizes[row];
       const Chain ch = load_chain(m, row);
-      double acc[K];
+      double acc[KA];
 #pragma unroll
-      for (int k = 0; k < K; k++) acc[k] = op_init<double, OP>();
+      for (int k = 0; k < KA; k++) acc[k] = op_init<double, OP>();
       int64_t before = 0;
 #pragma unroll
       for (int l = 0; l < MAX_SEGS; l++) {
@@ -599,17 +660,18 @@ __global__ void __launch_bounds__(RS_THREADS_) k_rows_reduce(Src src) {
             }
 #pragma unroll
             for (int i = 0; i < 4; i++)
-              if (b0 + 32 * i + lane < take) accum_entry<V, K, OP, VEC>(a[i], col[i], x, ldx, acc);
+              if (b0 + 32 * i + lane < take) accum_k<V, K, OP, VEC>(a[i], col[i], x, ldx, kr, vec, acc);
           }
           before += ch.cp[l];
         }
       }
 #pragma unroll
-      for (int k = 0; k < K; k++) {
+      for (int k = 0; k < KA; k++) {
+        if (K < 0 && k >= kr) break;
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) acc[k] = op_comb<double, OP>(acc[k], __shfl_xor_sync(FULL, acc[k], o));
       }
-      if (lane == 0) write_y<V, K, OP>(it.y, it.ldy, row, acc, it.alpha, it.beta, (int32_t)L);
+      if (lane == 0) write_y<V, K, OP>(it.y, it.ldy, row, acc, it.alpha, it.beta, (int32_t)L, kr);
     } else {
       // ---- short rows: a warp takes 32 consecutive rows
       const int64_t blk = lu * RS_WARPS + w;
@@ -619,9 +681,9 @@ __global__ void __launch_bounds__(RS_THREADS_) k_rows_reduce(Src src) {
         using P = typename std::conditional<sizeof(V) == 4, float, double>::type;  // window partials
         constexpr int U = 4;
         const RowBlock rb = load_block(m, blk * 32, lane, it.short_max);
-        double acc[K];
+        double acc[KA];
 #pragma unroll
-        for (int k = 0; k < K; k++) acc[k] = op_init<double, OP>();
+        for (int k = 0; k < KA; k++) acc[k] = op_init<double, OP>();
         int64_t cum = 0;  // capacity of this lane's row in the layers before l
         for (int l = 0; l < m.max_segs; l++) {
           int32_t len_l, st_l;
@@ -672,7 +734,8 @@ __global__ void __launch_bounds__(RS_THREADS_) k_rows_reduce(Src src) {
               for (int d = 1; d < 32; d <<= 1) {
                 const bool same = lane >= d && ((Mw[i] >> (lane - d + 1)) & ((1u << d) - 1u)) == 0;
 #pragma unroll
-                for (int k = 0; k < K; k++) {
+                for (int k = 0; k < KA; k++) {
+        if (K < 0 && k >= kr) break;
                   const P co = __shfl_up_sync(FULL, c[k], d);
                   if (same) c[k] = op_comb<P, OP>(c[k], co);
                 }
@@ -682,14 +745,15 @@ __global__ void __launch_bounds__(RS_THREADS_) k_rows_reduce(Src src) {
               const bool hit = len_l > 0 && excl < w0 + 32 && incl > w0;
               const int tail = (incl < w0 + 32 ? incl : w0 + 32) - 1 - w0;
 #pragma unroll
-              for (int k = 0; k < K; k++) {
+              for (int k = 0; k < KA; k++) {
+        if (K < 0 && k >= kr) break;
                 const P got = __shfl_sync(FULL, c[k], hit ? tail : 0);
                 if (hit) acc[k] = op_comb<double, OP>(acc[k], (double)got);
               }
             }
           }
         }
-        if (rb.row >= 0 && rb.len <= it.short_max) write_y<V, K, OP>(it.y, it.ldy, rb.row, acc, it.alpha, it.beta, rb.len);
+        if (rb.row >= 0 && rb.len <= it.short_max) write_y<V, K, OP>(it.y, it.ldy, rb.row, acc, it.alpha, it.beta, rb.len, kr);
       } else {
         // K values per entry: G lanes per row
         const RowBlock rb = load_block(m, blk * 32, lane, it.short_max);
@@ -701,11 +765,11 @@ __global__ void __launch_bounds__(RS_THREADS_) k_rows_reduce(Src src) {
           const int32_t row = __shfl_sync(FULL, rb.row, owner);
           const int32_t len = __shfl_sync(FULL, rb.len, owner);
           const Chain ch = shfl_chain(own, owner);
-          double acc[K];
+          double acc[KA];
 #pragma unroll
-          for (int k = 0; k < K; k++) acc[k] = op_init<double, OP>();
+          for (int k = 0; k < KA; k++) acc[k] = op_init<double, OP>();
           if (row >= 0 && len > 0 && len <= it.short_max) {
-            constexpr int UN = K <= 2 ? 8 : 4;  // entries in flight per lane
+            constexpr int UN = KArr<K>::N <= 2 ? 8 : 4;  // entries in flight per lane
             for_row_entries<UN>(ch, len, j, G, [&](int64_t st, int32_t p0, int32_t take, int32_t) {
               V a[UN];
               int32_t col[UN];
@@ -718,13 +782,15 @@ __global__ void __launch_bounds__(RS_THREADS_) k_rows_reduce(Src src) {
               }
 #pragma unroll
               for (int i = 0; i < UN; i++)
-                if (p0 + i * G < take) accum_entry<V, K, OP, VEC>((double)a[i], col[i], x, ldx, acc);
+                if (p0 + i * G < take) accum_k<V, K, OP, VEC>((double)a[i], col[i], x, ldx, kr, vec, acc);
             });
           }
 #pragma unroll
-          for (int k = 0; k < K; k++)
+          for (int k = 0; k < KA; k++) {
+            if (K < 0 && k >= kr) break;
             for (int o = G >> 1; o > 0; o >>= 1) acc[k] = op_comb<double, OP>(acc[k], __shfl_xor_sync(FULL, acc[k], o));
-          if (j == 0 && row >= 0 && len <= it.short_max) write_y<V, K, OP>(it.y, it.ldy, row, acc, it.alpha, it.beta, len);
+          }
+          if (j == 0 && row >= 0 && len <= it.short_max) write_y<V, K, OP>(it.y, it.ldy, row, acc, it.alpha, it.beta, len, kr);
         }
       }
     }
@@ -911,33 +977,25 @@ static int reduce_dispatch(dcsr_handle h, int32_t op, V *y, cudaStream_t s) {
   return DCSR_BAD_ARG;
 }
 
-// Batched SpMV over matrices that share k.
-template <typename V, int K, bool VEC>
-static int spmv_many_k(const RowItem<V> *its, int count, long long *pref, cudaStream_t s) {
+// Batched SpMV over a set of matrices of one k family: kf = 1 (k = 1,
+// streamed short rows), 2, 4 or 8 (each item's k <= kf, read by the kernel).
+template <typename V>
+static int spmv_many_t(const RowItem<V> *its, int count, int kf, long long *pref, cudaStream_t s) {
   DCSR_LAUNCH(k_unit_prefix<V>, 1, 1024, 0, s, its, count, pref);
   RowMany<V> src{its, count, pref};
-  return launch_reduce_src<V, K, OP_SPMV, VEC>(src, s);
-}
-
-template <typename V>
-static int spmv_many_t(const RowItem<V> *its, int count, int k, bool vec, long long *pref, cudaStream_t s) {
-  switch (k) {
-    case 1: return spmv_many_k<V, 1, false>(its, count, pref, s);
-    case 2: return vec ? spmv_many_k<V, 2, true>(its, count, pref, s) : spmv_many_k<V, 2, false>(its, count, pref, s);
-    case 3: return spmv_many_k<V, 3, false>(its, count, pref, s);
-    case 4: return vec ? spmv_many_k<V, 4, true>(its, count, pref, s) : spmv_many_k<V, 4, false>(its, count, pref, s);
-    case 5: return spmv_many_k<V, 5, false>(its, count, pref, s);
-    case 6: return vec ? spmv_many_k<V, 6, true>(its, count, pref, s) : spmv_many_k<V, 6, false>(its, count, pref, s);
-    case 7: return spmv_many_k<V, 7, false>(its, count, pref, s);
-    case 8: return vec ? spmv_many_k<V, 8, true>(its, count, pref, s) : spmv_many_k<V, 8, false>(its, count, pref, s);
+  switch (kf) {
+    case 1: return launch_reduce_src<V, 1, OP_SPMV, false>(src, s);
+    case 2: return launch_reduce_src<V, -2, OP_SPMV, false>(src, s);
+    case 4: return launch_reduce_src<V, -4, OP_SPMV, false>(src, s);
+    case 8: return launch_reduce_src<V, -8, OP_SPMV, false>(src, s);
   }
   return DCSR_BAD_ARG;
 }
 
-int spmv_many(const void *items_dev, int dtype, int count, int k, bool vec, long long *pref, cudaStream_t s) {
+int spmv_many(const void *items_dev, int dtype, int count, int k, long long *pref, cudaStream_t s) {
   if (count == 0) return DCSR_OK;
-  if (dtype == DCSR_F32) return spmv_many_t<float>((const RowItem<float> *)items_dev, count, k, vec, pref, s);
-  return spmv_many_t<double>((const RowItem<double> *)items_dev, count, k, vec, pref, s);
+  if (dtype == DCSR_F32) return spmv_many_t<float>((const RowItem<float> *)items_dev, count, k, pref, s);
+  return spmv_many_t<double>((const RowItem<double> *)items_dev, count, k, pref, s);
 }
 
 template <typename V>

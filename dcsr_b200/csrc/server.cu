@@ -22,8 +22,10 @@
 // other matrices in its launch.
 #include <chrono>
 #include <condition_variable>
+#include <cstdlib>
 #include <deque>
 #include <mutex>
+#include <string>
 #include <thread>
 #include <unordered_map>
 
@@ -63,6 +65,15 @@ struct Slot {
   int64_t cost = 0;
   bool statuses = false;
   int phase = 0;  // 1: batch in flight; 2: exports' entries being copied out
+  // tracing (DCSR_SERVER_TRACE): events around the batch's device work
+  cudaEvent_t t0 = nullptr, t1 = nullptr;
+  Clock::time_point h_start, h_launched;
+};
+
+struct TraceRow {
+  int n, upd, spmv, exp;
+  long long triples;
+  double host_us, gpu_us, turnaround_us;
 };
 
 }  // namespace
@@ -89,6 +100,8 @@ struct dcsr_server_s {
   int64_t completed = 0, batches = 0;
   int device = 0;
   int fatal = DCSR_OK;
+  std::string trace_path;  // DCSR_SERVER_TRACE: per-batch timings written at destroy
+  std::vector<TraceRow> trace;
 };
 
 namespace {
@@ -184,6 +197,8 @@ void form(dcsr_server s, std::vector<Req> &take) {
 int launch(dcsr_server s, Slot &sl, std::vector<Req> &take) {
   cudaStream_t st = sl.s;
   const auto now = Clock::now();
+  sl.h_start = now;
+  if (sl.t0) DCSR_CUDA(cudaEventRecord(sl.t0, st));
   sl.reqs.swap(take);
   sl.mats.clear();
   sl.items.clear();
@@ -348,13 +363,34 @@ int launch(dcsr_server s, Slot &sl, std::vector<Req> &take) {
         DCSR_CUDA(cudaMemcpyAsync(q.r.row_ptr, rp, 4 * ((size_t)h->n_rows + 1), cudaMemcpyDefault, st));
     }
   }
+  if (sl.t1) DCSR_CUDA(cudaEventRecord(sl.t1, st));
   DCSR_CUDA(cudaEventRecord(sl.done, st));
+  sl.h_launched = Clock::now();
   sl.phase = 1;
   return DCSR_OK;
 }
 
 // Release a finished batch and publish its results.
 int finish(dcsr_server s, Slot &sl) {
+  if (sl.t0) {
+    TraceRow t{(int)sl.reqs.size(), 0, 0, 0, 0, 0.0, 0.0, 0.0};
+    for (auto &q : sl.reqs) {
+      if (q.r.kind == DCSR_REQ_UPDATE) {
+        t.upd++;
+        t.triples += q.r.nnz;
+      } else if (q.r.kind == DCSR_REQ_SPMV) {
+        t.spmv++;
+      } else {
+        t.exp++;
+      }
+    }
+    float ms = 0;
+    cudaEventElapsedTime(&ms, sl.t0, sl.t1);
+    t.gpu_us = 1e3 * ms;
+    t.host_us = std::chrono::duration<double, std::micro>(sl.h_launched - sl.h_start).count();
+    t.turnaround_us = std::chrono::duration<double, std::micro>(Clock::now() - sl.h_start).count();
+    s->trace.push_back(t);
+  }
   if (sl.stage) DCSR_CUDA(cudaFreeAsync(sl.stage, sl.s));
   sl.stage = nullptr;
   sl.busy = false;
@@ -513,7 +549,7 @@ extern "C" {
 void dcsr_server_default_opts(dcsr_server_opts *o) {
   if (!o) return;
   o->max_batch = 256;
-  o->depth = 2;
+  o->depth = 4;
   o->mem_budget = 0;
   o->mem_reserve = 1ll << 30;
   o->plain = 0;
@@ -544,9 +580,16 @@ int dcsr_server_create(dcsr_server *out, const dcsr_handle *matrices, int32_t co
   }
   const int depth = o.plain ? 1 : o.depth;
   s->slots.resize(depth);
+  const char *tp = std::getenv("DCSR_SERVER_TRACE");
+  if (tp && *tp) s->trace_path = tp;
   for (auto &sl : s->slots) {
     if (cudaStreamCreateWithFlags(&sl.s, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming) != cudaSuccess) {
+      delete s;
+      return DCSR_CUDA_ERROR;
+    }
+    if (!s->trace_path.empty() &&
+        (cudaEventCreate(&sl.t0) != cudaSuccess || cudaEventCreate(&sl.t1) != cudaSuccess)) {
       delete s;
       return DCSR_CUDA_ERROR;
     }
@@ -603,8 +646,19 @@ int dcsr_server_destroy(dcsr_server s) {
   }
   s->cv_submit.notify_all();
   if (s->worker.joinable()) s->worker.join();
+  if (!s->trace_path.empty()) {
+    if (FILE *f = std::fopen(s->trace_path.c_str(), "w")) {
+      std::fprintf(f, "requests,updates,spmvs,exports,triples,host_launch_us,gpu_us,turnaround_us\n");
+      for (auto &t : s->trace)
+        std::fprintf(f, "%d,%d,%d,%d,%lld,%.1f,%.1f,%.1f\n", t.n, t.upd, t.spmv, t.exp, t.triples, t.host_us,
+                     t.gpu_us, t.turnaround_us);
+      std::fclose(f);
+    }
+  }
   for (auto &sl : s->slots) {
     if (sl.s) cudaStreamSynchronize(sl.s);
+    if (sl.t0) cudaEventDestroy(sl.t0);
+    if (sl.t1) cudaEventDestroy(sl.t1);
     sl.core.release();
     if (sl.status_host) cudaFreeHost(sl.status_host);
     if (sl.nnz_host) cudaFreeHost(sl.nnz_host);
