@@ -63,17 +63,22 @@ def peaks():
         return 6650.0, "fallback"
 
 
-def profiled_traffic(name):
-    """DRAM bytes per launch recorded by an ncu capture summarised under
-    profiles/ (a line `traffic_bytes_per_launch: N`), else None."""
+def profiled_traffic(name, algorithmic_bytes):
+    """DRAM bytes of one SpMV call on this workload, from the ncu summary
+    under profiles/: its measured traffic / algorithmic-bytes ratio applied to
+    this run's algorithmic bytes (the profiled matrix is smaller), else None."""
+    vals = {}
     try:
         with open(os.path.join(ROOT, "profiles", name)) as f:
             for line in f:
-                if line.strip().startswith("traffic_bytes_per_launch:"):
-                    return int(float(line.split(":", 1)[1]))
+                for key in ("traffic_bytes_per_launch:", "algorithmic_bytes_per_launch:"):
+                    if line.strip().startswith(key):
+                        vals[key] = float(line.split(":", 1)[1])
     except OSError:
-        pass
-    return None
+        return None
+    if len(vals) != 2:
+        return None
+    return int(algorithmic_bytes * vals["traffic_bytes_per_launch:"] / vals["algorithmic_bytes_per_launch:"])
 
 
 class ClockSampler:
@@ -577,6 +582,8 @@ def run_ours(args, rank, world, local_rank):
 
     stream = stream_part(args, dev, world) if not args.skip_stream else None
     batched = batched_part(args, dev) if not args.skip_batched else None
+    if args.skip_served:  # profiling runs of the other parts only
+        return {"stream": stream, "batched": batched}
     served = served_part(args, dev, rank, local_rank)
 
     # aggregate over ranks: requests of all ranks / the slowest rank's wall time
@@ -612,7 +619,7 @@ def run_ours(args, rank, world, local_rank):
     }
     if stream is not None:
         sp = stream["spmv"]
-        traffic = profiled_traffic("spmv_rmat_k1_f32.md")
+        traffic = profiled_traffic("spmv_rmat_k1_f32.md", sp["bytes"])
         out["spmv_gbs"] = sp["gbs"]
         out["roofline"] = {"kernel": "k_rows_reduce x3 (DCSR SpMV: long-row chunks, medium rows, short-row blocks; "
                                      "k=1, FP32, R-MAT 2^20 after the update stream)",
@@ -650,6 +657,7 @@ def main():
     ap.add_argument("--ref-requests", type=int, default=40)
     ap.add_argument("--skip-stream", action="store_true")
     ap.add_argument("--skip-batched", action="store_true")
+    ap.add_argument("--skip-served", action="store_true", help="profiling: no headline line")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
