@@ -208,6 +208,27 @@ def stream_part(args, dev, world):
     sb = spmv_bytes(nnz, n, n, segs)
     achieved = sb / (spmv_ms / 1e3) / 1e9
 
+    # gather ceiling: one 4-byte read of x per stored entry at the matrix's
+    # own columns in row order (its CSR export; torch.index_select, x warm in
+    # L2 as in the SpMV) -- the sector traffic the SpMV's x reads cost,
+    # whatever its kernel
+    assert L.dcsr_to_csr(h, P(out_rp), P(out_c), P(out_v), sp) == 0
+    gidx = out_c[:nnz].to(torch.int64)
+    gout = torch.empty(nnz, dtype=torch.float32, device=dev)
+    gt = []
+    for rep in range(args.spmv_reps + 3):
+        flush.fill_(float(rep))
+        x.add_(0.0)  # x back in L2 (the SpMV reads it many times, so it is warm there)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        torch.index_select(x, 0, gidx, out=gout)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        if rep >= 3:
+            gt.append(e0.elapsed_time(e1))
+    gather_ms = statistics.mean(gt)
+    del gidx, gout
+
     # the same steps through host buffers (pinned), copies inside the timed region
     hb = [tuple(torch.from_numpy(a).pin_memory() for a in b) for b in batches]
     y_h = torch.empty(n, dtype=torch.float32).pin_memory()
@@ -238,7 +259,8 @@ def stream_part(args, dev, world):
         "p99_ms": round(pct(per_step, 99), 4),
         "updates_per_s": round(world * args.steps * len(batches[0][0]) / (total_ms / 1e3), 1),
         "nnz_initial": nnz0, "nnz_final": nnz, "rows": n,
-        "spmv": {"ms": round(spmv_ms, 4), "bytes": int(sb), "gbs": round(achieved, 1)},
+        "spmv": {"ms": round(spmv_ms, 4), "bytes": int(sb), "gbs": round(achieved, 1),
+                 "gather_ceiling_ms": round(gather_ms, 4)},
     }
 
 
@@ -625,7 +647,13 @@ def run_ours(args, rank, world, local_rank):
                                      "k=1, FP32, R-MAT 2^20 after the update stream)",
                            "bound": "hbm", "achieved": sp["gbs"], "peak": hbm, "peak_kind": peak_kind, "unit": "GB/s",
                            "frac": round(sp["gbs"] / hbm, 4), "traffic": traffic, "bytes_per_launch": sp["bytes"],
-                           "avg_ms": sp["ms"]}
+                           "avg_ms": sp["ms"],
+                           "gather_ceiling": {
+                               "ms": sp["gather_ceiling_ms"],
+                               "frac": round(sp["gather_ceiling_ms"] / sp["ms"], 4),
+                               "note": "torch.index_select of x at the matrix's columns in row order (x warm in "
+                                       "L2): the sector traffic of the SpMV's x reads alone; frac = ceiling time / "
+                                       "SpMV time"}}
         out["stream"] = {k: v for k, v in stream.items() if not k.startswith("_")}
     if batched is not None:
         out["batched"] = batched

@@ -633,7 +633,7 @@ __global__ void __launch_bounds__(RS_THREADS_) k_rows_reduce(Src src) {
       }
       __syncthreads();
     } else if constexpr (PART == P_MED) {
-      // ---- one medium row per warp
+      // ---- one medium row per warp, UN loads in flight per lane
       const int64_t mi = lu * RS_WARPS + w;
       if (mi >= it.info[2]) continue;
       const int32_t row = it.med_rows[mi];
@@ -642,25 +642,26 @@ __global__ void __launch_bounds__(RS_THREADS_) k_rows_reduce(Src src) {
       double acc[KA];
 #pragma unroll
       for (int k = 0; k < KA; k++) acc[k] = op_init<double, OP>();
+      constexpr int UN = KArr<K>::N <= 2 ? 8 : 4;
       int64_t before = 0;
 #pragma unroll
       for (int l = 0; l < MAX_SEGS; l++) {
         if (l < ch.ns && before < L) {
           const int64_t take = (int64_t)ch.cp[l] < L - before ? (int64_t)ch.cp[l] : L - before;
           const int64_t st = ch.st[l];
-          for (int64_t b0 = 0; b0 < take; b0 += 32 * 4) {
-            double a[4];
-            int32_t col[4];
+          for (int64_t b0 = 0; b0 < take; b0 += 32 * UN) {
+            V a[UN];
+            int32_t col[UN];
 #pragma unroll
-            for (int i = 0; i < 4; i++) {
+            for (int i = 0; i < UN; i++) {
               const int64_t p = b0 + 32 * i + lane;
               const int64_t q = st + (p < take ? p : 0);
-              a[i] = (double)__ldcs(m.vals + q);
+              a[i] = __ldcs(m.vals + q);
               col[i] = OP == OP_SPMV ? __ldcs(m.cols + q) : 0;
             }
 #pragma unroll
-            for (int i = 0; i < 4; i++)
-              if (b0 + 32 * i + lane < take) accum_k<V, K, OP, VEC>(a[i], col[i], x, ldx, kr, vec, acc);
+            for (int i = 0; i < UN; i++)
+              if (b0 + 32 * i + lane < take) accum_k<V, K, OP, VEC>((double)a[i], col[i], x, ldx, kr, vec, acc);
           }
           before += ch.cp[l];
         }
