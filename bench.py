@@ -264,6 +264,53 @@ def stream_part(args, dev, world):
     }
 
 
+# ----------------------------------------------------------- SpGEMM part
+
+def spgemm_part(args, dev):
+    """C = A*A for the banded FP64 workload (2^17 rows, band half-width 2 +
+    8 random off-band columns per row), then 100k update triples into A and
+    C = A*A again; output entries per second, CUDA events."""
+    import torch
+    from dcsr_b200 import api
+    from dcsr_b200 import workloads as W
+
+    n, rp, cols, vals, (ur, uc, uv) = W.banded_spgemm(args.seed)
+    A = api.DcsrMatrix(n, n, torch.float64)
+    A.from_csr(torch.from_numpy(rp).to(dev), torch.from_numpy(cols).to(dev), torch.from_numpy(vals).to(dev))
+    C = api.DcsrMatrix(n, n, torch.float64)
+    stream = torch.cuda.current_stream()
+    for _ in range(2):  # warm-up
+        A.spgemm(A, C)
+    torch.cuda.synchronize()
+    times, outs = [], []
+    for rep in range(args.spgemm_reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        A.spgemm(A, C)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1))
+    nnz_c = C.nnz()
+    A.update(torch.from_numpy(ur).to(dev), torch.from_numpy(uc).to(dev), torch.from_numpy(uv).to(dev))
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    A.spgemm(A, C)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    after_ms = e0.elapsed_time(e1)
+    nnz_c2 = C.nnz()
+    ms = statistics.median(times)
+    del A, C
+    torch.cuda.synchronize()
+    return {"workload": f"C = A*A, A 2^17 x 2^17 FP64, band half-width 2 + 8 random off-band columns per row "
+                        f"({int(rp[-1])} nnz); then 100k update triples into A and C = A*A again",
+            "ms": round(ms, 3), "nnz_c": int(nnz_c), "output_nnz_per_s": round(nnz_c / (ms / 1e3), 1),
+            "after_update_ms": round(after_ms, 3), "after_update_nnz_c": int(nnz_c2),
+            "after_update_output_nnz_per_s": round(nnz_c2 / (after_ms / 1e3), 1),
+            "note": "includes the one host sync the operator makes (output size)"}
+
+
 # ----------------------------------------------------------- batched part
 
 def batched_part(args, dev):
@@ -292,6 +339,7 @@ def batched_part(args, dev):
     torch.cuda.synchronize()
     s = torch.cuda.Stream()
     batch = api.DcsrBatch(work, stream=s)
+    tuned = batch.autotune(s)  # row-class thresholds for this set (outputs untouched)
     batch.capture(s)
     T = sum(sp["updates"] for sp in specs)
 
@@ -342,6 +390,7 @@ def batched_part(args, dev):
         "workload": f"{len(specs)} matrices, rows log-uniform [1k,256k], mean degree U[4,64], FP32, "
                     f"{nnz / 1e6:.0f}M nnz; per matrix an update (log-uniform 100..100k, {T / 1e6:.2f}M triples "
                     "in all) + SpMV with k in {1,2,4,8}",
+        "autotuned_row_classes": {"short_max": tuned[0], "long_min": tuned[1], "spmv_pass_us": round(tuned[2], 1)},
         "batched_ms": round(batched_ms, 3), "plain_ms": round(plain_ms, 3),
         "speedup": round(plain_ms / batched_ms, 2),
         "batched_kernel_launches": round(batched_launches, 1), "plain_kernel_launches": round(plain_launches, 1),
@@ -603,9 +652,10 @@ def run_ours(args, rank, world, local_rank):
     hbm, peak_kind = peaks()
 
     stream = stream_part(args, dev, world) if not args.skip_stream else None
+    spgemm = spgemm_part(args, dev) if not args.skip_spgemm else None
     batched = batched_part(args, dev) if not args.skip_batched else None
     if args.skip_served:  # profiling runs of the other parts only
-        return {"stream": stream, "batched": batched}
+        return {"stream": stream, "batched": batched, "spgemm": spgemm}
     served = served_part(args, dev, rank, local_rank)
 
     # aggregate over ranks: requests of all ranks / the slowest rank's wall time
@@ -657,6 +707,8 @@ def run_ours(args, rank, world, local_rank):
         out["stream"] = {k: v for k, v in stream.items() if not k.startswith("_")}
     if batched is not None:
         out["batched"] = batched
+    if spgemm is not None:
+        out["spgemm"] = spgemm
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             out["cpu_baseline"] = reference_served_sample(args, n_req=args.ref_requests)
@@ -685,6 +737,8 @@ def main():
     ap.add_argument("--ref-requests", type=int, default=40)
     ap.add_argument("--skip-stream", action="store_true")
     ap.add_argument("--skip-batched", action="store_true")
+    ap.add_argument("--skip-spgemm", action="store_true")
+    ap.add_argument("--spgemm-reps", type=int, default=5)
     ap.add_argument("--skip-served", action="store_true", help="profiling: no headline line")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()

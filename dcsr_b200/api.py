@@ -111,6 +111,9 @@ _SIGS = {
     "dcsr_batch_status": (_i32, [_vp, _vp, _vp]),
     "dcsr_batch_repair": (_i32, [_vp, _vp, C.POINTER(_i32), _vp]),
     "dcsr_batch_destroy": (_i32, [_vp]),
+    "dcsr_batch_autotune": (_i32, [_vp, _vp, C.POINTER(_i32), C.POINTER(_i32), C.POINTER(C.c_float)]),
+    "dcsr_set_row_classes": (_i32, [_vp, _i32, _i32]),
+    "dcsr_get_row_classes": (_i32, [_vp, C.POINTER(_i32), C.POINTER(_i32)]),
     "dcsr_server_default_opts": (None, [_vp]),
     "dcsr_server_create": (_i32, [C.POINTER(_vp), _vp, _i32, _vp]),
     "dcsr_server_submit": (_i32, [_vp, _vp, C.POINTER(C.c_uint64)]),
@@ -264,6 +267,14 @@ class DcsrMatrix:
     def reserve(self, cap: int, stream=None):
         _check(lib().dcsr_reserve(self.h, cap, _stream(stream)), "dcsr_reserve")
 
+    def set_row_classes(self, short_max: int, long_min: int):
+        _check(lib().dcsr_set_row_classes(self.h, short_max, long_min), "dcsr_set_row_classes")
+
+    def row_classes(self):
+        sm, lm = _i32(), _i32()
+        _check(lib().dcsr_get_row_classes(self.h, C.byref(sm), C.byref(lm)), "dcsr_get_row_classes")
+        return sm.value, lm.value
+
     def bin_rows(self, stream=None):
         _check(lib().dcsr_bin_rows(self.h, _stream(stream)), "dcsr_bin_rows")
 
@@ -405,6 +416,14 @@ class DcsrBatch:
         st = np.zeros(self.count, dtype=np.int32)
         _check(lib().dcsr_batch_status(self.h, st.ctypes.data_as(C.c_void_p), _stream(stream)), "dcsr_batch_status")
         return st
+
+    def autotune(self, stream=None):
+        """Pick the row-class thresholds of the batch's matrices by timing
+        their SpMV passes; returns (short_max, long_min, us per run)."""
+        sm, lm, us = _i32(), _i32(), C.c_float()
+        _check(lib().dcsr_batch_autotune(self.h, _stream(stream), C.byref(sm), C.byref(lm), C.byref(us)),
+               "dcsr_batch_autotune")
+        return sm.value, lm.value, us.value
 
     def repair(self, statuses: np.ndarray, stream=None) -> int:
         st = np.ascontiguousarray(statuses, dtype=np.int32)

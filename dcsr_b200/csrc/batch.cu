@@ -392,6 +392,81 @@ int dcsr_batch_repair(dcsr_batch b, const int32_t *statuses, int32_t *repaired, 
   return DCSR_OK;
 }
 
+int dcsr_batch_autotune(dcsr_batch b, void *stream, int32_t *short_max, int32_t *long_min, float *best_us) {
+  if (!b) return DCSR_BAD_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  BatchCore &c = b->core;
+  // the batch's SpMV items without their updates, into scratch outputs
+  std::vector<dcsr_batch_item> items;
+  size_t ybytes = 0;
+  for (const auto &it : c.items)
+    if (it.x && it.matrix->n_rows > 0) ybytes += align_up((int64_t)(it.matrix->vsize() * it.k * it.matrix->n_rows), 256);
+  unsigned char *yscratch = nullptr;
+  if (ybytes) DCSR_CUDA(cudaMallocAsync((void **)&yscratch, ybytes, s));
+  size_t off = 0;
+  for (const auto &it : c.items) {
+    if (!it.x || it.matrix->n_rows == 0) continue;
+    dcsr_batch_item t = it;
+    t.rows = t.cols = nullptr;
+    t.vals = nullptr;
+    t.nnz = 0;
+    t.y = yscratch + off;
+    t.ldy = t.k;
+    t.beta = 0.0;
+    off += align_up((int64_t)(it.matrix->vsize() * it.k * it.matrix->n_rows), 256);
+    items.push_back(t);
+  }
+  int32_t best_s = c.items[0].matrix->short_max, best_l = c.items[0].matrix->long_min;
+  float best = -1.0f;
+  int st = DCSR_OK;
+  if (!items.empty()) {
+    BatchCore tmp;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    const int32_t shorts[] = {32, 64, 128};
+    const int32_t longs[] = {2048, 4096, 16384};
+    for (int32_t sm : shorts) {
+      for (int32_t lm : longs) {
+        for (auto &it : items) dcsr_set_row_classes(it.matrix, sm, lm);
+        if ((st = tmp.plan(items.data(), (int)items.size(), s, true)) != DCSR_OK) break;
+        if ((st = tmp.upload(s, true)) != DCSR_OK) break;
+        if ((st = tmp.reserve_scratch(s)) != DCSR_OK) break;
+        if ((st = tmp.enqueue(s)) != DCSR_OK) break;  // warm-up
+        float sum = 0.0f;
+        for (int rep = 0; rep < 3 && st == DCSR_OK; rep++) {
+          cudaEventRecord(e0, s);
+          st = tmp.enqueue(s);
+          cudaEventRecord(e1, s);
+          cudaEventSynchronize(e1);
+          float ms = 0.0f;
+          cudaEventElapsedTime(&ms, e0, e1);
+          sum += ms;
+        }
+        if (st != DCSR_OK) break;
+        if (best < 0.0f || sum < best) {
+          best = sum;
+          best_s = sm;
+          best_l = lm;
+        }
+      }
+      if (st != DCSR_OK) break;
+    }
+    cudaStreamSynchronize(s);
+    tmp.release();
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+  }
+  for (auto &it : c.items) dcsr_set_row_classes(it.matrix, best_s, best_l);
+  if (yscratch) cudaFreeAsync(yscratch, s);
+  DCSR_CUDA(cudaStreamSynchronize(s));
+  if (st != DCSR_OK) return st;
+  if (short_max) *short_max = best_s;
+  if (long_min) *long_min = best_l;
+  if (best_us) *best_us = best < 0.0f ? 0.0f : 1e3f * best / 3.0f;
+  return DCSR_OK;
+}
+
 int dcsr_batch_destroy(dcsr_batch b) {
   if (!b) return DCSR_BAD_ARG;
   release(b);

@@ -569,6 +569,24 @@ int dcsr_bin_rows(dcsr_handle h, void *stream) {
   return build_schedule(h, (cudaStream_t)stream);
 }
 
+int dcsr_set_row_classes(dcsr_handle h, int32_t short_max, int32_t long_min) {
+  if (!h || short_max < 1 || short_max > 256 || long_min < short_max || long_min < 256 || long_min > (1 << 20))
+    return DCSR_BAD_ARG;
+  if (h->short_max != short_max || h->long_min != long_min) {
+    h->short_max = short_max;
+    h->long_min = long_min;
+    h->bins_valid = false;  // rows change class: rebuild the schedule before the next pass
+  }
+  return DCSR_OK;
+}
+
+int dcsr_get_row_classes(dcsr_handle h, int32_t *short_max, int32_t *long_min) {
+  if (!h || !short_max || !long_min) return DCSR_BAD_ARG;
+  *short_max = h->short_max;
+  *long_min = h->long_min;
+  return DCSR_OK;
+}
+
 const char *dcsr_status_string(int st) {
   switch (st) {
     case DCSR_OK: return "OK";

@@ -149,6 +149,15 @@ int dcsr_reserve(dcsr_handle h, int64_t pool_cap, void *stream);
 /* Recompute the SpMV row bins.  Replaces device::BinRows (include/load.h:583-610);
  * bins live in the handle (no process-global __constant__ table). */
 int dcsr_bin_rows(dcsr_handle h, void *stream);
+/* Row-class thresholds of the row passes (SpMV, reductions, export): rows of
+ * at most short_max entries are streamed by 32-row blocks, rows above
+ * long_min are split into CTA chunks, the others get a warp each.  Defaults
+ * 64 / 4096; 1 <= short_max <= 256, max(short_max, 256) <= long_min <= 2^20.
+ * The classes change only the order of floating-point additions: every path
+ * (per call, batched, served) uses the handle's thresholds, so they agree
+ * bit for bit.  The reference's bins are fixed (include/sparse_update.inl:1121-1150). */
+int dcsr_set_row_classes(dcsr_handle h, int32_t short_max, int32_t long_min);
+int dcsr_get_row_classes(dcsr_handle h, int32_t *short_max, int32_t *long_min);
 
 /* ------------------------------------------------------------ operators */
 
@@ -216,6 +225,12 @@ int dcsr_batch_status(dcsr_batch b, int32_t *statuses, void *stream);
  * number of matrices repaired in *repaired (may be NULL). */
 int dcsr_batch_repair(dcsr_batch b, const int32_t *statuses, int32_t *repaired, void *stream);
 int dcsr_batch_destroy(dcsr_batch b);
+/* Autotune the row-class thresholds of the batch's matrices: time the
+ * batch's schedule rebuild + SpMV passes for a grid of candidates (outputs to
+ * scratch: the matrices' contents and the items' y are not touched), set the
+ * fastest on every matrix and return it (best_us: its time per run).
+ * Synchronises. */
+int dcsr_batch_autotune(dcsr_batch b, void *stream, int32_t *short_max, int32_t *long_min, float *best_us);
 
 /* ------------------------------------------------------------ serving */
 

@@ -222,3 +222,37 @@ def test_batch_rejects_bad_items(dcsr):
         dcsr.DcsrBatch([dict(matrix=a), dict(matrix=a)])  # a matrix twice
     with pytest.raises(dcsr.DcsrError):
         dcsr.DcsrBatch([dict(matrix=a), dict(matrix=b)])  # mixed dtypes
+
+
+def test_batch_autotune(dcsr):
+    """The autotuner picks row-class thresholds without touching the matrices
+    or the items' outputs; with the same thresholds on the per-call copies,
+    batched and per-call results stay bit-identical."""
+    rng = np.random.default_rng(15)
+    mats, refs, work = build_set(dcsr, rng, torch.float32, dcsr.MERGE)
+    y_before = [w["y"].clone() for w in work]
+    batch = dcsr.DcsrBatch(work)
+    sm, lm, us = batch.autotune()
+    assert (sm, lm) in {(a, b) for a in (32, 64, 128) for b in (2048, 4096, 16384)} and us > 0
+    torch.cuda.synchronize()
+    for w, y0, ref in zip(work, y_before, refs):
+        assert torch.equal(w["y"], y0), "autotune wrote an item's y"
+        assert w["matrix"].row_classes() == (sm, lm)
+        assert_same(w["matrix"], ref[0], "after autotune")
+        ref[0].set_row_classes(sm, lm)
+    batch.run()
+    batch.repair(batch.status())
+    for w, ref in zip(work, refs):
+        per_call(dcsr, w, ref, sync=True)
+    compare_all(work, refs, "tuned")
+    batch.close()
+
+
+def test_row_classes_api(dcsr):
+    a = dcsr.DcsrMatrix(100, 100, torch.float32)
+    assert a.row_classes() == (64, 4096)
+    a.set_row_classes(32, 512)
+    assert a.row_classes() == (32, 512)
+    for bad in ((0, 4096), (300, 4096), (64, 100), (64, 1 << 21)):
+        with pytest.raises(dcsr.DcsrError):
+            a.set_row_classes(*bad)
