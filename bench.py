@@ -18,8 +18,9 @@ served (headline)  2000 resident matrices (rows log-uniform [1k, 256k], mean
         from the first scheduled arrival to the last completion (the GPU is
         idle before and after); latency = scheduled arrival -> result visible
         to the caller.  `value` uses device-resident request buffers; `e2e`
-        repeats the same operating point with pinned host buffers (inputs copied
-        in, results copied out, inside each request).
+        applies the same rule with pinned host buffers (inputs copied in,
+        results copied out, inside each request; exports move whole matrices
+        over the host link, which bounds that mode).
 stream  the power-law update stream: R-MAT 2^20 rows, (a,b,c,d) =
         (.57,.19,.19,.05), mean degree 16, FP32; 16 batches of 1M triples with
         rows drawn by current row length; a step = dcsr_update_sync (merge,
@@ -534,27 +535,36 @@ def served_part(args, dev, rank, local_rank):
     out["plain"] = {"capacity_req_s": round(cap_p["req_s"], 1), "sweep": sweep_p,
                     "slo_point": {"load_frac": args.plain_fracs[-1], "req_s": ref_p["req_s"], "p99_ms": ref_p["p99_ms"]}}
     p99_plain = ref_p["p99_ms"]
-    # batched server
-    srv = api.DcsrServer(mats, max_batch=args.max_batch, depth=args.depth)
-    replay(api, srv, tr_dev, np.zeros(N))  # warm-up: one full pass
-    cap_s = replay(api, srv, tr_dev, np.zeros(N))
-    sweep, best, best_f = [], None, None
+    # batched server; the clock sampler starts before the warm-up pass (its
+    # start-up queries the driver, which must not fall in a measured sweep)
     sampler = ClockSampler(local_rank, "served")
     sampler.start()
-    for f in args.load_fracs:
-        launches0 = api.launch_count()
-        r = replay(api, srv, tr_dev, poisson_arrivals(f * cap_s["req_s"], N, args.seed + 9))
-        r["kernel_launches"] = api.launch_count() - launches0
-        r["offered_req_s"] = f * cap_s["req_s"]
-        sweep.append({k: round(v, 3) for k, v in r.items()})
-        if r["p99_ms"] <= p99_plain and r["errors"] == 0 and (best is None or r["req_s"] > best["req_s"]):
-            best, best_f = r, f
+
+    def sweep_at(tr):
+        """Capacity, then Poisson loads; the highest throughput whose p99 is at
+        or below the plain path's target (else the lowest-p99 point, flagged)."""
+        replay(api, srv, tr, np.zeros(N))  # warm-up: one full pass
+        cap = replay(api, srv, tr, np.zeros(N))
+        pts, best, best_f = [], None, None
+        for f in args.load_fracs:
+            launches0 = api.launch_count()
+            r = replay(api, srv, tr, poisson_arrivals(f * cap["req_s"], N, args.seed + 9))
+            r["kernel_launches"] = api.launch_count() - launches0
+            r["offered_req_s"] = f * cap["req_s"]
+            pts.append({k: round(v, 3) for k, v in r.items()})
+            if r["p99_ms"] <= p99_plain and r["errors"] == 0 and (best is None or r["req_s"] > best["req_s"]):
+                best, best_f = r, f
+        met = best is not None
+        if not met:
+            best, best_f = min(((s_, f) for s_, f in zip(pts, args.load_fracs)), key=lambda t: t[0]["p99_ms"])
+        return cap, pts, best, best_f, met
+
+    srv = api.DcsrServer(mats, max_batch=args.max_batch, depth=args.depth)
+    cap_s, sweep, best, best_f, met = sweep_at(tr_dev)
     clocks = sampler.stop()
-    met = best is not None
-    if not met:  # report the lowest load point, flagged
-        best, best_f = min(((s_, f) for s_, f in zip(sweep, args.load_fracs)), key=lambda t: t[0]["p99_ms"])
-    # the same operating point with host buffers
-    e2e = replay(api, srv, tr_host, poisson_arrivals(best_f * cap_s["req_s"], N, args.seed + 9))
+    # end to end: the same rule with pinned host buffers (inputs copied in,
+    # results copied out per request; exports move whole matrices to the host)
+    cap_h, sweep_h, e2e, e2e_f, e2e_met = sweep_at(tr_host)
     st = srv.stats()
     srv.close()
     # bytes each request of the host-buffer run moved (mean over the trace)
@@ -575,6 +585,8 @@ def served_part(args, dev, rank, local_rank):
     out["speedup_at_equal_p99"] = round(best["req_s"] / ref_p["req_s"], 2)
     out["speedup_vs_plain_capacity"] = round(best["req_s"] / cap_p["req_s"], 2)
     out["e2e"] = {k: round(v, 3) for k, v in e2e.items()}
+    out["e2e"].update({"capacity_req_s": round(cap_h["req_s"], 1), "chosen_load_frac": e2e_f,
+                       "p99_constraint_met": e2e_met, "sweep": sweep_h})
     out["e2e"]["h2d_bytes_per_request"] = int(h2d / N)
     out["e2e"]["d2h_bytes_per_request"] = int(d2h / N)
     out["launches"] = int(best["kernel_launches"])
@@ -690,6 +702,8 @@ def run_ours(args, rank, world, local_rank):
         "speedup_at_equal_p99": served["speedup_at_equal_p99"],
         "speedup_vs_plain_capacity": served["speedup_vs_plain_capacity"],
         "e2e": {"value": round(e2e_value, 3), "unit": "req/s", "p99_ms": served["e2e"]["p99_ms"],
+                "capacity_req_s": served["e2e"]["capacity_req_s"], "p99_constraint_met": served["e2e"]["p99_constraint_met"],
+                "sweep": served["e2e"]["sweep"],
                 "h2d_bytes_per_step": served["e2e"]["h2d_bytes_per_request"],
                 "d2h_bytes_per_step": served["e2e"]["d2h_bytes_per_request"],
                 "note": "a step is one request: its triples or x copied in from pinned host memory, its y or CSR "

@@ -77,8 +77,9 @@ void fill_image(const BatchCore &b, unsigned char *img) {
       RowItem<V> r = row_item<V>(it.matrix, it.x, it.y, it.ldx, it.ldy, it.alpha, it.beta);
       r.skip = b.skip + i;
       r.k = it.k;
-      // x rows as 8/16-byte vectors: even k, packed rows, aligned base
-      const size_t al = it.k * sizeof(V) >= 16 ? 16 : it.k * sizeof(V);
+      // x rows as 8/16/32-byte vectors: even k, packed rows, base aligned to
+      // the largest power of two (<= 32) dividing the row size
+      const size_t rb = it.k * sizeof(V), al = (rb & (0 - rb)) >= 32 ? 32 : (rb & (0 - rb));
       r.vec = it.k > 1 && it.k % 2 == 0 && it.ldx == it.k && ((uintptr_t)it.x % al) == 0;
       gi[j] = r;
     }
@@ -185,6 +186,26 @@ int BatchCore::plan(const dcsr_batch_item *its, int n, cudaStream_t s, bool all_
     DCSR_CUDA(cudaMallocAsync((void **)&gstat, sizeof(long long) * ST_WORDS, s));
     DCSR_CUDA(cudaMemsetAsync(gstat, 0, sizeof(long long) * ST_WORDS, s));
   }
+  return DCSR_OK;
+}
+
+int BatchCore::reserve_items(int n, int dt, cudaStream_t s) {
+  // BatchItem + schedule RowItem + SpMV RowItem per item, 256-byte section
+  // padding for the (at most 6) sections
+  const size_t bytes = align_up((int64_t)(n * (desc_size(dt, false) + 2 * desc_size(dt, true)) + 6 * 256), 256);
+  if (bytes > img_cap) {
+    if (img_host) DCSR_CUDA(cudaFreeHost(img_host));
+    img_host = nullptr;
+    DCSR_TRY(grow_dev(&img_dev, bytes, img_cap, s));
+    DCSR_CUDA(cudaMallocHost((void **)&img_host, bytes));
+    std::memset(img_host, 0, bytes);
+  }
+  size_t cc = cnt_cap;
+  DCSR_TRY(grow_dev(&skip, n, cc, s));
+  cc = 2 * (size_t)cnt_cap;
+  DCSR_TRY(grow_dev(&status_dev, 2 * (size_t)n, cc, s));
+  cnt_cap = n > cnt_cap ? n : cnt_cap;
+  DCSR_TRY(grow_dev(&pref, 3 * (size_t)(n + 4), pref_cap, s));
   return DCSR_OK;
 }
 

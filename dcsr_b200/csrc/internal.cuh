@@ -120,6 +120,10 @@ struct BatchCore {
   int plan(const dcsr_batch_item *items, int count, cudaStream_t s, bool all_schedules);
   // Size every matrix's schedule buffers for its pool (before an upload).
   int ensure_buffers(cudaStream_t s);
+  // Size the image and per-item buffers for up to `items` items at once, so
+  // later plans of that size allocate nothing (pinned host allocation and
+  // release synchronise the device).
+  int reserve_items(int items, int dtype, cudaStream_t s);
   // Rebuild the descriptor image from the handles and upload it if it changed.  sync=true waits for the
   // upload; otherwise the caller guarantees the previous upload of this core
   // has completed before the next call (the pinned image is reused).

@@ -395,16 +395,18 @@ __device__ __forceinline__ void for_row_entries(const Chain &ch, int32_t len, in
   }
 }
 
+// VEC: the rows of x are packed (ldx == K) and aligned to the largest power
+// of two (<= 32) dividing the row size, so a row is read with vector loads.
 template <typename T, typename V, int K, bool VEC>
 __device__ __forceinline__ void load_xk(const V *__restrict__ x, int64_t c, int64_t ldx, T (&xv)[K]) {
-  if constexpr (VEC && sizeof(V) == 4 && K == 4) {
-    const float4 t = __ldg(reinterpret_cast<const float4 *>(x + c * 4));
-    xv[0] = t.x; xv[1] = t.y; xv[2] = t.z; xv[3] = t.w;
-  } else if constexpr (VEC && sizeof(V) == 4 && K == 8) {
+  if constexpr (VEC && sizeof(V) == 4 && K == 8) {  // two 128-bit loads (measured faster than one 256-bit load)
     const float4 t = __ldg(reinterpret_cast<const float4 *>(x + c * 8));
     const float4 u = __ldg(reinterpret_cast<const float4 *>(x + c * 8) + 1);
     xv[0] = t.x; xv[1] = t.y; xv[2] = t.z; xv[3] = t.w;
     xv[4] = u.x; xv[5] = u.y; xv[6] = u.z; xv[7] = u.w;
+  } else if constexpr (VEC && sizeof(V) == 4 && K == 4) {
+    const float4 t = __ldg(reinterpret_cast<const float4 *>(x + c * 4));
+    xv[0] = t.x; xv[1] = t.y; xv[2] = t.z; xv[3] = t.w;
   } else if constexpr (VEC && sizeof(V) == 4 && K == 2) {
     const float2 t = __ldg(reinterpret_cast<const float2 *>(x + c * 2));
     xv[0] = t.x; xv[1] = t.y;
@@ -945,7 +947,7 @@ static int launch_reduce(dcsr_handle h, const V *x, int64_t ldx, V *y, int64_t l
 template <typename V, int K>
 static int spmv_k(dcsr_handle h, const V *x, int64_t ldx, V *y, int64_t ldy, double alpha, double beta,
                   cudaStream_t s) {
-  const size_t al = K * sizeof(V) >= 16 ? 16 : K * sizeof(V);
+  const size_t rb = K * sizeof(V), al = (rb & (0 - rb)) >= 32 ? 32 : (rb & (0 - rb));  // row alignment
   const bool vec = K > 1 && (K % 2 == 0) && ldx == K && ((uintptr_t)x % al) == 0;
   if (vec) return launch_reduce<V, K, OP_SPMV, true>(h, x, ldx, y, ldy, alpha, beta, s);
   return launch_reduce<V, K, OP_SPMV, false>(h, x, ldx, y, ldy, alpha, beta, s);

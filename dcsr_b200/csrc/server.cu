@@ -20,6 +20,7 @@
 // depend on how requests were batched: each matrix sees the same sequence of
 // operations, and every kernel's result for a matrix is independent of the
 // other matrices in its launch.
+#include <algorithm>
 #include <chrono>
 #include <condition_variable>
 #include <cstdlib>
@@ -67,13 +68,14 @@ struct Slot {
   int phase = 0;  // 1: batch in flight; 2: exports' entries being copied out
   // tracing (DCSR_SERVER_TRACE): events around the batch's device work
   cudaEvent_t t0 = nullptr, t1 = nullptr;
-  Clock::time_point h_start, h_launched;
+  Clock::time_point h_start, h_launched, h_retire;
+  int repairs = 0, grows = 0;
 };
 
 struct TraceRow {
-  int n, upd, spmv, exp;
+  int n, upd, spmv, exp, repairs, grows;
   long long triples;
-  double host_us, gpu_us, turnaround_us;
+  double host_us, gpu_us, turnaround_us, retire_us;
 };
 
 }  // namespace
@@ -326,6 +328,26 @@ int launch(dcsr_server s, Slot &sl, std::vector<Req> &take) {
       const dcsr_batch_item &bi = sl.items[q.item];
       DCSR_TRY(dcsr_spmv(h, bi.x, q.r.k, q.r.k, bi.y, q.r.k, q.r.alpha, q.r.beta, st));
     }
+  } else if (sl.reqs.size() == 1 && sl.items.size() == 1) {
+    // a lone update or SpMV (low load): its per-call operator, asynchronously --
+    // the same result as in a batch with fewer launches
+    Req &q = sl.reqs[0];
+    dcsr_handle h = s->mats[q.r.matrix];
+    const dcsr_batch_item &bi = sl.items[0];
+    if (q.r.kind == DCSR_REQ_UPDATE) {
+      DCSR_TRY(update_async(h, bi.rows, bi.cols, bi.vals, bi.nnz, st));
+      if (sl.status_cap < 1) {
+        DCSR_CUDA(cudaMallocHost((void **)&sl.status_host, sizeof(long long) * 2));
+        sl.status_cap = 1;
+      }
+      // (status, needed pool top) as the batch status kernel reports them
+      DCSR_CUDA(cudaMemcpyAsync(sl.status_host, h->stat + ST_STATUS, sizeof(long long), cudaMemcpyDeviceToHost, st));
+      DCSR_CUDA(cudaMemcpyAsync(sl.status_host + 1, h->stat + ST_NEED, sizeof(long long), cudaMemcpyDeviceToHost, st));
+      DCSR_CUDA(cudaMemsetAsync(h->stat + ST_STATUS, 0, sizeof(long long), st));
+      sl.statuses = true;
+    } else {
+      DCSR_TRY(dcsr_spmv(h, bi.x, bi.k, bi.ldx, bi.y, bi.ldy, bi.alpha, bi.beta, st));
+    }
   } else if (!sl.items.empty()) {
     DCSR_TRY(sl.core.plan(sl.items.data(), (int)sl.items.size(), st, false));
     DCSR_TRY(sl.core.upload(st, false, true));
@@ -373,7 +395,8 @@ int launch(dcsr_server s, Slot &sl, std::vector<Req> &take) {
 // Release a finished batch and publish its results.
 int finish(dcsr_server s, Slot &sl) {
   if (sl.t0) {
-    TraceRow t{(int)sl.reqs.size(), 0, 0, 0, 0, 0.0, 0.0, 0.0};
+    TraceRow t{(int)sl.reqs.size(), 0, 0, 0, sl.repairs, sl.grows, 0, 0.0, 0.0, 0.0, 0.0};
+    t.retire_us = std::chrono::duration<double, std::micro>(Clock::now() - sl.h_retire).count();
     for (auto &q : sl.reqs) {
       if (q.r.kind == DCSR_REQ_UPDATE) {
         t.upd++;
@@ -411,6 +434,8 @@ int finish(dcsr_server s, Slot &sl) {
 int retire(dcsr_server s, Slot &sl) {
   cudaStream_t st = sl.s;
   if (sl.phase == 2) return finish(s, sl);
+  sl.h_retire = Clock::now();
+  sl.repairs = sl.grows = 0;
   if (sl.statuses) {
     for (size_t i = 0; i < sl.items.size(); i++) {
       const int ui = sl.item_upd[i];
@@ -420,6 +445,7 @@ int retire(dcsr_server s, Slot &sl) {
       int status = (int)sl.status_host[2 * i];
       const long long need = sl.status_host[2 * i + 1];
       if (status != DCSR_OK) {
+        sl.repairs++;
         if (status == DCSR_POOL_EXHAUSTED || status == DCSR_LAYER_OVERFLOW)
           status = dcsr_update_sync(h, sl.items[i].rows, sl.items[i].cols, sl.items[i].vals, sl.items[i].nnz, st);
         const int si = sl.item_spmv[i];
@@ -434,6 +460,7 @@ int retire(dcsr_server s, Slot &sl) {
         DCSR_CUDA(cudaStreamSynchronize(st));
       } else if (h->pool_cap - need < h->pool_cap / 8) {
         // nearly full: grow ahead of the next update (stream-ordered, no sync)
+        sl.grows++;
         DCSR_TRY(reserve(h, pool_capacity(h->o, need), st));
       }
       q.status = status;
@@ -593,6 +620,26 @@ int dcsr_server_create(dcsr_server *out, const dcsr_handle *matrices, int32_t co
       delete s;
       return DCSR_CUDA_ERROR;
     }
+    // every per-batch buffer sized for a full batch now: the loop then never
+    // allocates pinned memory (whose release synchronises the device)
+    const int n = o.plain ? 1 : o.max_batch;
+    if (sl.core.reserve_items(n, s->mats[0]->dtype, sl.s) != DCSR_OK ||
+        cudaMallocHost((void **)&sl.status_host, sizeof(long long) * 2 * n) != cudaSuccess ||
+        cudaMallocHost((void **)&sl.nnz_host, sizeof(int32_t) * n) != cudaSuccess) {
+      delete s;
+      return DCSR_OOM;
+    }
+    sl.status_cap = n;
+    sl.nnz_cap = n;
+    cudaStreamSynchronize(sl.s);
+  }
+  // Pre-grow the stream-ordered pool the per-batch staging and scratch come
+  // from (freed blocks stay in it), so the loop's allocations map no memory.
+  {
+    const int64_t warm = std::min<int64_t>(std::max<int64_t>(s->budget / 16, 64ll << 20), 8ll << 30);
+    void *p = nullptr;
+    if (cudaMallocAsync(&p, (size_t)warm, s->slots[0].s) == cudaSuccess) cudaFreeAsync(p, s->slots[0].s);
+    cudaStreamSynchronize(s->slots[0].s);
   }
   s->worker = std::thread(worker_main, s);
   *out = s;
@@ -648,10 +695,11 @@ int dcsr_server_destroy(dcsr_server s) {
   if (s->worker.joinable()) s->worker.join();
   if (!s->trace_path.empty()) {
     if (FILE *f = std::fopen(s->trace_path.c_str(), "w")) {
-      std::fprintf(f, "requests,updates,spmvs,exports,triples,host_launch_us,gpu_us,turnaround_us\n");
+      std::fprintf(f, "requests,updates,spmvs,exports,repairs,grows,triples,host_launch_us,gpu_us,turnaround_us,"
+                      "retire_us\n");
       for (auto &t : s->trace)
-        std::fprintf(f, "%d,%d,%d,%d,%lld,%.1f,%.1f,%.1f\n", t.n, t.upd, t.spmv, t.exp, t.triples, t.host_us,
-                     t.gpu_us, t.turnaround_us);
+        std::fprintf(f, "%d,%d,%d,%d,%d,%d,%lld,%.1f,%.1f,%.1f,%.1f\n", t.n, t.upd, t.spmv, t.exp, t.repairs, t.grows,
+                     t.triples, t.host_us, t.gpu_us, t.turnaround_us, t.retire_us);
       std::fclose(f);
     }
   }
