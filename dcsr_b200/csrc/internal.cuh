@@ -20,8 +20,10 @@ int coo_to_csr64(dcsr_handle h, const int32_t *rows, const int32_t *cols, const 
                  Arena &ar, long long **rp, int32_t **ocols, void **ovals, int *bad, cudaStream_t s);
 size_t coo_to_csr_scratch(dcsr_handle h, int64_t nnz);
 
+// Per-call operators that take a scratch arena (default: the handle's own);
+// a server passes its slot's arena so resident matrices keep no scratch.
 int update_async(dcsr_handle h, const int32_t *rows, const int32_t *cols, const void *vals, int64_t nnz,
-                 cudaStream_t s);
+                 cudaStream_t s, Arena *ar = nullptr);
 
 // One matrix of a batched update (device-resident array element).
 template <typename V>
@@ -38,7 +40,9 @@ int update_many(const void *items_dev, int dtype, int count, int64_t T, bool mer
                 Arena &ar, cudaStream_t s);
 size_t update_scratch_bytes(int64_t T, size_t vsize);
 int compact(dcsr_handle h, cudaStream_t s);
-int build_schedule(dcsr_handle h, cudaStream_t s);
+int build_schedule(dcsr_handle h, cudaStream_t s, Arena *ar = nullptr);
+int spmv_call(dcsr_handle h, const void *x, int32_t k, int64_t ldx, void *y, int64_t ldy, double alpha, double beta,
+              cudaStream_t s, Arena *ar = nullptr);
 
 // One matrix of a row pass (SpMV / reduction) over a set of matrices.
 template <typename V>
@@ -80,7 +84,8 @@ int ensure_part(dcsr_handle h, int K, cudaStream_t s);
 int copy_rows(dcsr_handle h, const long long *dst_off, int32_t *out_cols, void *out_vals, int32_t *out_rows,
               int32_t *out_rowptr, cudaStream_t s, int64_t limit = INT64_MAX);
 // DCSR -> CSR writing at most `limit` entries (the row pointer is complete).
-int export_csr(dcsr_handle h, int32_t *row_ptr, int32_t *cols, void *vals, int64_t limit, cudaStream_t s);
+int export_csr(dcsr_handle h, int32_t *row_ptr, int32_t *cols, void *vals, int64_t limit, cudaStream_t s,
+               Arena *ar = nullptr);
 int reserve(dcsr_handle h, int64_t cap, cudaStream_t s);
 
 // The device side of a batch (batch.cu): a plan over a set of

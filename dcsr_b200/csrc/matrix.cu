@@ -491,10 +491,10 @@ int dcsr_nnz(dcsr_handle h, int64_t *nnz, void *stream) {
 }
 
 static int export_impl(dcsr_handle h, int32_t *row_ptr, int32_t *rows, int32_t *cols, void *vals, cudaStream_t s,
-                       int64_t limit = INT64_MAX) {
+                       int64_t limit = INT64_MAX, Arena *arp = nullptr) {
   const int32_t n = h->n_rows;
-  Arena &ar = h->scratch;
-  if (!h->bins_valid) DCSR_TRY(build_schedule(h, s));  // before taking arena memory
+  Arena &ar = arp ? *arp : h->scratch;
+  if (!h->bins_valid) DCSR_TRY(build_schedule(h, s, arp));  // before taking arena memory
   DCSR_TRY(ar.reserve(arena_bytes(n + 2, 8) + scan_scratch_bytes(n + 1), s));
   long long *rp = ar.take<long long>(n + 2);
   DCSR_LAUNCH(k_lens, grid_for(n + 1, 256), 256, 0, s, h->row_sizes, n, rp);
@@ -608,7 +608,8 @@ const char *dcsr_version(void) { return "dcsr_b200 0.1 (sm_100a)"; }
 }  // extern "C"
 
 namespace dcsr {
-int export_csr(dcsr_handle h, int32_t *row_ptr, int32_t *cols, void *vals, int64_t limit, cudaStream_t s) {
-  return export_impl(h, row_ptr, nullptr, cols, vals, s, limit);
+int export_csr(dcsr_handle h, int32_t *row_ptr, int32_t *cols, void *vals, int64_t limit, cudaStream_t s,
+               Arena *ar) {
+  return export_impl(h, row_ptr, nullptr, cols, vals, s, limit, ar);
 }
 }  // namespace dcsr

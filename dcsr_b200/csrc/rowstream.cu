@@ -244,18 +244,19 @@ int schedule_many(const void *items_dev, int dtype, int count, int64_t R, Arena 
 }
 
 template <typename V>
-static int build_schedule_t(dcsr_handle h, cudaStream_t s) {
+static int build_schedule_t(dcsr_handle h, cudaStream_t s, Arena &ar) {
   DCSR_TRY(ensure_part(h, 1, s));
-  DCSR_TRY(h->scratch.reserve(schedule_scratch_bytes(h->n_rows), s));
+  DCSR_TRY(ar.reserve(schedule_scratch_bytes(h->n_rows), s));
   RowOne<V> src{row_item<V>(h, nullptr, nullptr, 0, 0, 0.0, 0.0)};
-  DCSR_TRY(schedule_src<V>(src, 1, h->n_rows, h->scratch, s));
+  DCSR_TRY(schedule_src<V>(src, 1, h->n_rows, ar, s));
   h->bins_valid = true;
   return DCSR_OK;
 }
 
-int build_schedule(dcsr_handle h, cudaStream_t s) {
-  if (h->dtype == DCSR_F32) return build_schedule_t<float>(h, s);
-  return build_schedule_t<double>(h, s);
+int build_schedule(dcsr_handle h, cudaStream_t s, Arena *ar) {
+  Arena &a = ar ? *ar : h->scratch;
+  if (h->dtype == DCSR_F32) return build_schedule_t<float>(h, s, a);
+  return build_schedule_t<double>(h, s, a);
 }
 
 // Exclusive prefix over the matrices of each class's unit count (one block
@@ -1032,17 +1033,23 @@ int copy_rows(dcsr_handle h, const long long *dst_off, int32_t *out_cols, void *
 
 using namespace dcsr;
 
+namespace dcsr {
+int spmv_call(dcsr_handle h, const void *x, int32_t k, int64_t ldx, void *y, int64_t ldy, double alpha, double beta,
+              cudaStream_t s, Arena *ar) {
+  if (h->n_rows == 0) return DCSR_OK;
+  DCSR_TRY(ensure_part(h, k, s));
+  if (!h->bins_valid) DCSR_TRY(build_schedule(h, s, ar));
+  if (h->dtype == DCSR_F32)
+    return spmv_dispatch<float>(h, (const float *)x, k, ldx, (float *)y, ldy, alpha, beta, s);
+  return spmv_dispatch<double>(h, (const double *)x, k, ldx, (double *)y, ldy, alpha, beta, s);
+}
+}  // namespace dcsr
+
 extern "C" int dcsr_spmv(dcsr_handle h, const void *x, int32_t k, int64_t ldx, void *y, int64_t ldy, double alpha,
                          double beta, void *stream) {
   if (!h || k < 1 || k > 8 || ldx < k || ldy < k || (h->n_rows > 0 && !y) || (h->n_cols > 0 && !x))
     return DCSR_BAD_ARG;
-  cudaStream_t s = (cudaStream_t)stream;
-  if (h->n_rows == 0) return DCSR_OK;
-  DCSR_TRY(ensure_part(h, k, s));
-  if (!h->bins_valid) DCSR_TRY(build_schedule(h, s));
-  if (h->dtype == DCSR_F32)
-    return spmv_dispatch<float>(h, (const float *)x, k, ldx, (float *)y, ldy, alpha, beta, s);
-  return spmv_dispatch<double>(h, (const double *)x, k, ldx, (double *)y, ldy, alpha, beta, s);
+  return spmv_call(h, x, k, ldx, y, ldy, alpha, beta, (cudaStream_t)stream);
 }
 
 extern "C" int dcsr_row_reduce(dcsr_handle h, int32_t op, void *y, void *stream) {

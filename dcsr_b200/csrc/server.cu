@@ -335,7 +335,7 @@ int launch(dcsr_server s, Slot &sl, std::vector<Req> &take) {
     dcsr_handle h = s->mats[q.r.matrix];
     const dcsr_batch_item &bi = sl.items[0];
     if (q.r.kind == DCSR_REQ_UPDATE) {
-      DCSR_TRY(update_async(h, bi.rows, bi.cols, bi.vals, bi.nnz, st));
+      DCSR_TRY(update_async(h, bi.rows, bi.cols, bi.vals, bi.nnz, st, &sl.core.ar));
       if (sl.status_cap < 1) {
         DCSR_CUDA(cudaMallocHost((void **)&sl.status_host, sizeof(long long) * 2));
         sl.status_cap = 1;
@@ -346,7 +346,7 @@ int launch(dcsr_server s, Slot &sl, std::vector<Req> &take) {
       DCSR_CUDA(cudaMemsetAsync(h->stat + ST_STATUS, 0, sizeof(long long), st));
       sl.statuses = true;
     } else {
-      DCSR_TRY(dcsr_spmv(h, bi.x, bi.k, bi.ldx, bi.y, bi.ldy, bi.alpha, bi.beta, st));
+      DCSR_TRY(spmv_call(h, bi.x, bi.k, bi.ldx, (void *)bi.y, bi.ldy, bi.alpha, bi.beta, st, &sl.core.ar));
     }
   } else if (!sl.items.empty()) {
     DCSR_TRY(sl.core.plan(sl.items.data(), (int)sl.items.size(), st, false));
@@ -378,7 +378,7 @@ int launch(dcsr_server s, Slot &sl, std::vector<Req> &take) {
       int32_t *rp = q.direct ? q.r.row_ptr : (int32_t *)(b + q.off[0]);
       int32_t *oc = q.direct ? q.r.out_cols : (int32_t *)(b + q.off[1]);
       void *ov = q.direct ? q.r.out_vals : b + q.off[2];
-      DCSR_TRY(export_csr(h, rp, oc, ov, q.direct ? q.r.cap : INT64_MAX, st));
+      DCSR_TRY(export_csr(h, rp, oc, ov, q.direct ? q.r.cap : INT64_MAX, st, &sl.core.ar));
       DCSR_CUDA(cudaMemcpyAsync(sl.nnz_host + q.item, rp + h->n_rows, 4, cudaMemcpyDeviceToHost, st));
       // a staged export's row pointer now; its entries once their count is known
       if (!q.direct)

@@ -699,20 +699,21 @@ static int update_pipeline(const Src &src, int count, int64_t T, bool merge, int
 
 template <typename V>
 static int update_one(dcsr_handle h, const int32_t *rows, const int32_t *cols, const V *vals, int64_t T,
-                      cudaStream_t s) {
+                      cudaStream_t s, Arena &ar) {
   UpdOne<V> src{h->view<V>(), rows, cols, vals};
   DCSR_TRY(update_pipeline<V>(src, 1, T, h->o.mode == DCSR_MERGE, bits_for(h->n_rows), bits_for(h->n_cols), h->stat,
-                              h->scratch, s));
+                              ar, s));
   h->bins_valid = false;
   return DCSR_OK;
 }
 
 int update_async(dcsr_handle h, const int32_t *rows, const int32_t *cols, const void *vals, int64_t nnz,
-                 cudaStream_t s) {
+                 cudaStream_t s, Arena *ar) {
   if (nnz == 0) return DCSR_OK;
   if (nnz > 0x7ffffff0LL) return DCSR_BAD_ARG;
-  if (h->dtype == DCSR_F32) return update_one<float>(h, rows, cols, (const float *)vals, nnz, s);
-  return update_one<double>(h, rows, cols, (const double *)vals, nnz, s);
+  Arena &a = ar ? *ar : h->scratch;
+  if (h->dtype == DCSR_F32) return update_one<float>(h, rows, cols, (const float *)vals, nnz, s, a);
+  return update_one<double>(h, rows, cols, (const double *)vals, nnz, s, a);
 }
 
 template <typename V>
