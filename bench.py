@@ -258,6 +258,7 @@ def stream_part(args, dev, world):
         "ms_per_step": round(total_ms / args.steps, 4),
         "p50_ms": round(statistics.median(per_step), 4),
         "p99_ms": round(pct(per_step, 99), 4),
+        "step_ms": [round(t, 3) for t in per_step],
         "updates_per_s": round(world * args.steps * len(batches[0][0]) / (total_ms / 1e3), 1),
         "nnz_initial": nnz0, "nnz_final": nnz, "rows": n,
         "spmv": {"ms": round(spmv_ms, 4), "bytes": int(sb), "gbs": round(achieved, 1),
@@ -759,10 +760,10 @@ def main():
     ap.add_argument("--spmv-reps", type=int, default=20)
     ap.add_argument("--served-mats", type=int, default=2000)
     ap.add_argument("--served-requests", type=int, default=20000)
-    ap.add_argument("--plain-requests", type=int, default=3000)
+    ap.add_argument("--plain-requests", type=int, default=6000)
     ap.add_argument("--max-batch", type=int, default=256)
     ap.add_argument("--depth", type=int, default=6)
-    ap.add_argument("--load-fracs", type=float, nargs="+", default=[0.3, 0.5, 0.7, 0.85, 0.95])
+    ap.add_argument("--load-fracs", type=float, nargs="+", default=[0.3, 0.4, 0.45, 0.5, 0.55, 0.6, 0.7, 0.85])
     ap.add_argument("--plain-fracs", type=float, nargs="+", default=[0.5, 0.7, 0.9])
     ap.add_argument("--batched-mats", type=int, default=512)
     ap.add_argument("--batched-reps", type=int, default=5)

@@ -48,8 +48,8 @@ void fill_image(const BatchCore &b, unsigned char *img) {
   BatchItem<V> *up = (BatchItem<V> *)img;
   RowItem<V> *rows = (RowItem<V> *)(img + b.off_row);
   long long toff = 0, row0 = 0;
-  for (int i = 0; i < b.count; i++) {
-    const dcsr_batch_item &it = b.items[i];
+  for (size_t j = 0; j < b.upd.size(); j++) {
+    const dcsr_batch_item &it = b.items[b.upd[j]];
     dcsr_handle h = it.matrix;
     BatchItem<V> u;
     std::memset(&u, 0, sizeof(u));
@@ -59,7 +59,7 @@ void fill_image(const BatchCore &b, unsigned char *img) {
     u.vals = (const V *)it.vals;
     u.toff = toff;
     u.T = it.nnz;
-    up[i] = u;
+    up[j] = u;
     toff += it.nnz;
   }
   for (size_t q = 0; q < b.sched.size(); q++) {
@@ -75,7 +75,7 @@ void fill_image(const BatchCore &b, unsigned char *img) {
       const int i = g.idx[j];
       const dcsr_batch_item &it = b.items[i];
       RowItem<V> r = row_item<V>(it.matrix, it.x, it.y, it.ldx, it.ldy, it.alpha, it.beta);
-      r.skip = b.skip + i;
+      r.skip = b.upd_of[i] >= 0 ? b.skip + b.upd_of[i] : nullptr;  // only an update can be rejected
       r.k = it.k;
       // x rows as 8/16/32-byte vectors: even k, packed rows, base aligned to
       // the largest power of two (<= 32) dividing the row size
@@ -102,7 +102,6 @@ int grow_dev(T **p, size_t n, size_t &cap, cudaStream_t s) {
 int BatchCore::plan(const dcsr_batch_item *its, int n, cudaStream_t s, bool all_schedules) {
   if (n < 1 || !its || !its[0].matrix) return DCSR_BAD_ARG;
   const int dt = its[0].matrix->dtype, md = its[0].matrix->o.mode;
-  int32_t max_rows = 1, max_cols = 1;
   int64_t t = 0, r = 0;
   std::vector<dcsr_handle> seen;
   seen.reserve(n);
@@ -116,8 +115,6 @@ int BatchCore::plan(const dcsr_batch_item *its, int n, cudaStream_t s, bool all_
     seen.push_back(h);
     t += it.nnz;
     r += h->n_rows;
-    max_rows = h->n_rows > max_rows ? h->n_rows : max_rows;
-    max_cols = h->n_cols > max_cols ? h->n_cols : max_cols;
   }
   std::sort(seen.begin(), seen.end());
   if (std::adjacent_find(seen.begin(), seen.end()) != seen.end()) return DCSR_BAD_ARG;  // a matrix twice
@@ -127,8 +124,20 @@ int BatchCore::plan(const dcsr_batch_item *its, int n, cudaStream_t s, bool all_
   mode = md;
   items.assign(its, its + n);
   T = t;
-  rb = bits_for((int64_t)max_rows);
-  cb = bits_for((int64_t)max_cols);
+  // the update pipeline runs over the matrices with triples only; its key
+  // widths come from those matrices
+  upd.clear();
+  upd_of.assign(n, -1);
+  int32_t upd_rows = 1, upd_cols = 1;
+  for (int i = 0; i < n; i++)
+    if (its[i].nnz > 0) {
+      upd_of[i] = (int)upd.size();
+      upd.push_back(i);
+      upd_rows = its[i].matrix->n_rows > upd_rows ? its[i].matrix->n_rows : upd_rows;
+      upd_cols = its[i].matrix->n_cols > upd_cols ? its[i].matrix->n_cols : upd_cols;
+    }
+  rb = bits_for((int64_t)upd_rows);
+  cb = bits_for((int64_t)upd_cols);
   // SpMV groups by k family: 1, 2, 4 (k = 3, 4) and 8 (k = 5..8); the kernel
   // reads each item's k, so a run has at most four SpMV passes whatever the
   // mix of k
@@ -149,16 +158,30 @@ int BatchCore::plan(const dcsr_batch_item *its, int n, cudaStream_t s, bool all_
   }
   // schedules to rebuild: every matrix, or the updated ones and those whose
   // schedule is stale (after sizing their schedule buffers, which can
-  // invalidate a schedule)
+  // invalidate a schedule); the SpMVs of the others may run beside the update
   DCSR_TRY(ensure_buffers(s));
   sched.clear();
   R = 0;
+  std::vector<char> in_sched(n, 0);
   for (int i = 0; i < n; i++)
     if (all_schedules || its[i].nnz > 0 || !its[i].matrix->bins_valid) {
       sched.push_back(i);
+      in_sched[i] = 1;
       R += its[i].matrix->n_rows;
     }
-  size_t off = align_up((int64_t)(n * desc_size(dtype, false)), 256);
+  {
+    std::vector<Group> split;
+    for (auto &g : groups) {
+      Group main_g, side_g;
+      main_g.k = side_g.k = g.k;
+      side_g.side = true;
+      for (int i : g.idx) (in_sched[i] ? main_g : side_g).idx.push_back(i);
+      if (!main_g.idx.empty()) split.push_back(main_g);
+      if (!side_g.idx.empty()) split.push_back(side_g);
+    }
+    groups.swap(split);
+  }
+  size_t off = align_up((int64_t)(upd.size() * desc_size(dtype, false)), 256);
   off_row = off;
   off = align_up((int64_t)(off + sched.size() * desc_size(dtype, true)), 256);
   size_t poff = 0;
@@ -191,8 +214,9 @@ int BatchCore::plan(const dcsr_batch_item *its, int n, cudaStream_t s, bool all_
 
 int BatchCore::reserve_items(int n, int dt, cudaStream_t s) {
   // BatchItem + schedule RowItem + SpMV RowItem per item, 256-byte section
-  // padding for the (at most 6) sections
-  const size_t bytes = align_up((int64_t)(n * (desc_size(dt, false) + 2 * desc_size(dt, true)) + 6 * 256), 256);
+  // padding for the (at most 10: updates, schedules, 4 k families x main and
+  // side) sections
+  const size_t bytes = align_up((int64_t)(n * (desc_size(dt, false) + 2 * desc_size(dt, true)) + 10 * 256), 256);
   if (bytes > img_cap) {
     if (img_host) DCSR_CUDA(cudaFreeHost(img_host));
     img_host = nullptr;
@@ -205,7 +229,7 @@ int BatchCore::reserve_items(int n, int dt, cudaStream_t s) {
   cc = 2 * (size_t)cnt_cap;
   DCSR_TRY(grow_dev(&status_dev, 2 * (size_t)n, cc, s));
   cnt_cap = n > cnt_cap ? n : cnt_cap;
-  DCSR_TRY(grow_dev(&pref, 3 * (size_t)(n + 4), pref_cap, s));
+  DCSR_TRY(grow_dev(&pref, 3 * (size_t)(n + 8), pref_cap, s));
   return DCSR_OK;
 }
 
@@ -234,34 +258,46 @@ int BatchCore::reserve_scratch(cudaStream_t s) {
   return ar.reserve(upd > sch ? upd : sch, s);
 }
 
-int BatchCore::enqueue(cudaStream_t s) {
+int BatchCore::enqueue(cudaStream_t s, cudaStream_t s2, cudaEvent_t fork, cudaEvent_t join) {
   const bool merge = mode == DCSR_MERGE;
-  if (T > 0) {
-    DCSR_TRY(update_many(img_dev, dtype, count, T, merge, rb, cb, gstat, ar, s));
-    const int g = (count + 255) / 256;
+  bool beside = false;
+  for (auto &g : groups) beside |= g.side;
+  beside = beside && s2 && fork && join;
+  if (beside) {  // SpMVs of untouched matrices with valid schedules, on s2 beside the update
+    DCSR_CUDA(cudaEventRecord(fork, s));
+    DCSR_CUDA(cudaStreamWaitEvent(s2, fork, 0));
+    for (auto &g : groups)
+      if (g.side) DCSR_TRY(spmv_many(img_dev + g.off, dtype, (int)g.idx.size(), g.k, pref + g.pref_off, s2));
+    DCSR_CUDA(cudaEventRecord(join, s2));
+  }
+  const int nu = (int)upd.size();
+  if (T > 0 && nu > 0) {
+    DCSR_TRY(update_many(img_dev, dtype, nu, T, merge, rb, cb, gstat, ar, s));
+    const int g = (nu + 255) / 256;
     if (dtype == DCSR_F32)
-      DCSR_LAUNCH(k_batch_gate<float>, g, 256, 0, s, (const BatchItem<float> *)img_dev, count, skip);
+      DCSR_LAUNCH(k_batch_gate<float>, g, 256, 0, s, (const BatchItem<float> *)img_dev, nu, skip);
     else
-      DCSR_LAUNCH(k_batch_gate<double>, g, 256, 0, s, (const BatchItem<double> *)img_dev, count, skip);
-  } else {
-    DCSR_CUDA(cudaMemsetAsync(skip, 0, sizeof(int32_t) * count, s));
+      DCSR_LAUNCH(k_batch_gate<double>, g, 256, 0, s, (const BatchItem<double> *)img_dev, nu, skip);
   }
   if (!sched.empty()) {
     DCSR_TRY(ar.reserve(schedule_scratch_bytes(R), s));
     DCSR_TRY(schedule_many(img_dev + off_row, dtype, (int)sched.size(), R, ar, s));
   }
   for (auto &g : groups)
-    DCSR_TRY(spmv_many(img_dev + g.off, dtype, (int)g.idx.size(), g.k, pref + g.pref_off, s));
+    if (!g.side || !beside) DCSR_TRY(spmv_many(img_dev + g.off, dtype, (int)g.idx.size(), g.k, pref + g.pref_off, s));
+  if (beside) DCSR_CUDA(cudaStreamWaitEvent(s, join, 0));
   return DCSR_OK;
 }
 
 int BatchCore::status_async(long long *host, cudaStream_t s) {
-  const int g = (count + 255) / 256;
+  const int nu = (int)upd.size();
+  if (nu == 0) return DCSR_OK;
+  const int g = (nu + 255) / 256;
   if (dtype == DCSR_F32)
-    DCSR_LAUNCH(k_batch_status2<float>, g, 256, 0, s, (const BatchItem<float> *)img_dev, count, status_dev);
+    DCSR_LAUNCH(k_batch_status2<float>, g, 256, 0, s, (const BatchItem<float> *)img_dev, nu, status_dev);
   else
-    DCSR_LAUNCH(k_batch_status2<double>, g, 256, 0, s, (const BatchItem<double> *)img_dev, count, status_dev);
-  DCSR_CUDA(cudaMemcpyAsync(host, status_dev, sizeof(long long) * 2 * count, cudaMemcpyDeviceToHost, s));
+    DCSR_LAUNCH(k_batch_status2<double>, g, 256, 0, s, (const BatchItem<double> *)img_dev, nu, status_dev);
+  DCSR_CUDA(cudaMemcpyAsync(host, status_dev, sizeof(long long) * 2 * nu, cudaMemcpyDeviceToHost, s));
   return DCSR_OK;
 }
 
@@ -391,7 +427,10 @@ int dcsr_batch_status(dcsr_batch b, int32_t *statuses, void *stream) {
   cudaStream_t s = (cudaStream_t)stream;
   DCSR_TRY(b->core.status_async(b->status_host, s));
   DCSR_CUDA(cudaStreamSynchronize(s));
-  for (int i = 0; i < b->core.count; i++) statuses[i] = (int32_t)b->status_host[2 * i];
+  for (int i = 0; i < b->core.count; i++) {
+    const int j = b->core.upd_of[i];
+    statuses[i] = j >= 0 ? (int32_t)b->status_host[2 * j] : DCSR_OK;
+  }
   return DCSR_OK;
 }
 

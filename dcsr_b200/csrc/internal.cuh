@@ -94,7 +94,8 @@ int reserve(dcsr_handle h, int64_t cap, cudaStream_t s);
 // one core can serve many batches (the server re-plans one per slot).
 struct BatchCore {
   struct Group {
-    int k = 1;  // k family: 1, 2, 4 (k 3..4) or 8 (k 5..8)
+    int k = 1;          // k family: 1, 2, 4 (k 3..4) or 8 (k 5..8)
+    bool side = false;  // no update and a valid schedule: may run beside the update
     std::vector<int> idx;  // items of this group, in item order
     size_t off = 0;        // descriptor offset in the image
     size_t pref_off = 0;   // unit-prefix offset in pref
@@ -104,15 +105,17 @@ struct BatchCore {
   int64_t T = 0, R = 0;
   int rb = 1, cb = 1;
   std::vector<Group> groups;
-  std::vector<int> sched;  // items whose schedules the run rebuilds
-  // image: BatchItem[count] | RowItem[sched] (row space) | group RowItems
+  std::vector<int> sched;   // items whose schedules the run rebuilds
+  std::vector<int> upd;     // items with update triples (the update pipeline's items)
+  std::vector<int> upd_of;  // per item: its index in upd, or -1
+  // image: BatchItem[upd] | RowItem[sched] (row space) | group RowItems
   size_t off_row = 0, img_bytes = 0, img_cap = 0;
   unsigned char *img_dev = nullptr;
   unsigned char *img_host = nullptr;  // pinned copy of the last upload
   std::vector<unsigned char> img_new;
   int cnt_cap = 0;
-  int32_t *skip = nullptr;        // [count] 1: the matrix's update was rejected this run
-  long long *status_dev = nullptr;  // [2*count] (status, pool top needed) per matrix
+  int32_t *skip = nullptr;        // [upd] 1: the matrix's update was rejected this run
+  long long *status_dev = nullptr;  // [2*upd] (status, pool top needed) per updated matrix
   size_t pref_cap = 0;
   long long *pref = nullptr;
   long long *gstat = nullptr;
@@ -136,9 +139,12 @@ struct BatchCore {
   // Reserve the arena for this plan (before a capture: runs must not allocate).
   int reserve_scratch(cudaStream_t s);
   // Merged update, skip flags, schedule rebuild, grouped SpMV (capturable).
-  int enqueue(cudaStream_t s);
-  // (status, needed pool top) of every matrix into host memory (async);
-  // clears the device statuses.
+  // With a second stream s2 (and two events), the SpMVs of matrices without
+  // an update and with a valid schedule run on s2 beside the update; s waits
+  // for them before returning to the caller's stream order.
+  int enqueue(cudaStream_t s, cudaStream_t s2 = nullptr, cudaEvent_t fork = nullptr, cudaEvent_t join = nullptr);
+  // (status, needed pool top) of every updated matrix (item upd[j] -> words
+  // 2j, 2j+1) into host memory (async); clears the device statuses.
   int status_async(long long *host, cudaStream_t s);
   void mark_scheduled();
   void release();

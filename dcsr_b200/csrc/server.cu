@@ -52,6 +52,11 @@ struct Req {
 struct Slot {
   cudaStream_t s = nullptr;
   cudaEvent_t done = nullptr;
+  // second stream: SpMVs of matrices the batch does not update run on it
+  // beside the update pipeline, forked from and joined back into s
+  cudaStream_t s2 = nullptr;
+  cudaEvent_t fork = nullptr, join = nullptr;
+  bool single = false;  // the batch ran as one per-call operator
   BatchCore core;
   bool busy = false;
   std::vector<Req> reqs;
@@ -331,6 +336,7 @@ int launch(dcsr_server s, Slot &sl, std::vector<Req> &take) {
   } else if (sl.reqs.size() == 1 && sl.items.size() == 1) {
     // a lone update or SpMV (low load): its per-call operator, asynchronously --
     // the same result as in a batch with fewer launches
+    sl.single = true;
     Req &q = sl.reqs[0];
     dcsr_handle h = s->mats[q.r.matrix];
     const dcsr_batch_item &bi = sl.items[0];
@@ -352,7 +358,8 @@ int launch(dcsr_server s, Slot &sl, std::vector<Req> &take) {
     DCSR_TRY(sl.core.plan(sl.items.data(), (int)sl.items.size(), st, false));
     DCSR_TRY(sl.core.upload(st, false, true));
     DCSR_TRY(sl.core.reserve_scratch(st));
-    DCSR_TRY(sl.core.enqueue(st));
+    sl.single = false;
+    DCSR_TRY(sl.core.enqueue(st, sl.s2, sl.fork, sl.join));
     bool any_upd = false;
     for (int v : sl.item_upd) any_upd |= v >= 0;
     if (any_upd) {
@@ -442,8 +449,10 @@ int retire(dcsr_server s, Slot &sl) {
       if (ui < 0) continue;
       Req &q = sl.reqs[ui];
       dcsr_handle h = s->mats[q.r.matrix];
-      int status = (int)sl.status_host[2 * i];
-      const long long need = sl.status_host[2 * i + 1];
+      // the status words of updated matrices, in the order of the batch's updates
+      const int j = sl.single ? 0 : sl.core.upd_of[i];
+      int status = (int)sl.status_host[2 * j];
+      const long long need = sl.status_host[2 * j + 1];
       if (status != DCSR_OK) {
         sl.repairs++;
         if (status == DCSR_POOL_EXHAUSTED || status == DCSR_LAYER_OVERFLOW)
@@ -611,7 +620,10 @@ int dcsr_server_create(dcsr_server *out, const dcsr_handle *matrices, int32_t co
   if (tp && *tp) s->trace_path = tp;
   for (auto &sl : s->slots) {
     if (cudaStreamCreateWithFlags(&sl.s, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming) != cudaSuccess) {
+        cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&sl.s2, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&sl.fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&sl.join, cudaEventDisableTiming) != cudaSuccess) {
       delete s;
       return DCSR_CUDA_ERROR;
     }
@@ -711,6 +723,9 @@ int dcsr_server_destroy(dcsr_server s) {
     if (sl.status_host) cudaFreeHost(sl.status_host);
     if (sl.nnz_host) cudaFreeHost(sl.nnz_host);
     if (sl.done) cudaEventDestroy(sl.done);
+    if (sl.fork) cudaEventDestroy(sl.fork);
+    if (sl.join) cudaEventDestroy(sl.join);
+    if (sl.s2) cudaStreamDestroy(sl.s2);
     if (sl.s) cudaStreamDestroy(sl.s);
   }
   delete s;
