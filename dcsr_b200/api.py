@@ -123,6 +123,7 @@ _SIGS = {
     "dcsr_server_replay": (_i32, [_vp, _vp, _vp, _i64, _vp, C.POINTER(_dbl)]),
     "dcsr_status_string": (C.c_char_p, [_i32]),
     "dcsr_launch_count": (C.c_uint64, []),
+    "dcsr_spin_faults": (C.c_int, [C.POINTER(C.c_int64)]),
     "dcsr_version": (C.c_char_p, []),
 }
 

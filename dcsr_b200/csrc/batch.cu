@@ -255,7 +255,11 @@ int BatchCore::upload(cudaStream_t s, bool sync, bool force) {
 int BatchCore::reserve_scratch(cudaStream_t s) {
   const size_t upd = T > 0 ? update_scratch_bytes(T, dtype == DCSR_F64 ? 8 : 4) : 0;
   const size_t sch = schedule_scratch_bytes(R);
-  return ar.reserve(upd > sch ? upd : sch, s);
+  DCSR_TRY(ar.reserve(upd > sch ? upd : sch, s));
+  // look-back area for the update's sort and scans and the schedule's scans
+  // (sized here, outside any stream capture)
+  Lookback lb;
+  return ar.lookback(lookback_slots((T > R ? T : R) + 2), s, &lb);
 }
 
 int BatchCore::enqueue(cudaStream_t s, cudaStream_t s2, cudaEvent_t fork, cudaEvent_t join) {

@@ -90,11 +90,55 @@ struct Mat {
   dcsr_opts o;
 };
 
+// Device state of the single-pass scan and sort kernels (decoupled look-back):
+// an epoch that the last block of every such kernel advances, the dynamic
+// tile counter and the finished-block counter that block resets, the radix
+// digit histograms (re-zeroed by the sort's last pass), and per look-back slot
+// a flag word (epoch * 4 + 1: aggregate published, epoch * 4 + 2: inclusive
+// prefix published) with separate aggregate and inclusive value words.
+// Zeroed once at allocation: a slot left by an earlier kernel always carries
+// an older epoch, so nothing is cleared between kernels.
+struct Lookback {
+  unsigned long long *epoch;
+  unsigned *tiles, *done;
+  unsigned *hist;  // [8][256]
+  unsigned long long *flag, *agg, *inc;
+};
+constexpr size_t LB_HEADER = 64 + 8 * 256 * 4;
+
 // Stream-ordered scratch arena: one device buffer, bump-allocated per
-// operation, grown (stream-ordered free + malloc) when an operation needs more.
+// operation, grown (stream-ordered free + malloc) when an operation needs more;
+// plus the look-back area of the single-pass kernels.
 struct Arena {
   char *base = nullptr;
   size_t cap = 0, used = 0;
+  unsigned char *lb = nullptr;
+  size_t lb_slots = 0;
+  // Look-back area with at least `slots` slots (grown, and zeroed, outside
+  // stream capture only: a captured graph must find it sized already).
+  int lookback(size_t slots, cudaStream_t s, Lookback *out) {
+    if (slots > lb_slots || !lb) {
+      cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+      DCSR_CUDA(cudaStreamIsCapturing(s, &cs));
+      if (cs != cudaStreamCaptureStatusNone) return DCSR_NOT_SUPPORTED;
+      if (lb) DCSR_CUDA(cudaFreeAsync(lb, s));
+      lb = nullptr;
+      lb_slots = 0;
+      const size_t want = slots + slots / 4 + 1024;
+      const size_t bytes = LB_HEADER + 3 * 8 * want;
+      DCSR_CUDA(cudaMallocAsync((void **)&lb, bytes, s));
+      DCSR_CUDA(cudaMemsetAsync(lb, 0, bytes, s));
+      lb_slots = want;
+    }
+    out->epoch = (unsigned long long *)lb;
+    out->tiles = (unsigned *)(lb + 8);
+    out->done = (unsigned *)(lb + 12);
+    out->hist = (unsigned *)(lb + 64);
+    out->flag = (unsigned long long *)(lb + LB_HEADER);
+    out->agg = out->flag + lb_slots;
+    out->inc = out->agg + lb_slots;
+    return DCSR_OK;
+  }
   int reserve(size_t bytes, cudaStream_t s) {
     used = 0;
     if (bytes <= cap) return DCSR_OK;
@@ -118,8 +162,10 @@ struct Arena {
   }
   void release(cudaStream_t s) {
     if (base) cudaFreeAsync(base, s);
+    if (lb) cudaFreeAsync(lb, s);
     base = nullptr;
-    cap = used = 0;
+    lb = nullptr;
+    cap = used = lb_slots = 0;
   }
 };
 
@@ -323,6 +369,11 @@ size_t scan_scratch_bytes(int64_t n);
 int radix_sort_pairs(unsigned long long **keys, unsigned **vals, unsigned long long **keys_tmp,
                      unsigned **vals_tmp, int64_t n, int bits, Arena &ar, cudaStream_t s);
 size_t radix_scratch_bytes(int64_t n);
+// Look-back slots that a scan or a sort of n items needs (Arena::lookback).
+size_t lookback_slots(int64_t n);
+// Spin waits of the single-pass kernels that ran out of iterations (a bug
+// indicator: each wait has an owner that is running or finished).
+long long spin_faults();
 
 inline int bits_for(int64_t n) {  // bits to represent values in [0, n)
   int b = 1;

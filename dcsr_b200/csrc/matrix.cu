@@ -603,6 +603,14 @@ const char *dcsr_status_string(int st) {
 }
 
 uint64_t dcsr_launch_count(void) { return g_launches.load(); }
+
+int dcsr_spin_faults(int64_t *count) {
+  if (!count) return DCSR_BAD_ARG;
+  const long long v = dcsr::spin_faults();
+  if (v < 0) return DCSR_CUDA_ERROR;
+  *count = v;
+  return DCSR_OK;
+}
 const char *dcsr_version(void) { return "dcsr_b200 0.1 (sm_100a)"; }
 
 }  // extern "C"

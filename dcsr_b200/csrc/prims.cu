@@ -55,57 +55,147 @@ __device__ __forceinline__ T block_excl_scan(T v, T *total) {
   return out;
 }
 
-__global__ void k_scan_reduce(const long long *in, int64_t n, long long *partial) {
-  const int64_t base = (int64_t)blockIdx.x * SCAN_TILE;
-  long long s = 0;
-#pragma unroll
-  for (int j = 0; j < SCAN_ITEMS; j++) {
-    int64_t i = base + j * SCAN_THREADS + threadIdx.x;
-    if (i < n) s += in[i];
+// ------------------------------------------------- decoupled look-back
+//
+// Single-pass kernels: every block takes the next tile number from a device
+// counter (so all tiles before it are running or finished), publishes its
+// tile's aggregate, adds the aggregates of the tiles before it back to the
+// nearest published inclusive prefix, and publishes its own inclusive prefix.
+// A wait is only ever on an earlier tile, which therefore always finishes;
+// every wait still has an iteration limit, after which it counts a fault and
+// stops waiting.
+
+__device__ unsigned long long g_spin_faults = 0;
+constexpr int SPIN_LIMIT = 1 << 22;
+constexpr int LB_W = 8;  // earlier tiles whose flags one radix look-back step loads together
+
+__device__ __forceinline__ unsigned long long ld_vol(const unsigned long long *p) {
+  return *(const volatile unsigned long long *)p;
+}
+
+// The flag of slot q once published in epoch e (0 after a wait that gave up).
+__device__ __forceinline__ unsigned long long lb_wait(const Lookback &lb, int64_t q, unsigned long long e) {
+  const unsigned long long want = e * 4 + 1;
+  for (int it = 0; it < SPIN_LIMIT; it++) {
+    const unsigned long long f = ld_vol(lb.flag + q);
+    if (f >= want) return f;
+    if ((it & 1023) == 1023 && ld_vol(&g_spin_faults) != 0) break;  // an earlier wait gave up: stop at once
+    if (it >= 32) __nanosleep(64);
   }
-  s = warp_sum(s);
-  __shared__ long long ws[SCAN_THREADS / 32];
-  if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = s;
+  atomicAdd(&g_spin_faults, 1ull);
+  return 0;
+}
+
+// Publish slot q: kind 1 = the tile's aggregate, 2 = its inclusive prefix.
+__device__ __forceinline__ void lb_publish(const Lookback &lb, int64_t q, unsigned long long e, int kind,
+                                           unsigned long long v) {
+  *(volatile unsigned long long *)((kind == 1 ? lb.agg : lb.inc) + q) = v;
+  __threadfence();
+  *(volatile unsigned long long *)(lb.flag + q) = e * 4 + kind;
+}
+
+// Value of slot q whose flag f was read by lb_wait.
+__device__ __forceinline__ long long lb_value(const Lookback &lb, int64_t q, unsigned long long e,
+                                              unsigned long long f) {
+  __threadfence();
+  return (long long)ld_vol((f == e * 4 + 2 ? lb.inc : lb.agg) + q);
+}
+
+// Thread 0 of every block: the block's tile and the kernel's epoch.
+__device__ __forceinline__ void lb_begin(const Lookback &lb, unsigned *tile, unsigned long long *ep) {
+  if (threadIdx.x == 0) {
+    *tile = atomicAdd(lb.tiles, 1u);
+    *ep = ld_vol(lb.epoch);
+  }
+}
+
+// End of every block (all threads): true in the last block to finish.
+__device__ __forceinline__ bool lb_end(const Lookback &lb) {
+  __shared__ int last;
   __syncthreads();
   if (threadIdx.x == 0) {
-    long long t = 0;
-    for (int w = 0; w < SCAN_THREADS / 32; w++) t += ws[w];
-    partial[blockIdx.x] = t;
+    __threadfence();
+    last = atomicAdd(lb.done, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  return last;
+}
+
+// The last block: reset the counters and advance the epoch.
+__device__ __forceinline__ void lb_advance(const Lookback &lb) {
+  if (threadIdx.x == 0) {
+    *(volatile unsigned *)lb.tiles = 0;
+    *(volatile unsigned *)lb.done = 0;
+    *(volatile unsigned long long *)lb.epoch = ld_vol(lb.epoch) + 1;
+    __threadfence();
   }
 }
 
-// Single block: exclusive scan of the tile partials in place; total -> *total.
-__global__ void k_scan_partials(long long *partial, int64_t ntiles, long long *total) {
-  long long carry = 0;
-  for (int64_t b = 0; b < ntiles; b += blockDim.x) {
-    int64_t i = b + threadIdx.x;
-    long long v = i < ntiles ? partial[i] : 0;
-    long long bt;
-    long long ex = block_excl_scan(v, &bt);
-    if (i < ntiles) partial[i] = ex + carry;
-    carry += bt;
-  }
-  if (threadIdx.x == 0 && total) *total = carry;
+long long spin_faults() {
+  unsigned long long v = 0;
+  if (cudaMemcpyFromSymbol(&v, g_spin_faults, sizeof(v)) != cudaSuccess) return -1;
+  return (long long)v;
 }
 
-__global__ void k_scan_down(const long long *in, long long *out, int64_t n, const long long *partial) {
+// Exclusive scan, one pass: tiles of SCAN_TILE values; warp 0 looks back over
+// 32 earlier tiles at a time.  In place (in == out) is allowed.
+__global__ void __launch_bounds__(SCAN_THREADS) k_scan_1p(const long long *in, long long *out, int64_t n,
+                                                          long long *total, Lookback lb) {
   __shared__ long long tile[SCAN_TILE];
-  const int64_t base = (int64_t)blockIdx.x * SCAN_TILE;
+  __shared__ unsigned sh_tile;
+  __shared__ unsigned long long sh_ep;
+  __shared__ long long sh_prefix;
+  lb_begin(lb, &sh_tile, &sh_ep);
+  __syncthreads();
+  const int64_t t = sh_tile;
+  const unsigned long long e = sh_ep;
+  if (t >= gridDim.x) {  // a tile counter left non-zero (a bug): count it, touch nothing
+    if (threadIdx.x == 0) atomicAdd(&g_spin_faults, 1ull);
+    if (lb_end(lb)) lb_advance(lb);
+    return;
+  }
+  const int64_t base = t * SCAN_TILE;
 #pragma unroll
   for (int j = 0; j < SCAN_ITEMS; j++) {
-    int64_t i = base + j * SCAN_THREADS + threadIdx.x;
+    const int64_t i = base + j * SCAN_THREADS + threadIdx.x;
     tile[j * SCAN_THREADS + threadIdx.x] = i < n ? in[i] : 0;
   }
   __syncthreads();
   long long loc[SCAN_ITEMS];
-  long long s = 0;
+  long long sum = 0;
 #pragma unroll
   for (int j = 0; j < SCAN_ITEMS; j++) {
     loc[j] = tile[threadIdx.x * SCAN_ITEMS + j];
-    s += loc[j];
+    sum += loc[j];
   }
   long long bt;
-  long long ex = block_excl_scan(s, &bt) + partial[blockIdx.x];
+  long long ex = block_excl_scan(sum, &bt);
+  if (threadIdx.x < 32) {
+    const int lane = threadIdx.x;
+    long long excl = 0;
+    if (t == 0) {
+      if (lane == 0) lb_publish(lb, 0, e, 2, (unsigned long long)bt);
+    } else {
+      if (lane == 0) lb_publish(lb, t, e, 1, (unsigned long long)bt);
+      for (int64_t j = t - 1;; j -= 32) {
+        const int64_t q = j - lane;  // lane 0: the nearest earlier tile
+        const unsigned long long f = q >= 0 ? lb_wait(lb, q, e) : 0;
+        const bool stop = f != e * 4 + 1;  // inclusive prefix, before tile 0, or a wait that gave up
+        const long long v = (q >= 0 && f != 0) ? lb_value(lb, q, e, f) : 0;
+        const unsigned m = __ballot_sync(FULL, stop);
+        if (m) {
+          const int first = __ffs(m) - 1;
+          excl += warp_sum(lane <= first ? v : 0ll);
+          break;
+        }
+        excl += warp_sum(v);
+      }
+      if (lane == 0) lb_publish(lb, t, e, 2, (unsigned long long)(excl + bt));
+    }
+    if (lane == 0) sh_prefix = excl;
+  }
+  __syncthreads();
+  ex += sh_prefix;
 #pragma unroll
   for (int j = 0; j < SCAN_ITEMS; j++) {
     tile[threadIdx.x * SCAN_ITEMS + j] = ex;
@@ -114,9 +204,11 @@ __global__ void k_scan_down(const long long *in, long long *out, int64_t n, cons
   __syncthreads();
 #pragma unroll
   for (int j = 0; j < SCAN_ITEMS; j++) {
-    int64_t i = base + j * SCAN_THREADS + threadIdx.x;
+    const int64_t i = base + j * SCAN_THREADS + threadIdx.x;
     if (i < n) out[i] = tile[j * SCAN_THREADS + threadIdx.x];
   }
+  if (threadIdx.x == 0 && total && base + SCAN_TILE >= n) *total = sh_prefix + bt;
+  if (lb_end(lb)) lb_advance(lb);
 }
 
 // Small inputs: one block; coalesced loads into shared memory, each thread
@@ -156,28 +248,33 @@ int scan_i64(const long long *in, long long *out, int64_t n, long long *total, A
     DCSR_LAUNCH(k_scan_small, 1, 1024, 0, s, in, out, n, total);
     return DCSR_OK;
   }
-  int64_t nt = div_up(n, SCAN_TILE);
-  const size_t mark = ar.used;  // partials are stream-ordered scratch: released on return
-  long long *partial = ar.take<long long>(nt + 1);
-  DCSR_LAUNCH(k_scan_reduce, (unsigned)nt, SCAN_THREADS, 0, s, in, n, partial);
-  DCSR_LAUNCH(k_scan_partials, 1, 1024, 0, s, partial, nt, total);
-  DCSR_LAUNCH(k_scan_down, (unsigned)nt, SCAN_THREADS, 0, s, in, out, n, partial);
-  ar.used = mark;
+  const int64_t nt = div_up(n, SCAN_TILE);
+  Lookback lb;
+  DCSR_TRY(ar.lookback((size_t)nt, s, &lb));
+  DCSR_LAUNCH(k_scan_1p, (unsigned)nt, SCAN_THREADS, 0, s, in, out, n, total, lb);
   return DCSR_OK;
 }
 
 // ------------------------------------------------------------ radix sort
 //
-// Stable LSD radix sort, 8-bit digits.  Per pass: (1) per-tile digit
-// histograms, (2) exclusive scan over the digit-major histogram table, (3) a
-// stable scatter: each warp ranks its 512 consecutive items with match_any
-// (ties keep input order), warps are ordered by a per-digit prefix across the
-// block, and the block's global digit offsets come from the scanned table.
+// Stable LSD radix sort, 8-bit digits.  Up to RS_MID keys (where the launch
+// count of a sort matters more than its bandwidth), one pass over the keys per
+// digit plus one histogram pass: (1) one kernel counts the digits of every
+// pass at once into per-pass histograms; (2) per pass, one scatter kernel:
+// each block takes the next tile, ranks its items per warp with match_any
+// (ties keep input order), orders its warps by a per-digit prefix, and finds
+// the items of each digit in the tiles before it by decoupled look-back (one
+// thread per digit, LB_W earlier tiles per step); the digit's global start is
+// the exclusive scan of the pass's histogram.  Larger inputs use three
+// kernels per pass (tile histograms, the exclusive scan of the digit-major
+// histogram table, a scatter with the same ranking and the scanned offsets),
+// which keeps look-back latency off the critical path.
 
 constexpr int RS_THREADS = 256;
 constexpr int RS_WARPS = RS_THREADS / 32;
 constexpr int RS_BINS = 256;
-// items per lane: 16 for large inputs, 4 below RS_MID items (more, shorter tiles)
+// items per lane: 16 for large inputs (three kernels per pass), 8 up to RS_MID
+// items (single-pass scatter)
 constexpr int64_t RS_MID = 1 << 18;
 
 __device__ __forceinline__ unsigned lanemask_lt() {
@@ -253,6 +350,127 @@ __global__ void __launch_bounds__(RS_THREADS) k_radix_scatter(const unsigned lon
       keys_out[pos] = k[j];
       vals_out[pos] = vals[i];
     }
+  }
+}
+
+// Digit histograms of every pass (keys read once), into the look-back
+// area's histogram table (zero on entry: the previous sort's last pass left
+// it cleared).
+__global__ void __launch_bounds__(RS_THREADS) k_radix_hist_all(const unsigned long long *keys, int64_t n,
+                                                                int passes, Lookback lb) {
+  __shared__ unsigned h[8 * RS_BINS];
+  for (int i = threadIdx.x; i < 8 * RS_BINS; i += RS_THREADS) h[i] = 0;
+  __syncthreads();
+  for (int64_t i = (int64_t)blockIdx.x * RS_THREADS + threadIdx.x; i < n; i += (int64_t)gridDim.x * RS_THREADS) {
+    const unsigned long long k = keys[i];
+    for (int p = 0; p < passes; p++) atomicAdd(&h[p * RS_BINS + (unsigned)((k >> (8 * p)) & 0xff)], 1u);
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < passes * RS_BINS; i += RS_THREADS)
+    if (h[i]) atomicAdd(lb.hist + i, h[i]);
+}
+
+template <int RS_ITEMS>
+__global__ void __launch_bounds__(RS_THREADS, 2) k_radix_onesweep(const unsigned long long *keys,
+                                                                   const unsigned *vals, unsigned long long *keys_out,
+                                                                   unsigned *vals_out, int64_t n, int pass,
+                                                                   int last_pass, Lookback lb) {
+  constexpr int RS_TILE = RS_THREADS * RS_ITEMS;
+  __shared__ unsigned wcnt[RS_WARPS][RS_BINS];
+  __shared__ long long boff[RS_BINS];
+  __shared__ unsigned sh_tile;
+  __shared__ unsigned long long sh_ep;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, d = threadIdx.x;
+  const int shift = 8 * pass;
+  lb_begin(lb, &sh_tile, &sh_ep);
+  for (int w = 0; w < RS_WARPS; w++) wcnt[w][d] = 0;
+  // the digit's first position in the output: exclusive scan of the histogram
+  long long all;
+  const long long gbase = block_excl_scan((long long)__ldcg(lb.hist + pass * RS_BINS + d), &all);
+  const int64_t t = sh_tile;
+  const unsigned long long e = sh_ep;
+  if (t >= gridDim.x) {  // a tile counter left non-zero (a bug): count it, touch nothing
+    if (threadIdx.x == 0) atomicAdd(&g_spin_faults, 1ull);
+    if (lb_end(lb)) lb_advance(lb);
+    return;
+  }
+  const int64_t base = t * RS_TILE + (int64_t)warp * (32 * RS_ITEMS);
+  unsigned long long k[RS_ITEMS];
+  unsigned rank[RS_ITEMS];
+  const unsigned lt = lanemask_lt();
+#pragma unroll
+  for (int j = 0; j < RS_ITEMS; j++) {
+    const int64_t i = base + j * 32 + lane;
+    k[j] = i < n ? keys[i] : ~0ull;
+    const unsigned dg = i < n ? (unsigned)((k[j] >> shift) & 0xff) : 0x100u;
+    const unsigned peers = __match_any_sync(FULL, dg);
+    const unsigned pre = dg < 0x100u ? wcnt[warp][dg] : 0u;
+    rank[j] = pre + __popc(peers & lt);
+    __syncwarp();
+    if (dg < 0x100u && (__ffs(peers) - 1) == lane) wcnt[warp][dg] = pre + __popc(peers);
+    __syncwarp();
+  }
+  __syncthreads();
+  unsigned run = 0;  // exclusive prefix across warps per digit; run = the tile's count of digit d
+  for (int w = 0; w < RS_WARPS; w++) {
+    const unsigned c = wcnt[w][d];
+    wcnt[w][d] = run;
+    run += c;
+  }
+  // items of digit d in the tiles before this one: look back over windows of
+  // LB_W earlier tiles (their flags loaded together), consuming published
+  // aggregates up to the nearest published inclusive prefix
+  long long excl = 0;
+  const int64_t slot = t * RS_BINS + d;
+  if (t == 0) {
+    lb_publish(lb, slot, e, 2, run);
+  } else {
+    lb_publish(lb, slot, e, 1, run);
+    const unsigned long long want = e * 4 + 1, incf = e * 4 + 2;
+    int64_t q = t - 1;
+    int idle = 0;
+    bool done = false;
+    while (!done) {
+      unsigned long long f[LB_W];
+#pragma unroll
+      for (int j = 0; j < LB_W; j++) f[j] = q - j >= 0 ? ld_vol(lb.flag + (q - j) * RS_BINS + d) : incf;
+      __threadfence();
+      int used = 0;
+#pragma unroll
+      for (int j = 0; j < LB_W; j++) {
+        if (done || used < j || f[j] < want) continue;  // stop at the first unpublished tile
+        if (q - j >= 0) excl += (long long)ld_vol((f[j] == incf ? lb.inc : lb.agg) + (q - j) * RS_BINS + d);
+        used = j + 1;
+        done = f[j] == incf;
+      }
+      q -= used;
+      if (used == 0) {  // the nearest tile has not published yet
+        if (++idle >= SPIN_LIMIT || ((idle & 1023) == 1023 && ld_vol(&g_spin_faults) != 0)) {
+          atomicAdd(&g_spin_faults, 1ull);
+          break;
+        }
+        if (idle >= 32) __nanosleep(64);
+      }
+    }
+    lb_publish(lb, slot, e, 2, (unsigned long long)(excl + run));
+  }
+  boff[d] = gbase + excl;
+  __syncthreads();
+#pragma unroll
+  for (int j = 0; j < RS_ITEMS; j++) {
+    const int64_t i = base + j * 32 + lane;
+    if (i < n) {
+      const unsigned dg = (unsigned)((k[j] >> shift) & 0xff);
+      const int64_t pos = boff[dg] + wcnt[warp][dg] + rank[j];
+      keys_out[pos] = k[j];
+      vals_out[pos] = vals[i];
+    }
+  }
+  if (lb_end(lb)) {
+    if (last_pass)  // leave the histogram table cleared for the next sort
+      for (int i = threadIdx.x; i < 8 * RS_BINS; i += RS_THREADS) lb.hist[i] = 0;
+    __syncthreads();
+    lb_advance(lb);
   }
 }
 
@@ -344,20 +562,27 @@ __global__ void __launch_bounds__(1024) k_radix_small(const unsigned long long *
 }
 
 size_t radix_scratch_bytes(int64_t n) {
-  int64_t nt = div_up(n, RS_THREADS * 4);
-  return arena_bytes(nt * RS_BINS, 8) + scan_scratch_bytes(nt * RS_BINS);
+  if (n <= RS_MID) return 0;
+  return arena_bytes(div_up(n, RS_THREADS * 16) * RS_BINS, 8);
 }
 
-template <int ITEMS>
-static int radix_passes(unsigned long long **keys, unsigned **vals, unsigned long long **keys_tmp,
-                        unsigned **vals_tmp, int64_t n, int bits, Arena &ar, cudaStream_t s) {
+size_t lookback_slots(int64_t n) {
+  // mid-size sorts: one slot per (tile, digit); large sorts: the scan of their
+  // histogram table; scans: one slot per tile
+  const int64_t sort = n <= RS_MID ? div_up(n, RS_THREADS * 8) * RS_BINS
+                                   : div_up(div_up(n, RS_THREADS * 16) * RS_BINS, SCAN_TILE);
+  return (size_t)(std::max<int64_t>(sort, div_up(n, SCAN_TILE)) + 1);
+}
+
+// Large inputs: three kernels per pass (tile histograms, table scan, scatter).
+static int radix_passes_table(unsigned long long **keys, unsigned **vals, unsigned long long **keys_tmp,
+                              unsigned **vals_tmp, int64_t n, int bits, Arena &ar, cudaStream_t s) {
+  constexpr int ITEMS = 16;
   const int64_t nt = div_up(n, RS_THREADS * ITEMS);
   size_t mark = ar.used;
   long long *hist = ar.take<long long>(nt * RS_BINS);
-  size_t mark2 = ar.used;
   for (int shift = 0; shift < bits; shift += 8) {
     DCSR_LAUNCH(k_radix_hist<ITEMS>, (unsigned)nt, RS_THREADS, 0, s, *keys, n, shift, hist, nt);
-    ar.used = mark2;
     DCSR_TRY(scan_i64(hist, hist, nt * RS_BINS, nullptr, ar, s));
     DCSR_LAUNCH(k_radix_scatter<ITEMS>, (unsigned)nt, RS_THREADS, 0, s, *keys, *vals, *keys_tmp, *vals_tmp, n,
                 shift, hist, nt);
@@ -369,6 +594,30 @@ static int radix_passes(unsigned long long **keys, unsigned **vals, unsigned lon
     *vals_tmp = tv;
   }
   ar.used = mark;
+  return DCSR_OK;
+}
+
+// Mid-size inputs: one histogram kernel, then one single-pass scatter per pass.
+static int radix_passes_onesweep(unsigned long long **keys, unsigned **vals, unsigned long long **keys_tmp,
+                                 unsigned **vals_tmp, int64_t n, int bits, Arena &ar, cudaStream_t s) {
+  constexpr int ITEMS = 8;
+  const int passes = (int)div_up(bits, 8);
+  if (passes <= 0) return DCSR_OK;
+  const int64_t nt = div_up(n, RS_THREADS * ITEMS);
+  Lookback lb;
+  DCSR_TRY(ar.lookback((size_t)(nt * RS_BINS), s, &lb));
+  const int gh = (int)std::min<int64_t>(div_up(n, RS_THREADS * 8), 4 * sm_count());
+  DCSR_LAUNCH(k_radix_hist_all, gh, RS_THREADS, 0, s, *keys, n, passes, lb);
+  for (int p = 0; p < passes; p++) {
+    DCSR_LAUNCH(k_radix_onesweep<ITEMS>, (unsigned)nt, RS_THREADS, 0, s, *keys, *vals, *keys_tmp, *vals_tmp, n, p,
+                p == passes - 1 ? 1 : 0, lb);
+    unsigned long long *tk = *keys;
+    *keys = *keys_tmp;
+    *keys_tmp = tk;
+    unsigned *tv = *vals;
+    *vals = *vals_tmp;
+    *vals_tmp = tv;
+  }
   return DCSR_OK;
 }
 
@@ -390,8 +639,8 @@ int radix_sort_pairs(unsigned long long **keys, unsigned **vals, unsigned long l
     *vals_tmp = tv;
     return DCSR_OK;
   }
-  if (n <= RS_MID) return radix_passes<4>(keys, vals, keys_tmp, vals_tmp, n, bits, ar, s);
-  return radix_passes<16>(keys, vals, keys_tmp, vals_tmp, n, bits, ar, s);
+  if (n <= RS_MID) return radix_passes_onesweep(keys, vals, keys_tmp, vals_tmp, n, bits, ar, s);
+  return radix_passes_table(keys, vals, keys_tmp, vals_tmp, n, bits, ar, s);
 }
 
 // ------------------------------------------------- public segmented ops
@@ -437,13 +686,14 @@ __global__ void k_rbk_emit(const int32_t *keys, const V *vals, int64_t n, const 
 // ------------------------------------------- allocation-free reduce-by-key
 //
 // Scratch for dcsr_reduce_by_key_noalloc: head positions (one int64 per key)
-// and the scan's tile partials, in one static device array.  Every GPU that
-// loads the library holds it until exit.  Host code must not pass the
-// symbol itself to a kernel (in host code it names a host-side stand-in);
-// the device address is looked up once per device.
+// and the scan's look-back area, in one static device array (zero at module
+// load, as the look-back protocol needs).  Every GPU that loads the library
+// holds it until exit.  Host code must not pass the symbol itself to a
+// kernel (in host code it names a host-side stand-in); the device address is
+// looked up once per device.
 constexpr size_t NOALLOC_POS_BYTES = (size_t)DCSR_NOALLOC_MAX_KEYS * sizeof(long long);
-constexpr size_t NOALLOC_BYTES = NOALLOC_POS_BYTES + 2 * 256 +
-                                 ((DCSR_NOALLOC_MAX_KEYS + SCAN_TILE - 1) / SCAN_TILE + 1) * sizeof(long long);
+constexpr size_t NOALLOC_LB_SLOTS = (DCSR_NOALLOC_MAX_KEYS + SCAN_TILE - 1) / SCAN_TILE + 1;
+constexpr size_t NOALLOC_BYTES = NOALLOC_POS_BYTES + 256 + LB_HEADER + 3 * 8 * NOALLOC_LB_SLOTS;
 static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_BYTES];
 
 static int noalloc_scratch(void **out) {
@@ -478,10 +728,12 @@ extern "C" int dcsr_reduce_by_key_noalloc(const int32_t *keys, const void *vals,
   }
   void *base = nullptr;
   DCSR_TRY(noalloc_scratch(&base));
-  Arena ar;  // a view over the static array: take() only, never reserve()/release()
+  Arena ar;  // a view over the static array: take() and lookback() only, never reserve()/release()
   ar.base = (char *)base;
-  ar.cap = NOALLOC_BYTES;
+  ar.cap = NOALLOC_POS_BYTES + 256;
   ar.used = 0;
+  ar.lb = (unsigned char *)base + NOALLOC_POS_BYTES + 256;
+  ar.lb_slots = NOALLOC_LB_SLOTS;
   long long *pos = ar.take<long long>(n);  // fully rewritten below before any read
   const unsigned g = (unsigned)div_up(n, 256);
   DCSR_LAUNCH(k_rbk_flags, g, 256, 0, s, keys, n, pos);

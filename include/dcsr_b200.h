@@ -331,6 +331,12 @@ int dcsr_reduce_by_key_noalloc(const int32_t *keys, const void *vals, int64_t n,
 const char *dcsr_status_string(int status);
 /* Number of CUDA kernels this library has launched in this process. */
 uint64_t dcsr_launch_count(void);
+/* Waits of the single-pass scan and sort kernels (decoupled look-back) on
+ * the current device that reached their iteration limit and gave up, since
+ * the library was loaded.  Each such wait is on an earlier tile that is
+ * running or finished, so a non-zero count indicates a library bug (the
+ * affected result is wrong; nothing hangs).  Synchronises the device. */
+int dcsr_spin_faults(int64_t *count);
 /* Library version string. */
 const char *dcsr_version(void);
 
