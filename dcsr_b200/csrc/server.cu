@@ -107,6 +107,8 @@ struct dcsr_server_s {
   int64_t completed = 0, batches = 0;
   int device = 0;
   int fatal = DCSR_OK;
+  cudaMemPool_t pool = nullptr;     // the device's default pool (pre-grown at create)
+  uint64_t pool_reserved0 = 0;      // its reserved bytes before: trimmed back to them at destroy
   std::string trace_path;  // DCSR_SERVER_TRACE: per-batch timings written at destroy
   std::vector<TraceRow> trace;
 };
@@ -646,9 +648,15 @@ int dcsr_server_create(dcsr_server *out, const dcsr_handle *matrices, int32_t co
     cudaStreamSynchronize(sl.s);
   }
   // Pre-grow the stream-ordered pool the per-batch staging and scratch come
-  // from (freed blocks stay in it), so the loop's allocations map no memory.
+  // from (freed blocks stay in it), so the loop's allocations map no memory:
+  // a quarter of the budget covers the staging of `depth` full batches of
+  // host-buffer requests (a few GB each at max_batch 256).  Mapping new memory
+  // in the loop costs milliseconds to hundreds of milliseconds per call.
   {
-    const int64_t warm = std::min<int64_t>(std::max<int64_t>(s->budget / 16, 64ll << 20), 8ll << 30);
+    int dev = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetDefaultMemPool(&s->pool, dev) == cudaSuccess)
+      cudaMemPoolGetAttribute(s->pool, cudaMemPoolAttrReservedMemCurrent, &s->pool_reserved0);
+    const int64_t warm = std::min<int64_t>(std::max<int64_t>(s->budget / 4, 64ll << 20), 32ll << 30);
     void *p = nullptr;
     if (cudaMallocAsync(&p, (size_t)warm, s->slots[0].s) == cudaSuccess) cudaFreeAsync(p, s->slots[0].s);
     cudaStreamSynchronize(s->slots[0].s);
@@ -728,6 +736,8 @@ int dcsr_server_destroy(dcsr_server s) {
     if (sl.s2) cudaStreamDestroy(sl.s2);
     if (sl.s) cudaStreamDestroy(sl.s);
   }
+  // hand back the unused memory the pre-growth and the loop left in the pool
+  if (s->pool) cudaMemPoolTrimTo(s->pool, (size_t)s->pool_reserved0);
   delete s;
   return DCSR_OK;
 }
