@@ -489,7 +489,7 @@ int dcsr_batch_autotune(dcsr_batch b, void *stream, int32_t *short_max, int32_t 
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     const int32_t shorts[] = {32, 64, 128};
-    const int32_t longs[] = {2048, 4096, 16384};
+    const int32_t longs[] = {512, 1024, 4096, 16384};
     for (int32_t sm : shorts) {
       for (int32_t lm : longs) {
         for (auto &it : items) dcsr_set_row_classes(it.matrix, sm, lm);

@@ -196,7 +196,7 @@ struct dcsr_matrix_s {
   int32_t *med_rows = nullptr;   // [n_rows + 1] medium-length rows
   // Row-class thresholds of the row passes (rows of at most short_max
   // entries are streamed by row blocks, rows above long_min are chunked).
-  int32_t short_max = 64, long_min = 4096;
+  int32_t short_max = 64, long_min = 512;
   bool bins_valid = false;
   dcsr::Arena scratch;
   int device = 0;
