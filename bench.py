@@ -322,7 +322,7 @@ def batched_part(args, dev):
 
     specs = W.batched_specs(args.seed + 3, count=args.batched_mats)
     reps, warm = args.batched_reps, 3
-    mats, work, rounds = [], [], []
+    mats, work, per_mat = [], [], []
     nnz = 0
     for sp in specs:
         r, c, v = W.device_matrix(sp, dev)
@@ -333,11 +333,19 @@ def batched_part(args, dev):
         k = sp["k"]
         x = torch.rand(sp["n"], k, device=dev) * 2 - 1
         y = torch.zeros(sp["n"], k, device=dev)
-        rr = [W.device_updates(sp, dev, i) for i in range(warm + reps)]
-        live = tuple(t.clone() for t in rr[0])
+        per_mat.append([W.device_updates(sp, dev, i) for i in range(warm + reps)])
         mats.append(A)
-        rounds.append(rr)
-        work.append(dict(matrix=A, rows=live[0], cols=live[1], vals=live[2], x=x, y=y))
+        work.append(dict(matrix=A, x=x, y=y))
+    # every round's triples of all matrices in one buffer per array (the way
+    # a feed delivers a round); the batch reads them from one live buffer,
+    # matrix i at its fixed offset, refilled by one copy per array per round
+    sizes = [mr[0][0].numel() for mr in per_mat]
+    offs = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int64)
+    rounds = [tuple(torch.cat([mr[i][a] for mr in per_mat]) for a in range(3)) for i in range(warm + reps)]
+    per_mat.clear()
+    live = tuple(t.clone() for t in rounds[0])
+    for w, o0, o1 in zip(work, offs[:-1], offs[1:]):
+        w["rows"], w["cols"], w["vals"] = (t[o0:o1] for t in live)
     torch.cuda.synchronize()
     s = torch.cuda.Stream()
     batch = api.DcsrBatch(work, stream=s)
@@ -345,15 +353,15 @@ def batched_part(args, dev):
     batch.capture(s)
     T = sum(sp["updates"] for sp in specs)
 
+    repaired = [0]
+
     def batched_round(i):
-        for w, rr in zip(work, rounds):
-            w["rows"].copy_(rr[i][0], non_blocking=True)
-            w["cols"].copy_(rr[i][1], non_blocking=True)
-            w["vals"].copy_(rr[i][2], non_blocking=True)
+        for dst, src in zip(live, rounds[i]):
+            dst.copy_(src, non_blocking=True)
         batch.launch(s)
         st = batch.status(s)
         if (st != 0).any():
-            batch.repair(st, s)
+            repaired[0] += batch.repair(st, s)
 
     with torch.cuda.stream(s):
         for i in range(warm):
@@ -362,11 +370,13 @@ def batched_part(args, dev):
         launches0 = api.launch_count()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(s)
+        repaired[0] = 0
         for i in range(reps):
             batched_round(warm + i)
         e1.record(s)
         s.synchronize()
         batched_ms = e0.elapsed_time(e1) / reps
+        repairs_per_round = repaired[0] / reps
         batched_launches = (api.launch_count() - launches0) / reps
         # plain per-call sequences on the same matrices (fresh update rounds)
         L = api.lib()
@@ -375,8 +385,9 @@ def batched_part(args, dev):
         e0.record(s)
         launches0 = api.launch_count()
         for i in range(reps):
-            for w, rr in zip(work, rounds):
-                r, c, v = rr[(warm + i) % len(rr)]
+            rd = rounds[(warm + i) % len(rounds)]
+            for w, o0, o1 in zip(work, offs[:-1], offs[1:]):
+                r, c, v = (t[o0:o1] for t in rd)
                 st = L.dcsr_update_sync(w["matrix"].h, P(r), P(c), P(v), r.numel(), sp_)
                 assert st == 0, api.status_string(st)
                 k = w["x"].shape[1]
@@ -386,7 +397,7 @@ def batched_part(args, dev):
         plain_ms = e0.elapsed_time(e1) / reps
         plain_launches = (api.launch_count() - launches0) / reps
     batch.close()
-    del work, rounds, mats
+    del work, rounds, live, per_mat, mats
     torch.cuda.synchronize()
     return {
         "workload": f"{len(specs)} matrices, rows log-uniform [1k,256k], mean degree U[4,64], FP32, "
@@ -396,6 +407,7 @@ def batched_part(args, dev):
         "batched_ms": round(batched_ms, 3), "plain_ms": round(plain_ms, 3),
         "speedup": round(plain_ms / batched_ms, 2),
         "batched_kernel_launches": round(batched_launches, 1), "plain_kernel_launches": round(plain_launches, 1),
+        "repairs_per_round": repairs_per_round,
         "updates_per_s_batched": round(T / (batched_ms / 1e3), 1),
     }
 

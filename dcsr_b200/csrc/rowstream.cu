@@ -132,17 +132,19 @@ __global__ void k_sched_emit(Src src, int64_t R, const long long *lscan, const l
     const int32_t L = it.m.row_sizes[r];
     if (L > it.long_min) {
       const long long s = lscan[g] - lscan[it.row0];
-      const_cast<int32_t *>(it.long_rows)[s >> 32] = (int32_t)r;
-      const_cast<long long *>(it.long_off)[s >> 32] = s & 0xffffffff;
-      it.long_cnt[s >> 32] = 0;
+      const int32_t li = (int32_t)(s >> 32);
+      const long long c0 = s & 0xffffffff, nc = (L + CHUNK - 1) / CHUNK;
+      const_cast<int32_t *>(it.long_rows)[li] = (int32_t)r;
+      const_cast<long long *>(it.long_off)[li] = c0;
+      it.long_cnt[li] = 0;
+      for (long long c = c0; c < c0 + nc; c++) const_cast<int32_t *>(it.chunk_li)[c] = li;  // chunk -> long row
     } else if (L > it.short_max) {
       const_cast<int32_t *>(it.med_rows)[mscan[g] - mscan[it.row0]] = (int32_t)r;
     }
   }
 }
 
-// Per matrix (one warp each): class counts, the long-row offset sentinel and
-// the chunk -> long-row table.
+// Per matrix (one warp each): class counts and the long-row offset sentinel.
 template <typename V, typename Src>
 __global__ void k_sched_info(Src src, const long long *lscan, const long long *mscan) {
   const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
@@ -157,12 +159,6 @@ __global__ void k_sched_info(Src src, const long long *lscan, const long long *m
       it.info[1] = n_chunks;
       it.info[2] = (int32_t)(mscan[b] - mscan[a]);
       const_cast<long long *>(it.long_off)[n_long] = n_chunks;
-    }
-    __syncwarp();
-    for (int32_t li = lane; li < n_long; li += 32) {
-      const long long c0 = it.long_off[li];
-      const long long c1 = li + 1 < n_long ? it.long_off[li + 1] : n_chunks;
-      for (long long c = c0; c < c1; c++) const_cast<int32_t *>(it.chunk_li)[c] = li;
     }
   }
 }
@@ -529,8 +525,19 @@ __device__ __forceinline__ void write_y(V *y, int64_t ldy, int32_t row, const do
 
 // --------------------------------------------------------- reduction pass
 
+// Blocks per SM the row pass is compiled for: the runtime-k families hold up
+// to 8 FP64 accumulators and 8 x values per entry in flight, which left them
+// at 2-3 blocks (16-24 warps) per SM, too few to hide the gather latency.
+// Three blocks for k families 8 and 4 and four for family 2 (a few spilled
+// registers) ran the batched SpMV pass of 512 matrices 9% faster than the
+// unconstrained build (7.6 vs 8.4 ms).
+template <int K>
+struct RowsMinBlocks {
+  static constexpr int N = K == -8 ? 3 : K == -4 ? 3 : K == -2 ? 4 : 1;
+};
+
 template <typename V, int K, int OP, bool VEC, int PART, typename Src>
-__global__ void __launch_bounds__(RS_THREADS_) k_rows_reduce(Src src) {
+__global__ void __launch_bounds__(RS_THREADS_, RowsMinBlocks<K>::N) k_rows_reduce(Src src) {
   constexpr int KA = KArr<K>::N;
   __shared__ double red[RS_WARPS][KA];
   __shared__ int last_flag;
