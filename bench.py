@@ -580,7 +580,7 @@ def served_part(args, dev, rank, local_rank):
             best, best_f = min(((s_, f) for s_, f in zip(pts, args.load_fracs)), key=lambda t: t[0]["p99_ms"])
         return cap, pts, best, best_f, met
 
-    srv = api.DcsrServer(mats, max_batch=args.max_batch, depth=args.depth)
+    srv = api.DcsrServer(mats, max_batch=args.max_batch, depth=args.depth, workers=args.workers)
     cap_s, sweep, best, best_f, met = sweep_at(tr_dev, p99_plain)
     clocks = sampler.stop()
     # end to end: the same rule with pinned host buffers (inputs copied in,
@@ -598,7 +598,8 @@ def served_part(args, dev, rank, local_rank):
     torch.cuda.synchronize()
     out["served"] = {"capacity_req_s": round(cap_s["req_s"], 1), "mean_batch_at_capacity": round(cap_s["mean_batch"], 1),
                      "sweep": sweep, "chosen_load_frac": best_f, "p99_constraint_met": met,
-                     "batches": st["batches"], "max_batch": args.max_batch, "depth": args.depth}
+                     "batches": st["batches"], "max_batch": args.max_batch, "depth": args.depth,
+                     "workers": args.workers}
     out["value"] = best["req_s"]
     out["chosen"] = {"requests": best["requests"], "wall_ms": best["wall_ms"]}
     out["p50_ms"] = best["p50_ms"]
@@ -775,7 +776,8 @@ def main():
     ap.add_argument("--plain-requests", type=int, default=6000)
     ap.add_argument("--max-batch", type=int, default=256)
     ap.add_argument("--depth", type=int, default=6)
-    ap.add_argument("--load-fracs", type=float, nargs="+", default=[0.3, 0.4, 0.45, 0.5, 0.55, 0.6, 0.7, 0.85])
+    ap.add_argument("--workers", type=int, default=2)
+    ap.add_argument("--load-fracs", type=float, nargs="+", default=[0.3, 0.4, 0.5, 0.55, 0.6, 0.65, 0.7, 0.75, 0.85])
     ap.add_argument("--plain-fracs", type=float, nargs="+", default=[0.5, 0.7, 0.9])
     ap.add_argument("--batched-mats", type=int, default=512)
     ap.add_argument("--batched-reps", type=int, default=5)

@@ -52,7 +52,7 @@ class BatchItem(C.Structure):
 class ServerOpts(C.Structure):
     """dcsr_server_opts of the C ABI."""
     _fields_ = [("max_batch", C.c_int32), ("depth", C.c_int32), ("mem_budget", C.c_int64),
-                ("mem_reserve", C.c_int64), ("plain", C.c_int32)]
+                ("mem_reserve", C.c_int64), ("plain", C.c_int32), ("workers", C.c_int32)]
 
 
 class Request(C.Structure):
@@ -466,10 +466,11 @@ class DcsrServer:
     referenced until their result is taken with ``wait``.
     """
 
-    def __init__(self, matrices, max_batch=256, depth=4, mem_budget=0, mem_reserve=1 << 30, plain=False):
+    def __init__(self, matrices, max_batch=256, depth=4, mem_budget=0, mem_reserve=1 << 30, plain=False, workers=2):
         o = ServerOpts()
         lib().dcsr_server_default_opts(C.byref(o))
         o.max_batch, o.depth, o.mem_budget, o.mem_reserve, o.plain = max_batch, depth, mem_budget, mem_reserve, int(plain)
+        o.workers = workers
         self.matrices = list(matrices)
         arr = (C.c_void_p * len(self.matrices))(*[m.h.value for m in self.matrices])
         self.h = C.c_void_p()

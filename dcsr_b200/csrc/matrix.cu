@@ -2,6 +2,7 @@
 // CSR/COO export, compaction (defragmentation), pool growth, SpMV row bins,
 // the synchronous update repair policy and the status API.
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "internal.cuh"
@@ -283,9 +284,11 @@ int dcsr_create(dcsr_handle *out, int32_t n_rows, int32_t n_cols, int32_t dtype,
     // Pools and scratch use stream-ordered allocation; keep freed blocks in
     // the device's default pool instead of returning them at every sync, so a
     // compaction's fresh pool does not re-map memory each time.
+    static std::mutex mu;
     static bool configured[64] = {};
     int dev = 0;
     cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> lock(mu);
     if (dev >= 0 && dev < 64 && !configured[dev]) {
       cudaMemPool_t mp;
       if (cudaDeviceGetDefaultMemPool(&mp, dev) == cudaSuccess) {

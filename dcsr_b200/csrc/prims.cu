@@ -11,13 +11,14 @@ namespace dcsr {
 std::atomic<uint64_t> g_launches{0};
 
 int sm_count() {
-  static int n = 0;
-  if (!n) {
-    int dev = 0;
+  // function-local statics are initialised once, thread-safely (the server
+  // launches from several threads)
+  static const int n = [] {
+    int dev = 0, c = 0;
     cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
-    if (n <= 0) n = 148;
-  }
+    cudaDeviceGetAttribute(&c, cudaDevAttrMultiProcessorCount, dev);
+    return c > 0 ? c : 148;
+  }();
   return n;
 }
 
@@ -625,11 +626,9 @@ int radix_sort_pairs(unsigned long long **keys, unsigned **vals, unsigned long l
                      unsigned **vals_tmp, int64_t n, int bits, Arena &ar, cudaStream_t s) {
   if (n <= 1) return DCSR_OK;
   if (n <= RS_SMALL) {
-    static bool attr = false;
-    if (!attr) {
-      DCSR_CUDA(cudaFuncSetAttribute(k_radix_small, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)RS_SMALL_SMEM));
-      attr = true;
-    }
+    static const cudaError_t attr =
+        cudaFuncSetAttribute(k_radix_small, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)RS_SMALL_SMEM);
+    DCSR_CUDA(attr);
     DCSR_LAUNCH(k_radix_small, 1, 1024, RS_SMALL_SMEM, s, *keys, *vals, *keys_tmp, *vals_tmp, (int)n, bits);
     unsigned long long *tk = *keys;
     *keys = *keys_tmp;

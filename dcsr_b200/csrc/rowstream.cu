@@ -933,12 +933,9 @@ static int grid_of(const void *k) { return persistent_grid(k, RS_THREADS_, 0); }
 
 template <typename V, int K, int OP, bool VEC, typename Src>
 static int launch_reduce_src(const Src &src, cudaStream_t s) {
-  static int g0 = 0, g1 = 0, g2 = 0;
-  if (!g0) {
-    g0 = grid_of((const void *)k_rows_reduce<V, K, OP, VEC, P_BLOCKS, Src>);
-    g1 = grid_of((const void *)k_rows_reduce<V, K, OP, VEC, P_CHUNKS, Src>);
-    g2 = grid_of((const void *)k_rows_reduce<V, K, OP, VEC, P_MED, Src>);
-  }
+  static const int g0 = grid_of((const void *)k_rows_reduce<V, K, OP, VEC, P_BLOCKS, Src>);
+  static const int g1 = grid_of((const void *)k_rows_reduce<V, K, OP, VEC, P_CHUNKS, Src>);
+  static const int g2 = grid_of((const void *)k_rows_reduce<V, K, OP, VEC, P_MED, Src>);
   DCSR_LAUNCH((k_rows_reduce<V, K, OP, VEC, P_CHUNKS, Src>), g1, RS_THREADS_, 0, s, src);
   DCSR_LAUNCH((k_rows_reduce<V, K, OP, VEC, P_MED, Src>), g2, RS_THREADS_, 0, s, src);
   DCSR_LAUNCH((k_rows_reduce<V, K, OP, VEC, P_BLOCKS, Src>), g0, RS_THREADS_, 0, s, src);
@@ -1012,12 +1009,9 @@ int spmv_many(const void *items_dev, int dtype, int count, int k, long long *pre
 template <typename V>
 static int launch_copy(dcsr_handle h, const long long *dst_off, int32_t *out_cols, V *out_vals, int32_t *out_rows,
                        int32_t *out_rowptr, int64_t limit, cudaStream_t s) {
-  static int g0 = 0, g1 = 0, g2 = 0;
-  if (!g0) {
-    g0 = grid_of((const void *)k_rows_copy<V, P_BLOCKS>);
-    g1 = grid_of((const void *)k_rows_copy<V, P_CHUNKS>);
-    g2 = grid_of((const void *)k_rows_copy<V, P_MED>);
-  }
+  static const int g0 = grid_of((const void *)k_rows_copy<V, P_BLOCKS>);
+  static const int g1 = grid_of((const void *)k_rows_copy<V, P_CHUNKS>);
+  static const int g2 = grid_of((const void *)k_rows_copy<V, P_MED>);
   const RowItem<V> it = row_item<V>(h, nullptr, nullptr, 0, 0, 0.0, 0.0);
   DCSR_LAUNCH((k_rows_copy<V, P_CHUNKS>), g1, RS_THREADS_, 0, s, it, dst_off, out_cols, out_vals, out_rows, out_rowptr,
               limit);

@@ -1,7 +1,8 @@
 // server.cu -- the serving form: a request loop over resident matrices with
 // admission by device memory and continuous batching through BatchCore.
 //
-// One worker thread owns the device side.  Each turn it
+// Worker threads (opts.workers, default 2) own the device side; worker w owns
+// the slots w, w + workers, ...  Each turn a worker
 //   1. retires every in-flight batch whose completion event has fired:
 //      repairs rejected updates (compact / grow / retry, then the skipped
 //      SpMV), grows pools that are nearly full, frees the batch's staging,
@@ -16,10 +17,14 @@
 //      requests' inputs, the merged update + grouped SpMV of BatchCore, the
 //      exports, device -> host copies of the results, a completion event.
 // Up to `depth` batches are in flight on different streams, so copies and
-// kernels of consecutive batches overlap on the device.  Results do not
-// depend on how requests were batched: each matrix sees the same sequence of
-// operations, and every kernel's result for a matrix is independent of the
-// other matrices in its launch.
+// kernels of consecutive batches overlap on the device, and the host work of
+// forming and launching batches (tens of microseconds of launch calls each)
+// runs on several threads.  Batch formation is serialised by the server lock
+// and marks the batch's matrices busy and its bytes in use before the lock is
+// released, so two workers never take requests of one matrix out of order.
+// Results do not depend on how requests were batched: each matrix sees the
+// same sequence of operations, and every kernel's result for a matrix is
+// independent of the other matrices in its launch.
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
@@ -102,7 +107,7 @@ struct dcsr_server_s {
   std::unordered_map<uint64_t, dcsr_result> done;
   uint64_t next_ticket = 1;
   std::vector<Slot> slots;
-  std::thread worker;
+  std::vector<std::thread> workers;
   bool stop = false;
   int64_t completed = 0, batches = 0;
   int device = 0;
@@ -201,6 +206,14 @@ void form(dcsr_server s, std::vector<Req> &take) {
     take.push_back(std::move(q));
   }
   for (auto it = skipped.rbegin(); it != skipped.rend(); ++it) s->queue.push_front(std::move(*it));
+  // the batch owns its matrices and bytes from here (still under the lock)
+  if (!take.empty()) {
+    for (auto &q : take) {
+      s->in_use += q.cost;
+      s->busy[q.r.matrix] = 1;
+    }
+    s->batches++;
+  }
 }
 
 int launch(dcsr_server s, Slot &sl, std::vector<Req> &take) {
@@ -271,13 +284,7 @@ int launch(dcsr_server s, Slot &sl, std::vector<Req> &take) {
       item_of.emplace(q.r.matrix, -1);
     }
   }
-  sl.busy = true;  // from here on the slot owns its requests, matrices and memory
-  {
-    std::lock_guard<std::mutex> lk(s->mu);
-    s->in_use += sl.cost;
-    for (int m : sl.mats) s->busy[m] = 1;
-    s->batches++;
-  }
+  sl.busy = true;  // the slot owns its requests, matrices and memory (marked by form)
   if (n_exp > sl.nnz_cap) {
     if (sl.nnz_host) DCSR_CUDA(cudaFreeHost(sl.nnz_host));
     sl.nnz_host = nullptr;
@@ -421,6 +428,7 @@ int finish(dcsr_server s, Slot &sl) {
     t.gpu_us = 1e3 * ms;
     t.host_us = std::chrono::duration<double, std::micro>(sl.h_launched - sl.h_start).count();
     t.turnaround_us = std::chrono::duration<double, std::micro>(Clock::now() - sl.h_start).count();
+    std::lock_guard<std::mutex> lk(s->mu);
     s->trace.push_back(t);
   }
   if (sl.stage) DCSR_CUDA(cudaFreeAsync(sl.stage, sl.s));
@@ -520,11 +528,14 @@ void fail_slot(dcsr_server s, Slot &sl, int status) {
   sl.reqs.clear();
 }
 
-void worker_main(dcsr_server s) {
+void worker_main(dcsr_server s, int w, int W) {
   cudaSetDevice(s->device);
+  std::vector<Slot *> mine;
+  for (size_t i = w; i < s->slots.size(); i += W) mine.push_back(&s->slots[i]);
   for (;;) {
     bool progressed = false;
-    for (auto &sl : s->slots) {
+    for (Slot *slp : mine) {
+      Slot &sl = *slp;
       if (!sl.busy) continue;
       const cudaError_t e = cudaEventQuery(sl.done);
       if (e == cudaErrorNotReady) continue;
@@ -533,9 +544,9 @@ void worker_main(dcsr_server s) {
       progressed = true;
     }
     Slot *free_slot = nullptr;
-    for (auto &sl : s->slots)
-      if (!sl.busy) {
-        free_slot = &sl;
+    for (Slot *slp : mine)
+      if (!slp->busy) {
+        free_slot = slp;
         break;
       }
     if (free_slot) {
@@ -568,7 +579,7 @@ void worker_main(dcsr_server s) {
     if (!progressed) {
       std::unique_lock<std::mutex> lk(s->mu);
       bool inflight = false;
-      for (auto &sl : s->slots) inflight |= sl.busy;
+      for (Slot *slp : mine) inflight |= slp->busy;
       if (s->stop && s->queue.empty() && !inflight) break;
       if (!inflight) {
         s->cv_submit.wait_for(lk, std::chrono::milliseconds(2));
@@ -591,6 +602,7 @@ void dcsr_server_default_opts(dcsr_server_opts *o) {
   o->mem_budget = 0;
   o->mem_reserve = 1ll << 30;
   o->plain = 0;
+  o->workers = 2;
 }
 
 int dcsr_server_create(dcsr_server *out, const dcsr_handle *matrices, int32_t count, const dcsr_server_opts *opts) {
@@ -598,7 +610,9 @@ int dcsr_server_create(dcsr_server *out, const dcsr_handle *matrices, int32_t co
   dcsr_server_opts o;
   dcsr_server_default_opts(&o);
   if (opts) o = *opts;
-  if (o.max_batch < 1 || o.depth < 1 || o.depth > 16 || o.mem_budget < 0 || o.mem_reserve < 0) return DCSR_BAD_ARG;
+  if (o.max_batch < 1 || o.depth < 1 || o.depth > 16 || o.mem_budget < 0 || o.mem_reserve < 0 || o.workers < 1 ||
+      o.workers > 8)
+    return DCSR_BAD_ARG;
   for (int i = 0; i < count; i++)
     if (!matrices[i]) return DCSR_BAD_ARG;
   dcsr_server s = new dcsr_server_s;
@@ -661,7 +675,8 @@ int dcsr_server_create(dcsr_server *out, const dcsr_handle *matrices, int32_t co
     if (cudaMallocAsync(&p, (size_t)warm, s->slots[0].s) == cudaSuccess) cudaFreeAsync(p, s->slots[0].s);
     cudaStreamSynchronize(s->slots[0].s);
   }
-  s->worker = std::thread(worker_main, s);
+  const int nw = o.plain ? 1 : std::min(o.workers, depth);
+  for (int w = 0; w < nw; w++) s->workers.emplace_back(worker_main, s, w, nw);
   *out = s;
   return DCSR_OK;
 }
@@ -680,7 +695,7 @@ int dcsr_server_submit(dcsr_server s, const dcsr_request *req, uint64_t *ticket)
     *ticket = q.ticket;
     s->queue.push_back(std::move(q));
   }
-  s->cv_submit.notify_one();
+  s->cv_submit.notify_all();  // every worker: any of them may have a free slot
   return DCSR_OK;
 }
 
@@ -712,7 +727,8 @@ int dcsr_server_destroy(dcsr_server s) {
     s->stop = true;
   }
   s->cv_submit.notify_all();
-  if (s->worker.joinable()) s->worker.join();
+  for (auto &t : s->workers)
+    if (t.joinable()) t.join();
   if (!s->trace_path.empty()) {
     if (FILE *f = std::fopen(s->trace_path.c_str(), "w")) {
       std::fprintf(f, "requests,updates,spmvs,exports,repairs,grows,triples,host_launch_us,gpu_us,turnaround_us,"

@@ -329,17 +329,16 @@ static int spgemm_impl(dcsr_handle hA, dcsr_handle hB, dcsr_handle hC, cudaStrea
   DCSR_CUDA(cudaMallocAsync((void **)&tval, sizeof(V) * (P + 1), s));
   DCSR_CUDA(cudaMallocAsync((void **)&ucnt, sizeof(long long) * (n + 2), s));
   DCSR_CUDA(cudaMemsetAsync(ucnt, 0, sizeof(long long) * (n + 2), s));
-  static int g_warp = 0, g_cta = 0;
   const size_t cta_smem = SG_CTA_MAX * (sizeof(unsigned long long) + sizeof(V));
-  if (!g_warp) {
-    g_warp = persistent_grid((const void *)k_sg_warp<double>, SG_THREADS, 0);
+  static const int g_warp = persistent_grid((const void *)k_sg_warp<double>, SG_THREADS, 0);
+  static const int g_cta = [] {  // once, thread-safely: the CTA kernels' shared-memory limit, then their grid
     cudaFuncSetAttribute(k_sg_cta<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)(SG_CTA_MAX * (sizeof(unsigned long long) + sizeof(float))));
     cudaFuncSetAttribute(k_sg_cta<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)(SG_CTA_MAX * (sizeof(unsigned long long) + sizeof(double))));
-    g_cta = persistent_grid((const void *)k_sg_cta<double>, SG_THREADS,
-                            SG_CTA_MAX * (sizeof(unsigned long long) + sizeof(double)));
-  }
+    return persistent_grid((const void *)k_sg_cta<double>, SG_THREADS,
+                           SG_CTA_MAX * (sizeof(unsigned long long) + sizeof(double)));
+  }();
   if (host[SG_WARP + 1] > host[SG_WARP])
     DCSR_LAUNCH(k_sg_warp<V>, g_warp, SG_THREADS, 0, s, A, B, r0, starts, ub, tcol, tval, ucnt);
   if (host[SG_CTA + 1] > host[SG_CTA])

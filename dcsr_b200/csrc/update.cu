@@ -663,12 +663,9 @@ static int update_pipeline(const Src &src, int count, int64_t T, bool merge, int
   int32_t *tinfo = (int32_t *)p1;
   int32_t *ncol = (int32_t *)k1;
   int32_t *nins = ncol + T;
-  static int g_apply = 0, g_apply8 = 0, g_reloc = 0;
-  if (!g_apply) {
-    g_apply = persistent_grid((const void *)k_apply_merge<double, UpdOne<double>, 32>, UPD_THREADS, 0);
-    g_apply8 = persistent_grid((const void *)k_apply_merge<double, UpdOne<double>, 8>, UPD_THREADS, 0);
-    g_reloc = persistent_grid((const void *)k_relocate<double, UpdOne<double>>, RT_THREADS, 0);
-  }
+  static const int g_apply = persistent_grid((const void *)k_apply_merge<double, UpdOne<double>, 32>, UPD_THREADS, 0);
+  static const int g_apply8 = persistent_grid((const void *)k_apply_merge<double, UpdOne<double>, 8>, UPD_THREADS, 0);
+  static const int g_reloc = persistent_grid((const void *)k_relocate<double, UpdOne<double>>, RT_THREADS, 0);
   if (merge) {
     DCSR_LAUNCH((k_head_search<V, Src>), gT, 256, 0, s, src, k0, T, f, bcol, bpos, nflag);
     DCSR_TRY(scan_i64(nflag, nflag, T + 1, nullptr, ar, s));

@@ -237,7 +237,7 @@ int dcsr_batch_autotune(dcsr_batch b, void *stream, int32_t *short_max, int32_t 
 /* ------------------------------------------------------------ serving */
 
 /* A request server over a table of resident matrices.  Requests (update,
- * SpMV, export) carry HOST buffers; a worker thread admits queued requests
+ * SpMV, export) carry HOST buffers; worker threads admit queued requests
  * while their device memory fits the budget, coalesces them into batches
  * (merged update + grouped SpMV through the batched kernels, then exports),
  * keeps up to `depth` batches in flight on separate streams, and refills
@@ -255,6 +255,8 @@ typedef struct {
   int64_t mem_budget;  /* device bytes in-flight requests may hold; 0: free memory at creation - mem_reserve */
   int64_t mem_reserve; /* default 1 GiB */
   int32_t plain;       /* 1: no coalescing -- each request alone through the per-call operators */
+  int32_t workers;     /* host threads forming and launching batches, each owning every workers-th
+                          stream (default 2, 1..8, at most depth; plain uses 1) */
 } dcsr_server_opts;
 
 enum { DCSR_REQ_UPDATE = 0, DCSR_REQ_SPMV = 1, DCSR_REQ_EXPORT = 2 };
@@ -301,7 +303,7 @@ int dcsr_server_submit(dcsr_server s, const dcsr_request *req, uint64_t *ticket)
 int dcsr_server_wait(dcsr_server s, uint64_t ticket, int64_t timeout_us, dcsr_result *out);
 /* Counters: completed requests, batches launched, budget bytes in use. */
 int dcsr_server_stats(dcsr_server s, int64_t *completed, int64_t *batches, int64_t *mem_in_use);
-/* Drain the queue, stop the worker, release the server (not the matrices). */
+/* Drain the queue, stop the workers, release the server (not the matrices). */
 int dcsr_server_destroy(dcsr_server s);
 /* Load generator for measurements: submit requests[i] at arrival_us[i]
  * microseconds after the call starts (non-decreasing), then wait for all;

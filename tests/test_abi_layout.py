@@ -15,7 +15,7 @@ STRUCTS = {
                              "opts"]),
     "dcsr_batch_item": ("BatchItem", ["matrix", "rows", "cols", "vals", "nnz", "x", "y", "k", "ldx", "ldy", "alpha",
                                       "beta"]),
-    "dcsr_server_opts": ("ServerOpts", ["max_batch", "depth", "mem_budget", "mem_reserve", "plain"]),
+    "dcsr_server_opts": ("ServerOpts", ["max_batch", "depth", "mem_budget", "mem_reserve", "plain", "workers"]),
     "dcsr_request": ("Request", ["kind", "matrix", "rows", "cols", "vals", "nnz", "x", "y", "k", "alpha", "beta",
                                  "row_ptr", "out_cols", "out_vals", "cap", "on_device"]),
     "dcsr_result": ("Result", ["status", "batch_size", "nnz", "queue_us", "latency_us"]),
