@@ -267,11 +267,29 @@ int BatchCore::enqueue(cudaStream_t s, cudaStream_t s2, cudaEvent_t fork, cudaEv
   bool beside = false;
   for (auto &g : groups) beside |= g.side;
   beside = beside && s2 && fork && join;
+  // unit prefixes of a set of groups, one launch (a group's prefixes read
+  // its matrices' schedules: side groups' are valid now, the others' after
+  // the schedule rebuild below)
+  auto prefixes = [&](bool side) -> int {
+    const void *its[MAX_PREFIX_JOBS];
+    int cnt[MAX_PREFIX_JOBS];
+    long long *pr[MAX_PREFIX_JOBS];
+    int n = 0;
+    for (auto &g : groups)
+      if ((g.side && beside) == side && n < MAX_PREFIX_JOBS) {
+        its[n] = img_dev + g.off;
+        cnt[n] = (int)g.idx.size();
+        pr[n] = pref + g.pref_off;
+        n++;
+      }
+    return unit_prefix_many(its, cnt, pr, n, dtype, s);
+  };
   if (beside) {  // SpMVs of untouched matrices with valid schedules, on s2 beside the update
+    DCSR_TRY(prefixes(true));
     DCSR_CUDA(cudaEventRecord(fork, s));
     DCSR_CUDA(cudaStreamWaitEvent(s2, fork, 0));
     for (auto &g : groups)
-      if (g.side) DCSR_TRY(spmv_many(img_dev + g.off, dtype, (int)g.idx.size(), g.k, pref + g.pref_off, s2));
+      if (g.side) DCSR_TRY(spmv_many(img_dev + g.off, dtype, (int)g.idx.size(), g.k, pref + g.pref_off, s2, true));
     DCSR_CUDA(cudaEventRecord(join, s2));
   }
   const int nu = (int)upd.size();
@@ -287,8 +305,10 @@ int BatchCore::enqueue(cudaStream_t s, cudaStream_t s2, cudaEvent_t fork, cudaEv
     DCSR_TRY(ar.reserve(schedule_scratch_bytes(R), s));
     DCSR_TRY(schedule_many(img_dev + off_row, dtype, (int)sched.size(), R, ar, s));
   }
+  DCSR_TRY(prefixes(false));
   for (auto &g : groups)
-    if (!g.side || !beside) DCSR_TRY(spmv_many(img_dev + g.off, dtype, (int)g.idx.size(), g.k, pref + g.pref_off, s));
+    if (!g.side || !beside)
+      DCSR_TRY(spmv_many(img_dev + g.off, dtype, (int)g.idx.size(), g.k, pref + g.pref_off, s, true));
   if (beside) DCSR_CUDA(cudaStreamWaitEvent(s, join, 0));
   return DCSR_OK;
 }

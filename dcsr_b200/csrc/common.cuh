@@ -361,6 +361,9 @@ int sm_count();
 
 // Exclusive scan of int64 values; out may alias in; *total (device) = sum.
 int scan_i64(const long long *in, long long *out, int64_t n, long long *total, Arena &ar, cudaStream_t s);
+// Two independent exclusive scans of arrays of length n in one launch.
+int scan2_i64(const long long *in0, long long *out0, long long *total0, const long long *in1, long long *out1,
+              long long *total1, int64_t n, Arena &ar, cudaStream_t s);
 size_t scan_scratch_bytes(int64_t n);
 
 // Stable LSD radix sort of (uint64 key, uint32 value) pairs on bits [0, bits).

@@ -72,7 +72,13 @@ size_t schedule_scratch_bytes(int64_t R);
 // y = A x for `count` matrices (items: device RowItem<V>[count]) of one k
 // family: kf = 1, 2, 4 or 8, every item's k <= kf (each item's own k / vec
 // are read by the kernel); pref: device scratch of 3*(count+1) long longs.
-int spmv_many(const void *items_dev, int dtype, int count, int k, long long *pref, cudaStream_t s);
+// prefixed: the group's unit prefixes were computed already (unit_prefix_many)
+int spmv_many(const void *items_dev, int dtype, int count, int k, long long *pref, cudaStream_t s,
+              bool prefixed = false);
+// The unit prefixes of up to MAX_PREFIX_JOBS SpMV groups in one launch.
+constexpr int MAX_PREFIX_JOBS = 8;
+int unit_prefix_many(const void *const *items, const int *counts, long long *const *prefs, int n, int dtype,
+                     cudaStream_t s);
 template <typename V>
 RowItem<V> row_item(dcsr_handle h, const void *x, void *y, int64_t ldx, int64_t ldy, double alpha, double beta);
 // Size the handle's chunk table and chunk partials (K results per chunk).

@@ -138,10 +138,18 @@ long long spin_faults() {
   return (long long)v;
 }
 
+// Scan operands: one array, or two independent arrays of the same length
+// scanned by one launch (tiles [0, nt) scan the first, [nt, 2nt) the second).
+struct ScanArgs {
+  const long long *in[2];
+  long long *out[2];
+  long long *total[2];
+  int64_t n, nt;
+};
+
 // Exclusive scan, one pass: tiles of SCAN_TILE values; warp 0 looks back over
-// 32 earlier tiles at a time.  In place (in == out) is allowed.
-__global__ void __launch_bounds__(SCAN_THREADS) k_scan_1p(const long long *in, long long *out, int64_t n,
-                                                          long long *total, Lookback lb) {
+// 32 earlier tiles of its array at a time.  In place (in == out) is allowed.
+__global__ void __launch_bounds__(SCAN_THREADS) k_scan_1p(ScanArgs a, Lookback lb) {
   __shared__ long long tile[SCAN_TILE];
   __shared__ unsigned sh_tile;
   __shared__ unsigned long long sh_ep;
@@ -155,7 +163,12 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan_1p(const long long *in, l
     if (lb_end(lb)) lb_advance(lb);
     return;
   }
-  const int64_t base = t * SCAN_TILE;
+  const int arr = t >= a.nt ? 1 : 0;
+  const int64_t t0 = arr * a.nt;  // this array's first tile
+  const long long *__restrict__ in = a.in[arr];
+  long long *out = a.out[arr];
+  const int64_t n = a.n;
+  const int64_t base = (t - t0) * SCAN_TILE;
 #pragma unroll
   for (int j = 0; j < SCAN_ITEMS; j++) {
     const int64_t i = base + j * SCAN_THREADS + threadIdx.x;
@@ -174,15 +187,15 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan_1p(const long long *in, l
   if (threadIdx.x < 32) {
     const int lane = threadIdx.x;
     long long excl = 0;
-    if (t == 0) {
-      if (lane == 0) lb_publish(lb, 0, e, 2, (unsigned long long)bt);
+    if (t == t0) {
+      if (lane == 0) lb_publish(lb, t, e, 2, (unsigned long long)bt);
     } else {
       if (lane == 0) lb_publish(lb, t, e, 1, (unsigned long long)bt);
       for (int64_t j = t - 1;; j -= 32) {
         const int64_t q = j - lane;  // lane 0: the nearest earlier tile
-        const unsigned long long f = q >= 0 ? lb_wait(lb, q, e) : 0;
-        const bool stop = f != e * 4 + 1;  // inclusive prefix, before tile 0, or a wait that gave up
-        const long long v = (q >= 0 && f != 0) ? lb_value(lb, q, e, f) : 0;
+        const unsigned long long f = q >= t0 ? lb_wait(lb, q, e) : 0;
+        const bool stop = f != e * 4 + 1;  // inclusive prefix, before the array's first tile, or gave up
+        const long long v = (q >= t0 && f != 0) ? lb_value(lb, q, e, f) : 0;
         const unsigned m = __ballot_sync(FULL, stop);
         if (m) {
           const int first = __ffs(m) - 1;
@@ -208,15 +221,18 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan_1p(const long long *in, l
     const int64_t i = base + j * SCAN_THREADS + threadIdx.x;
     if (i < n) out[i] = tile[j * SCAN_THREADS + threadIdx.x];
   }
-  if (threadIdx.x == 0 && total && base + SCAN_TILE >= n) *total = sh_prefix + bt;
+  if (threadIdx.x == 0 && a.total[arr] && base + SCAN_TILE >= n) *a.total[arr] = sh_prefix + bt;
   if (lb_end(lb)) lb_advance(lb);
 }
 
 // Small inputs: one block; coalesced loads into shared memory, each thread
 // scans 4 consecutive values, one block scan, coalesced stores.
 constexpr int SCAN_SMALL = 1024 * 4;
-__global__ void __launch_bounds__(1024) k_scan_small(const long long *in, long long *out, int64_t n,
-                                                      long long *total) {
+__global__ void __launch_bounds__(1024) k_scan_small(ScanArgs a) {
+  const long long *__restrict__ in = a.in[blockIdx.x];
+  long long *out = a.out[blockIdx.x];
+  long long *total = a.total[blockIdx.x];
+  const int64_t n = a.n;
   __shared__ long long tile[SCAN_SMALL];
   for (int i = threadIdx.x; i < SCAN_SMALL; i += 1024) tile[i] = i < n ? in[i] : 0;
   __syncthreads();
@@ -245,14 +261,32 @@ int scan_i64(const long long *in, long long *out, int64_t n, long long *total, A
     if (total) DCSR_CUDA(cudaMemsetAsync(total, 0, sizeof(long long), s));
     return DCSR_OK;
   }
+  ScanArgs a{{in, nullptr}, {out, nullptr}, {total, nullptr}, n, div_up(n, SCAN_TILE)};
   if (n <= SCAN_SMALL) {
-    DCSR_LAUNCH(k_scan_small, 1, 1024, 0, s, in, out, n, total);
+    DCSR_LAUNCH(k_scan_small, 1, 1024, 0, s, a);
     return DCSR_OK;
   }
-  const int64_t nt = div_up(n, SCAN_TILE);
   Lookback lb;
-  DCSR_TRY(ar.lookback((size_t)nt, s, &lb));
-  DCSR_LAUNCH(k_scan_1p, (unsigned)nt, SCAN_THREADS, 0, s, in, out, n, total, lb);
+  DCSR_TRY(ar.lookback((size_t)a.nt, s, &lb));
+  DCSR_LAUNCH(k_scan_1p, (unsigned)a.nt, SCAN_THREADS, 0, s, a, lb);
+  return DCSR_OK;
+}
+
+int scan2_i64(const long long *in0, long long *out0, long long *total0, const long long *in1, long long *out1,
+              long long *total1, int64_t n, Arena &ar, cudaStream_t s) {
+  if (n <= 0) {
+    if (total0) DCSR_CUDA(cudaMemsetAsync(total0, 0, sizeof(long long), s));
+    if (total1) DCSR_CUDA(cudaMemsetAsync(total1, 0, sizeof(long long), s));
+    return DCSR_OK;
+  }
+  ScanArgs a{{in0, in1}, {out0, out1}, {total0, total1}, n, div_up(n, SCAN_TILE)};
+  if (n <= SCAN_SMALL) {
+    DCSR_LAUNCH(k_scan_small, 2, 1024, 0, s, a);
+    return DCSR_OK;
+  }
+  Lookback lb;
+  DCSR_TRY(ar.lookback((size_t)(2 * a.nt), s, &lb));
+  DCSR_LAUNCH(k_scan_1p, (unsigned)(2 * a.nt), SCAN_THREADS, 0, s, a, lb);
   return DCSR_OK;
 }
 
@@ -572,7 +606,7 @@ size_t lookback_slots(int64_t n) {
   // histogram table; scans: one slot per tile
   const int64_t sort = n <= RS_MID ? div_up(n, RS_THREADS * 8) * RS_BINS
                                    : div_up(div_up(n, RS_THREADS * 16) * RS_BINS, SCAN_TILE);
-  return (size_t)(std::max<int64_t>(sort, div_up(n, SCAN_TILE)) + 1);
+  return (size_t)(std::max<int64_t>(sort, 2 * div_up(n, SCAN_TILE)) + 1);
 }
 
 // Large inputs: three kernels per pass (tile histograms, table scan, scatter).

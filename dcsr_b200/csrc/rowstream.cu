@@ -225,8 +225,7 @@ static int schedule_src(const Src &src, int count, int64_t R, Arena &ar, cudaStr
   long long *lf = ar.take<long long>(R + 2), *mf = ar.take<long long>(R + 2);
   const int g = grid_for(R + 1, 256);
   DCSR_LAUNCH((k_sched_flags<V, Src>), g, 256, 0, s, src, R, lf, mf);
-  DCSR_TRY(scan_i64(lf, lf, R + 1, nullptr, ar, s));
-  DCSR_TRY(scan_i64(mf, mf, R + 1, nullptr, ar, s));
+  DCSR_TRY(scan2_i64(lf, lf, nullptr, mf, mf, nullptr, R + 1, ar, s));
   DCSR_LAUNCH((k_sched_emit<V, Src>), g, 256, 0, s, src, R, lf, mf);
   DCSR_LAUNCH((k_sched_info<V, Src>), grid_for((int64_t)count * 32, 256), 256, 0, s, src, lf, mf);
   return DCSR_OK;
@@ -258,7 +257,7 @@ int build_schedule(dcsr_handle h, cudaStream_t s, Arena *ar) {
 // Exclusive prefix over the matrices of each class's unit count (one block
 // of 1024 threads, 1024 matrices per round).
 template <typename V>
-__global__ void __launch_bounds__(1024) k_unit_prefix(const RowItem<V> *its, int count, long long *pref) {
+__device__ __forceinline__ void unit_prefix_block(const RowItem<V> *its, int count, long long *pref) {
   __shared__ long long wsum[3][32];
   __shared__ long long carry[3];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -291,6 +290,24 @@ __global__ void __launch_bounds__(1024) k_unit_prefix(const RowItem<V> *its, int
     __syncthreads();
   }
   if (threadIdx.x < 3) pref[threadIdx.x * (count + 1) + count] = carry[threadIdx.x];
+}
+
+template <typename V>
+__global__ void __launch_bounds__(1024) k_unit_prefix(const RowItem<V> *its, int count, long long *pref) {
+  unit_prefix_block(its, count, pref);
+}
+
+// Several SpMV groups' prefixes in one launch, one block per group.
+template <typename V>
+struct PrefixJobs {
+  const RowItem<V> *its[MAX_PREFIX_JOBS];
+  int count[MAX_PREFIX_JOBS];
+  long long *pref[MAX_PREFIX_JOBS];
+};
+
+template <typename V>
+__global__ void __launch_bounds__(1024) k_unit_prefix_many(PrefixJobs<V> jobs) {
+  unit_prefix_block(jobs.its[blockIdx.x], jobs.count[blockIdx.x], jobs.pref[blockIdx.x]);
 }
 
 // ------------------------------------------------------------- helpers
@@ -988,8 +1005,8 @@ static int reduce_dispatch(dcsr_handle h, int32_t op, V *y, cudaStream_t s) {
 // Batched SpMV over a set of matrices of one k family: kf = 1 (k = 1,
 // streamed short rows), 2, 4 or 8 (each item's k <= kf, read by the kernel).
 template <typename V>
-static int spmv_many_t(const RowItem<V> *its, int count, int kf, long long *pref, cudaStream_t s) {
-  DCSR_LAUNCH(k_unit_prefix<V>, 1, 1024, 0, s, its, count, pref);
+static int spmv_many_t(const RowItem<V> *its, int count, int kf, long long *pref, bool prefixed, cudaStream_t s) {
+  if (!prefixed) DCSR_LAUNCH(k_unit_prefix<V>, 1, 1024, 0, s, its, count, pref);
   RowMany<V> src{its, count, pref};
   switch (kf) {
     case 1: return launch_reduce_src<V, 1, OP_SPMV, false>(src, s);
@@ -1000,10 +1017,32 @@ static int spmv_many_t(const RowItem<V> *its, int count, int kf, long long *pref
   return DCSR_BAD_ARG;
 }
 
-int spmv_many(const void *items_dev, int dtype, int count, int k, long long *pref, cudaStream_t s) {
+int spmv_many(const void *items_dev, int dtype, int count, int k, long long *pref, cudaStream_t s, bool prefixed) {
   if (count == 0) return DCSR_OK;
-  if (dtype == DCSR_F32) return spmv_many_t<float>((const RowItem<float> *)items_dev, count, k, pref, s);
-  return spmv_many_t<double>((const RowItem<double> *)items_dev, count, k, pref, s);
+  if (dtype == DCSR_F32) return spmv_many_t<float>((const RowItem<float> *)items_dev, count, k, pref, prefixed, s);
+  return spmv_many_t<double>((const RowItem<double> *)items_dev, count, k, pref, prefixed, s);
+}
+
+template <typename V>
+static int unit_prefix_many_t(const void *const *items, const int *counts, long long *const *prefs, int n,
+                              cudaStream_t s) {
+  PrefixJobs<V> jobs;
+  std::memset(&jobs, 0, sizeof(jobs));
+  for (int i = 0; i < n; i++) {
+    jobs.its[i] = (const RowItem<V> *)items[i];
+    jobs.count[i] = counts[i];
+    jobs.pref[i] = prefs[i];
+  }
+  DCSR_LAUNCH(k_unit_prefix_many<V>, n, 1024, 0, s, jobs);
+  return DCSR_OK;
+}
+
+int unit_prefix_many(const void *const *items, const int *counts, long long *const *prefs, int n, int dtype,
+                     cudaStream_t s) {
+  if (n < 1) return DCSR_OK;
+  if (n > MAX_PREFIX_JOBS) return DCSR_BAD_ARG;
+  if (dtype == DCSR_F32) return unit_prefix_many_t<float>(items, counts, prefs, n, s);
+  return unit_prefix_many_t<double>(items, counts, prefs, n, s);
 }
 
 template <typename V>

@@ -675,8 +675,10 @@ static int update_pipeline(const Src &src, int count, int64_t T, bool merge, int
   } else {
     DCSR_LAUNCH((k_plan_append<V, Src>), gT, 256, 0, s, src, T, gstat, trow, tb0, tmat, tcap, ttiles, tmnew, tinfo);
   }
-  DCSR_TRY(scan_i64(tcap, tcap, T + 1, gstat + ST_TOTAL, ar, s));
-  if (merge) DCSR_TRY(scan_i64(ttiles, ttiles, T + 1, gstat + ST_TILES, ar, s));
+  if (merge)
+    DCSR_TRY(scan2_i64(tcap, tcap, gstat + ST_TOTAL, ttiles, ttiles, gstat + ST_TILES, T + 1, ar, s));
+  else
+    DCSR_TRY(scan_i64(tcap, tcap, T + 1, gstat + ST_TOTAL, ar, s));
   DCSR_LAUNCH((k_check<V, Src>), gI, 256, 0, s, src, count, tcap);
   if (merge) {
     DCSR_LAUNCH((k_apply_existing<V, Src>), gT, 256, 0, s, src, k0, T, f, bval, bpos);
