@@ -11,10 +11,13 @@ served (headline)  2000 resident matrices (rows log-uniform [1k, 256k], mean
         dcsr_spmv / dcsr_to_csr) is measured first: its capacity (all requests
         queued at once) and its p99 latency under Poisson arrivals at 50, 70
         and 90% of that capacity; the 90% point (its best sustained
-        throughput) sets the latency target.  The batched server (continuous batching, memory
-        admission) then runs Poisson arrivals at fractions of its own capacity;
-        `value` = its request throughput at the highest load whose p99 stays
-        at or below the plain path's p99.  Throughput = requests / wall time
+        throughput) sets the latency target.  The batched server (continuous
+        batching, memory admission) then runs Poisson arrivals at fractions of
+        its own capacity; `value` = its request throughput at the highest load
+        whose p99 stays at or below the plain path's p99.  Every load point
+        of both servers is replayed three times with different arrival seeds
+        and stands as its median-p99 run (one run's p99 rests on its 1%
+        slowest requests and moved by +-30% between runs).  Throughput = requests / wall time
         from the first scheduled arrival to the last completion (the GPU is
         idle before and after); latency = scheduled arrival -> result visible
         to the caller.  `value` uses device-resident request buffers; `e2e`
@@ -150,6 +153,10 @@ def stream_part(args, dev, world):
     A = api.DcsrMatrix(n, n, torch.float32)
     A.from_csr(torch.from_numpy(rp).to(dev), torch.from_numpy(cols).to(dev), torch.from_numpy(vals).to(dev))
     dbatch = [tuple(torch.from_numpy(a).to(dev) for a in b) for b in batches]
+    # set-up: room in the device pool for the matrix to grow into (compaction
+    # and repair allocate new pools; mapping new memory during the stream
+    # would time the driver, not the library)
+    api.pool_reserve(8 << 30)
     rng = np.random.default_rng(args.seed + 1)
     x = torch.from_numpy(rng.uniform(-1, 1, n).astype(np.float32)).to(dev)
     y = torch.empty(n, dtype=torch.float32, device=dev)
@@ -347,6 +354,7 @@ def batched_part(args, dev):
     for w, o0, o1 in zip(work, offs[:-1], offs[1:]):
         w["rows"], w["cols"], w["vals"] = (t[o0:o1] for t in live)
     torch.cuda.synchronize()
+    api.pool_reserve(16 << 30)  # set-up: room for repairs to grow matrices into
     s = torch.cuda.Stream()
     batch = api.DcsrBatch(work, stream=s)
     tuned = batch.autotune(s)  # row-class thresholds for this set (outputs untouched)
@@ -488,6 +496,23 @@ def replay(api, srv, trace, arrivals, lo=0, hi=None):
             "p99_ms": pct(lat, 99), "errors": bad, "mean_batch": float(sizes.mean())}
 
 
+def replay_point(api, srv, trace, rate, n, seed, repeats, lo=0, hi=None):
+    """`repeats` Poisson replays at one offered rate (different arrival seeds);
+    the run with the median p99 stands for the point (a single run's p99 rests
+    on its 1% slowest requests), with every run's p99 listed beside it."""
+    runs = []
+    for j in range(repeats):
+        launches0 = api.launch_count()
+        r = replay(api, srv, trace, poisson_arrivals(rate, n, seed + 1000 * j), lo, hi)
+        r["kernel_launches"] = api.launch_count() - launches0
+        runs.append(r)
+    order = sorted(range(len(runs)), key=lambda j: runs[j]["p99_ms"])
+    pick = dict(runs[order[len(runs) // 2]])
+    pick["p99_ms_runs"] = [round(r["p99_ms"], 3) for r in runs]
+    pick["offered_req_s"] = rate
+    return pick
+
+
 def poisson_arrivals(rate_per_s, n, seed):
     rng = np.random.default_rng(seed)
     return np.cumsum(rng.exponential(1e6 / rate_per_s, n))
@@ -543,9 +568,8 @@ def served_part(args, dev, rank, local_rank):
         cap = replay(api, srv, tr, np.zeros(Np), 0, Np)
         pts = []
         for f in args.plain_fracs:
-            r = replay(api, srv, tr, poisson_arrivals(f * cap["req_s"], Np, args.seed + 8), 0, Np)
-            r["offered_req_s"] = f * cap["req_s"]
-            pts.append({k: round(v, 3) for k, v in r.items()})
+            r = replay_point(api, srv, tr, f * cap["req_s"], Np, args.seed + 8, args.repeats, 0, Np)
+            pts.append({k: (round(v, 3) if not isinstance(v, list) else v) for k, v in r.items()})
         srv.close()
         ref = pts[-1]
         return {"capacity_req_s": round(cap["req_s"], 1), "sweep": pts,
@@ -568,11 +592,8 @@ def served_part(args, dev, rank, local_rank):
         cap = replay(api, srv, tr, np.zeros(N))
         pts, best, best_f = [], None, None
         for f in args.load_fracs:
-            launches0 = api.launch_count()
-            r = replay(api, srv, tr, poisson_arrivals(f * cap["req_s"], N, args.seed + 9))
-            r["kernel_launches"] = api.launch_count() - launches0
-            r["offered_req_s"] = f * cap["req_s"]
-            pts.append({k: round(v, 3) for k, v in r.items()})
+            r = replay_point(api, srv, tr, f * cap["req_s"], N, args.seed + 9, args.repeats)
+            pts.append({k: (round(v, 3) if not isinstance(v, list) else v) for k, v in r.items()})
             if r["p99_ms"] <= p99_plain and r["errors"] == 0 and (best is None or r["req_s"] > best["req_s"]):
                 best, best_f = r, f
         met = best is not None
@@ -606,7 +627,7 @@ def served_part(args, dev, rank, local_rank):
     out["p99_ms"] = best["p99_ms"]
     out["speedup_at_equal_p99"] = round(best["req_s"] / ref_p["req_s"], 2)
     out["speedup_vs_plain_capacity"] = round(best["req_s"] / cap_p["req_s"], 2)
-    out["e2e"] = {k: round(v, 3) for k, v in e2e.items()}
+    out["e2e"] = {k: (round(v, 3) if not isinstance(v, list) else v) for k, v in e2e.items()}
     out["e2e"].update({"capacity_req_s": round(cap_h["req_s"], 1), "chosen_load_frac": e2e_f,
                        "p99_constraint_met": e2e_met, "sweep": sweep_h,
                        "speedup_at_equal_p99": round(e2e["req_s"] / out["plain_host_buffers"]["slo_point"]["req_s"], 2)})
@@ -717,7 +738,7 @@ def run_ours(args, rank, world, local_rank):
         "config": {"workload": "served: " + served["workload"],
                    "headline": "batched-server req/s at the highest Poisson load whose p99 <= the plain per-call "
                                "server's p99 at its highest load (90% of its capacity); device-resident request "
-                               "buffers",
+                               f"buffers; each load point the median-p99 of {args.repeats} replays",
                    "parallelism": f"matrix shards x{world} (no data-path collective)",
                    "l2": "working sets > L2 (60 GB resident; SpMV roofline flushes L2 between launches)"},
         "p50_ms": served["p50_ms"], "p99_ms": served["p99_ms"],
@@ -777,6 +798,7 @@ def main():
     ap.add_argument("--max-batch", type=int, default=256)
     ap.add_argument("--depth", type=int, default=6)
     ap.add_argument("--workers", type=int, default=2)
+    ap.add_argument("--repeats", type=int, default=3, help="Poisson replays per served load point (median p99)")
     ap.add_argument("--load-fracs", type=float, nargs="+", default=[0.3, 0.4, 0.5, 0.55, 0.6, 0.65, 0.7, 0.75, 0.85])
     ap.add_argument("--plain-fracs", type=float, nargs="+", default=[0.5, 0.7, 0.9])
     ap.add_argument("--batched-mats", type=int, default=512)

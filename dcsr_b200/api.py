@@ -124,6 +124,7 @@ _SIGS = {
     "dcsr_status_string": (C.c_char_p, [_i32]),
     "dcsr_launch_count": (C.c_uint64, []),
     "dcsr_spin_faults": (C.c_int, [C.POINTER(C.c_int64)]),
+    "dcsr_pool_reserve": (C.c_int, [C.c_int64, C.c_void_p]),
     "dcsr_version": (C.c_char_p, []),
 }
 
@@ -149,6 +150,12 @@ def status_string(st: int) -> str:
 
 def launch_count() -> int:
     return int(lib().dcsr_launch_count())
+
+
+def pool_reserve(nbytes: int, stream=None):
+    """Pre-grow the device memory pool the library allocates from (kept for
+    later growth of matrices, scratch and staging)."""
+    _check(lib().dcsr_pool_reserve(int(nbytes), _stream(stream)), "dcsr_pool_reserve")
 
 
 def _check(st: int, what: str):

@@ -103,6 +103,7 @@ struct Lookback {
   unsigned *tiles, *done;
   unsigned *hist;  // [8][256]
   unsigned long long *flag, *agg, *inc;
+  unsigned long long slots;  // entries of flag / agg / inc
 };
 constexpr size_t LB_HEADER = 64 + 8 * 256 * 4;
 
@@ -137,6 +138,7 @@ struct Arena {
     out->flag = (unsigned long long *)(lb + LB_HEADER);
     out->agg = out->flag + lb_slots;
     out->inc = out->agg + lb_slots;
+    out->slots = lb_slots;
     return DCSR_OK;
   }
   int reserve(size_t bytes, cudaStream_t s) {

@@ -205,6 +205,25 @@ int reserve(dcsr_handle h, int64_t cap, cudaStream_t s) {
   return DCSR_OK;
 }
 
+// Pools and scratch use stream-ordered allocation; keep freed blocks in the
+// device's default pool instead of returning them at every sync, so a
+// compaction's fresh pool does not re-map memory each time (once per device).
+void keep_pool_memory() {
+  static std::mutex mu;
+  static bool configured[64] = {};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lock(mu);
+  if (dev >= 0 && dev < 64 && !configured[dev]) {
+    cudaMemPool_t mp;
+    if (cudaDeviceGetDefaultMemPool(&mp, dev) == cudaSuccess) {
+      uint64_t thr = UINT64_MAX;
+      cudaMemPoolSetAttribute(mp, cudaMemPoolAttrReleaseThreshold, &thr);
+    }
+    configured[dev] = true;
+  }
+}
+
 int compact(dcsr_handle h, cudaStream_t s) {
   const int32_t n = h->n_rows;
   Arena &ar = h->scratch;
@@ -280,24 +299,7 @@ int dcsr_create(dcsr_handle *out, int32_t n_rows, int32_t n_cols, int32_t dtype,
   if (o.max_segs < 1 || o.max_segs > MAX_SEGS || o.factor_x16 < 16 || o.align < 1 || (o.align & (o.align - 1)) ||
       o.min_cap < 0 || o.alpha < 0 || o.spare_x16 < 0 || o.min_spare < 0 || (o.mode != DCSR_MERGE && o.mode != DCSR_APPEND))
     return DCSR_BAD_ARG;
-  {
-    // Pools and scratch use stream-ordered allocation; keep freed blocks in
-    // the device's default pool instead of returning them at every sync, so a
-    // compaction's fresh pool does not re-map memory each time.
-    static std::mutex mu;
-    static bool configured[64] = {};
-    int dev = 0;
-    cudaGetDevice(&dev);
-    std::lock_guard<std::mutex> lock(mu);
-    if (dev >= 0 && dev < 64 && !configured[dev]) {
-      cudaMemPool_t mp;
-      if (cudaDeviceGetDefaultMemPool(&mp, dev) == cudaSuccess) {
-        uint64_t thr = UINT64_MAX;
-        cudaMemPoolSetAttribute(mp, cudaMemPoolAttrReleaseThreshold, &thr);
-      }
-      configured[dev] = true;
-    }
-  }
+  keep_pool_memory();
   dcsr_matrix_s *h = new dcsr_matrix_s;
   h->n_rows = n_rows;
   h->n_cols = n_cols;
@@ -606,6 +608,18 @@ const char *dcsr_status_string(int st) {
 }
 
 uint64_t dcsr_launch_count(void) { return g_launches.load(); }
+
+int dcsr_pool_reserve(int64_t bytes, void *stream) {
+  if (bytes < 0) return DCSR_BAD_ARG;
+  if (bytes == 0) return DCSR_OK;
+  cudaStream_t s = (cudaStream_t)stream;
+  keep_pool_memory();
+  void *p = nullptr;
+  DCSR_CUDA(cudaMallocAsync(&p, (size_t)bytes, s));
+  DCSR_CUDA(cudaFreeAsync(p, s));
+  DCSR_CUDA(cudaStreamSynchronize(s));
+  return DCSR_OK;
+}
 
 int dcsr_spin_faults(int64_t *count) {
   if (!count) return DCSR_BAD_ARG;

@@ -75,11 +75,12 @@ __device__ __forceinline__ unsigned long long ld_vol(const unsigned long long *p
 }
 
 // The flag of slot q once published in epoch e (0 after a wait that gave up).
+// Exact match: the slot may hold a word of any earlier kernel, a scan's
+// (epoch * 4 + kind) or a radix sort's packed word.
 __device__ __forceinline__ unsigned long long lb_wait(const Lookback &lb, int64_t q, unsigned long long e) {
-  const unsigned long long want = e * 4 + 1;
   for (int it = 0; it < SPIN_LIMIT; it++) {
     const unsigned long long f = ld_vol(lb.flag + q);
-    if (f >= want) return f;
+    if (f == e * 4 + 1 || f == e * 4 + 2) return f;
     if ((it & 1023) == 1023 && ld_vol(&g_spin_faults) != 0) break;  // an earlier wait gave up: stop at once
     if (it >= 32) __nanosleep(64);
   }
@@ -102,6 +103,18 @@ __device__ __forceinline__ long long lb_value(const Lookback &lb, int64_t q, uns
   return (long long)ld_vol((f == e * 4 + 2 ? lb.inc : lb.agg) + q);
 }
 
+// Radix look-back slots are single 64-bit words: tag (the epoch's low 30
+// bits, kind) above a 32-bit count, so a slot is published and read in one
+// access -- no fences, no second load.  A scan's flag (epoch * 4 + kind, far
+// below 2^32) has kind bits 0 here, and a packed word (at least 2^32) never
+// equals a scan's flag.  The tag repeats every 2^30 kernels on one area: the
+// kernel whose last block advances the epoch to such a multiple clears the
+// area (lb_advance), so a stale word never matches.
+constexpr unsigned long long LB_EMASK = (1ull << 30) - 1;
+__device__ __forceinline__ unsigned long long lb_pack(unsigned long long e, int kind, unsigned v) {
+  return ((e & LB_EMASK) << 34) | ((unsigned long long)kind << 32) | v;
+}
+
 // Thread 0 of every block: the block's tile and the kernel's epoch.
 __device__ __forceinline__ void lb_begin(const Lookback &lb, unsigned *tile, unsigned long long *ep) {
   if (threadIdx.x == 0) {
@@ -114,21 +127,26 @@ __device__ __forceinline__ void lb_begin(const Lookback &lb, unsigned *tile, uns
 __device__ __forceinline__ bool lb_end(const Lookback &lb) {
   __shared__ int last;
   __syncthreads();
-  if (threadIdx.x == 0) {
-    __threadfence();
-    last = atomicAdd(lb.done, 1u) == gridDim.x - 1;
-  }
+  // (no fence: this block's results reach later kernels at the launch boundary)
+  if (threadIdx.x == 0) last = atomicAdd(lb.done, 1u) == gridDim.x - 1;
   __syncthreads();
   return last;
 }
 
-// The last block: reset the counters and advance the epoch.
+// The last block (all its threads): reset the counters and advance the
+// epoch; at a multiple of 2^30 clear the slots first (packed radix tags).
 __device__ __forceinline__ void lb_advance(const Lookback &lb) {
+  __shared__ unsigned long long next;
+  if (threadIdx.x == 0) next = ld_vol(lb.epoch) + 1;
+  __syncthreads();
+  if ((next & LB_EMASK) == 0)
+    for (unsigned long long i = threadIdx.x; i < lb.slots; i += blockDim.x) lb.flag[i] = 0;
+  __syncthreads();
   if (threadIdx.x == 0) {
     *(volatile unsigned *)lb.tiles = 0;
     *(volatile unsigned *)lb.done = 0;
-    *(volatile unsigned long long *)lb.epoch = ld_vol(lb.epoch) + 1;
     __threadfence();
+    *(volatile unsigned long long *)lb.epoch = next;
   }
 }
 
@@ -405,23 +423,25 @@ __global__ void __launch_bounds__(RS_THREADS) k_radix_hist_all(const unsigned lo
     if (h[i]) atomicAdd(lb.hist + i, h[i]);
 }
 
-template <int RS_ITEMS>
-__global__ void __launch_bounds__(RS_THREADS, 2) k_radix_onesweep(const unsigned long long *keys,
+template <int OS_THREADS, int RS_ITEMS, int MIN_BLOCKS>
+__global__ void __launch_bounds__(OS_THREADS, MIN_BLOCKS) k_radix_onesweep(const unsigned long long *keys,
                                                                    const unsigned *vals, unsigned long long *keys_out,
                                                                    unsigned *vals_out, int64_t n, int pass,
                                                                    int last_pass, Lookback lb) {
-  constexpr int RS_TILE = RS_THREADS * RS_ITEMS;
-  __shared__ unsigned wcnt[RS_WARPS][RS_BINS];
+  constexpr int RS_TILE = OS_THREADS * RS_ITEMS, OS_WARPS = OS_THREADS / 32;
+  __shared__ unsigned wcnt[OS_WARPS][RS_BINS];
   __shared__ long long boff[RS_BINS];
   __shared__ unsigned sh_tile;
   __shared__ unsigned long long sh_ep;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, d = threadIdx.x;
   const int shift = 8 * pass;
   lb_begin(lb, &sh_tile, &sh_ep);
-  for (int w = 0; w < RS_WARPS; w++) wcnt[w][d] = 0;
-  // the digit's first position in the output: exclusive scan of the histogram
+  for (int i = threadIdx.x; i < OS_WARPS * RS_BINS; i += OS_THREADS) (&wcnt[0][0])[i] = 0;
+  // the digit's first position in the output: exclusive scan of the
+  // histogram (thread d < RS_BINS owns digit d from here on)
   long long all;
-  const long long gbase = block_excl_scan((long long)__ldcg(lb.hist + pass * RS_BINS + d), &all);
+  const long long gbase =
+      block_excl_scan((long long)(d < RS_BINS ? __ldcg(lb.hist + pass * RS_BINS + d) : 0u), &all);
   const int64_t t = sh_tile;
   const unsigned long long e = sh_ep;
   if (t >= gridDim.x) {  // a tile counter left non-zero (a bug): count it, touch nothing
@@ -431,12 +451,17 @@ __global__ void __launch_bounds__(RS_THREADS, 2) k_radix_onesweep(const unsigned
   }
   const int64_t base = t * RS_TILE + (int64_t)warp * (32 * RS_ITEMS);
   unsigned long long k[RS_ITEMS];
-  unsigned rank[RS_ITEMS];
+  unsigned rank[RS_ITEMS], val[RS_ITEMS];
   const unsigned lt = lanemask_lt();
+#pragma unroll
+  for (int j = 0; j < RS_ITEMS; j++) {  // keys and values in one round of loads
+    const int64_t i = base + j * 32 + lane;
+    k[j] = i < n ? keys[i] : ~0ull;
+    val[j] = i < n ? vals[i] : 0u;
+  }
 #pragma unroll
   for (int j = 0; j < RS_ITEMS; j++) {
     const int64_t i = base + j * 32 + lane;
-    k[j] = i < n ? keys[i] : ~0ull;
     const unsigned dg = i < n ? (unsigned)((k[j] >> shift) & 0xff) : 0x100u;
     const unsigned peers = __match_any_sync(FULL, dg);
     const unsigned pre = dg < 0x100u ? wcnt[warp][dg] : 0u;
@@ -447,36 +472,40 @@ __global__ void __launch_bounds__(RS_THREADS, 2) k_radix_onesweep(const unsigned
   }
   __syncthreads();
   unsigned run = 0;  // exclusive prefix across warps per digit; run = the tile's count of digit d
-  for (int w = 0; w < RS_WARPS; w++) {
-    const unsigned c = wcnt[w][d];
-    wcnt[w][d] = run;
-    run += c;
-  }
+  if (d < RS_BINS)
+    for (int w = 0; w < OS_WARPS; w++) {
+      const unsigned c = wcnt[w][d];
+      wcnt[w][d] = run;
+      run += c;
+    }
   // items of digit d in the tiles before this one: look back over windows of
   // LB_W earlier tiles (their flags loaded together), consuming published
   // aggregates up to the nearest published inclusive prefix
   long long excl = 0;
   const int64_t slot = t * RS_BINS + d;
-  if (t == 0) {
-    lb_publish(lb, slot, e, 2, run);
+  if (d >= RS_BINS) {
+    // no digit: nothing to look back for
+  } else if (t == 0) {
+    *(volatile unsigned long long *)(lb.flag + slot) = lb_pack(e, 2, run);
   } else {
-    lb_publish(lb, slot, e, 1, run);
-    const unsigned long long want = e * 4 + 1, incf = e * 4 + 2;
+    *(volatile unsigned long long *)(lb.flag + slot) = lb_pack(e, 1, run);
+    const unsigned long long tag = e & LB_EMASK;
     int64_t q = t - 1;
     int idle = 0;
     bool done = false;
     while (!done) {
       unsigned long long f[LB_W];
 #pragma unroll
-      for (int j = 0; j < LB_W; j++) f[j] = q - j >= 0 ? ld_vol(lb.flag + (q - j) * RS_BINS + d) : incf;
-      __threadfence();
+      for (int j = 0; j < LB_W; j++)
+        f[j] = q - j >= 0 ? ld_vol(lb.flag + (q - j) * RS_BINS + d) : lb_pack(e, 2, 0);  // before tile 0: 0
       int used = 0;
 #pragma unroll
       for (int j = 0; j < LB_W; j++) {
-        if (done || used < j || f[j] < want) continue;  // stop at the first unpublished tile
-        if (q - j >= 0) excl += (long long)ld_vol((f[j] == incf ? lb.inc : lb.agg) + (q - j) * RS_BINS + d);
+        // stop at the first tile that has not published in this epoch
+        if (done || used < j || (f[j] >> 34) != tag || ((f[j] >> 32) & 3) == 0) continue;
+        excl += (long long)(f[j] & 0xffffffffull);
         used = j + 1;
-        done = f[j] == incf;
+        done = ((f[j] >> 32) & 3) == 2;
       }
       q -= used;
       if (used == 0) {  // the nearest tile has not published yet
@@ -487,9 +516,9 @@ __global__ void __launch_bounds__(RS_THREADS, 2) k_radix_onesweep(const unsigned
         if (idle >= 32) __nanosleep(64);
       }
     }
-    lb_publish(lb, slot, e, 2, (unsigned long long)(excl + run));
+    *(volatile unsigned long long *)(lb.flag + slot) = lb_pack(e, 2, (unsigned)(excl + run));
   }
-  boff[d] = gbase + excl;
+  if (d < RS_BINS) boff[d] = gbase + excl;
   __syncthreads();
 #pragma unroll
   for (int j = 0; j < RS_ITEMS; j++) {
@@ -498,12 +527,12 @@ __global__ void __launch_bounds__(RS_THREADS, 2) k_radix_onesweep(const unsigned
       const unsigned dg = (unsigned)((k[j] >> shift) & 0xff);
       const int64_t pos = boff[dg] + wcnt[warp][dg] + rank[j];
       keys_out[pos] = k[j];
-      vals_out[pos] = vals[i];
+      vals_out[pos] = val[j];
     }
   }
   if (lb_end(lb)) {
     if (last_pass)  // leave the histogram table cleared for the next sort
-      for (int i = threadIdx.x; i < 8 * RS_BINS; i += RS_THREADS) lb.hist[i] = 0;
+      for (int i = threadIdx.x; i < 8 * RS_BINS; i += OS_THREADS) lb.hist[i] = 0;
     __syncthreads();
     lb_advance(lb);
   }
@@ -633,9 +662,13 @@ static int radix_passes_table(unsigned long long **keys, unsigned **vals, unsign
 }
 
 // Mid-size inputs: one histogram kernel, then one single-pass scatter per pass.
+// Tile shape of the single-pass scatter: OS_T threads x OS_I keys per thread
+// (tiles of 4096 and 8192 keys, with 256-1024 threads, ran no faster: the
+// pass time is the chain of memory round trips of one tile, not its size).
+constexpr int OS_T = 256, OS_I = 8, OS_MB = 2;
 static int radix_passes_onesweep(unsigned long long **keys, unsigned **vals, unsigned long long **keys_tmp,
                                  unsigned **vals_tmp, int64_t n, int bits, Arena &ar, cudaStream_t s) {
-  constexpr int ITEMS = 8;
+  constexpr int ITEMS = OS_T * OS_I / RS_THREADS;  // keys per tile / RS_THREADS
   const int passes = (int)div_up(bits, 8);
   if (passes <= 0) return DCSR_OK;
   const int64_t nt = div_up(n, RS_THREADS * ITEMS);
@@ -644,7 +677,8 @@ static int radix_passes_onesweep(unsigned long long **keys, unsigned **vals, uns
   const int gh = (int)std::min<int64_t>(div_up(n, RS_THREADS * 8), 4 * sm_count());
   DCSR_LAUNCH(k_radix_hist_all, gh, RS_THREADS, 0, s, *keys, n, passes, lb);
   for (int p = 0; p < passes; p++) {
-    DCSR_LAUNCH(k_radix_onesweep<ITEMS>, (unsigned)nt, RS_THREADS, 0, s, *keys, *vals, *keys_tmp, *vals_tmp, n, p,
+    DCSR_LAUNCH((k_radix_onesweep<OS_T, OS_I, OS_MB>), (unsigned)nt, OS_T, 0, s, *keys, *vals, *keys_tmp, *vals_tmp,
+                n, p,
                 p == passes - 1 ? 1 : 0, lb);
     unsigned long long *tk = *keys;
     *keys = *keys_tmp;

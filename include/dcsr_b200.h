@@ -341,6 +341,15 @@ uint64_t dcsr_launch_count(void);
  * running or finished, so a non-zero count indicates a library bug (the
  * affected result is wrong; nothing hangs).  Synchronises the device. */
 int dcsr_spin_faults(int64_t *count);
+/* Pre-grow the current device's stream-ordered memory pool, from which
+ * every matrix pool, scratch arena and staging buffer of this library is
+ * allocated, by `bytes` (allocated and freed on `stream`, then kept by the
+ * pool; the library sets the pool never to release memory it holds).
+ * Growing a matrix (compaction, repair) or staging a large batch then takes
+ * memory the pool already maps: mapping new device memory inside the loop
+ * cost 2 to several hundred milliseconds per allocation on some machines.
+ * Synchronises the stream.  No counterpart in the reference (host memory). */
+int dcsr_pool_reserve(int64_t bytes, void *stream);
 /* Library version string. */
 const char *dcsr_version(void);
 

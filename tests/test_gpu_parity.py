@@ -363,3 +363,17 @@ def test_spgemm_after_updates(dcsr):
     oC = oA.spgemm(oA, oracle_opts_of(dC))
     assert_layout_equal(dC, oC, "C")
     assert_content_equal(dC, oC, "C")
+
+
+def test_pool_reserve(dcsr):
+    """Pre-growing the device pool succeeds, rejects a negative size, and
+    later matrices allocate from it as before (results unchanged)."""
+    import ctypes as C
+    s = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    assert dcsr.lib().dcsr_pool_reserve(-1, s) == dcsr.BAD_ARG
+    assert dcsr.lib().dcsr_pool_reserve(0, s) == 0
+    dcsr.pool_reserve(256 << 20)
+    dev = dcsr.DcsrMatrix(64, 64)
+    dev.from_coo(np.arange(64, dtype=np.int32), np.arange(64, dtype=np.int32), np.full(64, 2.0, np.float32))
+    y = dev.spmv(torch.ones(64, device="cuda"))
+    assert torch.equal(y, torch.full((64,), 2.0, device="cuda"))
