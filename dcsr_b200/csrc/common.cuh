@@ -93,17 +93,16 @@ struct Mat {
 // Device state of the single-pass scan and sort kernels (decoupled look-back):
 // an epoch that the last block of every such kernel advances, the dynamic
 // tile counter and the finished-block counter that block resets, the radix
-// digit histograms (re-zeroed by the sort's last pass), and per look-back slot
-// a flag word (epoch * 4 + 1: aggregate published, epoch * 4 + 2: inclusive
-// prefix published) with separate aggregate and inclusive value words.
-// Zeroed once at allocation: a slot left by an earlier kernel always carries
-// an older epoch, so nothing is cleared between kernels.
+// digit histograms (re-zeroed by the sort's last pass), and the look-back
+// words, each tagged with the epoch that wrote it (prims.cu).  Zeroed once at
+// allocation: a word left by an earlier kernel carries another epoch, so
+// nothing is cleared between kernels.
 struct Lookback {
   unsigned long long *epoch;
   unsigned *tiles, *done;
-  unsigned *hist;  // [8][256]
-  unsigned long long *flag, *agg, *inc;
-  unsigned long long slots;  // entries of flag / agg / inc
+  unsigned *hist;             // [8][256]
+  unsigned long long *flag;   // look-back words
+  unsigned long long slots;   // entries of flag
 };
 constexpr size_t LB_HEADER = 64 + 8 * 256 * 4;
 
@@ -126,7 +125,7 @@ struct Arena {
       lb = nullptr;
       lb_slots = 0;
       const size_t want = slots + slots / 4 + 1024;
-      const size_t bytes = LB_HEADER + 3 * 8 * want;
+      const size_t bytes = LB_HEADER + 8 * want;
       DCSR_CUDA(cudaMallocAsync((void **)&lb, bytes, s));
       DCSR_CUDA(cudaMemsetAsync(lb, 0, bytes, s));
       lb_slots = want;
@@ -136,8 +135,6 @@ struct Arena {
     out->done = (unsigned *)(lb + 12);
     out->hist = (unsigned *)(lb + 64);
     out->flag = (unsigned long long *)(lb + LB_HEADER);
-    out->agg = out->flag + lb_slots;
-    out->inc = out->agg + lb_slots;
     out->slots = lb_slots;
     return DCSR_OK;
   }

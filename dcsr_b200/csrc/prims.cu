@@ -74,42 +74,15 @@ __device__ __forceinline__ unsigned long long ld_vol(const unsigned long long *p
   return *(const volatile unsigned long long *)p;
 }
 
-// The flag of slot q once published in epoch e (0 after a wait that gave up).
-// Exact match: the slot may hold a word of any earlier kernel, a scan's
-// (epoch * 4 + kind) or a radix sort's packed word.
-__device__ __forceinline__ unsigned long long lb_wait(const Lookback &lb, int64_t q, unsigned long long e) {
-  for (int it = 0; it < SPIN_LIMIT; it++) {
-    const unsigned long long f = ld_vol(lb.flag + q);
-    if (f == e * 4 + 1 || f == e * 4 + 2) return f;
-    if ((it & 1023) == 1023 && ld_vol(&g_spin_faults) != 0) break;  // an earlier wait gave up: stop at once
-    if (it >= 32) __nanosleep(64);
-  }
-  atomicAdd(&g_spin_faults, 1ull);
-  return 0;
-}
-
-// Publish slot q: kind 1 = the tile's aggregate, 2 = its inclusive prefix.
-__device__ __forceinline__ void lb_publish(const Lookback &lb, int64_t q, unsigned long long e, int kind,
-                                           unsigned long long v) {
-  *(volatile unsigned long long *)((kind == 1 ? lb.agg : lb.inc) + q) = v;
-  __threadfence();
-  *(volatile unsigned long long *)(lb.flag + q) = e * 4 + kind;
-}
-
-// Value of slot q whose flag f was read by lb_wait.
-__device__ __forceinline__ long long lb_value(const Lookback &lb, int64_t q, unsigned long long e,
-                                              unsigned long long f) {
-  __threadfence();
-  return (long long)ld_vol((f == e * 4 + 2 ? lb.inc : lb.agg) + q);
-}
-
-// Radix look-back slots are single 64-bit words: tag (the epoch's low 30
-// bits, kind) above a 32-bit count, so a slot is published and read in one
-// access -- no fences, no second load.  A scan's flag (epoch * 4 + kind, far
-// below 2^32) has kind bits 0 here, and a packed word (at least 2^32) never
-// equals a scan's flag.  The tag repeats every 2^30 kernels on one area: the
-// kernel whose last block advances the epoch to such a multiple clears the
-// area (lb_advance), so a stale word never matches.
+// Look-back words are packed: a tag (the epoch's low 30 bits, a 2-bit kind)
+// above a 32-bit value, so a word is published with one store and read with
+// one load -- no fences, no second load.  A sort's word per (tile, digit)
+// holds a count (kind 1: the tile's aggregate, 2: its inclusive prefix); a
+// scan's four words per tile hold the halves of its 64-bit aggregate and
+// inclusive prefix (kind 1: written).  A word is current when its tag is the
+// kernel's; the tag repeats every 2^30 kernels on one area, so the kernel
+// whose last block advances the epoch to such a multiple clears the area
+// (lb_advance) and a stale word never matches.
 constexpr unsigned long long LB_EMASK = (1ull << 30) - 1;
 __device__ __forceinline__ unsigned long long lb_pack(unsigned long long e, int kind, unsigned v) {
   return ((e & LB_EMASK) << 34) | ((unsigned long long)kind << 32) | v;
@@ -203,26 +176,59 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan_1p(ScanArgs a, Lookback l
   long long bt;
   long long ex = block_excl_scan(sum, &bt);
   if (threadIdx.x < 32) {
+    // look-back: slot words 4t..4t+3 hold the tile's aggregate (low, high
+    // half) and inclusive prefix (low, high half), each a packed word written
+    // once per epoch, so a reader that sees both halves of one pair current
+    // has a consistent value -- no fences
     const int lane = threadIdx.x;
+    const unsigned long long tag = e & LB_EMASK;
+    unsigned long long *w = lb.flag;
+    auto cur = [&](unsigned long long x) { return (x >> 34) == tag && ((x >> 32) & 3) == 1; };
     long long excl = 0;
     if (t == t0) {
-      if (lane == 0) lb_publish(lb, t, e, 2, (unsigned long long)bt);
+      if (lane == 0) {
+        *(volatile unsigned long long *)(w + 4 * t + 2) = lb_pack(e, 1, (unsigned)bt);
+        *(volatile unsigned long long *)(w + 4 * t + 3) = lb_pack(e, 1, (unsigned)((unsigned long long)bt >> 32));
+      }
     } else {
-      if (lane == 0) lb_publish(lb, t, e, 1, (unsigned long long)bt);
-      for (int64_t j = t - 1;; j -= 32) {
+      if (lane == 0) {
+        *(volatile unsigned long long *)(w + 4 * t + 0) = lb_pack(e, 1, (unsigned)bt);
+        *(volatile unsigned long long *)(w + 4 * t + 1) = lb_pack(e, 1, (unsigned)((unsigned long long)bt >> 32));
+      }
+      int idle = 0;
+      for (int64_t j = t - 1;;) {
         const int64_t q = j - lane;  // lane 0: the nearest earlier tile
-        const unsigned long long f = q >= t0 ? lb_wait(lb, q, e) : 0;
-        const bool stop = f != e * 4 + 1;  // inclusive prefix, before the array's first tile, or gave up
-        const long long v = (q >= t0 && f != 0) ? lb_value(lb, q, e, f) : 0;
-        const unsigned m = __ballot_sync(FULL, stop);
-        if (m) {
-          const int first = __ffs(m) - 1;
+        bool ready = true, inc = true;
+        long long v = 0;
+        if (q >= t0) {  // before the array's first tile: an inclusive prefix of 0
+          const unsigned long long a0 = ld_vol(w + 4 * q), a1 = ld_vol(w + 4 * q + 1);
+          const unsigned long long i0 = ld_vol(w + 4 * q + 2), i1 = ld_vol(w + 4 * q + 3);
+          inc = cur(i0) && cur(i1);
+          ready = inc || (cur(a0) && cur(a1));
+          const unsigned long long lo = inc ? i0 : a0, hi = inc ? i1 : a1;
+          v = (long long)(((hi & 0xffffffffull) << 32) | (lo & 0xffffffffull));
+        }
+        const unsigned rm = __ballot_sync(FULL, ready), im = __ballot_sync(FULL, ready && inc);
+        const int first = im ? __ffs(im) - 1 : 32;  // nearest inclusive prefix in this window
+        const unsigned need = first >= 31 ? FULL : ((2u << first) - 1u);
+        if ((rm & need) == need) {  // everything up to it published
           excl += warp_sum(lane <= first ? v : 0ll);
+          if (first < 32) break;
+          j -= 32;
+          idle = 0;
+          continue;
+        }
+        if (++idle >= SPIN_LIMIT || ((idle & 1023) == 1023 && __any_sync(FULL, ld_vol(&g_spin_faults) != 0))) {
+          if (lane == 0) atomicAdd(&g_spin_faults, 1ull);
           break;
         }
-        excl += warp_sum(v);
+        if (idle >= 32) __nanosleep(64);
       }
-      if (lane == 0) lb_publish(lb, t, e, 2, (unsigned long long)(excl + bt));
+      if (lane == 0) {
+        const unsigned long long p = (unsigned long long)(excl + bt);
+        *(volatile unsigned long long *)(w + 4 * t + 2) = lb_pack(e, 1, (unsigned)p);
+        *(volatile unsigned long long *)(w + 4 * t + 3) = lb_pack(e, 1, (unsigned)(p >> 32));
+      }
     }
     if (lane == 0) sh_prefix = excl;
   }
@@ -285,7 +291,7 @@ int scan_i64(const long long *in, long long *out, int64_t n, long long *total, A
     return DCSR_OK;
   }
   Lookback lb;
-  DCSR_TRY(ar.lookback((size_t)a.nt, s, &lb));
+  DCSR_TRY(ar.lookback((size_t)(4 * a.nt), s, &lb));  // four look-back words per tile
   DCSR_LAUNCH(k_scan_1p, (unsigned)a.nt, SCAN_THREADS, 0, s, a, lb);
   return DCSR_OK;
 }
@@ -303,7 +309,7 @@ int scan2_i64(const long long *in0, long long *out0, long long *total0, const lo
     return DCSR_OK;
   }
   Lookback lb;
-  DCSR_TRY(ar.lookback((size_t)(2 * a.nt), s, &lb));
+  DCSR_TRY(ar.lookback((size_t)(8 * a.nt), s, &lb));
   DCSR_LAUNCH(k_scan_1p, (unsigned)(2 * a.nt), SCAN_THREADS, 0, s, a, lb);
   return DCSR_OK;
 }
@@ -635,7 +641,7 @@ size_t lookback_slots(int64_t n) {
   // histogram table; scans: one slot per tile
   const int64_t sort = n <= RS_MID ? div_up(n, RS_THREADS * 8) * RS_BINS
                                    : div_up(div_up(n, RS_THREADS * 16) * RS_BINS, SCAN_TILE);
-  return (size_t)(std::max<int64_t>(sort, 2 * div_up(n, SCAN_TILE)) + 1);
+  return (size_t)(std::max<int64_t>(sort, 8 * div_up(n, SCAN_TILE)) + 1);  // two-array scans: 4 words x 2 tiles
 }
 
 // Large inputs: three kernels per pass (tile histograms, table scan, scatter).
@@ -759,8 +765,8 @@ __global__ void k_rbk_emit(const int32_t *keys, const V *vals, int64_t n, const 
 // kernel (in host code it names a host-side stand-in); the device address is
 // looked up once per device.
 constexpr size_t NOALLOC_POS_BYTES = (size_t)DCSR_NOALLOC_MAX_KEYS * sizeof(long long);
-constexpr size_t NOALLOC_LB_SLOTS = (DCSR_NOALLOC_MAX_KEYS + SCAN_TILE - 1) / SCAN_TILE + 1;
-constexpr size_t NOALLOC_BYTES = NOALLOC_POS_BYTES + 256 + LB_HEADER + 3 * 8 * NOALLOC_LB_SLOTS;
+constexpr size_t NOALLOC_LB_SLOTS = 4 * ((DCSR_NOALLOC_MAX_KEYS + SCAN_TILE - 1) / SCAN_TILE) + 4;
+constexpr size_t NOALLOC_BYTES = NOALLOC_POS_BYTES + 256 + LB_HEADER + 8 * NOALLOC_LB_SLOTS;
 static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_BYTES];
 
 static int noalloc_scratch(void **out) {
