@@ -190,6 +190,9 @@ int BatchCore::plan(const dcsr_batch_item *its, int n, cudaStream_t s, bool all_
     off = align_up((int64_t)(off + g.idx.size() * desc_size(dtype, true)), 256);
     g.pref_off = poff;
     poff += 3 * (g.idx.size() + 1);
+    int64_t blocks = 0;
+    for (int i : g.idx) blocks += div_up(its[i].matrix->n_rows, 32);
+    g.split = short_split(blocks, g.k);
   }
   img_bytes = off;
   if (img_bytes > img_cap) {
@@ -272,7 +275,7 @@ int BatchCore::enqueue(cudaStream_t s, cudaStream_t s2, cudaEvent_t fork, cudaEv
   // the schedule rebuild below)
   auto prefixes = [&](bool side) -> int {
     const void *its[MAX_PREFIX_JOBS];
-    int cnt[MAX_PREFIX_JOBS];
+    int cnt[MAX_PREFIX_JOBS], spl[MAX_PREFIX_JOBS];
     long long *pr[MAX_PREFIX_JOBS];
     int n = 0;
     for (auto &g : groups)
@@ -280,16 +283,18 @@ int BatchCore::enqueue(cudaStream_t s, cudaStream_t s2, cudaEvent_t fork, cudaEv
         its[n] = img_dev + g.off;
         cnt[n] = (int)g.idx.size();
         pr[n] = pref + g.pref_off;
+        spl[n] = g.split;
         n++;
       }
-    return unit_prefix_many(its, cnt, pr, n, dtype, s);
+    return unit_prefix_many(its, cnt, pr, spl, n, dtype, s);
   };
   if (beside) {  // SpMVs of untouched matrices with valid schedules, on s2 beside the update
     DCSR_TRY(prefixes(true));
     DCSR_CUDA(cudaEventRecord(fork, s));
     DCSR_CUDA(cudaStreamWaitEvent(s2, fork, 0));
     for (auto &g : groups)
-      if (g.side) DCSR_TRY(spmv_many(img_dev + g.off, dtype, (int)g.idx.size(), g.k, pref + g.pref_off, s2, true));
+      if (g.side)
+        DCSR_TRY(spmv_many(img_dev + g.off, dtype, (int)g.idx.size(), g.k, pref + g.pref_off, s2, true, g.split));
     DCSR_CUDA(cudaEventRecord(join, s2));
   }
   const int nu = (int)upd.size();
@@ -308,7 +313,7 @@ int BatchCore::enqueue(cudaStream_t s, cudaStream_t s2, cudaEvent_t fork, cudaEv
   DCSR_TRY(prefixes(false));
   for (auto &g : groups)
     if (!g.side || !beside)
-      DCSR_TRY(spmv_many(img_dev + g.off, dtype, (int)g.idx.size(), g.k, pref + g.pref_off, s, true));
+      DCSR_TRY(spmv_many(img_dev + g.off, dtype, (int)g.idx.size(), g.k, pref + g.pref_off, s, true, g.split));
   if (beside) DCSR_CUDA(cudaStreamWaitEvent(s, join, 0));
   return DCSR_OK;
 }

@@ -72,13 +72,16 @@ size_t schedule_scratch_bytes(int64_t R);
 // y = A x for `count` matrices (items: device RowItem<V>[count]) of one k
 // family: kf = 1, 2, 4 or 8, every item's k <= kf (each item's own k / vec
 // are read by the kernel); pref: device scratch of 3*(count+1) long longs.
-// prefixed: the group's unit prefixes were computed already (unit_prefix_many)
+// prefixed: the group's unit prefixes were computed already (unit_prefix_many,
+// with the same split); split: warps per 32-row block of short rows (short_split)
 int spmv_many(const void *items_dev, int dtype, int count, int k, long long *pref, cudaStream_t s,
-              bool prefixed = false);
+              bool prefixed = false, int split = 1);
+// Warps per 32-row short-row block for an SpMV pass over `blocks` blocks with k RHS.
+int short_split(int64_t blocks, int k);
 // The unit prefixes of up to MAX_PREFIX_JOBS SpMV groups in one launch.
 constexpr int MAX_PREFIX_JOBS = 8;
-int unit_prefix_many(const void *const *items, const int *counts, long long *const *prefs, int n, int dtype,
-                     cudaStream_t s);
+int unit_prefix_many(const void *const *items, const int *counts, long long *const *prefs, const int *splits, int n,
+                     int dtype, cudaStream_t s);
 template <typename V>
 RowItem<V> row_item(dcsr_handle h, const void *x, void *y, int64_t ldx, int64_t ldy, double alpha, double beta);
 // Size the handle's chunk table and chunk partials (K results per chunk).
@@ -102,6 +105,7 @@ struct BatchCore {
   struct Group {
     int k = 1;          // k family: 1, 2, 4 (k 3..4) or 8 (k 5..8)
     bool side = false;  // no update and a valid schedule: may run beside the update
+    int split = 1;      // warps per 32-row short-row block (short_split of its rows)
     std::vector<int> idx;  // items of this group, in item order
     size_t off = 0;        // descriptor offset in the image
     size_t pref_off = 0;   // unit-prefix offset in pref

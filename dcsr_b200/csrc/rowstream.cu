@@ -51,16 +51,20 @@ enum { P_BLOCKS = 0, P_CHUNKS = 1, P_MED = 2 };
 // set of matrices laid end to end in one row space (RowMany, descriptors in
 // device memory, per-class unit prefixes computed on the device).
 
+// split: warps sharing one 32-row block of short rows in the k >= 2 pass
+// (each takes every split-th group pass), so a small matrix's few blocks
+// still fill the GPU; 1 for everything else.
 template <typename V>
 struct RowOne {
   RowItem<V> it;
+  int split = 1;
   __device__ __forceinline__ int n_items() const { return 1; }
   __device__ __forceinline__ const RowItem<V> &item(int) const { return it; }
   __device__ __forceinline__ int find_row(int64_t) const { return 0; }
   __device__ __forceinline__ int64_t units(int part) const {
     if (part == P_CHUNKS) return it.info[1];
     if (part == P_MED) return div_up(it.info[2], RS_WARPS);
-    return div_up(div_up(it.m.n_rows, 32), RS_WARPS);
+    return div_up(div_up(it.m.n_rows, 32) * split, RS_WARPS);
   }
   __device__ __forceinline__ int locate(int, int64_t u, int64_t &lu) const {
     lu = u;
@@ -72,7 +76,8 @@ template <typename V>
 struct RowMany {
   const RowItem<V> *its;
   int count;
-  const long long *pref;  // [3][count+1] unit prefixes per class
+  const long long *pref;  // [3][count+1] unit prefixes per class (short blocks counted split times)
+  int split = 1;
   __device__ __forceinline__ int n_items() const { return count; }
   __device__ __forceinline__ const RowItem<V> &item(int i) const { return its[i]; }
   __device__ __forceinline__ int find_row(int64_t g) const {  // matrix holding global row g
@@ -257,7 +262,7 @@ int build_schedule(dcsr_handle h, cudaStream_t s, Arena *ar) {
 // Exclusive prefix over the matrices of each class's unit count (one block
 // of 1024 threads, 1024 matrices per round).
 template <typename V>
-__device__ __forceinline__ void unit_prefix_block(const RowItem<V> *its, int count, long long *pref) {
+__device__ __forceinline__ void unit_prefix_block(const RowItem<V> *its, int count, long long *pref, int split) {
   __shared__ long long wsum[3][32];
   __shared__ long long carry[3];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -267,7 +272,7 @@ __device__ __forceinline__ void unit_prefix_block(const RowItem<V> *its, int cou
     const int i = b + threadIdx.x;
     long long u[3] = {0, 0, 0}, inc[3];
     if (i < count) {
-      u[P_BLOCKS] = div_up(div_up(its[i].m.n_rows, 32), RS_WARPS);
+      u[P_BLOCKS] = div_up(div_up(its[i].m.n_rows, 32) * split, RS_WARPS);
       u[P_CHUNKS] = its[i].info[1];
       u[P_MED] = div_up(its[i].info[2], RS_WARPS);
     }
@@ -293,8 +298,8 @@ __device__ __forceinline__ void unit_prefix_block(const RowItem<V> *its, int cou
 }
 
 template <typename V>
-__global__ void __launch_bounds__(1024) k_unit_prefix(const RowItem<V> *its, int count, long long *pref) {
-  unit_prefix_block(its, count, pref);
+__global__ void __launch_bounds__(1024) k_unit_prefix(const RowItem<V> *its, int count, long long *pref, int split) {
+  unit_prefix_block(its, count, pref, split);
 }
 
 // Several SpMV groups' prefixes in one launch, one block per group.
@@ -303,11 +308,12 @@ struct PrefixJobs {
   const RowItem<V> *its[MAX_PREFIX_JOBS];
   int count[MAX_PREFIX_JOBS];
   long long *pref[MAX_PREFIX_JOBS];
+  int split[MAX_PREFIX_JOBS];
 };
 
 template <typename V>
 __global__ void __launch_bounds__(1024) k_unit_prefix_many(PrefixJobs<V> jobs) {
-  unit_prefix_block(jobs.its[blockIdx.x], jobs.count[blockIdx.x], jobs.pref[blockIdx.x]);
+  unit_prefix_block(jobs.its[blockIdx.x], jobs.count[blockIdx.x], jobs.pref[blockIdx.x], jobs.split[blockIdx.x]);
 }
 
 // ------------------------------------------------------------- helpers
@@ -702,7 +708,10 @@ __global__ void __launch_bounds__(RS_THREADS_, RowsMinBlocks<K>::N) k_rows_reduc
       if (lane == 0) write_y<V, K, OP>(it.y, it.ldy, row, acc, it.alpha, it.beta, (int32_t)L, kr);
     } else {
       // ---- short rows: a warp takes 32 consecutive rows
-      const int64_t blk = lu * RS_WARPS + w;
+      const int S = K == 1 ? 1 : src.split;  // warps per 32-row block (k >= 2 pass only)
+      const int64_t wu = lu * RS_WARPS + w;
+      const int64_t blk = wu / S;
+      const int sub = (int)(wu - blk * S);
       if (blk * 32 >= m.n_rows) continue;
       if constexpr (K == 1) {
         // one value per entry: stream the block's entries across the lanes
@@ -788,7 +797,7 @@ __global__ void __launch_bounds__(RS_THREADS_, RowsMinBlocks<K>::N) k_rows_reduc
         const Chain own = load_chain_used(m, rb.row >= 0 ? rb.row : 0, rb.stream ? rb.len : 0);
         const int G = group_width(warp_sum(rb.stream ? rb.len : 0));
         const int per = 32 / G, j = lane & (G - 1), g = lane / G;
-        for (int pass = 0; pass < G; pass++) {
+        for (int pass = sub; pass < G; pass += S) {
           const int owner = pass * per + g;
           const int32_t row = __shfl_sync(FULL, rb.row, owner);
           const int32_t len = __shfl_sync(FULL, rb.len, owner);
@@ -959,10 +968,22 @@ static int launch_reduce_src(const Src &src, cudaStream_t s) {
   return DCSR_OK;
 }
 
+// Warps per 32-row block of short rows for the k >= 2 pass: doubled (up to
+// 8) while the blocks times the split stay under 12 warps per SM, so a
+// matrix of a few thousand rows is not left to a few dozen warps, each
+// walking 32 rows' groups one after another.
+int short_split(int64_t blocks, int k) {
+  if (k == 1) return 1;
+  int S = 1;
+  while (S < 8 && blocks * S * 2 <= (int64_t)sm_count() * 12) S *= 2;
+  return S;
+}
+
 template <typename V, int K, int OP, bool VEC>
 static int launch_reduce(dcsr_handle h, const V *x, int64_t ldx, V *y, int64_t ldy, double alpha, double beta,
                          cudaStream_t s) {
   RowOne<V> src{row_item<V>(h, x, y, ldx, ldy, alpha, beta)};
+  src.split = OP == OP_SPMV ? short_split(div_up(h->n_rows, 32), K) : 1;
   return launch_reduce_src<V, K, OP, VEC>(src, s);
 }
 
@@ -1005,9 +1026,11 @@ static int reduce_dispatch(dcsr_handle h, int32_t op, V *y, cudaStream_t s) {
 // Batched SpMV over a set of matrices of one k family: kf = 1 (k = 1,
 // streamed short rows), 2, 4 or 8 (each item's k <= kf, read by the kernel).
 template <typename V>
-static int spmv_many_t(const RowItem<V> *its, int count, int kf, long long *pref, bool prefixed, cudaStream_t s) {
-  if (!prefixed) DCSR_LAUNCH(k_unit_prefix<V>, 1, 1024, 0, s, its, count, pref);
-  RowMany<V> src{its, count, pref};
+static int spmv_many_t(const RowItem<V> *its, int count, int kf, long long *pref, bool prefixed, int split,
+                       cudaStream_t s) {
+  if (kf == 1) split = 1;
+  if (!prefixed) DCSR_LAUNCH(k_unit_prefix<V>, 1, 1024, 0, s, its, count, pref, split);
+  RowMany<V> src{its, count, pref, split};
   switch (kf) {
     case 1: return launch_reduce_src<V, 1, OP_SPMV, false>(src, s);
     case 2: return launch_reduce_src<V, -2, OP_SPMV, false>(src, s);
@@ -1017,32 +1040,35 @@ static int spmv_many_t(const RowItem<V> *its, int count, int kf, long long *pref
   return DCSR_BAD_ARG;
 }
 
-int spmv_many(const void *items_dev, int dtype, int count, int k, long long *pref, cudaStream_t s, bool prefixed) {
+int spmv_many(const void *items_dev, int dtype, int count, int k, long long *pref, cudaStream_t s, bool prefixed,
+              int split) {
   if (count == 0) return DCSR_OK;
-  if (dtype == DCSR_F32) return spmv_many_t<float>((const RowItem<float> *)items_dev, count, k, pref, prefixed, s);
-  return spmv_many_t<double>((const RowItem<double> *)items_dev, count, k, pref, prefixed, s);
+  if (dtype == DCSR_F32)
+    return spmv_many_t<float>((const RowItem<float> *)items_dev, count, k, pref, prefixed, split, s);
+  return spmv_many_t<double>((const RowItem<double> *)items_dev, count, k, pref, prefixed, split, s);
 }
 
 template <typename V>
-static int unit_prefix_many_t(const void *const *items, const int *counts, long long *const *prefs, int n,
-                              cudaStream_t s) {
+static int unit_prefix_many_t(const void *const *items, const int *counts, long long *const *prefs,
+                              const int *splits, int n, cudaStream_t s) {
   PrefixJobs<V> jobs;
   std::memset(&jobs, 0, sizeof(jobs));
   for (int i = 0; i < n; i++) {
     jobs.its[i] = (const RowItem<V> *)items[i];
     jobs.count[i] = counts[i];
     jobs.pref[i] = prefs[i];
+    jobs.split[i] = splits[i];
   }
   DCSR_LAUNCH(k_unit_prefix_many<V>, n, 1024, 0, s, jobs);
   return DCSR_OK;
 }
 
-int unit_prefix_many(const void *const *items, const int *counts, long long *const *prefs, int n, int dtype,
-                     cudaStream_t s) {
+int unit_prefix_many(const void *const *items, const int *counts, long long *const *prefs, const int *splits, int n,
+                     int dtype, cudaStream_t s) {
   if (n < 1) return DCSR_OK;
   if (n > MAX_PREFIX_JOBS) return DCSR_BAD_ARG;
-  if (dtype == DCSR_F32) return unit_prefix_many_t<float>(items, counts, prefs, n, s);
-  return unit_prefix_many_t<double>(items, counts, prefs, n, s);
+  if (dtype == DCSR_F32) return unit_prefix_many_t<float>(items, counts, prefs, splits, n, s);
+  return unit_prefix_many_t<double>(items, counts, prefs, splits, n, s);
 }
 
 template <typename V>
