@@ -796,7 +796,7 @@ def main():
     ap.add_argument("--served-requests", type=int, default=20000)
     ap.add_argument("--plain-requests", type=int, default=6000)
     ap.add_argument("--max-batch", type=int, default=256)
-    ap.add_argument("--depth", type=int, default=6)
+    ap.add_argument("--depth", type=int, default=8)
     ap.add_argument("--workers", type=int, default=2)
     ap.add_argument("--repeats", type=int, default=3, help="Poisson replays per served load point (median p99)")
     ap.add_argument("--load-fracs", type=float, nargs="+", default=[0.3, 0.4, 0.5, 0.55, 0.6, 0.65, 0.7, 0.75, 0.85])

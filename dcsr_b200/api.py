@@ -473,7 +473,7 @@ class DcsrServer:
     referenced until their result is taken with ``wait``.
     """
 
-    def __init__(self, matrices, max_batch=256, depth=4, mem_budget=0, mem_reserve=1 << 30, plain=False, workers=2):
+    def __init__(self, matrices, max_batch=256, depth=8, mem_budget=0, mem_reserve=1 << 30, plain=False, workers=2):
         o = ServerOpts()
         lib().dcsr_server_default_opts(C.byref(o))
         o.max_batch, o.depth, o.mem_budget, o.mem_reserve, o.plain = max_batch, depth, mem_budget, mem_reserve, int(plain)

@@ -598,7 +598,7 @@ extern "C" {
 void dcsr_server_default_opts(dcsr_server_opts *o) {
   if (!o) return;
   o->max_batch = 256;
-  o->depth = 4;
+  o->depth = 8;
   o->mem_budget = 0;
   o->mem_reserve = 1ll << 30;
   o->plain = 0;

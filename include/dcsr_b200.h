@@ -251,7 +251,7 @@ typedef struct dcsr_server_s *dcsr_server;
 
 typedef struct {
   int32_t max_batch;   /* requests coalesced into one batch (default 256) */
-  int32_t depth;       /* batches in flight, one stream each (default 4) */
+  int32_t depth;       /* batches in flight, one stream each (default 8, at most 16) */
   int64_t mem_budget;  /* device bytes in-flight requests may hold; 0: free memory at creation - mem_reserve */
   int64_t mem_reserve; /* default 1 GiB */
   int32_t plain;       /* 1: no coalescing -- each request alone through the per-call operators */
