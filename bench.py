@@ -362,14 +362,18 @@ def batched_part(args, dev):
     T = sum(sp["updates"] for sp in specs)
 
     repaired = [0]
+    repair_s = [0.0]
 
     def batched_round(i):
         for dst, src in zip(live, rounds[i]):
             dst.copy_(src, non_blocking=True)
         batch.launch(s)
-        st = batch.status(s)
+        st = batch.status(s)  # synchronises: the graph's work is done here
         if (st != 0).any():
+            t0 = time.perf_counter()
             repaired[0] += batch.repair(st, s)
+            s.synchronize()
+            repair_s[0] += time.perf_counter() - t0
 
     with torch.cuda.stream(s):
         for i in range(warm):
@@ -379,12 +383,14 @@ def batched_part(args, dev):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(s)
         repaired[0] = 0
+        repair_s[0] = 0.0
         for i in range(reps):
             batched_round(warm + i)
         e1.record(s)
         s.synchronize()
         batched_ms = e0.elapsed_time(e1) / reps
         repairs_per_round = repaired[0] / reps
+        repair_ms_per_round = 1e3 * repair_s[0] / reps
         batched_launches = (api.launch_count() - launches0) / reps
         # plain per-call sequences on the same matrices (fresh update rounds)
         L = api.lib()
@@ -415,7 +421,7 @@ def batched_part(args, dev):
         "batched_ms": round(batched_ms, 3), "plain_ms": round(plain_ms, 3),
         "speedup": round(plain_ms / batched_ms, 2),
         "batched_kernel_launches": round(batched_launches, 1), "plain_kernel_launches": round(plain_launches, 1),
-        "repairs_per_round": repairs_per_round,
+        "repairs_per_round": repairs_per_round, "repair_ms_per_round": round(repair_ms_per_round, 3),
         "updates_per_s_batched": round(T / (batched_ms / 1e3), 1),
     }
 
