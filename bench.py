@@ -369,11 +369,11 @@ def batched_part(args, dev):
             dst.copy_(src, non_blocking=True)
         batch.launch(s)
         st = batch.status(s)  # synchronises: the graph's work is done here
+        t0 = time.perf_counter()
         if (st != 0).any():
-            t0 = time.perf_counter()
             repaired[0] += batch.repair(st, s)
-            s.synchronize()
-            repair_s[0] += time.perf_counter() - t0
+        s.synchronize()
+        repair_s[0] += time.perf_counter() - t0
 
     with torch.cuda.stream(s):
         for i in range(warm):

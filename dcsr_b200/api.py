@@ -110,6 +110,7 @@ _SIGS = {
     "dcsr_batch_launch": (_i32, [_vp, _vp]),
     "dcsr_batch_status": (_i32, [_vp, _vp, _vp]),
     "dcsr_batch_repair": (_i32, [_vp, _vp, C.POINTER(_i32), _vp]),
+    "dcsr_batch_grow": (_i32, [_vp, C.POINTER(_i32), _vp]),
     "dcsr_batch_destroy": (_i32, [_vp]),
     "dcsr_batch_autotune": (_i32, [_vp, _vp, C.POINTER(_i32), C.POINTER(_i32), C.POINTER(C.c_float)]),
     "dcsr_set_row_classes": (_i32, [_vp, _i32, _i32]),
@@ -432,6 +433,13 @@ class DcsrBatch:
         _check(lib().dcsr_batch_autotune(self.h, _stream(stream), C.byref(sm), C.byref(lm), C.byref(us)),
                "dcsr_batch_autotune")
         return sm.value, lm.value, us.value
+
+    def grow(self, stream=None) -> int:
+        """After status(): grow pools that the last run left more than 7/8
+        full (returns how many)."""
+        n = _i32(0)
+        _check(lib().dcsr_batch_grow(self.h, C.byref(n), _stream(stream)), "dcsr_batch_grow")
+        return int(n.value)
 
     def repair(self, statuses: np.ndarray, stream=None) -> int:
         st = np.ascontiguousarray(statuses, dtype=np.int32)

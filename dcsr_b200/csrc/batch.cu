@@ -356,6 +356,7 @@ using namespace dcsr;
 struct dcsr_batch_s {
   BatchCore core;
   long long *status_host = nullptr;  // pinned [2*count]
+  bool status_read = false;          // status_host holds the last status read (for dcsr_batch_grow)
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   uint64_t graph_kernels = 0;  // kernel nodes of the captured graph
@@ -460,6 +461,27 @@ int dcsr_batch_status(dcsr_batch b, int32_t *statuses, void *stream) {
     const int j = b->core.upd_of[i];
     statuses[i] = j >= 0 ? (int32_t)b->status_host[2 * j] : DCSR_OK;
   }
+  b->status_read = true;
+  return DCSR_OK;
+}
+
+int dcsr_batch_grow(dcsr_batch b, int32_t *grown, void *stream) {
+  if (!b) return DCSR_BAD_ARG;
+  int n = 0;
+  if (b->status_read) {  // the words of the last status read: (status, pool top needed) per update
+    for (int i = 0; i < b->core.count; i++) {
+      const int j = b->core.upd_of[i];
+      if (j < 0 || b->status_host[2 * j] != DCSR_OK) continue;
+      dcsr_handle h = b->core.items[i].matrix;
+      const long long need = b->status_host[2 * j + 1];
+      if (h->pool_cap - need < h->pool_cap / 8) {
+        DCSR_TRY(reserve(h, grow_target(h, need), (cudaStream_t)stream));
+        n++;
+      }
+    }
+    b->status_read = false;
+  }
+  if (grown) *grown = n;
   return DCSR_OK;
 }
 

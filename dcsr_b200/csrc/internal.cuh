@@ -96,6 +96,14 @@ int copy_rows(dcsr_handle h, const long long *dst_off, int32_t *out_cols, void *
 int export_csr(dcsr_handle h, int32_t *row_ptr, int32_t *cols, void *vals, int64_t limit, cudaStream_t s,
                Arena *ar = nullptr);
 int reserve(dcsr_handle h, int64_t cap, cudaStream_t s);
+// Pool capacity for a matrix whose pool top reached `need` and is nearly
+// full: the policy's capacity for that top, and at least a quarter more than
+// the current capacity (so the growth is never a no-op).
+inline int64_t grow_target(dcsr_handle h, int64_t need) {
+  const int64_t p = pool_capacity(h->o, need), q = h->pool_cap + h->pool_cap / 4;
+  const int64_t t = p > q ? p : q;
+  return t < 0x7fffffffLL ? t : 0x7fffffffLL;  // the pool's index range
+}
 
 // The device side of a batch (batch.cu): a plan over a set of
 // dcsr_batch_items, their descriptor image, and the enqueue of the merged

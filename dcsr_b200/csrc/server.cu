@@ -480,7 +480,7 @@ int retire(dcsr_server s, Slot &sl) {
       } else if (h->pool_cap - need < h->pool_cap / 8) {
         // nearly full: grow ahead of the next update (stream-ordered, no sync)
         sl.grows++;
-        DCSR_TRY(reserve(h, pool_capacity(h->o, need), st));
+        DCSR_TRY(reserve(h, grow_target(h, need), st));
       }
       q.status = status;
     }

@@ -222,6 +222,12 @@ int dcsr_batch_capture(dcsr_batch b, void *stream);
 int dcsr_batch_launch(dcsr_batch b, void *stream);
 /* Per-matrix statuses of the last run (synchronises, clears them). */
 int dcsr_batch_status(dcsr_batch b, int32_t *statuses, void *stream);
+/* After dcsr_batch_status: grow the pool of every matrix whose accepted
+ * update left it more than 7/8 full (stream-ordered, the server's rule), so
+ * the next run's update is not rejected for space and needs no repair.
+ * Contents, row lengths and segment tables are unchanged; only the pool
+ * capacity grows.  *grown (may be NULL) = matrices grown. */
+int dcsr_batch_grow(dcsr_batch b, int32_t *grown, void *stream);
 /* For matrices whose update was rejected: apply the repair policy
  * (compact, grow) and redo their update and SpMV per call.  Returns the
  * number of matrices repaired in *repaired (may be NULL). */

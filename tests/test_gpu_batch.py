@@ -256,3 +256,41 @@ def test_row_classes_api(dcsr):
     for bad in ((0, 4096), (300, 4096), (64, 100), (64, 1 << 21)):
         with pytest.raises(dcsr.DcsrError):
             a.set_row_classes(*bad)
+
+
+def test_grow_nearly_full_pools(dcsr):
+    """dcsr_batch_grow after a status read grows exactly the pools that the
+    run left more than 7/8 full (here every pool: 1/16 spare), and only
+    their capacity: contents, row lengths and segments stay the per-call
+    ones round after round."""
+    rng = np.random.default_rng(31)
+    shapes = [(3000, 3000, 6, (), 3000, 2), (2000, 2000, 4, (), 200, 1)]
+    mats, refs, work = build_set(dcsr, rng, torch.float32, dcsr.MERGE, shapes=shapes, spare_x16=1, min_spare=16)
+    batch = dcsr.DcsrBatch(work)
+    grown_total = 0
+    for rnd in range(4):
+        for w in work:  # fresh triples in the batch's input buffers
+            n, m, T = w["matrix"].n_rows, w["matrix"].n_cols, w["rows"].numel()
+            w["rows"].copy_(torch.tensor(rng.integers(0, n, T).astype(np.int32)))
+            w["cols"].copy_(torch.tensor(rng.integers(0, m, T).astype(np.int32)))
+            w["vals"].copy_(torch.tensor(rng.uniform(-1, 1, T), dtype=w["vals"].dtype))
+        batch.run()
+        st = batch.status()
+        batch.repair(st)
+        caps_before = [w["matrix"].layout().pool_cap for w in work]
+        grown = batch.grow()
+        grown_total += grown
+        torch.cuda.synchronize()
+        caps_after = [w["matrix"].layout().pool_cap for w in work]
+        assert sum(a > b for a, b in zip(caps_after, caps_before)) == grown
+        for w, ref in zip(work, refs):
+            per_call(dcsr, w, ref, sync=True)
+            la, lb = w["matrix"].layout(), ref[0].layout()
+            np.testing.assert_array_equal(la.row_sizes, lb.row_sizes)
+            np.testing.assert_array_equal(la.seg, lb.seg)
+            for ta, tb in zip(w["matrix"].to_csr(), ref[0].to_csr()):
+                assert torch.equal(ta, tb)
+            assert torch.equal(w["y"], ref[1])
+            ref[0].reserve(la.pool_cap)  # the reference follows the growth
+    assert grown_total >= 1
+    batch.close()
