@@ -145,7 +145,8 @@ int BatchCore::plan(const dcsr_batch_item *its, int n, cudaStream_t s, bool all_
   for (int i = 0; i < n; i++) {
     const dcsr_batch_item &it = its[i];
     if (!it.x || it.matrix->n_rows == 0) continue;
-    const int gk = it.k <= 2 ? it.k : it.k <= 4 ? 4 : 8;
+    // k families 1 (large matrices), 2 (k <= 2; k = 1 of small matrices), 4, 8
+    const int gk = it.k == 1 ? (it.matrix->n_rows <= K1_GROUP_ROWS ? 2 : 1) : it.k <= 2 ? 2 : it.k <= 4 ? 4 : 8;
     int gi = -1;
     for (size_t q = 0; q < groups.size(); q++)
       if (groups[q].k == gk) gi = (int)q;

@@ -78,6 +78,11 @@ int spmv_many(const void *items_dev, int dtype, int count, int k, long long *pre
               bool prefixed = false, int split = 1);
 // Warps per 32-row short-row block for an SpMV pass over `blocks` blocks with k RHS.
 int short_split(int64_t blocks, int k);
+// A k = 1 SpMV of a matrix of at most this many rows runs in the runtime-k
+// (k <= 2) pass -- row groups of G lanes, blocks split across warps -- instead
+// of the one-value stream, whose 32-row blocks leave a small matrix to a few
+// dozen warps.  A per-matrix rule, so the per-call and batched paths agree.
+constexpr int32_t K1_GROUP_ROWS = 32768;
 // The unit prefixes of up to MAX_PREFIX_JOBS SpMV groups in one launch.
 constexpr int MAX_PREFIX_JOBS = 8;
 int unit_prefix_many(const void *const *items, const int *counts, long long *const *prefs, const int *splits, int n,

@@ -999,6 +999,11 @@ static int spmv_k(dcsr_handle h, const V *x, int64_t ldx, V *y, int64_t ldy, dou
 template <typename V>
 static int spmv_dispatch(dcsr_handle h, const V *x, int32_t k, int64_t ldx, V *y, int64_t ldy, double alpha,
                          double beta, cudaStream_t s) {
+  if (k == 1 && h->n_rows <= K1_GROUP_ROWS) {  // the runtime-k pass with the item's k = 1
+    RowOne<V> src{row_item<V>(h, x, y, ldx, ldy, alpha, beta)};
+    src.split = short_split(div_up(h->n_rows, 32), 2);
+    return launch_reduce_src<V, -2, OP_SPMV, false>(src, s);
+  }
   switch (k) {
     case 1: return spmv_k<V, 1>(h, x, ldx, y, ldy, alpha, beta, s);
     case 2: return spmv_k<V, 2>(h, x, ldx, y, ldy, alpha, beta, s);
@@ -1103,7 +1108,7 @@ namespace dcsr {
 int spmv_call(dcsr_handle h, const void *x, int32_t k, int64_t ldx, void *y, int64_t ldy, double alpha, double beta,
               cudaStream_t s, Arena *ar) {
   if (h->n_rows == 0) return DCSR_OK;
-  DCSR_TRY(ensure_part(h, k, s));
+  DCSR_TRY(ensure_part(h, k == 1 && h->n_rows <= K1_GROUP_ROWS ? 2 : k, s));  // partials of the k <= 2 pass
   if (!h->bins_valid) DCSR_TRY(build_schedule(h, s, ar));
   if (h->dtype == DCSR_F32)
     return spmv_dispatch<float>(h, (const float *)x, k, ldx, (float *)y, ldy, alpha, beta, s);
