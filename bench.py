@@ -548,6 +548,17 @@ def served_part(args, dev, rank, local_rank):
         resident += inf.pool_cap * 8 + (sp["n"] + 1) * 4 + inf.pitch * 4 * inf.opts.max_segs
         mats.append(A)
     torch.cuda.synchronize()
+    # set-up: row-class thresholds of the served matrices from the batch
+    # autotuner (an SpMV of every matrix, k = 4; both servers use the result)
+    tuned = None
+    if not args.no_served_autotune:
+        xs = [torch.zeros(sp["n"], 4, device=dev) for sp in specs]
+        ys = [torch.zeros(sp["n"], 4, device=dev) for sp in specs]
+        tb = api.DcsrBatch([dict(matrix=A, x=x, y=y) for A, x, y in zip(mats, xs, ys)])
+        tuned = tb.autotune()
+        tb.close()
+        del xs, ys
+        torch.cuda.synchronize()
     # the global trace; this rank serves the requests addressed to its matrices
     kind_g, mat_g, size_g = W.served_trace(args.seed + 6, len(specs_all), args.served_requests * world)
     sel, local = shard.route(mat_g, owner, rank)
@@ -626,7 +637,8 @@ def served_part(args, dev, rank, local_rank):
     out["served"] = {"capacity_req_s": round(cap_s["req_s"], 1), "mean_batch_at_capacity": round(cap_s["mean_batch"], 1),
                      "sweep": sweep, "chosen_load_frac": best_f, "p99_constraint_met": met,
                      "batches": st["batches"], "max_batch": args.max_batch, "depth": args.depth,
-                     "workers": args.workers}
+                     "workers": args.workers,
+                     "row_classes": None if tuned is None else {"short_max": tuned[0], "long_min": tuned[1]}}
     out["value"] = best["req_s"]
     out["chosen"] = {"requests": best["requests"], "wall_ms": best["wall_ms"]}
     out["p50_ms"] = best["p50_ms"]
@@ -864,6 +876,7 @@ def main():
     ap.add_argument("--spgemm-reps", type=int, default=5)
     ap.add_argument("--skip-served", action="store_true", help="profiling: no headline line")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-served-autotune", action="store_true", help="served matrices keep the default row classes")
     ap.add_argument("--small-batch-profile", action="store_true",
                     help="profiling aid: time one small batch and run it once inside a profiler range")
     args = ap.parse_args()
