@@ -6,8 +6,9 @@ them):
 served (headline)  2000 resident matrices (rows log-uniform [1k, 256k], mean
         degree U[4, 64], Poisson row lengths, FP32; ~60 GB of HBM) and a
         request stream: 40% updates (log-uniform 10..100k triples), 50% SpMV
-        (k uniform in 1..8), 10% DCSR->CSR exports, matrices uniform.  The
-        plain per-call server (each request alone through dcsr_update_sync /
+        (k uniform in 1..8), 10% DCSR->CSR exports, matrices uniform.  At
+        set-up the batch autotuner picks the matrices' row-class thresholds
+        (both servers then use them).  The plain per-call server (each request alone through dcsr_update_sync /
         dcsr_spmv / dcsr_to_csr) is measured first: its capacity (all requests
         queued at once) and its p99 latency under Poisson arrivals at 50, 70
         and 90% of that capacity; the 90% point (its best sustained
