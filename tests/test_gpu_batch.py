@@ -50,6 +50,7 @@ SHAPES = [  # (rows, cols, mean degree, long rows, update size, k)
     (1, 1, 1, (), 3, 1),
     (40000, 10000, 3, ((1, 70000 // 7),), 100000, 2),
     (1200, 1200, 100, (), 5000, 1),
+    (36000, 36000, 5, ((9, 700),), 4000, 1),  # k = 1 above the row-group threshold: the one-value stream
 ]
 
 

@@ -377,3 +377,27 @@ def test_pool_reserve(dcsr):
     dev.from_coo(np.arange(64, dtype=np.int32), np.arange(64, dtype=np.int32), np.full(64, 2.0, np.float32))
     y = dev.spmv(torch.ones(64, device="cuda"))
     assert torch.equal(y, torch.full((64,), 2.0, device="cuda"))
+
+
+@pytest.mark.parametrize("n", [32768, 32769, 70000])
+def test_spmv_k1_both_paths(dcsr, n):
+    """k = 1 SpMV on both sides of the row threshold where a matrix moves from
+    the row-group pass to the one-value stream (32768 rows), against the
+    oracle, before and after an update."""
+    rng = np.random.default_rng(n)
+    lens = rng.poisson(9, n)
+    m = 50000
+    rp = np.concatenate([[0], np.cumsum(lens)]).astype(np.int32)
+    cols = np.concatenate([np.sort(rng.choice(m, L, replace=False)) for L in lens]).astype(np.int32)
+    vals = rng.uniform(-1, 1, cols.size).astype(np.float32)
+    dev, orc = make_pair(dcsr, n, m, 0, 0)
+    dev.from_csr(rp, cols, vals)
+    orc.load_csr(rp, cols, vals.astype(np.float64))
+    check_spmv(dev, orc, rng)
+    check_spmv(dev, orc, rng, alpha=2.0, beta=-0.5)
+    T = 20000
+    r = rng.integers(0, n, T).astype(np.int32)
+    c = rng.integers(0, m, T).astype(np.int32)
+    v = rng.uniform(-1, 1, T).astype(np.float32)
+    assert dev.update(r, c, v) == orc.update_auto(r, c, v.astype(np.float64)) == 0
+    check_spmv(dev, orc, rng)
