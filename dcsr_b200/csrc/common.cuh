@@ -198,6 +198,16 @@ struct dcsr_matrix_s {
   int32_t short_max = 64, long_min = 512;
   bool bins_valid = false;
   dcsr::Arena scratch;
+  // Pool buffers: buf_cap >= pool_cap entries are allocated.  The buffers a
+  // compaction or growth replaced stay as this matrix's spare (within a
+  // process-wide byte budget), so the next compaction or growth of the
+  // matrix -- a repair's -- takes them instead of allocating; spare_ev orders
+  // their reuse after the kernels that last read them.
+  int64_t buf_cap = 0;
+  int32_t *spare_cols = nullptr;
+  void *spare_vals = nullptr;
+  int64_t spare_cap = 0;
+  cudaEvent_t spare_ev = nullptr;
   int device = 0;
 
   template <typename V>

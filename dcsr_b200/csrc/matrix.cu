@@ -1,6 +1,7 @@
 // matrix.cu -- DCSR handle lifecycle, CSR/COO/HYB -> DCSR loading, DCSR ->
 // CSR/COO export, compaction (defragmentation), pool growth, SpMV row bins,
 // the synchronous update repair policy and the status API.
+#include <atomic>
 #include <cstring>
 #include <mutex>
 #include <vector>
@@ -135,17 +136,64 @@ static int grid_for(int64_t n, int block) {
 
 // ------------------------------------------------------------ host side
 
-static int alloc_pool(dcsr_handle h, int64_t cap, int32_t **cols, void **vals, cudaStream_t s) {
+// Spare pool buffers kept by all matrices together (bytes), and the budget.
+static std::atomic<int64_t> g_spare_bytes{0};
+constexpr int64_t SPARE_BUDGET = 8ll << 30;
+
+static int64_t pool_bytes(dcsr_handle h, int64_t cap) { return cap * (int64_t)(sizeof(int32_t) + h->vsize()); }
+
+static void drop_spare(dcsr_handle h, cudaStream_t s) {
+  if (!h->spare_cols) return;
+  cudaFreeAsync(h->spare_cols, s);
+  cudaFreeAsync(h->spare_vals, s);
+  g_spare_bytes -= pool_bytes(h, h->spare_cap);
+  h->spare_cols = nullptr;
+  h->spare_vals = nullptr;
+  h->spare_cap = 0;
+}
+
+// New pool buffers of at least cap entries (*got: their capacity): the
+// matrix's spare when it is large enough, else a stream-ordered allocation.
+static int alloc_pool(dcsr_handle h, int64_t cap, int32_t **cols, void **vals, int64_t *got, cudaStream_t s) {
   if (cap < 1) cap = 1;
+  if (h->spare_cols && h->spare_cap >= cap) {
+    DCSR_CUDA(cudaStreamWaitEvent(s, h->spare_ev, 0));
+    *cols = h->spare_cols;
+    *vals = h->spare_vals;
+    *got = h->spare_cap;
+    g_spare_bytes -= pool_bytes(h, h->spare_cap);
+    h->spare_cols = nullptr;
+    h->spare_vals = nullptr;
+    h->spare_cap = 0;
+    return DCSR_OK;
+  }
   DCSR_CUDA(cudaMallocAsync((void **)cols, cap * sizeof(int32_t), s));
   DCSR_CUDA(cudaMallocAsync(vals, cap * h->vsize(), s));
+  *got = cap;
   return DCSR_OK;
 }
+
+// Retire the current pool buffers (after the kernels enqueued on s that read
+// them): kept as the spare when the budget allows, else freed.
 static void free_pool(dcsr_handle h, cudaStream_t s) {
-  if (h->cols) cudaFreeAsync(h->cols, s);
-  if (h->vals) cudaFreeAsync(h->vals, s);
+  if (h->cols) {
+    const int64_t b = pool_bytes(h, h->buf_cap);
+    if (h->spare_cols && h->spare_cap < h->buf_cap) drop_spare(h, s);
+    if (!h->spare_cols && g_spare_bytes + b <= SPARE_BUDGET &&
+        (h->spare_ev || cudaEventCreateWithFlags(&h->spare_ev, cudaEventDisableTiming) == cudaSuccess) &&
+        cudaEventRecord(h->spare_ev, s) == cudaSuccess) {
+      h->spare_cols = h->cols;
+      h->spare_vals = h->vals;
+      h->spare_cap = h->buf_cap;
+      g_spare_bytes += b;
+    } else {
+      cudaFreeAsync(h->cols, s);
+      cudaFreeAsync(h->vals, s);
+    }
+  }
   h->cols = nullptr;
   h->vals = nullptr;
+  h->buf_cap = 0;
 }
 
 size_t load_scratch_bytes(dcsr_handle h) { return arena_bytes(h->n_rows + 2, 8) + scan_scratch_bytes(h->n_rows + 1); }
@@ -169,10 +217,12 @@ int load_from_csr64(dcsr_handle h, const long long *rp, const int32_t *cols, con
   if (cap > 0x7fffffffLL) cap = 0x7fffffffLL;
   int32_t *nc;
   void *nv;
-  DCSR_TRY(alloc_pool(h, cap, &nc, &nv, s));
+  int64_t got;
+  DCSR_TRY(alloc_pool(h, cap, &nc, &nv, &got, s));
   free_pool(h, s);
   h->cols = nc;
   h->vals = nv;
+  h->buf_cap = got;
   h->pool_cap = cap;
   DCSR_LAUNCH(k_layout, grid_for(n + 1, 256), 256, 0, s, h->seg, h->row_sizes, n, h->pitch, h->o.max_segs, caps, rp);
   if (h->dtype == DCSR_F32)
@@ -191,9 +241,14 @@ int load_from_csr64(dcsr_handle h, const long long *rp, const int32_t *cols, con
 int reserve(dcsr_handle h, int64_t cap, cudaStream_t s) {
   if (cap <= h->pool_cap && h->vals) return DCSR_OK;
   if (cap > 0x7fffffffLL) return DCSR_OOM;
+  if (h->vals && cap <= h->buf_cap) {  // the buffers (a spare taken earlier) are large enough already
+    h->pool_cap = cap;
+    return DCSR_OK;
+  }
   int32_t *nc;
   void *nv;
-  DCSR_TRY(alloc_pool(h, cap, &nc, &nv, s));
+  int64_t got;
+  DCSR_TRY(alloc_pool(h, cap, &nc, &nv, &got, s));
   if (h->vals && h->pool_cap > 0) {
     DCSR_CUDA(cudaMemcpyAsync(nc, h->cols, h->pool_cap * sizeof(int32_t), cudaMemcpyDeviceToDevice, s));
     DCSR_CUDA(cudaMemcpyAsync(nv, h->vals, h->pool_cap * h->vsize(), cudaMemcpyDeviceToDevice, s));
@@ -201,6 +256,7 @@ int reserve(dcsr_handle h, int64_t cap, cudaStream_t s) {
   free_pool(h, s);
   h->cols = nc;
   h->vals = nv;
+  h->buf_cap = got;
   h->pool_cap = cap;
   return DCSR_OK;
 }
@@ -241,7 +297,8 @@ int compact(dcsr_handle h, cudaStream_t s) {
   if (cap > 0x7fffffffLL) cap = 0x7fffffffLL;
   int32_t *nc;
   void *nv;
-  DCSR_TRY(alloc_pool(h, cap, &nc, &nv, s));
+  int64_t got;
+  DCSR_TRY(alloc_pool(h, cap, &nc, &nv, &got, s));
   // row lengths are unchanged, so the schedule stays valid across compaction
   DCSR_TRY(copy_rows(h, caps, nc, nv, nullptr, nullptr, s));
   DCSR_LAUNCH(k_layout, grid_for(n + 1, 256), 256, 0, s, h->seg, h->row_sizes, n, h->pitch, h->o.max_segs, caps,
@@ -249,8 +306,10 @@ int compact(dcsr_handle h, cudaStream_t s) {
   free_pool(h, s);
   h->cols = nc;
   h->vals = nv;
+  h->buf_cap = got;
   h->pool_cap = cap;
-  h->scratch.release(s);
+  // the scratch (sized by this matrix's earlier updates) stays for the
+  // update a repair runs next: re-allocating it there stalled repairs
   return DCSR_OK;
 }
 
@@ -339,7 +398,10 @@ int dcsr_destroy(dcsr_handle h) {
   if (!h) return DCSR_BAD_ARG;
   cudaDeviceSynchronize();
   h->scratch.release(0);
-  free_pool(h, 0);
+  drop_spare(h, 0);
+  if (h->cols) cudaFreeAsync(h->cols, 0);
+  if (h->vals) cudaFreeAsync(h->vals, 0);
+  if (h->spare_ev) cudaEventDestroy(h->spare_ev);
   cudaFree(h->row_sizes);
   cudaFree(h->seg);
   cudaFree(h->stat);
