@@ -190,7 +190,7 @@ struct dcsr_matrix_s {
   int32_t *sched_info = nullptr; // [32]: [0] long rows, [1] chunks, [2] medium rows
   double *part = nullptr;        // chunk partials (reductions)
   int64_t part_cap = 0;
-  int32_t *chunk_li = nullptr;   // long-row index of every chunk
+  int2 *chunk_rl = nullptr;      // (row, long-row index) of every chunk
   int64_t chunk_cap = 0;
   int32_t *med_rows = nullptr;   // [n_rows + 1] medium-length rows
   // Row-class thresholds of the row passes (rows of at most short_max

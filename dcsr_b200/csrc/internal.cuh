@@ -50,7 +50,7 @@ struct RowItem {
   Mat<V> m;
   const int32_t *long_rows;
   const long long *long_off;
-  const int32_t *chunk_li;
+  const int2 *chunk_rl;  // per chunk: (row, long-row index)
   const int32_t *med_rows;
   int32_t *info;  // [0] long rows, [1] chunks, [2] medium rows
   int32_t *long_cnt;

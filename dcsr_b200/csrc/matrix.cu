@@ -411,7 +411,7 @@ int dcsr_destroy(dcsr_handle h) {
   cudaFree(h->med_rows);
   cudaFree(h->sched_info);
   if (h->part) cudaFree(h->part);
-  if (h->chunk_li) cudaFree(h->chunk_li);
+  if (h->chunk_rl) cudaFree(h->chunk_rl);
   cudaDeviceSynchronize();
   delete h;
   return DCSR_OK;

@@ -142,7 +142,7 @@ __global__ void k_sched_emit(Src src, int64_t R, const long long *lscan, const l
       const_cast<int32_t *>(it.long_rows)[li] = (int32_t)r;
       const_cast<long long *>(it.long_off)[li] = c0;
       it.long_cnt[li] = 0;
-      for (long long c = c0; c < c0 + nc; c++) const_cast<int32_t *>(it.chunk_li)[c] = li;  // chunk -> long row
+      for (long long c = c0; c < c0 + nc; c++) const_cast<int2 *>(it.chunk_rl)[c] = make_int2((int32_t)r, li);
     } else if (L > it.short_max) {
       const_cast<int32_t *>(it.med_rows)[mscan[g] - mscan[it.row0]] = (int32_t)r;
     }
@@ -172,9 +172,9 @@ static int64_t max_chunks(dcsr_handle h) { return h->pool_cap / CHUNK + h->pool_
 
 int ensure_part(dcsr_handle h, int K, cudaStream_t s) {
   if (max_chunks(h) > h->chunk_cap) {
-    if (h->chunk_li) DCSR_CUDA(cudaFreeAsync(h->chunk_li, s));
-    h->chunk_li = nullptr;
-    DCSR_CUDA(cudaMallocAsync((void **)&h->chunk_li, sizeof(int32_t) * max_chunks(h), s));
+    if (h->chunk_rl) DCSR_CUDA(cudaFreeAsync(h->chunk_rl, s));
+    h->chunk_rl = nullptr;
+    DCSR_CUDA(cudaMallocAsync((void **)&h->chunk_rl, sizeof(int2) * max_chunks(h), s));
     h->chunk_cap = max_chunks(h);
     h->bins_valid = false;  // the chunk table is gone
   }
@@ -194,7 +194,7 @@ RowItem<V> row_item(dcsr_handle h, const void *x, void *y, int64_t ldx, int64_t 
   it.m = h->view<V>();
   it.long_rows = h->long_rows;
   it.long_off = h->long_off;
-  it.chunk_li = h->chunk_li;
+  it.chunk_rl = h->chunk_rl;
   it.med_rows = h->med_rows;
   it.info = h->sched_info;
   it.long_cnt = h->long_cnt;
@@ -576,12 +576,14 @@ __global__ void __launch_bounds__(RS_THREADS_, RowsMinBlocks<K>::N) k_rows_reduc
     const int kr = K < 0 ? it.k : K;
     const bool vec = K < 0 ? it.vec != 0 : VEC;
     if constexpr (PART == P_CHUNKS) {
-      // ---- one chunk of a long row, whole CTA
-      const int64_t li = it.chunk_li[lu];
-      const int32_t row = it.long_rows[li];
-      const int64_t chunk = lu - it.long_off[li];
-      const int64_t nch = it.long_off[li + 1] - it.long_off[li];
+      // ---- one chunk of a long row, whole CTA (the chunk's row comes with
+      // it; its chunk number and the long-row tables only for multi-chunk rows)
+      const int2 rl = it.chunk_rl[lu];
+      const int32_t row = rl.x;
+      const int64_t li = rl.y;
       const int64_t L = m.row_sizes[row];
+      const int64_t nch = (L + CHUNK - 1) / CHUNK;
+      const int64_t chunk = nch == 1 ? 0 : lu - it.long_off[li];
       const Chain ch = load_chain(m, row);
       const int64_t c0 = chunk * CHUNK, c1 = c0 + CHUNK < L ? c0 + CHUNK : L;
       double acc[KA];
@@ -857,10 +859,10 @@ __global__ void __launch_bounds__(RS_THREADS_) k_rows_copy(RowItem<V> it, const 
       int64_t c0, c1, L;
       int tid, nthr;
       if (PART == P_CHUNKS) {
-        const int64_t li = it.chunk_li[u];
-        row = it.long_rows[li];
-        const int64_t chunk = u - it.long_off[li];
+        const int2 rl = it.chunk_rl[u];
+        row = rl.x;
         L = m.row_sizes[row];
+        const int64_t chunk = L <= CHUNK ? 0 : u - it.long_off[rl.y];
         c0 = chunk * CHUNK;
         c1 = c0 + CHUNK < L ? c0 + CHUNK : L;
         tid = threadIdx.x;
