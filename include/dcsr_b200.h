@@ -345,7 +345,8 @@ uint64_t dcsr_launch_count(void);
  * the current device that reached their iteration limit and gave up, since
  * the library was loaded.  Each such wait is on an earlier tile that is
  * running or finished, so a non-zero count indicates a library bug (the
- * affected result is wrong; nothing hangs).  Synchronises the device. */
+ * affected result is wrong; nothing hangs).  Synchronises the device.  No
+ * counterpart in the reference (its scans and sorts come from Thrust/CUB). */
 int dcsr_spin_faults(int64_t *count);
 /* Pre-grow the current device's stream-ordered memory pool, from which
  * every matrix pool, scratch arena and staging buffer of this library is
