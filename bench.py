@@ -48,6 +48,7 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -94,7 +95,10 @@ class ClockSampler:
     def __init__(self, index: int, tag: str):
         self.index = index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{tag}_rank{index}.csv")
+        # raw samples: $DCSR_BENCH_OUT if set, else the temp directory (the
+        # JSON line carries their summary)
+        out = os.environ.get("DCSR_BENCH_OUT") or tempfile.gettempdir()
+        self.path = os.path.join(out, f"clocks_{tag}_rank{index}.csv")
 
     def start(self):
         try:
