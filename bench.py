@@ -807,54 +807,6 @@ def run_ours(args, rank, world, local_rank):
     return out
 
 
-def small_batch_profile(args):
-    """Profiling aid, not a bench line: one small batch -- six matrices of the
-    served kind, two with updates (10k and 50k triples), four with an SpMV
-    (k = 1, 3, 6, 8) -- run 3 + 20 times (mean time printed), then once
-    between cudaProfilerStart/Stop (for `ncu --profile-from-start off`)."""
-    import torch
-    from dcsr_b200 import api
-    from dcsr_b200 import workloads as W
-    dev = torch.device("cuda", 0)
-    g = torch.Generator(device=dev)
-    g.manual_seed(args.seed + 11)
-    work = []
-    for i, sp in enumerate(W.batched_specs(5, count=40)[:6]):
-        r, c, v = W.device_matrix(sp, dev)
-        A = api.DcsrMatrix(sp["n"], sp["n"], torch.float32)
-        A.from_coo(r, c, v)
-        w = dict(matrix=A)
-        if i < 2:
-            T = (10000, 50000)[i]
-            w["rows"] = torch.randint(0, sp["n"], (T,), dtype=torch.int32, device=dev, generator=g)
-            w["cols"] = torch.randint(0, sp["n"], (T,), dtype=torch.int32, device=dev, generator=g)
-            w["vals"] = torch.rand(T, device=dev, generator=g)
-        else:
-            k = (1, 3, 6, 8)[i - 2]
-            w["x"] = torch.rand(sp["n"], k, device=dev, generator=g)
-            w["y"] = torch.zeros(sp["n"], k, device=dev)
-        work.append(w)
-    s = torch.cuda.Stream()
-    b = api.DcsrBatch(work, stream=s)
-    with torch.cuda.stream(s):
-        for _ in range(3):
-            b.run(s)
-        s.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(s)
-        for _ in range(20):
-            b.run(s)
-        e1.record(s)
-        s.synchronize()
-        ms = e0.elapsed_time(e1) / 20
-        torch.cuda.profiler.start()
-        b.run(s)
-        s.synchronize()
-        torch.cuda.profiler.stop()
-    b.close()
-    return {"small_batch_run_ms": round(ms, 4)}
-
-
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -882,16 +834,11 @@ def main():
     ap.add_argument("--skip-served", action="store_true", help="profiling: no headline line")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-served-autotune", action="store_true", help="served matrices keep the default row classes")
-    ap.add_argument("--small-batch-profile", action="store_true",
-                    help="profiling aid: time one small batch and run it once inside a profiler range")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
     local_rank = int(os.environ.get("LOCAL_RANK", 0))
-    if args.small_batch_profile:
-        print(json.dumps(small_batch_profile(args)), flush=True)
-        return
     if args.impl == "reference":
         if rank != 0:
             return

@@ -125,6 +125,12 @@ _SIGS = {
     "dcsr_status_string": (C.c_char_p, [_i32]),
     "dcsr_launch_count": (C.c_uint64, []),
     "dcsr_spin_faults": (C.c_int, [C.POINTER(C.c_int64)]),
+    "dcsr_debug_lookback": (_i32, [_i32, _i32]),
+    "dcsr_snapshot_bytes": (_i32, [_vp, C.POINTER(_i64), _vp]),
+    "dcsr_snapshot": (_i32, [_vp, _vp, _i64, _vp]),
+    "dcsr_snapshot_header": (_i32, [_vp, _i64, C.POINTER(_i32), C.POINTER(_i32), C.POINTER(_i32), C.POINTER(Opts)]),
+    "dcsr_restore": (_i32, [_vp, _vp, _i64, _vp]),
+    "dcsr_cg": (_i32, [_vp, _vp, _vp, _i32, _dbl, _dbl, C.POINTER(_i32), C.POINTER(_dbl), _vp]),
     "dcsr_pool_reserve": (C.c_int, [C.c_int64, C.c_void_p]),
     "dcsr_version": (C.c_char_p, []),
 }
@@ -151,6 +157,18 @@ def status_string(st: int) -> str:
 
 def launch_count() -> int:
     return int(lib().dcsr_launch_count())
+
+
+def spin_faults() -> int:
+    """Look-back waits that gave up since the library was loaded (synchronises)."""
+    v = C.c_int64(-1)
+    _check(lib().dcsr_spin_faults(C.byref(v)), "dcsr_spin_faults")
+    return v.value
+
+
+def debug_lookback(spin_limit: int = 0, stall_first_tile: bool = False):
+    """Test hook: look-back wait limit (0: default) and the first-tile stall switch."""
+    _check(lib().dcsr_debug_lookback(spin_limit, 1 if stall_first_tile else 0), "dcsr_debug_lookback")
 
 
 def pool_reserve(nbytes: int, stream=None):
@@ -324,6 +342,34 @@ class DcsrMatrix:
         _check(lib().dcsr_info(self.h, C.byref(i)), "dcsr_info")
         return i
 
+    # ---------------------------------------------------------- snapshot
+    def snapshot(self, stream=None) -> bytes:
+        """Binary image of the layout (dcsr_snapshot); restores bit-exact."""
+        nb = _i64()
+        _check(lib().dcsr_snapshot_bytes(self.h, C.byref(nb), _stream(stream)), "dcsr_snapshot_bytes")
+        buf = (C.c_char * nb.value)()
+        _check(lib().dcsr_snapshot(self.h, buf, nb.value, _stream(stream)), "dcsr_snapshot")
+        return bytes(buf)
+
+    def save(self, path: str, stream=None):
+        with open(path, "wb") as f:
+            f.write(self.snapshot(stream))
+
+    @classmethod
+    def from_snapshot(cls, data: bytes, stream=None) -> "DcsrMatrix":
+        nr, nc, dt, o = _i32(), _i32(), _i32(), Opts()
+        buf = C.create_string_buffer(data, len(data))
+        _check(lib().dcsr_snapshot_header(buf, len(data), C.byref(nr), C.byref(nc), C.byref(dt), C.byref(o)),
+               "dcsr_snapshot_header")
+        A = cls(nr.value, nc.value, _TORCH_DT[dt.value], opts=o)
+        _check(lib().dcsr_restore(A.h, buf, len(data), _stream(stream)), "dcsr_restore")
+        return A
+
+    @classmethod
+    def load(cls, path: str, stream=None) -> "DcsrMatrix":
+        with open(path, "rb") as f:
+            return cls.from_snapshot(f.read(), stream)
+
     # -------------------------------------------------------- operators
     def spmv(self, x: torch.Tensor, y: torch.Tensor | None = None, alpha: float = 1.0, beta: float = 0.0,
              stream=None) -> torch.Tensor:
@@ -335,6 +381,17 @@ class DcsrMatrix:
             beta = 0.0
         _check(lib().dcsr_spmv(self.h, _ptr(x), k, k, _ptr(y), k, alpha, beta, _stream(stream)), "dcsr_spmv")
         return y
+
+    def cg(self, b: torch.Tensor, x0: torch.Tensor | None = None, max_iter: int = 500, rel_tol: float = 1e-5,
+           abs_tol: float = 0.0, stream=None):
+        """Conjugate gradient (dcsr_cg, cusp::krylov::cg's iteration and stop
+        rule): returns (x, iterations, final residual norm)."""
+        b = self._v(b)
+        x = torch.zeros_like(b) if x0 is None else self._v(x0).clone()
+        it, res = _i32(), _dbl()
+        _check(lib().dcsr_cg(self.h, _ptr(b), _ptr(x), max_iter, rel_tol, abs_tol, C.byref(it), C.byref(res),
+                             _stream(stream)), "dcsr_cg")
+        return x, it.value, res.value
 
     def row_reduce(self, op: int = REDUCE_SUM, y: torch.Tensor | None = None, stream=None) -> torch.Tensor:
         if y is None:

@@ -26,11 +26,14 @@ __global__ void k_batch_gate(const BatchItem<V> *its, int count, int32_t *skip) 
     skip[i] = its[i].m.stat[ST_GO] == 0;
 }
 
+// (status, pool top needed) per updated matrix; a look-back timeout of the
+// batch's merged sort or scans (the batch-global status word) is reported
+// for every matrix that has no status of its own.
 template <typename V>
-__global__ void k_batch_status2(const BatchItem<V> *its, int count, long long *out) {
+__global__ void k_batch_status2(const BatchItem<V> *its, int count, const long long *gstat, long long *out) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
     long long *st = its[i].m.stat;
-    out[2 * i] = st[ST_STATUS];
+    out[2 * i] = st[ST_STATUS] ? st[ST_STATUS] : gstat[ST_STATUS];
     out[2 * i + 1] = st[ST_NEED];
     st[ST_STATUS] = 0;
   }
@@ -190,13 +193,14 @@ int BatchCore::plan(const dcsr_batch_item *its, int n, cudaStream_t s, bool all_
     g.off = off;
     off = align_up((int64_t)(off + g.idx.size() * desc_size(dtype, true)), 256);
     g.pref_off = poff;
-    poff += 3 * (g.idx.size() + 1);
+    poff += 3 * (g.idx.size() + 1) + 1;  // unit prefixes + the k = 1 pass's counter word
     int64_t blocks = 0;
     for (int i : g.idx) blocks += div_up(its[i].matrix->n_rows, 32);
     g.split = short_split(blocks, g.k);
   }
   img_bytes = off;
   if (img_bytes > img_cap) {
+    if (up_ev) DCSR_CUDA(cudaEventSynchronize(up_ev));  // the last upload has left the pinned image
     if (img_host) DCSR_CUDA(cudaFreeHost(img_host));
     img_host = nullptr;
     DCSR_TRY(grow_dev(&img_dev, img_bytes, img_cap, s));
@@ -222,6 +226,7 @@ int BatchCore::reserve_items(int n, int dt, cudaStream_t s) {
   // side) sections
   const size_t bytes = align_up((int64_t)(n * (desc_size(dt, false) + 2 * desc_size(dt, true)) + 10 * 256), 256);
   if (bytes > img_cap) {
+    if (up_ev) DCSR_CUDA(cudaEventSynchronize(up_ev));  // the last upload has left the pinned image
     if (img_host) DCSR_CUDA(cudaFreeHost(img_host));
     img_host = nullptr;
     DCSR_TRY(grow_dev(&img_dev, bytes, img_cap, s));
@@ -233,7 +238,7 @@ int BatchCore::reserve_items(int n, int dt, cudaStream_t s) {
   cc = 2 * (size_t)cnt_cap;
   DCSR_TRY(grow_dev(&status_dev, 2 * (size_t)n, cc, s));
   cnt_cap = n > cnt_cap ? n : cnt_cap;
-  DCSR_TRY(grow_dev(&pref, 3 * (size_t)(n + 8), pref_cap, s));
+  DCSR_TRY(grow_dev(&pref, 3 * (size_t)(n + 8) + 8, pref_cap, s));
   return DCSR_OK;
 }
 
@@ -251,6 +256,8 @@ int BatchCore::upload(cudaStream_t s, bool sync, bool force) {
   if (force || std::memcmp(img_new.data(), img_host, img_bytes) != 0) {
     std::memcpy(img_host, img_new.data(), img_bytes);
     DCSR_CUDA(cudaMemcpyAsync(img_dev, img_host, img_bytes, cudaMemcpyHostToDevice, s));
+    if (!up_ev) DCSR_CUDA(cudaEventCreateWithFlags(&up_ev, cudaEventDisableTiming));
+    DCSR_CUDA(cudaEventRecord(up_ev, s));
     if (sync) DCSR_CUDA(cudaStreamSynchronize(s));
   }
   return DCSR_OK;
@@ -268,6 +275,7 @@ int BatchCore::reserve_scratch(cudaStream_t s) {
 
 int BatchCore::enqueue(cudaStream_t s, cudaStream_t s2, cudaEvent_t fork, cudaEvent_t join) {
   const bool merge = mode == DCSR_MERGE;
+  ar.status = gstat + ST_STATUS;  // look-back timeouts of the run's sorts and scans
   bool beside = false;
   for (auto &g : groups) beside |= g.side;
   beside = beside && s2 && fork && join;
@@ -324,9 +332,10 @@ int BatchCore::status_async(long long *host, cudaStream_t s) {
   if (nu == 0) return DCSR_OK;
   const int g = (nu + 255) / 256;
   if (dtype == DCSR_F32)
-    DCSR_LAUNCH(k_batch_status2<float>, g, 256, 0, s, (const BatchItem<float> *)img_dev, nu, status_dev);
+    DCSR_LAUNCH(k_batch_status2<float>, g, 256, 0, s, (const BatchItem<float> *)img_dev, nu, gstat, status_dev);
   else
-    DCSR_LAUNCH(k_batch_status2<double>, g, 256, 0, s, (const BatchItem<double> *)img_dev, nu, status_dev);
+    DCSR_LAUNCH(k_batch_status2<double>, g, 256, 0, s, (const BatchItem<double> *)img_dev, nu, gstat, status_dev);
+  DCSR_CUDA(cudaMemsetAsync(gstat + ST_STATUS, 0, sizeof(long long), s));
   DCSR_CUDA(cudaMemcpyAsync(host, status_dev, sizeof(long long) * 2 * nu, cudaMemcpyDeviceToHost, s));
   return DCSR_OK;
 }
@@ -336,15 +345,21 @@ void BatchCore::mark_scheduled() {
 }
 
 void BatchCore::release() {
-  cudaDeviceSynchronize();
-  if (img_dev) cudaFree(img_dev);
+  // Device buffers: stream-ordered frees on the legacy default stream (after
+  // the work queued on blocking streams; the host does not wait).  The pinned
+  // image: once its last upload has been copied.
+  if (img_dev) cudaFreeAsync(img_dev, 0);
+  if (skip) cudaFreeAsync(skip, 0);
+  if (status_dev) cudaFreeAsync(status_dev, 0);
+  if (pref) cudaFreeAsync(pref, 0);
+  if (gstat) cudaFreeAsync(gstat, 0);
+  ar.release(0);
+  if (up_ev) {
+    cudaEventSynchronize(up_ev);
+    cudaEventDestroy(up_ev);
+    up_ev = nullptr;
+  }
   if (img_host) cudaFreeHost(img_host);
-  if (skip) cudaFree(skip);
-  if (status_dev) cudaFree(status_dev);
-  if (pref) cudaFree(pref);
-  if (gstat) cudaFree(gstat);
-  ar.release(nullptr);
-  cudaDeviceSynchronize();
   img_dev = img_host = nullptr;
   skip = nullptr;
   status_dev = pref = gstat = nullptr;

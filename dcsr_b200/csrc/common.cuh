@@ -97,12 +97,18 @@ struct Mat {
 // words, each tagged with the epoch that wrote it (prims.cu).  Zeroed once at
 // allocation: a word left by an earlier kernel carries another epoch, so
 // nothing is cleared between kernels.
+// A wait that reaches its iteration limit gives up: it counts a fault,
+// marks the area's fault word with the kernel's epoch (the other waits of
+// that kernel then give up early instead of each spinning to the limit) and
+// sets the operation's status word (when it has one) to DCSR_TIMEOUT.
 struct Lookback {
   unsigned long long *epoch;
   unsigned *tiles, *done;
+  unsigned long long *fault;  // epoch tag + 1 of the last kernel whose wait gave up
   unsigned *hist;             // [8][256]
   unsigned long long *flag;   // look-back words
   unsigned long long slots;   // entries of flag
+  long long *status;          // the operation's status word, or null
 };
 constexpr size_t LB_HEADER = 64 + 8 * 256 * 4;
 
@@ -114,6 +120,13 @@ struct Arena {
   size_t cap = 0, used = 0;
   unsigned char *lb = nullptr;
   size_t lb_slots = 0;
+  // Status word (device) of the operation using the arena: a look-back wait
+  // that gives up sets it to DCSR_TIMEOUT.  Set by the operation (null: the
+  // fault is only counted, see dcsr_spin_faults).
+  long long *status = nullptr;
+  // Set when take() could not fit a request (a sizing bug): the caller
+  // returns DCSR_OOM instead of launching with the null pointer.
+  bool overflow = false;
   // Look-back area with at least `slots` slots (grown, and zeroed, outside
   // stream capture only: a captured graph must find it sized already).
   int lookback(size_t slots, cudaStream_t s, Lookback *out) {
@@ -133,13 +146,16 @@ struct Arena {
     out->epoch = (unsigned long long *)lb;
     out->tiles = (unsigned *)(lb + 8);
     out->done = (unsigned *)(lb + 12);
+    out->fault = (unsigned long long *)(lb + 16);
     out->hist = (unsigned *)(lb + 64);
     out->flag = (unsigned long long *)(lb + LB_HEADER);
     out->slots = lb_slots;
+    out->status = status;
     return DCSR_OK;
   }
   int reserve(size_t bytes, cudaStream_t s) {
     used = 0;
+    overflow = false;
     if (bytes <= cap) return DCSR_OK;
     if (base) DCSR_CUDA(cudaFreeAsync(base, s));
     base = nullptr;
@@ -149,14 +165,18 @@ struct Arena {
     cap = want;
     return DCSR_OK;
   }
+  // Bump allocation from the reserved buffer; nullptr (and overflow set)
+  // when the request does not fit -- a sizing bug in the library, which the
+  // caller reports as DCSR_OOM before any kernel sees the pointer.
   template <typename T>
   T *take(size_t n) {
     size_t off = align_up((int64_t)used, 256);
-    used = off + n * sizeof(T);
-    if (used > cap) {  // a sizing bug in the library: stop before any kernel sees the pointer
-      fprintf(stderr, "dcsr: scratch arena overflow (%zu > %zu bytes)\n", used, cap);
-      abort();
+    if (off + n * sizeof(T) > cap) {
+      fprintf(stderr, "dcsr: scratch arena overflow (%zu > %zu bytes)\n", off + n * sizeof(T), cap);
+      overflow = true;
+      return nullptr;
     }
+    used = off + n * sizeof(T);
     return (T *)(base + off);
   }
   void release(cudaStream_t s) {
@@ -192,7 +212,10 @@ struct dcsr_matrix_s {
   int64_t part_cap = 0;
   int2 *chunk_rl = nullptr;      // (row, long-row index) of every chunk
   int64_t chunk_cap = 0;
-  int32_t *med_rows = nullptr;   // [n_rows + 1] medium-length rows
+  // medium-length rows, one descriptor each: (row, length, layer-0 start,
+  // layer-0 capacity)
+  int4 *med_desc = nullptr;      // [n_rows + 1]
+  int4 *chunk_desc = nullptr;    // [chunk_cap] per chunk: its row's (row, length, layer-0 start, capacity)
   // Row-class thresholds of the row passes (rows of at most short_max
   // entries are streamed by row blocks, rows above long_min are chunked).
   int32_t short_max = 64, long_min = 512;
@@ -386,6 +409,10 @@ size_t lookback_slots(int64_t n);
 // Spin waits of the single-pass kernels that ran out of iterations (a bug
 // indicator: each wait has an owner that is running or finished).
 long long spin_faults();
+// Test hook: wait limit of the look-back kernels (<= 0: the default) and a
+// switch that keeps the first tile of each single-pass kernel from
+// publishing.  Synchronises the device.
+int debug_lookback(int spin_limit, int stall);
 
 inline int bits_for(int64_t n) {  // bits to represent values in [0, n)
   int b = 1;

@@ -50,8 +50,9 @@ struct RowItem {
   Mat<V> m;
   const int32_t *long_rows;
   const long long *long_off;
-  const int2 *chunk_rl;  // per chunk: (row, long-row index)
-  const int32_t *med_rows;
+  const int2 *chunk_rl;   // per chunk: (row, long-row index)
+  const int4 *chunk_desc; // per chunk: (row, length, layer-0 start, layer-0 capacity)
+  const int4 *med_desc;   // per medium row: the same descriptor
   int32_t *info;  // [0] long rows, [1] chunks, [2] medium rows
   int32_t *long_cnt;
   double *part;
@@ -71,7 +72,8 @@ int schedule_many(const void *items_dev, int dtype, int count, int64_t R, Arena 
 size_t schedule_scratch_bytes(int64_t R);
 // y = A x for `count` matrices (items: device RowItem<V>[count]) of one k
 // family: kf = 1, 2, 4 or 8, every item's k <= kf (each item's own k / vec
-// are read by the kernel); pref: device scratch of 3*(count+1) long longs.
+// are read by the kernel); pref: device scratch of 3*(count+1)+1 long longs
+// (the unit prefixes, then the k = 1 pass's counter word).
 // prefixed: the group's unit prefixes were computed already (unit_prefix_many,
 // with the same split); split: warps per 32-row block of short rows (short_split)
 int spmv_many(const void *items_dev, int dtype, int count, int k, long long *pref, cudaStream_t s,
@@ -135,6 +137,7 @@ struct BatchCore {
   size_t off_row = 0, img_bytes = 0, img_cap = 0;
   unsigned char *img_dev = nullptr;
   unsigned char *img_host = nullptr;  // pinned copy of the last upload
+  cudaEvent_t up_ev = nullptr;        // recorded after the last upload from img_host
   std::vector<unsigned char> img_new;
   int cnt_cap = 0;
   int32_t *skip = nullptr;        // [upd] 1: the matrix's update was rejected this run

@@ -196,17 +196,24 @@ static void free_pool(dcsr_handle h, cudaStream_t s) {
   h->buf_cap = 0;
 }
 
+static int clear_status(dcsr_handle h, cudaStream_t s);
+
 size_t load_scratch_bytes(dcsr_handle h) { return arena_bytes(h->n_rows + 2, 8) + scan_scratch_bytes(h->n_rows + 1); }
 
 int load_from_csr64(dcsr_handle h, const long long *rp, const int32_t *cols, const void *vals, cudaStream_t s) {
   Arena &ar = h->scratch;  // caller reserved load_scratch_bytes() beyond its own use
   const int32_t n = h->n_rows;
   long long *caps = ar.take<long long>(n + 2);
+  if (ar.overflow) return DCSR_OOM;  // scratch sizing bug: no kernel sees a null pointer
   DCSR_LAUNCH(k_caps_from_rp, grid_for(n + 1, 256), 256, 0, s, rp, n, h->o, caps);
   DCSR_TRY(scan_i64(caps, caps, n + 1, h->stat + ST_TOTAL, ar, s));
   long long host[ST_WORDS];
   DCSR_CUDA(cudaMemcpyAsync(host, h->stat, sizeof(host), cudaMemcpyDeviceToHost, s));
   DCSR_CUDA(cudaStreamSynchronize(s));
+  if (host[ST_STATUS] == DCSR_TIMEOUT) {  // a look-back wait of the sort or scan gave up
+    DCSR_TRY(clear_status(h, s));
+    return DCSR_TIMEOUT;
+  }
   if (host[ST_AUX] & AUX_BAD_INDEX) {
     DCSR_CUDA(cudaMemsetAsync(h->stat + ST_AUX, 0, sizeof(long long), s));
     return DCSR_BAD_INDEX;
@@ -280,17 +287,36 @@ void keep_pool_memory() {
   }
 }
 
+// The library's own non-blocking stream on the current device (created once
+// per device): matrix creation allocates and initialises on it and waits for
+// it alone.
+int lifecycle_stream(cudaStream_t *out) {
+  static std::mutex mu;
+  static cudaStream_t streams[64] = {};
+  int dev = 0;
+  DCSR_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return DCSR_NOT_SUPPORTED;
+  std::lock_guard<std::mutex> lock(mu);
+  if (!streams[dev]) DCSR_CUDA(cudaStreamCreateWithFlags(&streams[dev], cudaStreamNonBlocking));
+  *out = streams[dev];
+  return DCSR_OK;
+}
+
 int compact(dcsr_handle h, cudaStream_t s) {
   const int32_t n = h->n_rows;
   Arena &ar = h->scratch;
+  ar.status = h->stat + ST_STATUS;
   if (!h->bins_valid) DCSR_TRY(build_schedule(h, s));  // before taking arena memory
   DCSR_TRY(ar.reserve(arena_bytes(n + 2, 8) + scan_scratch_bytes(n + 1), s));
   long long *caps = ar.take<long long>(n + 2);
+  if (ar.overflow) return DCSR_OOM;  // scratch sizing bug: no kernel sees a null pointer
   DCSR_LAUNCH(k_caps_from_sizes, grid_for(n + 1, 256), 256, 0, s, h->row_sizes, n, h->o, caps);
   DCSR_TRY(scan_i64(caps, caps, n + 1, h->stat + ST_TOTAL, ar, s));
-  long long top;
-  DCSR_CUDA(cudaMemcpyAsync(&top, h->stat + ST_TOTAL, sizeof(top), cudaMemcpyDeviceToHost, s));
+  long long host[ST_WORDS];
+  DCSR_CUDA(cudaMemcpyAsync(host, h->stat, sizeof(host), cudaMemcpyDeviceToHost, s));
   DCSR_CUDA(cudaStreamSynchronize(s));
+  if (host[ST_STATUS] == DCSR_TIMEOUT) return DCSR_TIMEOUT;  // the scan's look-back gave up (status kept)
+  const long long top = host[ST_TOTAL];
   if (top > 0x7fffffffLL) return DCSR_OOM;
   int64_t cap = pool_capacity(h->o, top);
   if (cap < h->pool_cap) cap = h->pool_cap;
@@ -299,7 +325,6 @@ int compact(dcsr_handle h, cudaStream_t s) {
   void *nv;
   int64_t got;
   DCSR_TRY(alloc_pool(h, cap, &nc, &nv, &got, s));
-  // row lengths are unchanged, so the schedule stays valid across compaction
   DCSR_TRY(copy_rows(h, caps, nc, nv, nullptr, nullptr, s));
   DCSR_LAUNCH(k_layout, grid_for(n + 1, 256), 256, 0, s, h->seg, h->row_sizes, n, h->pitch, h->o.max_segs, caps,
               (const long long *)nullptr);
@@ -308,6 +333,8 @@ int compact(dcsr_handle h, cudaStream_t s) {
   h->vals = nv;
   h->buf_cap = got;
   h->pool_cap = cap;
+  // the schedule's row descriptors hold segment starts, which moved
+  h->bins_valid = false;
   // the scratch (sized by this matrix's earlier updates) stays for the
   // update a repair runs next: re-allocating it there stalled repairs
   return DCSR_OK;
@@ -359,6 +386,8 @@ int dcsr_create(dcsr_handle *out, int32_t n_rows, int32_t n_cols, int32_t dtype,
       o.min_cap < 0 || o.alpha < 0 || o.spare_x16 < 0 || o.min_spare < 0 || (o.mode != DCSR_MERGE && o.mode != DCSR_APPEND))
     return DCSR_BAD_ARG;
   keep_pool_memory();
+  cudaStream_t ls = nullptr;
+  DCSR_TRY(lifecycle_stream(&ls));
   dcsr_matrix_s *h = new dcsr_matrix_s;
   h->n_rows = n_rows;
   h->n_cols = n_cols;
@@ -367,24 +396,29 @@ int dcsr_create(dcsr_handle *out, int32_t n_rows, int32_t n_cols, int32_t dtype,
   h->pitch = (int32_t)align_up(2 * (int64_t)n_rows, 32);
   cudaGetDevice(&h->device);
   const size_t nseg = (size_t)h->pitch * o.max_segs;
+  // Stream-ordered allocation and initialisation on the library's own
+  // non-blocking stream, then a wait for that stream only: creating a matrix
+  // does not stall work on other streams.
   int st = DCSR_OK;
-  if (cudaMalloc((void **)&h->row_sizes, sizeof(int32_t) * (n_rows + 1)) != cudaSuccess ||
-      cudaMalloc((void **)&h->seg, sizeof(int32_t) * (nseg ? nseg : 1)) != cudaSuccess ||
-      cudaMalloc((void **)&h->stat, sizeof(long long) * ST_WORDS) != cudaSuccess ||
-      cudaMalloc((void **)&h->long_rows, sizeof(int32_t) * (n_rows + 1)) != cudaSuccess ||
-      cudaMalloc((void **)&h->long_off, sizeof(long long) * (n_rows + 2)) != cudaSuccess ||
-      cudaMalloc((void **)&h->long_cnt, sizeof(int32_t) * (n_rows + 1)) != cudaSuccess ||
-      cudaMalloc((void **)&h->med_rows, sizeof(int32_t) * (n_rows + 1)) != cudaSuccess ||
-      cudaMalloc((void **)&h->sched_info, sizeof(int32_t) * 32) != cudaSuccess)
+  if (cudaMallocAsync((void **)&h->row_sizes, sizeof(int32_t) * (n_rows + 1), ls) != cudaSuccess ||
+      cudaMallocAsync((void **)&h->seg, sizeof(int32_t) * (nseg ? nseg : 1), ls) != cudaSuccess ||
+      cudaMallocAsync((void **)&h->stat, sizeof(long long) * ST_WORDS, ls) != cudaSuccess ||
+      cudaMallocAsync((void **)&h->long_rows, sizeof(int32_t) * (n_rows + 1), ls) != cudaSuccess ||
+      cudaMallocAsync((void **)&h->long_off, sizeof(long long) * (n_rows + 2), ls) != cudaSuccess ||
+      cudaMallocAsync((void **)&h->long_cnt, sizeof(int32_t) * (n_rows + 1), ls) != cudaSuccess ||
+      cudaMallocAsync((void **)&h->med_desc, sizeof(int4) * (n_rows + 1), ls) != cudaSuccess ||
+      cudaMallocAsync((void **)&h->sched_info, sizeof(int32_t) * 32, ls) != cudaSuccess)
     st = DCSR_OOM;
   if (st == DCSR_OK) {
-    cudaMemset(h->row_sizes, 0, sizeof(int32_t) * (n_rows + 1));
-    cudaMemset(h->seg, 0xff, sizeof(int32_t) * (nseg ? nseg : 1));
-    cudaMemset(h->stat, 0, sizeof(long long) * ST_WORDS);
-    cudaMemset(h->sched_info, 0, sizeof(int32_t) * 32);
-    cudaMemset(h->long_cnt, 0, sizeof(int32_t) * (n_rows + 1));
-    st = reserve(h, pool_capacity(o, 0), 0);
-    if (cudaDeviceSynchronize() != cudaSuccess) st = DCSR_CUDA_ERROR;
+    h->scratch.status = h->stat + ST_STATUS;  // look-back timeouts of this matrix's operations
+    if (cudaMemsetAsync(h->row_sizes, 0, sizeof(int32_t) * (n_rows + 1), ls) != cudaSuccess ||
+        cudaMemsetAsync(h->seg, 0xff, sizeof(int32_t) * (nseg ? nseg : 1), ls) != cudaSuccess ||
+        cudaMemsetAsync(h->stat, 0, sizeof(long long) * ST_WORDS, ls) != cudaSuccess ||
+        cudaMemsetAsync(h->sched_info, 0, sizeof(int32_t) * 32, ls) != cudaSuccess ||
+        cudaMemsetAsync(h->long_cnt, 0, sizeof(int32_t) * (n_rows + 1), ls) != cudaSuccess)
+      st = DCSR_CUDA_ERROR;
+    if (st == DCSR_OK) st = reserve(h, pool_capacity(o, 0), ls);
+    if (cudaStreamSynchronize(ls) != cudaSuccess && st == DCSR_OK) st = DCSR_CUDA_ERROR;
   }
   if (st != DCSR_OK) {
     dcsr_destroy(h);
@@ -396,23 +430,18 @@ int dcsr_create(dcsr_handle *out, int32_t n_rows, int32_t n_cols, int32_t dtype,
 
 int dcsr_destroy(dcsr_handle h) {
   if (!h) return DCSR_BAD_ARG;
-  cudaDeviceSynchronize();
-  h->scratch.release(0);
-  drop_spare(h, 0);
-  if (h->cols) cudaFreeAsync(h->cols, 0);
-  if (h->vals) cudaFreeAsync(h->vals, 0);
+  // Stream-ordered frees on the legacy default stream, which follows the work
+  // already queued on blocking streams; the host does not wait.  Work on
+  // non-blocking streams that uses the matrix must be complete (or ordered
+  // before the legacy stream) first.
+  cudaStream_t s0 = 0;
+  h->scratch.release(s0);
+  drop_spare(h, s0);
+  void *bufs[] = {h->cols, h->vals, h->row_sizes, h->seg, h->stat, h->long_rows, h->long_off,
+                  h->long_cnt, h->med_desc, h->sched_info, h->part, h->chunk_rl, h->chunk_desc};
+  for (void *p : bufs)
+    if (p) cudaFreeAsync(p, s0);
   if (h->spare_ev) cudaEventDestroy(h->spare_ev);
-  cudaFree(h->row_sizes);
-  cudaFree(h->seg);
-  cudaFree(h->stat);
-  cudaFree(h->long_rows);
-  cudaFree(h->long_off);
-  cudaFree(h->long_cnt);
-  cudaFree(h->med_rows);
-  cudaFree(h->sched_info);
-  if (h->part) cudaFree(h->part);
-  if (h->chunk_rl) cudaFree(h->chunk_rl);
-  cudaDeviceSynchronize();
   delete h;
   return DCSR_OK;
 }
@@ -451,6 +480,7 @@ int dcsr_from_csr(dcsr_handle h, const int32_t *row_ptr, const int32_t *cols, co
   Arena &ar = h->scratch;
   DCSR_TRY(ar.reserve(arena_bytes(n + 2, 8) + load_scratch_bytes(h), s));
   long long *rp = ar.take<long long>(n + 2);
+  if (ar.overflow) return DCSR_OOM;  // scratch sizing bug: no kernel sees a null pointer
   DCSR_CUDA(cudaMemsetAsync(h->stat + ST_AUX, 0, sizeof(long long), s));
   if (n > 0) DCSR_LAUNCH(k_csr_check, grid_for((int64_t)n * 32, 256), 256, 0, s, row_ptr, cols, n, h->n_cols, rp, h->stat);
   else DCSR_CUDA(cudaMemsetAsync(rp, 0, sizeof(long long), s));
@@ -471,6 +501,7 @@ int dcsr_from_csr(dcsr_handle h, const int32_t *row_ptr, const int32_t *cols, co
                             load_scratch_bytes(h), s));
     long long *rp2 = ar.take<long long>(n + 2);
     int32_t *rows = ar.take<int32_t>(nnz + 1);
+    if (ar.overflow) return DCSR_OOM;  // scratch sizing bug: no kernel sees a null pointer
     DCSR_LAUNCH(k_csr_check, grid_for((int64_t)n * 32, 256), 256, 0, s, row_ptr, cols, n, h->n_cols, rp2, h->stat);
     DCSR_LAUNCH(k_expand_rows, grid_for((int64_t)n * 32, 256), 256, 0, s, rp2, n, rows);
     DCSR_CUDA(cudaMemsetAsync(h->stat + ST_AUX, 0, sizeof(long long), s));
@@ -515,6 +546,7 @@ int dcsr_from_hyb(dcsr_handle h, const int32_t *ell_cols, const void *ell_vals, 
   DCSR_CUDA(cudaMallocAsync(&vals, h->vsize() * (T + 1), s));
   DCSR_CUDA(cudaMallocAsync((void **)&flag, sizeof(long long) * (slots + 1), s));
   Arena tmp;
+  tmp.status = h->stat + ST_STATUS;
   DCSR_TRY(tmp.reserve(scan_scratch_bytes(slots + 1), s));
   long long nell = 0;
   if (slots > 0) {
@@ -561,9 +593,11 @@ static int export_impl(dcsr_handle h, int32_t *row_ptr, int32_t *rows, int32_t *
                        int64_t limit = INT64_MAX, Arena *arp = nullptr) {
   const int32_t n = h->n_rows;
   Arena &ar = arp ? *arp : h->scratch;
+  ar.status = h->stat + ST_STATUS;
   if (!h->bins_valid) DCSR_TRY(build_schedule(h, s, arp));  // before taking arena memory
   DCSR_TRY(ar.reserve(arena_bytes(n + 2, 8) + scan_scratch_bytes(n + 1), s));
   long long *rp = ar.take<long long>(n + 2);
+  if (ar.overflow) return DCSR_OOM;  // scratch sizing bug: no kernel sees a null pointer
   DCSR_LAUNCH(k_lens, grid_for(n + 1, 256), 256, 0, s, h->row_sizes, n, rp);
   DCSR_TRY(scan_i64(rp, rp, n + 1, nullptr, ar, s));
   return copy_rows(h, rp, cols, vals, rows, row_ptr, s, limit);
@@ -631,6 +665,126 @@ int dcsr_reserve(dcsr_handle h, int64_t pool_cap, void *stream) {
   return reserve(h, pool_cap, (cudaStream_t)stream);
 }
 
+// ---------------------------------------------------------------- snapshot
+// Binary image of a matrix's layout: a fixed header, then row_sizes[n+1],
+// seg[max_segs*pitch], cols[top] and vals[top] (top = row_sizes[n], the
+// pool's bump pointer; slots beyond it hold nothing).  Little-endian, as the
+// host writes it.
+namespace {
+struct SnapHeader {
+  char magic[8];  // "DCSRSNP1"
+  int32_t version, n_rows, n_cols, dtype;
+  dcsr_opts opts;
+  int32_t pitch;
+  int64_t pool_cap, top;
+  int64_t reserved[4];
+};
+constexpr char SNAP_MAGIC[8] = {'D', 'C', 'S', 'R', 'S', 'N', 'P', '1'};
+
+int64_t snap_bytes(dcsr_handle h, int64_t top) {
+  return (int64_t)sizeof(SnapHeader) + 4 * ((int64_t)h->n_rows + 1) + 4 * (int64_t)h->pitch * h->o.max_segs +
+         (4 + (int64_t)h->vsize()) * top;
+}
+int read_top(dcsr_handle h, cudaStream_t s, int64_t *top) {
+  int32_t t = 0;
+  DCSR_CUDA(cudaMemcpyAsync(&t, h->row_sizes + h->n_rows, sizeof(t), cudaMemcpyDeviceToHost, s));
+  DCSR_CUDA(cudaStreamSynchronize(s));
+  *top = t;
+  return DCSR_OK;
+}
+}  // namespace
+
+int dcsr_snapshot_bytes(dcsr_handle h, int64_t *bytes, void *stream) {
+  if (!h || !bytes) return DCSR_BAD_ARG;
+  int64_t top;
+  DCSR_TRY(read_top(h, (cudaStream_t)stream, &top));
+  *bytes = snap_bytes(h, top);
+  return DCSR_OK;
+}
+
+int dcsr_snapshot(dcsr_handle h, void *host_buf, int64_t buf_bytes, void *stream) {
+  if (!h || !host_buf) return DCSR_BAD_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  int64_t top;
+  DCSR_TRY(read_top(h, s, &top));
+  if (buf_bytes < snap_bytes(h, top)) return DCSR_BAD_ARG;
+  SnapHeader hd;
+  std::memset(&hd, 0, sizeof(hd));
+  std::memcpy(hd.magic, SNAP_MAGIC, 8);
+  hd.version = 1;
+  hd.n_rows = h->n_rows;
+  hd.n_cols = h->n_cols;
+  hd.dtype = h->dtype;
+  hd.opts = h->o;
+  hd.pitch = h->pitch;
+  hd.pool_cap = h->pool_cap;
+  hd.top = top;
+  char *p = (char *)host_buf;
+  std::memcpy(p, &hd, sizeof(hd));
+  p += sizeof(hd);
+  const size_t rs = 4 * ((size_t)h->n_rows + 1), sg = 4 * (size_t)h->pitch * h->o.max_segs;
+  DCSR_CUDA(cudaMemcpyAsync(p, h->row_sizes, rs, cudaMemcpyDeviceToHost, s));
+  p += rs;
+  DCSR_CUDA(cudaMemcpyAsync(p, h->seg, sg, cudaMemcpyDeviceToHost, s));
+  p += sg;
+  if (top > 0) {
+    DCSR_CUDA(cudaMemcpyAsync(p, h->cols, 4 * (size_t)top, cudaMemcpyDeviceToHost, s));
+    p += 4 * (size_t)top;
+    DCSR_CUDA(cudaMemcpyAsync(p, h->vals, h->vsize() * (size_t)top, cudaMemcpyDeviceToHost, s));
+  }
+  DCSR_CUDA(cudaStreamSynchronize(s));
+  return DCSR_OK;
+}
+
+int dcsr_snapshot_header(const void *host_buf, int64_t buf_bytes, int32_t *n_rows, int32_t *n_cols, int32_t *dtype,
+                         dcsr_opts *opts) {
+  if (!host_buf || buf_bytes < (int64_t)sizeof(SnapHeader)) return DCSR_BAD_ARG;
+  SnapHeader hd;
+  std::memcpy(&hd, host_buf, sizeof(hd));
+  if (std::memcmp(hd.magic, SNAP_MAGIC, 8) != 0 || hd.version != 1) return DCSR_BAD_ARG;
+  if (n_rows) *n_rows = hd.n_rows;
+  if (n_cols) *n_cols = hd.n_cols;
+  if (dtype) *dtype = hd.dtype;
+  if (opts) *opts = hd.opts;
+  return DCSR_OK;
+}
+
+int dcsr_restore(dcsr_handle h, const void *host_buf, int64_t buf_bytes, void *stream) {
+  if (!h || !host_buf || buf_bytes < (int64_t)sizeof(SnapHeader)) return DCSR_BAD_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  SnapHeader hd;
+  std::memcpy(&hd, host_buf, sizeof(hd));
+  if (std::memcmp(hd.magic, SNAP_MAGIC, 8) != 0 || hd.version != 1 || hd.n_rows != h->n_rows ||
+      hd.n_cols != h->n_cols || hd.dtype != h->dtype || hd.opts.max_segs != h->o.max_segs || hd.pitch != h->pitch ||
+      hd.top < 0 || hd.pool_cap < hd.top || hd.pool_cap > 0x7fffffffLL)
+    return DCSR_BAD_ARG;
+  h->o = hd.opts;  // the layout policy the image was built under
+  if (buf_bytes < snap_bytes(h, hd.top)) return DCSR_BAD_ARG;
+  const char *p = (const char *)host_buf + sizeof(hd);
+  const size_t rs = 4 * ((size_t)h->n_rows + 1), sg = 4 * (size_t)h->pitch * h->o.max_segs;
+  int32_t *nc;
+  void *nv;
+  int64_t got;
+  DCSR_TRY(alloc_pool(h, hd.pool_cap, &nc, &nv, &got, s));
+  free_pool(h, s);
+  h->cols = nc;
+  h->vals = nv;
+  h->buf_cap = got;
+  h->pool_cap = hd.pool_cap;
+  DCSR_CUDA(cudaMemcpyAsync(h->row_sizes, p, rs, cudaMemcpyHostToDevice, s));
+  p += rs;
+  DCSR_CUDA(cudaMemcpyAsync(h->seg, p, sg, cudaMemcpyHostToDevice, s));
+  p += sg;
+  if (hd.top > 0) {
+    DCSR_CUDA(cudaMemcpyAsync(h->cols, p, 4 * (size_t)hd.top, cudaMemcpyHostToDevice, s));
+    p += 4 * (size_t)hd.top;
+    DCSR_CUDA(cudaMemcpyAsync(h->vals, p, h->vsize() * (size_t)hd.top, cudaMemcpyHostToDevice, s));
+  }
+  h->bins_valid = false;
+  DCSR_CUDA(cudaStreamSynchronize(s));  // the host buffer may be released on return
+  return DCSR_OK;
+}
+
 int dcsr_bin_rows(dcsr_handle h, void *stream) {
   if (!h) return DCSR_BAD_ARG;
   return build_schedule(h, (cudaStream_t)stream);
@@ -681,6 +835,10 @@ int dcsr_pool_reserve(int64_t bytes, void *stream) {
   DCSR_CUDA(cudaFreeAsync(p, s));
   DCSR_CUDA(cudaStreamSynchronize(s));
   return DCSR_OK;
+}
+
+int dcsr_debug_lookback(int32_t spin_limit, int32_t stall_first_tile) {
+  return dcsr::debug_lookback(spin_limit, stall_first_tile ? 1 : 0);
 }
 
 int dcsr_spin_faults(int64_t *count) {

@@ -68,6 +68,11 @@ __device__ __forceinline__ T block_excl_scan(T v, T *total) {
 
 __device__ unsigned long long g_spin_faults = 0;
 constexpr int SPIN_LIMIT = 1 << 22;
+// Wait limit of the look-back kernels (SPIN_LIMIT unless a test lowered it)
+// and a test switch that keeps the first tile of every single-pass kernel
+// from publishing, so the waits on it run out (dcsr_debug_lookback).
+__device__ int g_spin_limit = SPIN_LIMIT;
+__device__ int g_lb_stall = 0;
 constexpr int LB_W = 8;  // earlier tiles whose flags one radix look-back step loads together
 
 __device__ __forceinline__ unsigned long long ld_vol(const unsigned long long *p) {
@@ -86,6 +91,19 @@ __device__ __forceinline__ unsigned long long ld_vol(const unsigned long long *p
 constexpr unsigned long long LB_EMASK = (1ull << 30) - 1;
 __device__ __forceinline__ unsigned long long lb_pack(unsigned long long e, int kind, unsigned v) {
   return ((e & LB_EMASK) << 34) | ((unsigned long long)kind << 32) | v;
+}
+
+// A wait that gave up: count it, mark the area's fault word with this
+// kernel's epoch (its other waits then give up early) and report
+// DCSR_TIMEOUT in the operation's status word.
+__device__ __forceinline__ void lb_give_up(const Lookback &lb, unsigned long long e) {
+  atomicAdd(&g_spin_faults, 1ull);
+  *(volatile unsigned long long *)lb.fault = (e & LB_EMASK) + 1;
+  if (lb.status) atomicCAS(reinterpret_cast<unsigned long long *>(lb.status), 0ull, (unsigned long long)DCSR_TIMEOUT);
+}
+// True when another wait of this kernel (epoch e) gave up already.
+__device__ __forceinline__ bool lb_faulted(const Lookback &lb, unsigned long long e) {
+  return ld_vol(lb.fault) == (e & LB_EMASK) + 1;
 }
 
 // Thread 0 of every block: the block's tile and the kernel's epoch.
@@ -129,6 +147,14 @@ long long spin_faults() {
   return (long long)v;
 }
 
+int debug_lookback(int spin_limit, int stall) {
+  const int lim = spin_limit > 0 ? spin_limit : SPIN_LIMIT;
+  DCSR_CUDA(cudaMemcpyToSymbol(g_spin_limit, &lim, sizeof(int)));
+  DCSR_CUDA(cudaMemcpyToSymbol(g_lb_stall, &stall, sizeof(int)));
+  DCSR_CUDA(cudaDeviceSynchronize());
+  return DCSR_OK;
+}
+
 // Scan operands: one array, or two independent arrays of the same length
 // scanned by one launch (tiles [0, nt) scan the first, [nt, 2nt) the second).
 struct ScanArgs {
@@ -149,8 +175,8 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan_1p(ScanArgs a, Lookback l
   __syncthreads();
   const int64_t t = sh_tile;
   const unsigned long long e = sh_ep;
-  if (t >= gridDim.x) {  // a tile counter left non-zero (a bug): count it, touch nothing
-    if (threadIdx.x == 0) atomicAdd(&g_spin_faults, 1ull);
+  if (t >= gridDim.x) {  // a tile counter left non-zero (a bug): report it, touch nothing
+    if (threadIdx.x == 0) lb_give_up(lb, e);
     if (lb_end(lb)) lb_advance(lb);
     return;
   }
@@ -186,7 +212,7 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan_1p(ScanArgs a, Lookback l
     auto cur = [&](unsigned long long x) { return (x >> 34) == tag && ((x >> 32) & 3) == 1; };
     long long excl = 0;
     if (t == t0) {
-      if (lane == 0) {
+      if (lane == 0 && !(g_lb_stall && t == 0)) {
         *(volatile unsigned long long *)(w + 4 * t + 2) = lb_pack(e, 1, (unsigned)bt);
         *(volatile unsigned long long *)(w + 4 * t + 3) = lb_pack(e, 1, (unsigned)((unsigned long long)bt >> 32));
       }
@@ -218,8 +244,8 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan_1p(ScanArgs a, Lookback l
           idle = 0;
           continue;
         }
-        if (++idle >= SPIN_LIMIT || ((idle & 1023) == 1023 && __any_sync(FULL, ld_vol(&g_spin_faults) != 0))) {
-          if (lane == 0) atomicAdd(&g_spin_faults, 1ull);
+        if (++idle >= g_spin_limit || ((idle & 1023) == 1023 && __any_sync(FULL, lb_faulted(lb, e)))) {
+          if (lane == 0) lb_give_up(lb, e);
           break;
         }
         if (idle >= 32) __nanosleep(64);
@@ -450,8 +476,8 @@ __global__ void __launch_bounds__(OS_THREADS, MIN_BLOCKS) k_radix_onesweep(const
       block_excl_scan((long long)(d < RS_BINS ? __ldcg(lb.hist + pass * RS_BINS + d) : 0u), &all);
   const int64_t t = sh_tile;
   const unsigned long long e = sh_ep;
-  if (t >= gridDim.x) {  // a tile counter left non-zero (a bug): count it, touch nothing
-    if (threadIdx.x == 0) atomicAdd(&g_spin_faults, 1ull);
+  if (t >= gridDim.x) {  // a tile counter left non-zero (a bug): report it, touch nothing
+    if (threadIdx.x == 0) lb_give_up(lb, e);
     if (lb_end(lb)) lb_advance(lb);
     return;
   }
@@ -492,7 +518,7 @@ __global__ void __launch_bounds__(OS_THREADS, MIN_BLOCKS) k_radix_onesweep(const
   if (d >= RS_BINS) {
     // no digit: nothing to look back for
   } else if (t == 0) {
-    *(volatile unsigned long long *)(lb.flag + slot) = lb_pack(e, 2, run);
+    if (!g_lb_stall) *(volatile unsigned long long *)(lb.flag + slot) = lb_pack(e, 2, run);
   } else {
     *(volatile unsigned long long *)(lb.flag + slot) = lb_pack(e, 1, run);
     const unsigned long long tag = e & LB_EMASK;
@@ -515,8 +541,8 @@ __global__ void __launch_bounds__(OS_THREADS, MIN_BLOCKS) k_radix_onesweep(const
       }
       q -= used;
       if (used == 0) {  // the nearest tile has not published yet
-        if (++idle >= SPIN_LIMIT || ((idle & 1023) == 1023 && ld_vol(&g_spin_faults) != 0)) {
-          atomicAdd(&g_spin_faults, 1ull);
+        if (++idle >= g_spin_limit || ((idle & 1023) == 1023 && lb_faulted(lb, e))) {
+          lb_give_up(lb, e);
           break;
         }
         if (idle >= 32) __nanosleep(64);
@@ -651,6 +677,7 @@ static int radix_passes_table(unsigned long long **keys, unsigned **vals, unsign
   const int64_t nt = div_up(n, RS_THREADS * ITEMS);
   size_t mark = ar.used;
   long long *hist = ar.take<long long>(nt * RS_BINS);
+  if (ar.overflow) return DCSR_OOM;  // scratch sizing bug: no kernel sees a null pointer
   for (int shift = 0; shift < bits; shift += 8) {
     DCSR_LAUNCH(k_radix_hist<ITEMS>, (unsigned)nt, RS_THREADS, 0, s, *keys, n, shift, hist, nt);
     DCSR_TRY(scan_i64(hist, hist, nt * RS_BINS, nullptr, ar, s));
@@ -808,6 +835,7 @@ extern "C" int dcsr_reduce_by_key_noalloc(const int32_t *keys, const void *vals,
   ar.lb = (unsigned char *)base + NOALLOC_POS_BYTES + 256;
   ar.lb_slots = NOALLOC_LB_SLOTS;
   long long *pos = ar.take<long long>(n);  // fully rewritten below before any read
+  if (ar.overflow) return DCSR_OOM;  // scratch sizing bug: no kernel sees a null pointer
   const unsigned g = (unsigned)div_up(n, 256);
   DCSR_LAUNCH(k_rbk_flags, g, 256, 0, s, keys, n, pos);
   DCSR_TRY(scan_i64(pos, pos, n, (long long *)n_out, ar, s));
@@ -839,6 +867,7 @@ extern "C" int dcsr_reduce_by_key(const int32_t *keys, const void *vals, int64_t
   Arena ar;
   DCSR_TRY(ar.reserve(arena_bytes(n, 8) + scan_scratch_bytes(n), s));
   long long *pos = ar.take<long long>(n);
+  if (ar.overflow) return DCSR_OOM;  // scratch sizing bug: no kernel sees a null pointer
   unsigned g = (unsigned)div_up(n, 256);
   DCSR_LAUNCH(k_rbk_flags, g, 256, 0, s, keys, n, pos);
   DCSR_TRY(scan_i64(pos, pos, n, (long long *)n_out, ar, s));

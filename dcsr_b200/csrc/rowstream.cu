@@ -42,7 +42,11 @@ namespace dcsr {
 
 constexpr int RS_THREADS_ = 256;
 constexpr int RS_WARPS = RS_THREADS_ / 32;
-constexpr int CHUNK = 65536;  // long-row entries per CTA unit
+// Long-row entries per chunk unit: one warp's unit in the k = 1 pass
+// (k_rows1), one CTA's in the k >= 2 and copy passes.  Small enough that a
+// power-law matrix's hottest rows spread over many warps; multi-chunk rows
+// combine their partials in chunk order.
+constexpr int CHUNK = 2048;
 constexpr int STEP = 4096;    // entries a CTA has in flight per step
 enum { P_BLOCKS = 0, P_CHUNKS = 1, P_MED = 2 };
 
@@ -58,6 +62,10 @@ template <typename V>
 struct RowOne {
   RowItem<V> it;
   int split = 1;
+  // unit counter and finished-warp counter of the k = 1 pass (the handle's
+  // schedule words 8 and 9: zeroed by the schedule rebuild, reset by the
+  // last warp of every pass)
+  __device__ __forceinline__ unsigned *ctr() const { return reinterpret_cast<unsigned *>(it.info + 8); }
   __device__ __forceinline__ int n_items() const { return 1; }
   __device__ __forceinline__ const RowItem<V> &item(int) const { return it; }
   __device__ __forceinline__ int find_row(int64_t) const { return 0; }
@@ -76,8 +84,12 @@ template <typename V>
 struct RowMany {
   const RowItem<V> *its;
   int count;
-  const long long *pref;  // [3][count+1] unit prefixes per class (short blocks counted split times)
+  const long long *pref;  // [3][count+1] unit prefixes per class (short blocks counted split times),
+                          // then one word: the k = 1 pass's unit and finished-warp counters
   int split = 1;
+  __device__ __forceinline__ unsigned *ctr() const {
+    return reinterpret_cast<unsigned *>(const_cast<long long *>(pref + 3 * (count + 1)));
+  }
   __device__ __forceinline__ int n_items() const { return count; }
   __device__ __forceinline__ const RowItem<V> &item(int i) const { return its[i]; }
   __device__ __forceinline__ int find_row(int64_t g) const {  // matrix holding global row g
@@ -135,16 +147,23 @@ __global__ void k_sched_emit(Src src, int64_t R, const long long *lscan, const l
     const RowItem<V> &it = src.item(src.find_row(g));
     const int64_t r = g - it.row0;
     const int32_t L = it.m.row_sizes[r];
-    if (L > it.long_min) {
-      const long long s = lscan[g] - lscan[it.row0];
-      const int32_t li = (int32_t)(s >> 32);
-      const long long c0 = s & 0xffffffff, nc = (L + CHUNK - 1) / CHUNK;
-      const_cast<int32_t *>(it.long_rows)[li] = (int32_t)r;
-      const_cast<long long *>(it.long_off)[li] = c0;
-      it.long_cnt[li] = 0;
-      for (long long c = c0; c < c0 + nc; c++) const_cast<int2 *>(it.chunk_rl)[c] = make_int2((int32_t)r, li);
-    } else if (L > it.short_max) {
-      const_cast<int32_t *>(it.med_rows)[mscan[g] - mscan[it.row0]] = (int32_t)r;
+    if (L > it.short_max) {
+      const int2 s0 = *reinterpret_cast<const int2 *>(it.m.seg + 2 * r);  // layer 0
+      const int4 d = make_int4((int32_t)r, L, s0.x, s0.y - s0.x);
+      if (L > it.long_min) {
+        const long long s = lscan[g] - lscan[it.row0];
+        const int32_t li = (int32_t)(s >> 32);
+        const long long c0 = s & 0xffffffff, nc = (L + CHUNK - 1) / CHUNK;
+        const_cast<int32_t *>(it.long_rows)[li] = (int32_t)r;
+        const_cast<long long *>(it.long_off)[li] = c0;
+        it.long_cnt[li] = 0;
+        for (long long c = c0; c < c0 + nc; c++) {
+          const_cast<int2 *>(it.chunk_rl)[c] = make_int2((int32_t)r, li);
+          const_cast<int4 *>(it.chunk_desc)[c] = d;
+        }
+      } else {
+        const_cast<int4 *>(it.med_desc)[mscan[g] - mscan[it.row0]] = d;
+      }
     }
   }
 }
@@ -163,6 +182,8 @@ __global__ void k_sched_info(Src src, const long long *lscan, const long long *m
       it.info[0] = n_long;
       it.info[1] = n_chunks;
       it.info[2] = (int32_t)(mscan[b] - mscan[a]);
+      it.info[8] = 0;  // k = 1 pass counters
+      it.info[9] = 0;
       const_cast<long long *>(it.long_off)[n_long] = n_chunks;
     }
   }
@@ -173,8 +194,11 @@ static int64_t max_chunks(dcsr_handle h) { return h->pool_cap / CHUNK + h->pool_
 int ensure_part(dcsr_handle h, int K, cudaStream_t s) {
   if (max_chunks(h) > h->chunk_cap) {
     if (h->chunk_rl) DCSR_CUDA(cudaFreeAsync(h->chunk_rl, s));
+    if (h->chunk_desc) DCSR_CUDA(cudaFreeAsync(h->chunk_desc, s));
     h->chunk_rl = nullptr;
+    h->chunk_desc = nullptr;
     DCSR_CUDA(cudaMallocAsync((void **)&h->chunk_rl, sizeof(int2) * max_chunks(h), s));
+    DCSR_CUDA(cudaMallocAsync((void **)&h->chunk_desc, sizeof(int4) * max_chunks(h), s));
     h->chunk_cap = max_chunks(h);
     h->bins_valid = false;  // the chunk table is gone
   }
@@ -195,7 +219,8 @@ RowItem<V> row_item(dcsr_handle h, const void *x, void *y, int64_t ldx, int64_t 
   it.long_rows = h->long_rows;
   it.long_off = h->long_off;
   it.chunk_rl = h->chunk_rl;
-  it.med_rows = h->med_rows;
+  it.med_desc = h->med_desc;
+  it.chunk_desc = h->chunk_desc;
   it.info = h->sched_info;
   it.long_cnt = h->long_cnt;
   it.part = h->part;
@@ -228,6 +253,7 @@ size_t schedule_scratch_bytes(int64_t R) { return 2 * arena_bytes(R + 2, 8) + sc
 template <typename V, typename Src>
 static int schedule_src(const Src &src, int count, int64_t R, Arena &ar, cudaStream_t s) {
   long long *lf = ar.take<long long>(R + 2), *mf = ar.take<long long>(R + 2);
+  if (ar.overflow) return DCSR_OOM;  // scratch sizing bug: no kernel sees a null pointer
   const int g = grid_for(R + 1, 256);
   DCSR_LAUNCH((k_sched_flags<V, Src>), g, 256, 0, s, src, R, lf, mf);
   DCSR_TRY(scan2_i64(lf, lf, nullptr, mf, mf, nullptr, R + 1, ar, s));
@@ -255,6 +281,7 @@ static int build_schedule_t(dcsr_handle h, cudaStream_t s, Arena &ar) {
 
 int build_schedule(dcsr_handle h, cudaStream_t s, Arena *ar) {
   Arena &a = ar ? *ar : h->scratch;
+  a.status = h->stat + ST_STATUS;
   if (h->dtype == DCSR_F32) return build_schedule_t<float>(h, s, a);
   return build_schedule_t<double>(h, s, a);
 }
@@ -295,6 +322,7 @@ __device__ __forceinline__ void unit_prefix_block(const RowItem<V> *its, int cou
     __syncthreads();
   }
   if (threadIdx.x < 3) pref[threadIdx.x * (count + 1) + count] = carry[threadIdx.x];
+  if (threadIdx.x == 0) pref[3 * (count + 1)] = 0;  // the k = 1 pass's counters
 }
 
 template <typename V>
@@ -546,6 +574,91 @@ __device__ __forceinline__ void write_y(V *y, int64_t ldy, int32_t row, const do
   }
 }
 
+// ------------------------------------------------- k = 1 short-row block
+// One warp, one block of 32 consecutive rows: one value per entry (SpMV
+// k = 1, row reductions), the block's entries streamed across the lanes in
+// windows of 32, U windows' loads in flight; a lane's row comes from ballots
+// over the window's row starts, sums use a segmented warp scan.
+// d0: the lane's row, its length and its layer-0 segment (start, capacity),
+// loaded ahead by the caller (row -1 past the matrix's end).
+template <typename V, int OP>
+__device__ __forceinline__ void short_block_k1(const RowItem<V> &it, int4 d0, int lane) {
+  using P = typename std::conditional<sizeof(V) == 4, float, double>::type;  // window partials
+  constexpr int U = 4;
+  const Mat<V> &m = it.m;
+  const V *__restrict__ x = it.x;
+  RowBlock rb;
+  rb.row = d0.x;
+  rb.len = d0.y;
+  rb.stream = rb.len > 0 && rb.len <= it.short_max;
+  double acc = op_init<double, OP>();
+  int64_t cum = 0;  // capacity of this lane's row in the layers before l
+  for (int l = 0; l < m.max_segs; l++) {
+    int32_t len_l = 0, st_l = 0;
+    if (l == 0) {
+      if (rb.stream) {  // the layer-0 segment came with the descriptor
+        len_l = rb.len < d0.w ? rb.len : d0.w;
+        st_l = d0.z;
+        cum = d0.w;
+      }
+    } else {
+      next_layer(m, rb, l, cum, len_l, st_l);
+    }
+    if (!__any_sync(FULL, len_l > 0)) break;
+    const int32_t incl = warp_incl_scan(len_l);  // block-local (<= 32 * short_max)
+    const int32_t excl = incl - len_l;
+    const int32_t E = __shfl_sync(FULL, incl, 31);
+    for (int32_t base = 0; base < E; base += 32 * U) {
+      int32_t q[U];
+      unsigned Mw[U];
+      bool ok[U];
+#pragma unroll
+      for (int i = 0; i < U; i++) {
+        const int32_t w0 = base + 32 * i;
+        const WinMap wm = window_map(w0, excl, incl, len_l, lane);
+        const int32_t ej = __shfl_sync(FULL, excl, wm.j);
+        const int32_t sj = __shfl_sync(FULL, st_l, wm.j);
+        ok[i] = w0 + lane < E;
+        Mw[i] = wm.M;
+        q[i] = sj + (ok[i] ? w0 + lane - ej : 0);
+      }
+      V a[U];
+      int32_t col[U];
+#pragma unroll
+      for (int i = 0; i < U; i++) {
+        a[i] = __ldcs(m.vals + q[i]);
+        col[i] = OP == OP_SPMV ? __ldcs(m.cols + q[i]) : 0;
+      }
+#pragma unroll
+      for (int i = 0; i < U; i++) {
+        P c = op_init<P, OP>();
+        if (ok[i]) {
+          if constexpr (OP == OP_SPMV) c = mul_rn((P)a[i], (P)__ldg(x + (int64_t)col[i] * it.ldx));
+          else c = OP == OP_COUNT ? (P)1 : (P)a[i];
+        }
+        // segmented inclusive scan: lanes p-d and p share a row unless a
+        // row starts in (p-d, p] (bit test on the window's start mask)
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+          const bool same = lane >= d && ((Mw[i] >> (lane - d + 1)) & ((1u << d) - 1u)) == 0;
+          const P co = __shfl_up_sync(FULL, c, d);
+          if (same) c = op_comb<P, OP>(c, co);
+        }
+        // lane j collects the tail of its row's run in this window
+        const int32_t w0 = base + 32 * i;
+        const bool hit = len_l > 0 && excl < w0 + 32 && incl > w0;
+        const int tail = (incl < w0 + 32 ? incl : w0 + 32) - 1 - w0;
+        const P got = __shfl_sync(FULL, c, hit ? tail : 0);
+        if (hit) acc = op_comb<double, OP>(acc, (double)got);
+      }
+    }
+  }
+  if (rb.row >= 0 && rb.len <= it.short_max) {
+    const double accs[1] = {acc};
+    write_y<V, 1, OP>(it.y, it.ldy, rb.row, accs, it.alpha, it.beta, rb.len, 1);
+  }
+}
+
 // --------------------------------------------------------- reduction pass
 
 // Blocks per SM the row pass is compiled for: the runtime-k families hold up
@@ -671,7 +784,7 @@ __global__ void __launch_bounds__(RS_THREADS_, RowsMinBlocks<K>::N) k_rows_reduc
       // ---- one medium row per warp, UN loads in flight per lane
       const int64_t mi = lu * RS_WARPS + w;
       if (mi >= it.info[2]) continue;
-      const int32_t row = it.med_rows[mi];
+      const int32_t row = it.med_desc[mi].x;
       const int64_t L = m.row_sizes[row];
       const Chain ch = load_chain(m, row);
       double acc[KA];
@@ -716,83 +829,13 @@ __global__ void __launch_bounds__(RS_THREADS_, RowsMinBlocks<K>::N) k_rows_reduc
       const int sub = (int)(wu - blk * S);
       if (blk * 32 >= m.n_rows) continue;
       if constexpr (K == 1) {
-        // one value per entry: stream the block's entries across the lanes
-        using P = typename std::conditional<sizeof(V) == 4, float, double>::type;  // window partials
-        constexpr int U = 4;
-        const RowBlock rb = load_block(m, blk * 32, lane, it.short_max);
-        double acc[KA];
-#pragma unroll
-        for (int k = 0; k < KA; k++) acc[k] = op_init<double, OP>();
-        int64_t cum = 0;  // capacity of this lane's row in the layers before l
-        for (int l = 0; l < m.max_segs; l++) {
-          int32_t len_l, st_l;
-          next_layer(m, rb, l, cum, len_l, st_l);
-          if (!__any_sync(FULL, len_l > 0)) break;
-          const int32_t incl = warp_incl_scan(len_l);  // block-local (<= 32 * short_max)
-          const int32_t excl = incl - len_l;
-          const int32_t E = __shfl_sync(FULL, incl, 31);
-          for (int32_t base = 0; base < E; base += 32 * U) {
-            int32_t q[U];
-            unsigned Mw[U];
-            bool ok[U];
-#pragma unroll
-            for (int i = 0; i < U; i++) {
-              const int32_t w0 = base + 32 * i;
-              const WinMap wm = window_map(w0, excl, incl, len_l, lane);
-              const int32_t ej = __shfl_sync(FULL, excl, wm.j);
-              const int32_t sj = __shfl_sync(FULL, st_l, wm.j);
-              ok[i] = w0 + lane < E;
-              Mw[i] = wm.M;
-              q[i] = sj + (ok[i] ? w0 + lane - ej : 0);
-            }
-            V a[U];
-            int32_t col[U];
-#pragma unroll
-            for (int i = 0; i < U; i++) {
-              a[i] = __ldcs(m.vals + q[i]);
-              col[i] = OP == OP_SPMV ? __ldcs(m.cols + q[i]) : 0;
-            }
-#pragma unroll
-            for (int i = 0; i < U; i++) {
-              P c[K];
-#pragma unroll
-              for (int k = 0; k < K; k++) c[k] = op_init<P, OP>();
-              if (ok[i]) {
-                if constexpr (OP == OP_SPMV) {
-                  P xv[K];
-                  load_xk<P, V, K, VEC>(x, col[i], ldx, xv);
-#pragma unroll
-                  for (int k = 0; k < K; k++) c[k] = mul_rn((P)a[i], xv[k]);
-                } else {
-                  c[0] = OP == OP_COUNT ? (P)1 : (P)a[i];
-                }
-              }
-              // segmented inclusive scan: lanes p-d and p share a row unless a
-              // row starts in (p-d, p] (bit test on the window's start mask)
-#pragma unroll
-              for (int d = 1; d < 32; d <<= 1) {
-                const bool same = lane >= d && ((Mw[i] >> (lane - d + 1)) & ((1u << d) - 1u)) == 0;
-#pragma unroll
-                for (int k = 0; k < KA; k++) {
-        if (K < 0 && k >= kr) break;
-                  const P co = __shfl_up_sync(FULL, c[k], d);
-                  if (same) c[k] = op_comb<P, OP>(c[k], co);
-                }
-              }
-              // lane j collects the tail of its row's run in this window
-              const int32_t w0 = base + 32 * i;
-              const bool hit = len_l > 0 && excl < w0 + 32 && incl > w0;
-              const int tail = (incl < w0 + 32 ? incl : w0 + 32) - 1 - w0;
-#pragma unroll
-              for (int k = 0; k < KA; k++) {
-        if (K < 0 && k >= kr) break;
-                const P got = __shfl_sync(FULL, c[k], hit ? tail : 0);
-                if (hit) acc[k] = op_comb<double, OP>(acc[k], (double)got);
-              }
-            }
-          }
+        const int64_t r = blk * 32 + lane;
+        int4 d0 = make_int4(-1, 0, 0, 0);
+        if (r < m.n_rows) {
+          const int2 s0 = __ldg(reinterpret_cast<const int2 *>(m.seg + 2 * r));
+          d0 = make_int4((int32_t)r, __ldg(m.row_sizes + r), s0.x, s0.y - s0.x);
         }
-        if (rb.row >= 0 && rb.len <= it.short_max) write_y<V, K, OP>(it.y, it.ldy, rb.row, acc, it.alpha, it.beta, rb.len, kr);
+        short_block_k1<V, OP>(it, d0, lane);
       } else {
         // K values per entry: G lanes per row
         const RowBlock rb = load_block(m, blk * 32, lane, it.short_max);
@@ -836,6 +879,252 @@ __global__ void __launch_bounds__(RS_THREADS_, RowsMinBlocks<K>::N) k_rows_reduc
   }
 }
 
+// ---------------------------------------------------- k = 1 single pass
+// SpMV with one right-hand side and the row reductions: every class in one
+// launch of warp units, taken from a device counter (longest first: long-row
+// chunks, then medium rows, then 32-row short blocks), so no class waits for
+// another's tail and a warp's next unit number is fetched while it works on
+// the current one.  A chunk or medium row is streamed lane-consecutively
+// (UN windows of 32 entries in flight per warp), the products of one window
+// step summed in the matrix type in a fixed order and the step sums
+// accumulated in FP64; a row of several chunks combines their partials in
+// chunk order (the warp that finishes its last chunk does it).  The pass is
+// bound by the x gathers (random 4-byte reads of x, one L1 line each).
+
+// Entries [c0, c1) of a row (chain ch) streamed across the warp; returns the
+// lane's partial.
+// Windows of 32 entries a warp has in flight per step, and blocks per SM the
+// k = 1 pass is compiled for.
+#ifndef DCSR_K1_UN
+#define DCSR_K1_UN 4
+#endif
+#ifndef DCSR_K1_MINB
+#define DCSR_K1_MINB 4
+#endif
+
+// Entries [c0, c1) of a row whose range lies in one segment starting at pool
+// slot st: two sets of UN windows, the loads of the next set in flight while
+// the current set's x values are gathered and summed.  Returns the lane's
+// partial.
+template <typename V, int OP>
+__device__ __forceinline__ double stream_seg(const RowItem<V> &it, int64_t st, int64_t c0, int64_t c1, int lane) {
+  using P = typename std::conditional<sizeof(V) == 4, float, double>::type;
+  constexpr int UN = sizeof(V) == 8 && DCSR_K1_UN > 1 ? DCSR_K1_UN / 2 : DCSR_K1_UN;  // FP64: half the windows
+  const V *__restrict__ vals = it.m.vals + st;
+  const int32_t *__restrict__ cols = it.m.cols + st;
+  const V *__restrict__ x = it.x;
+  V a[UN], an[UN];
+  int32_t col[UN], coln[UN];
+#pragma unroll
+  for (int i = 0; i < UN; i++) {
+    const int64_t p = c0 + 32 * i + lane, q = p < c1 ? p : c0;
+    a[i] = __ldcs(vals + q);
+    col[i] = OP == OP_SPMV ? __ldcs(cols + q) : 0;
+  }
+  double acc = op_init<double, OP>();
+  for (int64_t b0 = c0; b0 < c1; b0 += 32 * UN) {
+    const int64_t nb = b0 + 32 * UN;
+    if (nb < c1) {
+#pragma unroll
+      for (int i = 0; i < UN; i++) {
+        const int64_t p = nb + 32 * i + lane, q = p < c1 ? p : c0;
+        an[i] = __ldcs(vals + q);
+        coln[i] = OP == OP_SPMV ? __ldcs(cols + q) : 0;
+      }
+    }
+    P w = op_init<P, OP>();
+#pragma unroll
+    for (int i = 0; i < UN; i++) {
+      if (b0 + 32 * i + lane < c1) {
+        P t;
+        if constexpr (OP == OP_SPMV) t = mul_rn((P)a[i], (P)__ldg(x + (int64_t)col[i] * it.ldx));
+        else t = OP == OP_COUNT ? (P)1 : (P)a[i];
+        w = op_comb<P, OP>(w, t);
+      }
+    }
+    acc = op_comb<double, OP>(acc, (double)w);
+#pragma unroll
+    for (int i = 0; i < UN; i++) {
+      a[i] = an[i];
+      col[i] = coln[i];
+    }
+  }
+  return acc;
+}
+
+// The same over a range that crosses segments (a chained row): UN windows
+// per step, each entry's slot found through the chain.  Same summation
+// order as stream_seg.
+template <typename V, int OP>
+__device__ __noinline__ double stream_chain(const RowItem<V> &it, const Chain &ch, int64_t c0, int64_t c1, int lane) {
+  using P = typename std::conditional<sizeof(V) == 4, float, double>::type;
+  constexpr int UN = sizeof(V) == 8 && DCSR_K1_UN > 1 ? DCSR_K1_UN / 2 : DCSR_K1_UN;
+  const Mat<V> &m = it.m;
+  const int64_t first = ch.phys(c0);
+  double acc = op_init<double, OP>();
+  for (int64_t b0 = c0; b0 < c1; b0 += 32 * UN) {
+    V a[UN];
+    int32_t col[UN];
+#pragma unroll
+    for (int i = 0; i < UN; i++) {
+      const int64_t p = b0 + 32 * i + lane;
+      const int64_t q = p < c1 ? ch.phys(p) : first;
+      a[i] = __ldcs(m.vals + q);
+      col[i] = OP == OP_SPMV ? __ldcs(m.cols + q) : 0;
+    }
+    P w = op_init<P, OP>();
+#pragma unroll
+    for (int i = 0; i < UN; i++) {
+      if (b0 + 32 * i + lane < c1) {
+        P t;
+        if constexpr (OP == OP_SPMV) t = mul_rn((P)a[i], (P)__ldg(it.x + (int64_t)col[i] * it.ldx));
+        else t = OP == OP_COUNT ? (P)1 : (P)a[i];
+        w = op_comb<P, OP>(w, t);
+      }
+    }
+    acc = op_comb<double, OP>(acc, (double)w);
+  }
+  return acc;
+}
+
+template <int OP>
+__device__ __forceinline__ double warp_comb(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = op_comb<double, OP>(v, __shfl_xor_sync(FULL, v, o));
+  return v;
+}
+
+// A unit of the k = 1 pass, decoded and with its descriptor loaded: for a
+// chunk or a medium row every lane holds the row's descriptor (row, length,
+// layer-0 start, layer-0 capacity); for a block of short rows each lane holds
+// its own row's.
+enum { U1_CHUNK = 0, U1_MED = 1, U1_BLOCK = 2, U1_NONE = 3 };
+struct Unit1 {
+  int kind;
+  int item;    // matrix of the unit
+  int64_t lu;  // chunk number within the matrix (chunks)
+  int4 d;
+};
+
+template <typename V, typename Src>
+__device__ __forceinline__ Unit1 unit1_load(const Src &src, int64_t u, int64_t NC, int64_t NM, int64_t total,
+                                            int lane) {
+  Unit1 x;
+  x.kind = U1_NONE;
+  x.item = 0;
+  x.lu = 0;
+  x.d = make_int4(-1, 0, 0, 0);
+  if (u >= total) return x;
+  int64_t lu;
+  if (u < NC) {
+    x.item = src.locate(P_CHUNKS, u, lu);
+    const RowItem<V> &it = src.item(x.item);
+    if (it.skip && *it.skip) return x;
+    x.kind = U1_CHUNK;
+    x.lu = lu;
+    x.d = it.chunk_desc[lu];
+  } else if (u < NC + NM) {
+    x.item = src.locate(P_MED, (u - NC) / RS_WARPS, lu);
+    const RowItem<V> &it = src.item(x.item);
+    const int64_t mi = lu * RS_WARPS + (u - NC) % RS_WARPS;
+    if ((it.skip && *it.skip) || mi >= it.info[2]) return x;
+    x.kind = U1_MED;
+    x.d = it.med_desc[mi];
+  } else {
+    const int64_t bu = u - NC - NM;
+    x.item = src.locate(P_BLOCKS, bu / RS_WARPS, lu);
+    const RowItem<V> &it = src.item(x.item);
+    const int64_t blk = lu * RS_WARPS + bu % RS_WARPS;
+    if ((it.skip && *it.skip) || blk * 32 >= it.m.n_rows) return x;
+    x.kind = U1_BLOCK;
+    const int64_t r = blk * 32 + lane;
+    if (r < it.m.n_rows) {
+      const int2 s0 = __ldg(reinterpret_cast<const int2 *>(it.m.seg + 2 * r));
+      x.d = make_int4((int32_t)r, __ldg(it.m.row_sizes + r), s0.x, s0.y - s0.x);
+    }
+  }
+  return x;
+}
+
+template <typename V, int OP, typename Src>
+__global__ void __launch_bounds__(RS_THREADS_, DCSR_K1_MINB) k_rows1(Src src) {
+  const int lane = threadIdx.x & 31;
+  const int64_t NC = src.units(P_CHUNKS), NM = src.units(P_MED) * RS_WARPS, NB = src.units(P_BLOCKS) * RS_WARPS;
+  const int64_t total = NC + NM + NB;
+  unsigned *ctr = src.ctr();
+  auto fetch = [&]() -> int64_t {
+    unsigned v = 0;
+    if (lane == 0) v = atomicAdd(ctr, 1u);
+    return (int64_t)__shfl_sync(FULL, v, 0);
+  };
+  // three units in flight per warp: the one being worked on (its descriptor
+  // loaded), the next (its descriptor loads issued at the top of this
+  // iteration), and the one after (its number being fetched)
+  int64_t u = fetch();
+  Unit1 cur = unit1_load<V>(src, u, NC, NM, total, lane);
+  int64_t n1 = fetch();
+  while (u < total) {
+    const int64_t n2 = fetch();
+    const Unit1 nx = unit1_load<V>(src, n1, NC, NM, total, lane);
+    if (cur.kind == U1_CHUNK || cur.kind == U1_MED) {
+      // ---- a long-row chunk or a medium row
+      const RowItem<V> &it = src.item(cur.item);
+      const Mat<V> &m = it.m;
+      const int32_t row = cur.d.x;
+      const int64_t L = cur.d.y;
+      int64_t chunk = 0, nch = 1;
+      if (cur.kind == U1_CHUNK) nch = (L + CHUNK - 1) / CHUNK;
+      int64_t li = 0;
+      if (nch > 1) {
+        li = it.chunk_rl[cur.lu].y;
+        chunk = cur.lu - it.long_off[li];
+      }
+      const int64_t c0 = chunk * CHUNK, c1 = cur.kind == U1_CHUNK ? (c0 + CHUNK < L ? c0 + CHUNK : L) : L;
+      const double part = c1 <= cur.d.w ? stream_seg<V, OP>(it, cur.d.z, c0, c1, lane)  // inside layer 0
+                                        : stream_chain<V, OP>(it, load_chain(m, row), c0, c1, lane);
+      const double t = warp_comb<OP>(part);
+      if (nch == 1) {
+        if (lane == 0) {
+          const double o[1] = {t};
+          write_y<V, 1, OP>(it.y, it.ldy, row, o, it.alpha, it.beta, (int32_t)L, 1);
+        }
+      } else {
+        const int64_t p0 = it.long_off[li];
+        int last = 0;
+        if (lane == 0) {
+          it.part[p0 + chunk] = t;
+          __threadfence();
+          last = atomicAdd(&it.long_cnt[li], 1) == nch - 1;
+        }
+        if (__shfl_sync(FULL, last, 0)) {
+          // every chunk's partial is published: lanes take partials
+          // lane, lane+32, ... in order, then a fixed xor tree
+          __threadfence();
+          double v = op_init<double, OP>();
+          for (int64_t q = lane; q < nch; q += 32) v = op_comb<double, OP>(v, __ldcg(it.part + p0 + q));
+          v = warp_comb<OP>(v);
+          if (lane == 0) {
+            const double o[1] = {v};
+            write_y<V, 1, OP>(it.y, it.ldy, row, o, it.alpha, it.beta, (int32_t)L, 1);
+            it.long_cnt[li] = 0;
+          }
+        }
+      }
+    } else if (cur.kind == U1_BLOCK) {
+      // ---- a block of 32 short rows
+      short_block_k1<V, OP>(src.item(cur.item), cur.d, lane);
+    }
+    u = n1;
+    cur = nx;
+    n1 = n2;
+  }
+  // the last warp to finish resets the counters for the next pass
+  if (lane == 0 && atomicAdd(ctr + 1, 1u) == gridDim.x * RS_WARPS - 1) {
+    ctr[0] = 0;
+    ctr[1] = 0;
+  }
+}
+
 // -------------------------------------------------------------- copy pass
 // Copies each row's logical entries to dst_off[r] in (out_cols, out_vals),
 // optionally writing COO row ids and an int32 row pointer (one matrix).
@@ -870,7 +1159,7 @@ __global__ void __launch_bounds__(RS_THREADS_) k_rows_copy(RowItem<V> it, const 
       } else {
         const int64_t mi = u * RS_WARPS + w;
         if (mi >= it.info[2]) continue;
-        row = it.med_rows[mi];
+        row = it.med_desc[mi].x;
         L = m.row_sizes[row];
         c0 = 0;
         c1 = L;
@@ -961,13 +1250,19 @@ static int grid_of(const void *k) { return persistent_grid(k, RS_THREADS_, 0); }
 
 template <typename V, int K, int OP, bool VEC, typename Src>
 static int launch_reduce_src(const Src &src, cudaStream_t s) {
-  static const int g0 = grid_of((const void *)k_rows_reduce<V, K, OP, VEC, P_BLOCKS, Src>);
-  static const int g1 = grid_of((const void *)k_rows_reduce<V, K, OP, VEC, P_CHUNKS, Src>);
-  static const int g2 = grid_of((const void *)k_rows_reduce<V, K, OP, VEC, P_MED, Src>);
-  DCSR_LAUNCH((k_rows_reduce<V, K, OP, VEC, P_CHUNKS, Src>), g1, RS_THREADS_, 0, s, src);
-  DCSR_LAUNCH((k_rows_reduce<V, K, OP, VEC, P_MED, Src>), g2, RS_THREADS_, 0, s, src);
-  DCSR_LAUNCH((k_rows_reduce<V, K, OP, VEC, P_BLOCKS, Src>), g0, RS_THREADS_, 0, s, src);
-  return DCSR_OK;
+  if constexpr (K == 1) {  // one value per entry: every class in one launch
+    static const int g = grid_of((const void *)k_rows1<V, OP, Src>);
+    DCSR_LAUNCH((k_rows1<V, OP, Src>), g, RS_THREADS_, 0, s, src);
+    return DCSR_OK;
+  } else {
+    static const int g0 = grid_of((const void *)k_rows_reduce<V, K, OP, VEC, P_BLOCKS, Src>);
+    static const int g1 = grid_of((const void *)k_rows_reduce<V, K, OP, VEC, P_CHUNKS, Src>);
+    static const int g2 = grid_of((const void *)k_rows_reduce<V, K, OP, VEC, P_MED, Src>);
+    DCSR_LAUNCH((k_rows_reduce<V, K, OP, VEC, P_CHUNKS, Src>), g1, RS_THREADS_, 0, s, src);
+    DCSR_LAUNCH((k_rows_reduce<V, K, OP, VEC, P_MED, Src>), g2, RS_THREADS_, 0, s, src);
+    DCSR_LAUNCH((k_rows_reduce<V, K, OP, VEC, P_BLOCKS, Src>), g0, RS_THREADS_, 0, s, src);
+    return DCSR_OK;
+  }
 }
 
 // Warps per 32-row block of short rows for the k >= 2 pass: doubled (up to

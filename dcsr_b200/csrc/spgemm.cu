@@ -302,12 +302,14 @@ static int spgemm_impl(dcsr_handle hA, dcsr_handle hB, dcsr_handle hC, cudaStrea
   const int32_t n = hA->n_rows;
   Mat<V> A = hA->view<V>(), B = hB->view<V>();
   Arena ar;
+  ar.status = hC->stat + ST_STATUS;  // look-back timeouts reach C's status
   DCSR_TRY(ar.reserve(arena_bytes(n + 2, 8) * 3 + arena_bytes(n + 2, 4) * 2 + arena_bytes(8, 8) +
                           radix_scratch_bytes(n) + scan_scratch_bytes(n + 2), s));
   long long *cnt = ar.take<long long>(n + 2);
   unsigned long long *k0 = ar.take<unsigned long long>(n + 2), *k1 = ar.take<unsigned long long>(n + 2);
   unsigned *r0 = ar.take<unsigned>(n + 2), *r1 = ar.take<unsigned>(n + 2);
   long long *starts = ar.take<long long>(8);
+  if (ar.overflow) return DCSR_OOM;  // scratch sizing bug: no kernel sees a null pointer
   long long *ub = cnt;  // scanned in place
   if (n > 0) {
     DCSR_LAUNCH(k_sg_count<V>, grid_for((int64_t)n * 32, SG_THREADS), SG_THREADS, 0, s, A, B, cnt, k0, r0);
@@ -347,8 +349,10 @@ static int spgemm_impl(dcsr_handle hA, dcsr_handle hB, dcsr_handle hC, cudaStrea
     // products of all large rows, laid out densely by slot, then one stable
     // radix sort by (slot, column) keeps every column's products in p order
     Arena g;
+    g.status = hC->stat + ST_STATUS;  // look-back timeouts reach C's status
     DCSR_TRY(g.reserve(arena_bytes(n_global + 2, 8) + scan_scratch_bytes(n_global + 2), s));
     long long *goff = g.take<long long>(n_global + 2);
+    if (g.overflow) return DCSR_OOM;  // scratch sizing bug: no kernel sees a null pointer
     DCSR_LAUNCH(k_sg_global_sizes, grid_for(n_global + 1, 256), 256, 0, s, r0, starts, ub, goff);
     DCSR_TRY(scan_i64(goff, goff, n_global + 1, hC->stat + ST_AUX + 1, g, s));
     long long Pg = 0;
@@ -356,12 +360,14 @@ static int spgemm_impl(dcsr_handle hA, dcsr_handle hB, dcsr_handle hC, cudaStrea
     DCSR_CUDA(cudaStreamSynchronize(s));
     if (Pg > 0xffffffffLL) return DCSR_NOT_SUPPORTED;
     Arena gg;
+    gg.status = hC->stat + ST_STATUS;  // look-back timeouts reach C's status
     DCSR_TRY(gg.reserve(2 * arena_bytes(Pg, 8) + 2 * arena_bytes(Pg, 4) + arena_bytes(Pg, sizeof(V)) +
                             arena_bytes(Pg + 1, 8) + radix_scratch_bytes(Pg) + scan_scratch_bytes(Pg + 1), s));
     unsigned long long *gk0 = gg.take<unsigned long long>(Pg), *gk1 = gg.take<unsigned long long>(Pg);
     unsigned *gi0 = gg.take<unsigned>(Pg), *gi1 = gg.take<unsigned>(Pg);
     V *gprod = (V *)gg.take<double>(Pg);
     long long *hpos = gg.take<long long>(Pg + 1);
+    if (gg.overflow) return DCSR_OOM;  // scratch sizing bug: no kernel sees a null pointer
     const int cb = bits_for(hB->n_cols);
     DCSR_LAUNCH(k_sg_global_expand<V>, grid_for(n_global * 32, 256), 256, 0, s, A, B, r0, starts, goff, cb, gk0, gi0,
                 gprod);
@@ -378,8 +384,10 @@ static int spgemm_impl(dcsr_handle hA, dcsr_handle hB, dcsr_handle hC, cudaStrea
   int32_t *ccol = nullptr;
   V *cval = nullptr;
   Arena c;
+  c.status = hC->stat + ST_STATUS;  // look-back timeouts reach C's status
   DCSR_TRY(c.reserve(arena_bytes(n + 2, 8) + scan_scratch_bytes(n + 2), s));
   rp = c.take<long long>(n + 2);
+  if (c.overflow) return DCSR_OOM;  // scratch sizing bug: no kernel sees a null pointer
   DCSR_TRY(scan_i64(ucnt, rp, n + 1, hC->stat + ST_TOTAL, c, s));
   long long nnzc = 0;
   DCSR_CUDA(cudaMemcpyAsync(&nnzc, hC->stat + ST_TOTAL, sizeof(nnzc), cudaMemcpyDeviceToHost, s));

@@ -650,6 +650,7 @@ static int update_pipeline(const Src &src, int count, int64_t T, bool merge, int
   V *bval = ar.take<V>(T), *nval = ar.take<V>(T);
   long long *hflag = ar.take<long long>(T + 2), *tcap = ar.take<long long>(T + 2);
   long long *ttiles = ar.take<long long>(T + 2), *nflag = ar.take<long long>(T + 2);
+  if (ar.overflow) return DCSR_OOM;  // scratch sizing bug: no kernel sees a null pointer
   const int gT = grid_for(T + 1, 256);
   const int gI = grid_for(count, 256);
 
@@ -711,6 +712,7 @@ int update_async(dcsr_handle h, const int32_t *rows, const int32_t *cols, const 
   if (nnz == 0) return DCSR_OK;
   if (nnz > 0x7ffffff0LL) return DCSR_BAD_ARG;
   Arena &a = ar ? *ar : h->scratch;
+  a.status = h->stat + ST_STATUS;  // a look-back wait that gives up reports DCSR_TIMEOUT here
   if (h->dtype == DCSR_F32) return update_one<float>(h, rows, cols, (const float *)vals, nnz, s, a);
   return update_one<double>(h, rows, cols, (const double *)vals, nnz, s, a);
 }
@@ -725,6 +727,7 @@ static int update_many_t(const BatchItem<V> *items_dev, int count, int64_t T, bo
 int update_many(const void *items_dev, int dtype, int count, int64_t T, bool merge, int rb, int cb, long long *gstat,
                 Arena &ar, cudaStream_t s) {
   if (T == 0 || count == 0) return DCSR_OK;
+  ar.status = gstat + ST_STATUS;  // a look-back wait that gives up reports DCSR_TIMEOUT for the batch
   if (dtype == DCSR_F32)
     return update_many_t<float>((const BatchItem<float> *)items_dev, count, T, merge, rb, cb, gstat, ar, s);
   return update_many_t<double>((const BatchItem<double> *)items_dev, count, T, merge, rb, cb, gstat, ar, s);
@@ -790,6 +793,7 @@ static int coo_impl(dcsr_handle h, const int32_t *rows, const int32_t *cols, con
   int32_t *oc = ar.take<int32_t>(T);
   V *ov = (V *)ar.take<double>(T);
   long long *cnt = ar.take<long long>(h->n_rows + 2);
+  if (ar.overflow) return DCSR_OOM;  // scratch sizing bug: no kernel sees a null pointer
   DCSR_CUDA(cudaMemsetAsync(cnt, 0, sizeof(long long) * (h->n_rows + 2), s));
   if (T > 0) {
     DCSR_LAUNCH(k_coo_keys, grid_for(T, 256), 256, 0, s, rows, cols, T, h->n_rows, h->n_cols, cb, merge ? 1 : 0, k0,

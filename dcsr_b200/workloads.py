@@ -18,6 +18,9 @@ workloads:
                        U[4, 64] with Poisson row lengths, FP32 U(-1,1); update
                        batches log-uniform [100, 100k]; SpMV with k in {1,2,4,8}.
 * ``served``           2000 resident matrices drawn like ``batched``.
+* ``spd_matrix``       a symmetric, strictly diagonally dominant (so positive
+                       definite) matrix for the CG solver, and update batches
+                       that keep it so.
 
 Generators return CSR (row_ptr, cols, vals) with rows sorted and unique, and
 update batches as COO (rows, cols, vals) in batch order.
@@ -216,3 +219,44 @@ def served_trace(seed: int, n_mats: int, count: int, min_upd: int = 10, max_upd:
     k = rng.integers(1, 9, count).astype(np.int32)
     size = np.where(kind == 0, upd, np.where(kind == 1, k, 0))
     return kind, mat, size
+
+
+def spd_matrix(seed: int = 0, n: int = 4096, degree: float = 6.0):
+    """Symmetric, strictly diagonally dominant matrix with a positive diagonal
+    (hence positive definite): returns CSR (row_ptr, cols, vals[f64]) with
+    rows sorted and unique."""
+    rng = np.random.default_rng(seed)
+    rp, cols = poisson_matrix(rng, n, n, degree / 2)
+    rows = np.repeat(np.arange(n, dtype=np.int64), np.diff(rp))
+    off = rows != cols
+    rows, cols = rows[off], cols[off].astype(np.int64)
+    v = rng.uniform(-1.0, 1.0, rows.size)
+    # symmetric: (i, j) and (j, i) with the same value, duplicates summed
+    keys = np.concatenate([rows * n + cols, cols * n + rows])
+    vals = np.concatenate([v, v])
+    order = np.argsort(keys, kind="stable")
+    keys, vals = keys[order], vals[order]
+    uk, start = np.unique(keys, return_index=True)
+    sv = np.add.reduceat(vals, start) if keys.size else vals
+    r, c = uk // n, uk % n
+    absrow = np.bincount(r, weights=np.abs(sv), minlength=n)
+    keys = np.concatenate([uk, np.arange(n, dtype=np.int64) * (n + 1)])
+    vals = np.concatenate([sv, absrow + 1.0])
+    order = np.argsort(keys, kind="stable")
+    keys, vals = keys[order], vals[order]
+    row_ptr = np.zeros(n + 1, np.int64)
+    np.cumsum(np.bincount(keys // n, minlength=n), out=row_ptr[1:])
+    return row_ptr.astype(np.int32), (keys % n).astype(np.int32), vals
+
+
+def spd_updates(seed: int, n: int, pairs: int):
+    """COO update batch that keeps spd_matrix's properties: each pair (i, j),
+    i != j, adds v at (i, j) and (j, i) and 2|v| at (i, i) and (j, j)."""
+    rng = np.random.default_rng(seed)
+    i = rng.integers(0, n, pairs)
+    j = (i + rng.integers(1, n, pairs)) % n
+    v = rng.uniform(-1.0, 1.0, pairs)
+    rows = np.concatenate([i, j, i, j]).astype(np.int32)
+    cols = np.concatenate([j, i, i, j]).astype(np.int32)
+    vals = np.concatenate([v, v, 2 * np.abs(v), 2 * np.abs(v)])
+    return rows, cols, vals

@@ -125,6 +125,25 @@ int dcsr_to_csr(dcsr_handle h, int32_t *row_ptr, int32_t *cols, void *vals, void
 /* DCSR -> COO in row order (rows, cols, vals of length nnz). */
 int dcsr_to_coo(dcsr_handle h, int32_t *rows, int32_t *cols, void *vals, void *stream);
 
+/* Binary snapshot and restore (Matrix Market / checkpoint IO; the
+ * reference keeps matrices in device memory only and reads text files with
+ * ReadMatrixFile, include/load_matrix.h:48-119).  The image is a fixed
+ * header (magic "DCSRSNP1", shape, dtype, layout policy, pitch, pool
+ * capacity, pool top) followed by row_sizes[n_rows+1], seg[max_segs*pitch]
+ * and the pool's cols/vals up to its top.  Restoring it reproduces the layout
+ * bit for bit (row lengths, every segment pair, pool capacity and contents),
+ * so a compacted or chained matrix comes back exactly as it was saved.
+ * All three synchronise the stream; buffers are host memory. */
+int dcsr_snapshot_bytes(dcsr_handle h, int64_t *bytes, void *stream);
+int dcsr_snapshot(dcsr_handle h, void *host_buf, int64_t buf_bytes, void *stream);
+/* Shape, dtype and policy stored in an image (to create the handle to
+ * restore into); DCSR_BAD_ARG if the buffer is not a snapshot. */
+int dcsr_snapshot_header(const void *host_buf, int64_t buf_bytes, int32_t *n_rows, int32_t *n_cols, int32_t *dtype,
+                         dcsr_opts *opts);
+/* Into a handle of the image's shape, dtype and max_segs (its policy is set
+ * from the image); the handle's previous content is replaced. */
+int dcsr_restore(dcsr_handle h, const void *host_buf, int64_t buf_bytes, void *stream);
+
 /* -------------------------------------------------------------- updates */
 
 /* In-place batch update with COO triples in any order.  Replaces
@@ -177,6 +196,20 @@ int dcsr_row_reduce(dcsr_handle h, int32_t op, void *y, void *stream);
  * zeros kept, all rows computed.  Replaces device::spmm (include/spmm.h:30-391).
  * Synchronises once (output size). */
 int dcsr_spgemm(dcsr_handle A, dcsr_handle B, dcsr_handle C, void *stream);
+
+/* Conjugate gradient on a symmetric positive definite matrix (square),
+ * unpreconditioned: the solver the reference tree ships for its matrices
+ * (cusp::krylov::cg, cusp/krylov/detail/cg.inl) with cusp::monitor's stop
+ * rule (cusp/detail/monitor.inl: stop when ||r||_2 <= abs_tol +
+ * rel_tol*||b||_2, tested before every iteration, or after max_iter
+ * iterations; cusp's defaults are 500, 1e-5 and 0).  b and x are device
+ * vectors of the matrix dtype; x holds the initial guess on entry and the
+ * iterate on return.  *iters / *resid (host, may be NULL) receive the
+ * iteration count and the last residual norm.  Every step runs on the device
+ * (the SpMV is dcsr_spmv's); the host reads the stop flag between chunks of
+ * iterations.  Synchronises. */
+int dcsr_cg(dcsr_handle A, const void *b, void *x, int32_t max_iter, double rel_tol, double abs_tol, int32_t *iters,
+            double *resid, void *stream);
 
 /* X[I[n]] += 1 for a sorted index array I.  Replaces
  * device::count_sorted_indices (include/primitives.h:417-464). */
@@ -348,6 +381,17 @@ uint64_t dcsr_launch_count(void);
  * affected result is wrong; nothing hangs).  Synchronises the device.  No
  * counterpart in the reference (its scans and sorts come from Thrust/CUB). */
 int dcsr_spin_faults(int64_t *count);
+/* Failure-handling test hook (no counterpart in the reference).  Sets the
+ * iteration limit of the look-back waits (spin_limit <= 0 restores the
+ * default, about a second) and, with stall_first_tile != 0, keeps the first
+ * tile of every single-pass scan and sort from publishing its prefix, so the
+ * waits on it run out: each such wait gives up after the limit, the kernel
+ * finishes (its result is wrong) and the operation's status word -- read by
+ * dcsr_get_status, dcsr_batch_status, or returned by the synchronising
+ * calls -- reports DCSR_TIMEOUT.  Nothing hangs and no GPU fault is raised.
+ * For tests only; synchronises the device; not thread-safe with running
+ * operations. */
+int dcsr_debug_lookback(int32_t spin_limit, int32_t stall_first_tile);
 /* Pre-grow the current device's stream-ordered memory pool, from which
  * every matrix pool, scratch arena and staging buffer of this library is
  * allocated, by `bytes` (allocated and freed on `stream`, then kept by the

@@ -43,9 +43,18 @@ class OrDcsr(C.Structure):
                 ("cols", C.POINTER(C.c_int32)), ("vals", C.POINTER(C.c_double))]
 
 
+def reference_tree() -> str | None:
+    """The reference source tree: $DCSR_REFERENCE, else its conventional
+    location in the build container when present; None elsewhere (the GPU
+    box uses the prebuilt oracle/_ref only)."""
+    p = os.environ.get("DCSR_REFERENCE") or "/root/reference"
+    return p if os.path.isdir(p) else None
+
+
 def build() -> None:
     """Compile the oracle (and oracle/_ref when the reference tree exists)."""
-    subprocess.run(["make", "-s", "-C", HERE], check=True)
+    ref = reference_tree()
+    subprocess.run(["make", "-s", "-C", HERE] + ([f"REF={ref}"] if ref else []), check=True)
 
 
 _lib = None
@@ -185,6 +194,29 @@ class OracleDcsr:
         lib().or_row_reduce(self.p, op, y)
         return y
 
+    def cg(self, b, x0=None, max_iter=500, rel_tol=1e-5, abs_tol=0.0):
+        """Unpreconditioned CG in FP64 over this matrix's SpMV: the steps of
+        cusp::krylov::cg (reference cusp/krylov/detail/cg.inl:62-128) with
+        cusp::monitor's stop rule (cusp/detail/monitor.inl: ||r||_2 <=
+        abs_tol + rel_tol*||b||_2 tested before every iteration, at most
+        max_iter iterations).  Returns (x, iterations, final residual norm)."""
+        b = _f64(b)
+        x = np.zeros(self.n_rows) if x0 is None else _f64(x0).copy()
+        r = b - self.spmv(x)
+        p = r.copy()
+        rz = float(r @ r)
+        tol = abs_tol + rel_tol * float(np.sqrt(b @ b))
+        it = 0
+        while not (np.sqrt(rz) <= tol or it >= max_iter):
+            y = self.spmv(p)
+            alpha = rz / float(y @ p)
+            x += alpha * p
+            r -= alpha * y
+            rz_old, rz = rz, float(r @ r)
+            p = r + (rz / rz_old) * p
+            it += 1
+        return x, it, float(np.sqrt(rz))
+
     def spgemm(self, B: "OracleDcsr", opts: OrOpts | None = None) -> "OracleDcsr":
         o = opts if opts is not None else default_opts()
         st = C.c_int(0)
@@ -223,6 +255,23 @@ def reduce_by_key(keys, vals, dtype=F64):
 
 # ------------------------------------------------------------ cusp harness
 
+def ref_read_mtx(path: str, cap: int = 1 << 22):
+    """The reference's own ReadMatrixFile<int, double> (oracle/_ref/libref_mtx.so):
+    (n_rows, n_cols, rows, cols, vals) with 0-based indices, file order."""
+    lib_path = os.path.join(REFDIR, "libref_mtx.so")
+    if not os.path.exists(lib_path):
+        raise FileNotFoundError(lib_path)
+    L = C.CDLL(lib_path)
+    L.ref_read_mtx.argtypes = [C.c_char_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_long, _i32p, _i32p, _f64p]
+    L.ref_read_mtx.restype = C.c_int
+    r = np.zeros(cap, np.int32)
+    c = np.zeros(cap, np.int32)
+    v = np.zeros(cap, np.float64)
+    nr, nc = C.c_int(), C.c_int()
+    nnz = L.ref_read_mtx(path.encode(), C.byref(nr), C.byref(nc), cap, r, c, v)
+    return nr.value, nc.value, r[:nnz].copy(), c[:nnz].copy(), v[:nnz].copy()
+
+
 class Ref:
     """The reference's own cusp host path (oracle/_ref); ``seq`` picks the
     sequential host system (bit-reproducible), else the OpenMP one."""
@@ -242,6 +291,8 @@ class Ref:
                                  _i32p, _f64p]
         L.ref_spgemm.restype = C.c_void_p
         L.ref_sort_by_row.argtypes = [C.c_int32, _i32p, _i32p, _f64p, C.c_int64]
+        L.ref_cg.argtypes = [C.c_int32, C.c_int32, _i32p, _i32p, _f64p, _f64p, _f64p, C.c_int32, C.c_double,
+                             C.c_double, C.POINTER(C.c_int32), C.POINTER(C.c_double)]
         L.ref_result_nnz.argtypes = [C.c_void_p]
         L.ref_result_nnz.restype = C.c_int64
         L.ref_result_rows_len.argtypes = [C.c_void_p]
@@ -297,6 +348,15 @@ class Ref:
         """cusp::multiply(csr, csr): returns CSR (row_ptr, cols, vals); rows unsorted, zeros dropped."""
         h = self.L.ref_spgemm(dtype, n, k, m, _i32(arp), _i32(aci), _f64(av), _i32(brp), _i32(bci), _f64(bv))
         return self._take(h)
+
+    def cg(self, dtype, n, rp, ci, vv, b, x0, max_iter=500, rel_tol=1e-5, abs_tol=0.0):
+        """cusp::krylov::cg with a cusp::monitor(b, max_iter, rel_tol, abs_tol):
+        (x, iterations, residual norm)."""
+        x = _f64(x0).copy()
+        it, res = C.c_int32(), C.c_double()
+        self.L.ref_cg(dtype, n, _i32(rp), _i32(ci), _f64(vv), _f64(b), x, max_iter, rel_tol, abs_tol,
+                      C.byref(it), C.byref(res))
+        return x, it.value, res.value
 
     def sort_by_row(self, dtype, rows, cols, vals):
         r, c, v = _i32(rows).copy(), _i32(cols).copy(), _f64(vals).copy()

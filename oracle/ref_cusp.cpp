@@ -11,11 +11,14 @@
 //   cusp::add(coo, coo, coo)         cusp/system/detail/generic/elementwise.inl:75-231
 //   cusp::multiply(csr, csr, csr)    cusp/system/detail/sequential/multiply/csr_spgemm.h:38-182
 //   cusp::sort_by_row(r, c, v)       cusp/detail/sort.inl:38-67 (stable)
+//   cusp::krylov::cg(A, x, b, mon)   cusp/krylov/detail/cg.inl (the reference's included solver)
 // which are the CSR comparison / update operations the reference's drivers
 // time (src/Fill_Test.inl:236-264, src/SPMM_Test.inl:142).
 #include <cusp/coo_matrix.h>
 #include <cusp/csr_matrix.h>
 #include <cusp/elementwise.h>
+#include <cusp/krylov/cg.h>
+#include <cusp/monitor.h>
 #include <cusp/multiply.h>
 #include <cusp/sort.h>
 
@@ -137,9 +140,35 @@ struct Stream {
   cusp::array1d<V, DM> x, ones, y, rs;
 };
 
+// Unpreconditioned CG with cusp's monitor (stop when ||r|| <= abs + rel*||b||
+// or after max_iter iterations); x holds the initial guess on entry.
+template <typename V>
+void cg_impl(int32_t n, const int32_t *rp, const int32_t *ci, const double *vv, const double *b, double *x,
+             int32_t max_iter, double rel, double abs_tol, int32_t *iters, double *resid) {
+  cusp::csr_matrix<int, V, DM> A = host_csr<V>(n, n, rp, ci, vv);
+  cusp::array1d<V, HM> bh(n), xh(n);
+  for (int32_t i = 0; i < n; i++) {
+    bh[i] = (V)b[i];
+    xh[i] = (V)x[i];
+  }
+  cusp::array1d<V, DM> bd = bh, xd = xh;
+  cusp::monitor<V> mon(bd, (size_t)max_iter, (V)rel, (V)abs_tol);
+  cusp::krylov::cg(A, xd, bd, mon);
+  xh = xd;
+  for (int32_t i = 0; i < n; i++) x[i] = (double)xh[i];
+  *iters = (int32_t)mon.iteration_count();
+  *resid = (double)mon.residual_norm();
+}
+
 }  // namespace
 
 extern "C" {
+
+void ref_cg(int32_t dtype, int32_t n, const int32_t *rp, const int32_t *ci, const double *vv, const double *b,
+            double *x, int32_t max_iter, double rel, double abs_tol, int32_t *iters, double *resid) {
+  if (dtype == 0) cg_impl<float>(n, rp, ci, vv, b, x, max_iter, rel, abs_tol, iters, resid);
+  else cg_impl<double>(n, rp, ci, vv, b, x, max_iter, rel, abs_tol, iters, resid);
+}
 
 int ref_threads(void) {
 #ifdef _OPENMP

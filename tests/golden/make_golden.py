@@ -9,6 +9,9 @@ synthetic inputs and the outputs of the reference's cusp host path
   append_small.npz   cusp::sort_by_row(A entries ++ batch) (append semantics)
   spmv_small.npz     cusp::multiply(A, x) in FP32
   spgemm_small.npz   cusp::multiply(A, A) in FP64 (rows unsorted, zeros dropped)
+  mtx_values.npz     ReadMatrixFile (the reference's Matrix Market reader) on
+                     the texts of mtx_corpus.py
+  cg_small.npz       cusp::krylov::cg (cusp::monitor defaults) on an SPD matrix
 """
 import os
 import sys
@@ -17,6 +20,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+sys.path.insert(0, HERE)
 
 from dcsr_b200 import workloads as W  # noqa: E402
 from oracle import oracle as O  # noqa: E402
@@ -63,6 +67,24 @@ def main():
     C = ref.spgemm(O.F64, m, m, m, grp, gcols, gvals, grp, gcols, gvals)
     np.savez_compressed(os.path.join(HERE, "spgemm_small.npz"), n=m, rp=grp, cols=gcols, vals=gvals, c_rp=C[0],
                         c_cols=C[1], c_vals=C[2])
+    import tempfile
+    from mtx_corpus import corpus
+    mtx = {}
+    with tempfile.TemporaryDirectory() as d:
+        for name, text in corpus().items():
+            path = os.path.join(d, name + ".mtx")
+            with open(path, "w", newline="") as f:
+                f.write(text)
+            nr, nc, r, c, v = O.ref_read_mtx(path)
+            mtx.update({f"{name}_shape": np.array([nr, nc]), f"{name}_rows": r, f"{name}_cols": c,
+                        f"{name}_vals": v})
+    np.savez_compressed(os.path.join(HERE, "mtx_values.npz"), **mtx)
+    n = 600
+    rp, cg_c, cg_v = W.spd_matrix(21, n)
+    b = np.random.default_rng(22).uniform(-1, 1, n)
+    x, it, res = ref.cg(O.F64, n, rp, cg_c, cg_v, b, np.zeros(n))
+    np.savez_compressed(os.path.join(HERE, "cg_small.npz"), rp=rp, cols=cg_c, vals=cg_v, b=b, x=x, iters=it,
+                        resid=res, max_iter=500, rel_tol=1e-5)
     print("wrote fixtures to", HERE)
 
 

@@ -23,7 +23,7 @@ from dcsr_b200 import workloads as W
 from oracle import oracle as O
 
 GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
-REF_TREE = "/root/reference"
+REF_TREE = O.reference_tree() or ""
 
 
 def load(name):

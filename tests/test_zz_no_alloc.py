@@ -4,10 +4,11 @@ dcsr_reduce_by_key_noalloc exists for callers that cannot allocate device
 memory at call time (fixed up-front memory budgets, or a foreign allocator
 that must not have CUDA's allocator run underneath it).  Its scratch is a
 static device array in the library, shared by every call.  This test calls
-both entry points through the C ABI on two different inputs in a row and
+both entry points through the C ABI on three different inputs in a row and
 requires identical results (the same bit-exact bar as the other
-reduce-by-key tests), so a second call cannot see stale scratch from the
-first.  It sits in its own file, collected last.
+reduce-by-key tests), so a later call cannot see stale scratch (head
+positions, look-back epochs and tile counters) from an earlier one.  It sits
+in its own file, collected last.
 """
 import ctypes as C
 
@@ -45,14 +46,18 @@ def test_noalloc_matches_allocating_entry_point_twice(dcsr, dtype):
     L, fn_noalloc = _bind(dcsr)
     code = dcsr.F32 if dtype == torch.float32 else dcsr.F64
     rng = np.random.default_rng(123)
-    # two calls in a row: a large input, then a smaller one with other keys
-    for n, span in ((dcsr_max(L) // 2 + 12345, 70000), (3001, 900)):
+    faults = dcsr.spin_faults()
+    # calls in a row, all above one scan block (4096 keys), so each reuses the
+    # static array's look-back area after the previous call: the full
+    # capacity, then a smaller input with other keys, then one single run
+    for n, span in ((dcsr_max(L), 70000), (dcsr_max(L) // 3 + 12345, 900), (5000, 1)):
         keys = torch.tensor(np.sort(rng.integers(0, span, n)).astype(np.int32), device="cuda")
         vals = torch.tensor(rng.standard_normal(n), dtype=dtype, device="cuda")
         k_ref, v_ref = dcsr.reduce_by_key(keys, vals)
         k_na, v_na = _run(fn_noalloc, keys, vals, code)
         np.testing.assert_array_equal(k_na, k_ref.cpu().numpy())
         np.testing.assert_array_equal(v_na, v_ref.cpu().numpy())
+    assert dcsr.spin_faults() == faults  # no look-back wait gave up
 
 
 def dcsr_max(L):
