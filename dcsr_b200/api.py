@@ -130,6 +130,10 @@ _SIGS = {
     "dcsr_snapshot": (_i32, [_vp, _vp, _i64, _vp]),
     "dcsr_snapshot_header": (_i32, [_vp, _i64, C.POINTER(_i32), C.POINTER(_i32), C.POINTER(_i32), C.POINTER(Opts)]),
     "dcsr_restore": (_i32, [_vp, _vp, _i64, _vp]),
+    "dcsr_hyb_overflow": (_i32, [_vp, _i32, C.POINTER(_i64), _vp]),
+    "dcsr_to_hyb": (_i32, [_vp, _i32, _i64, _vp, _vp, _vp, _vp, _vp, _i64, C.POINTER(_i64), _vp]),
+    "dcsr_hyb_spmv": (_i32, [_i32, _i32, _i32, _i64, _vp, _vp, _i64, _vp, _vp, _vp, _vp, _vp, _dbl, _dbl, _vp]),
+    "dcsr_measure_gather": (_i32, [_vp, _vp, _i64, _vp, _vp, _i32, _vp]),
     "dcsr_cg": (_i32, [_vp, _vp, _vp, _i32, _dbl, _dbl, C.POINTER(_i32), C.POINTER(_dbl), _vp]),
     "dcsr_pool_reserve": (C.c_int, [C.c_int64, C.c_void_p]),
     "dcsr_version": (C.c_char_p, []),
@@ -320,6 +324,24 @@ class DcsrMatrix:
         _check(lib().dcsr_to_csr(self.h, _ptr(rp), _ptr(c), _ptr(v), _stream(stream)), "dcsr_to_csr")
         return rp, c[:nnz], v[:nnz]
 
+    def to_hyb(self, ell_width: int, ell_pitch: int | None = None, stream=None):
+        """DCSR -> HYB: returns (ell_cols [width, pitch], ell_vals, coo_rows, coo_cols, coo_vals)."""
+        pitch = self.n_rows if ell_pitch is None else int(ell_pitch)
+        n = _i64()
+        _check(lib().dcsr_hyb_overflow(self.h, ell_width, C.byref(n), _stream(stream)), "dcsr_hyb_overflow")
+        dev = torch.device("cuda", torch.cuda.current_device())
+        ec = torch.empty((ell_width, pitch), dtype=torch.int32, device=dev)
+        ev = torch.empty((ell_width, pitch), dtype=self.dtype, device=dev)
+        m = max(n.value, 1)
+        cr = torch.empty(m, dtype=torch.int32, device=dev)
+        cc = torch.empty(m, dtype=torch.int32, device=dev)
+        cv = torch.empty(m, dtype=self.dtype, device=dev)
+        got = _i64()
+        _check(lib().dcsr_to_hyb(self.h, ell_width, pitch, _ptr(ec), _ptr(ev), _ptr(cr), _ptr(cc), _ptr(cv), m,
+                                 C.byref(got), _stream(stream)), "dcsr_to_hyb")
+        k = got.value
+        return ec, ev, cr[:k], cc[:k], cv[:k]
+
     def to_coo(self, stream=None):
         nnz = self.nnz(stream)
         dev = torch.device("cuda", torch.cuda.current_device())
@@ -417,6 +439,19 @@ class DcsrMatrix:
         if not t.is_cuda:
             t = t.cuda()
         return t.to(self.dtype).contiguous()
+
+
+def hyb_spmv(ell_cols, ell_vals, coo_rows, coo_cols, coo_vals, x, y=None, alpha=1.0, beta=0.0, stream=None):
+    """y = alpha * A x + beta * y for a HYB matrix (dcsr_hyb_spmv); ell_* are [width, pitch]."""
+    width, pitch = (ell_cols.shape[0], ell_cols.shape[1]) if ell_cols.dim() == 2 else (0, x.numel())
+    n_rows = pitch if y is None else y.numel()
+    if y is None:
+        y = torch.empty(n_rows, dtype=ell_vals.dtype, device=ell_vals.device)
+        beta = 0.0
+    _check(lib().dcsr_hyb_spmv(n_rows, _dtype_code(ell_vals.dtype), width, pitch, _ptr(ell_cols), _ptr(ell_vals),
+                               coo_rows.numel(), _ptr(coo_rows), _ptr(coo_cols), _ptr(coo_vals), _ptr(x), _ptr(y),
+                               alpha, beta, _stream(stream)), "dcsr_hyb_spmv")
+    return y
 
 
 def count_sorted_indices(I: torch.Tensor, X: torch.Tensor, stream=None) -> torch.Tensor:

@@ -11,6 +11,12 @@ namespace dcsr {
 // content copy.  Synchronises once (pool size).
 int load_from_csr64(dcsr_handle h, const long long *rp, const int32_t *cols, const void *vals, cudaStream_t s);
 size_t load_scratch_bytes(dcsr_handle h);
+// Rows staged elsewhere (row r: lens[r] entries at src_off[r]) become the
+// matrix's content with policy capacities, in a pool allocated at cap_bound
+// entries (an upper bound of the pool capacity the rows need); synchronises
+// once at the end (pool top).  Uses the handle's scratch arena.
+int load_from_rows(dcsr_handle h, const long long *src_off, const long long *lens, const int32_t *scols,
+                   const void *svals, int64_t cap_bound, cudaStream_t s);
 
 // Sort + group a COO batch (any order) into CSR form in the arena:
 // MERGE: sorted by (row, col), duplicates summed in input order;

@@ -245,6 +245,81 @@ int load_from_csr64(dcsr_handle h, const long long *rp, const int32_t *cols, con
   return DCSR_OK;
 }
 
+// Rows staged elsewhere (row r: lens[r] entries at src_off[r] in scols /
+// svals, int64 offsets) become the matrix's content with the layout policy's
+// capacities -- the CSR load without its host round trip before the copy:
+// the pool is allocated at cap_bound entries (the caller's upper bound of
+// pool_capacity(top)), the rows are placed, and one synchronisation reads
+// the pool top to set the pool capacity.
+template <typename V>
+__global__ void k_place_rows(int32_t n, const long long *offs, const long long *src_off, const long long *lens,
+                             const int32_t *scols, const V *svals, int32_t *pcols, V *pvals) {
+  const int lane = threadIdx.x & 31;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t r = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < n; r += nw) {
+    const int64_t s0 = src_off[r], L = lens[r], d = offs[r];
+    for (int64_t j = lane; j < L; j += 32) {
+      pcols[d + j] = scols[s0 + j];
+      pvals[d + j] = svals[s0 + j];
+    }
+  }
+}
+__global__ void k_caps_from_lens(const long long *lens, int32_t n, dcsr_opts o, long long *caps) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r <= n; r += stride)
+    caps[r] = r < n ? policy_cap(o, lens[r]) : 0;
+}
+__global__ void k_sizes_from_lens(const long long *lens, int32_t n, int32_t *row_sizes) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += stride) row_sizes[r] = (int32_t)lens[r];
+}
+
+int load_from_rows(dcsr_handle h, const long long *src_off, const long long *lens, const int32_t *scols,
+                   const void *svals, int64_t cap_bound, cudaStream_t s) {
+  const int32_t n = h->n_rows;
+  Arena &ar = h->scratch;
+  ar.status = h->stat + ST_STATUS;
+  DCSR_TRY(ar.reserve(arena_bytes(n + 2, 8) + scan_scratch_bytes(n + 1), s));
+  long long *caps = ar.take<long long>(n + 2);
+  if (ar.overflow) return DCSR_OOM;  // scratch sizing bug: no kernel sees a null pointer
+  if (cap_bound > 0x7fffffffLL) return DCSR_OOM;
+  DCSR_LAUNCH(k_caps_from_lens, grid_for(n + 1, 256), 256, 0, s, lens, n, h->o, caps);
+  DCSR_TRY(scan_i64(caps, caps, n + 1, h->stat + ST_TOTAL, ar, s));
+  int32_t *nc;
+  void *nv;
+  int64_t got;
+  DCSR_TRY(alloc_pool(h, cap_bound, &nc, &nv, &got, s));
+  free_pool(h, s);
+  h->cols = nc;
+  h->vals = nv;
+  h->buf_cap = got;
+  DCSR_LAUNCH(k_layout, grid_for(n + 1, 256), 256, 0, s, h->seg, h->row_sizes, n, h->pitch, h->o.max_segs, caps,
+              (const long long *)nullptr);
+  if (n > 0) DCSR_LAUNCH(k_sizes_from_lens, grid_for(n, 256), 256, 0, s, lens, n, h->row_sizes);
+  if (n > 0) {
+    if (h->dtype == DCSR_F32)
+      DCSR_LAUNCH(k_place_rows<float>, grid_for((int64_t)n * 32, 256), 256, 0, s, n, caps, src_off, lens, scols,
+                  (const float *)svals, h->cols, (float *)h->vals);
+    else
+      DCSR_LAUNCH(k_place_rows<double>, grid_for((int64_t)n * 32, 256), 256, 0, s, n, caps, src_off, lens, scols,
+                  (const double *)svals, h->cols, (double *)h->vals);
+  }
+  long long host[ST_WORDS];
+  DCSR_CUDA(cudaMemcpyAsync(host, h->stat, sizeof(host), cudaMemcpyDeviceToHost, s));
+  DCSR_CUDA(cudaStreamSynchronize(s));
+  h->bins_valid = false;
+  h->scratch.release(s);
+  if (host[ST_STATUS] == DCSR_TIMEOUT) {
+    DCSR_TRY(clear_status(h, s));
+    return DCSR_TIMEOUT;
+  }
+  int64_t cap = pool_capacity(h->o, host[ST_TOTAL]);
+  if (cap > 0x7fffffffLL) cap = 0x7fffffffLL;
+  if (cap > got) return DCSR_OOM;  // the caller's bound was not one (a bug)
+  h->pool_cap = cap;
+  return DCSR_OK;
+}
+
 int reserve(dcsr_handle h, int64_t cap, cudaStream_t s) {
   if (cap <= h->pool_cap && h->vals) return DCSR_OK;
   if (cap > 0x7fffffffLL) return DCSR_OOM;

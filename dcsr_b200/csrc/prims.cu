@@ -765,35 +765,82 @@ __global__ void k_count_sorted(const int32_t *I, int64_t n, int32_t *X) {
   }
 }
 
-// Reduce-by-key: heads flagged, head positions compacted by scan, then each
-// head sums its run left to right (deterministic order).
+// Reduce-by-key: heads flagged, head positions compacted by scan.  A run is
+// summed in pieces of at most RBK_PIECE keys (a piece starts at the run's
+// head or at a multiple of RBK_PIECE inside the run), each piece left to
+// right by one thread; the thread at the head writes its piece's sum and the
+// pieces that continue a run leave theirs in cpart; a second kernel adds a
+// run's continuation pieces to its head piece in order.  The order of the
+// additions is fixed by the input alone, so results are deterministic, and no
+// thread sums more than RBK_PIECE values (a run of 2^20 equal keys is summed
+// by 4096 threads, then 4096 partials by one).
+constexpr int64_t RBK_PIECE = 256;
 __global__ void k_rbk_flags(const int32_t *keys, int64_t n, long long *flag) {
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) flag[i] = (i == 0 || keys[i] != keys[i - 1]) ? 1 : 0;
 }
 template <typename V>
 __global__ void k_rbk_emit(const int32_t *keys, const V *vals, int64_t n, const long long *pos,
-                           int32_t *keys_out, V *vals_out) {
+                           int32_t *keys_out, V *vals_out, V *cpart) {
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  if (i > 0 && keys[i] == keys[i - 1]) return;
+  const bool head = i == 0 || keys[i] != keys[i - 1];
+  if (!head && i % RBK_PIECE != 0) return;
+  const int64_t end = (i / RBK_PIECE + 1) * RBK_PIECE < n ? (i / RBK_PIECE + 1) * RBK_PIECE : n;
   V acc = vals[i];
-  for (int64_t j = i + 1; j < n && keys[j] == keys[i]; j++) acc = acc + vals[j];
-  keys_out[pos[i]] = keys[i];
-  vals_out[pos[i]] = acc;
+  for (int64_t j = i + 1; j < end && keys[j] == keys[i]; j++) acc = acc + vals[j];
+  if (head) {
+    keys_out[pos[i]] = keys[i];
+    vals_out[pos[i]] = acc;
+  } else {
+    cpart[i / RBK_PIECE] = acc;
+  }
+}
+// One thread per piece boundary b = s * RBK_PIECE (s >= 1): the owner of a
+// run that crosses b is the boundary whose previous piece holds the run's
+// head; it adds the run's continuation pieces s, s+1, ... to the head piece.
+template <typename V>
+__global__ void k_rbk_fix(const int32_t *keys, int64_t n, const long long *pos, V *vals_out, const V *cpart) {
+  const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int64_t b = s * RBK_PIECE;
+  if (b >= n || keys[b] != keys[b - 1]) return;       // no run crosses b
+  if (pos[b] == pos[b - RBK_PIECE]) return;  // no head in [b - RBK_PIECE, b): an earlier boundary owns the run
+  const int64_t out = pos[b] - 1;  // the run's output slot (heads before b, minus one)
+  V acc = vals_out[out];
+  const int32_t key = keys[b];
+  for (int64_t t = s; t * RBK_PIECE < n; t++) {
+    if (keys[t * RBK_PIECE] != key) break;  // the run ended before this piece (keys are sorted)
+    acc = acc + cpart[t];
+  }
+  vals_out[out] = acc;
+}
+
+template <typename V>
+static int rbk_launch(const int32_t *keys, const V *vals, int64_t n, long long *pos, long long *n_out, int32_t *keys_out,
+                      V *vals_out, V *cpart, Arena &ar, cudaStream_t s) {
+  const unsigned g = (unsigned)div_up(n, 256);
+  DCSR_LAUNCH(k_rbk_flags, g, 256, 0, s, keys, n, pos);
+  DCSR_TRY(scan_i64(pos, pos, n, n_out, ar, s));
+  DCSR_LAUNCH(k_rbk_emit<V>, g, 256, 0, s, keys, vals, n, pos, keys_out, vals_out, cpart);
+  const int64_t nb = (n - 1) / RBK_PIECE;  // piece boundaries inside [1, n)
+  if (nb > 0) DCSR_LAUNCH(k_rbk_fix<V>, (unsigned)div_up(nb, 256), 256, 0, s, keys, n, pos, vals_out, cpart);
+  return DCSR_OK;
 }
 
 // ------------------------------------------- allocation-free reduce-by-key
 //
-// Scratch for dcsr_reduce_by_key_noalloc: head positions (one int64 per key)
-// and the scan's look-back area, in one static device array (zero at module
+// Scratch for dcsr_reduce_by_key_noalloc: head positions (one int64 per key),
+// the continuation-piece partials and the scan's look-back area, in one
+// static device array (zero at module
 // load, as the look-back protocol needs).  Every GPU that loads the library
 // holds it until exit.  Host code must not pass the symbol itself to a
 // kernel (in host code it names a host-side stand-in); the device address is
 // looked up once per device.
 constexpr size_t NOALLOC_POS_BYTES = (size_t)DCSR_NOALLOC_MAX_KEYS * sizeof(long long);
+constexpr size_t NOALLOC_PART_BYTES = (size_t)(DCSR_NOALLOC_MAX_KEYS / RBK_PIECE + 1) * sizeof(double);
 constexpr size_t NOALLOC_LB_SLOTS = 4 * ((DCSR_NOALLOC_MAX_KEYS + SCAN_TILE - 1) / SCAN_TILE) + 4;
-constexpr size_t NOALLOC_BYTES = NOALLOC_POS_BYTES + 256 + LB_HEADER + 8 * NOALLOC_LB_SLOTS;
+constexpr size_t NOALLOC_ARENA_BYTES = NOALLOC_POS_BYTES + 256 + NOALLOC_PART_BYTES + 256;
+constexpr size_t NOALLOC_BYTES = NOALLOC_ARENA_BYTES + LB_HEADER + 8 * NOALLOC_LB_SLOTS;
 static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_BYTES];
 
 static int noalloc_scratch(void **out) {
@@ -830,21 +877,20 @@ extern "C" int dcsr_reduce_by_key_noalloc(const int32_t *keys, const void *vals,
   DCSR_TRY(noalloc_scratch(&base));
   Arena ar;  // a view over the static array: take() and lookback() only, never reserve()/release()
   ar.base = (char *)base;
-  ar.cap = NOALLOC_POS_BYTES + 256;
+  ar.cap = NOALLOC_ARENA_BYTES;
   ar.used = 0;
-  ar.lb = (unsigned char *)base + NOALLOC_POS_BYTES + 256;
+  ar.lb = (unsigned char *)base + NOALLOC_ARENA_BYTES;
   ar.lb_slots = NOALLOC_LB_SLOTS;
-  long long *pos = ar.take<long long>(n);  // fully rewritten below before any read
+  // every word below is written before it is read in each call: positions
+  // by the flag kernel, a partial by the piece that owns it
+  long long *pos = ar.take<long long>(n);
+  double *cpart = ar.take<double>(n / RBK_PIECE + 1);
   if (ar.overflow) return DCSR_OOM;  // scratch sizing bug: no kernel sees a null pointer
-  const unsigned g = (unsigned)div_up(n, 256);
-  DCSR_LAUNCH(k_rbk_flags, g, 256, 0, s, keys, n, pos);
-  DCSR_TRY(scan_i64(pos, pos, n, (long long *)n_out, ar, s));
   if (dtype == DCSR_F32)
-    DCSR_LAUNCH(k_rbk_emit<float>, g, 256, 0, s, keys, (const float *)vals, n, pos, keys_out, (float *)vals_out);
-  else
-    DCSR_LAUNCH(k_rbk_emit<double>, g, 256, 0, s, keys, (const double *)vals, n, pos, keys_out,
-                (double *)vals_out);
-  return DCSR_OK;
+    return rbk_launch<float>(keys, (const float *)vals, n, pos, (long long *)n_out, keys_out, (float *)vals_out,
+                             (float *)cpart, ar, s);
+  return rbk_launch<double>(keys, (const double *)vals, n, pos, (long long *)n_out, keys_out, (double *)vals_out,
+                            cpart, ar, s);
 }
 
 extern "C" int dcsr_count_sorted_indices(const int32_t *I, int64_t n, int32_t *X, void *stream) {
@@ -865,17 +911,14 @@ extern "C" int dcsr_reduce_by_key(const int32_t *keys, const void *vals, int64_t
     return DCSR_OK;
   }
   Arena ar;
-  DCSR_TRY(ar.reserve(arena_bytes(n, 8) + scan_scratch_bytes(n), s));
+  DCSR_TRY(ar.reserve(arena_bytes(n, 8) + arena_bytes(n / RBK_PIECE + 1, 8) + scan_scratch_bytes(n), s));
   long long *pos = ar.take<long long>(n);
+  double *cpart = ar.take<double>(n / RBK_PIECE + 1);
   if (ar.overflow) return DCSR_OOM;  // scratch sizing bug: no kernel sees a null pointer
-  unsigned g = (unsigned)div_up(n, 256);
-  DCSR_LAUNCH(k_rbk_flags, g, 256, 0, s, keys, n, pos);
-  DCSR_TRY(scan_i64(pos, pos, n, (long long *)n_out, ar, s));
-  if (dtype == DCSR_F32)
-    DCSR_LAUNCH(k_rbk_emit<float>, g, 256, 0, s, keys, (const float *)vals, n, pos, keys_out, (float *)vals_out);
-  else
-    DCSR_LAUNCH(k_rbk_emit<double>, g, 256, 0, s, keys, (const double *)vals, n, pos, keys_out,
-                (double *)vals_out);
+  const int rc = dtype == DCSR_F32 ? rbk_launch<float>(keys, (const float *)vals, n, pos, (long long *)n_out, keys_out,
+                                                       (float *)vals_out, (float *)cpart, ar, s)
+                                   : rbk_launch<double>(keys, (const double *)vals, n, pos, (long long *)n_out,
+                                                        keys_out, (double *)vals_out, cpart, ar, s);
   ar.release(s);
-  return DCSR_OK;
+  return rc;
 }

@@ -12,7 +12,11 @@
 //                           of (row, column) keys (no row is skipped; the
 //                           reference left rows > 2048 products uncomputed,
 //                           include/spmm.h:368-389)
-// 4. layout  C's rows with its own slack policy (CSR load path).
+// 4. layout  C's rows placed straight from the staging area into C's pool
+//            with C's slack policy; the pool is allocated at an upper bound
+//            (the policy capacity of P_i per row) so nothing waits for the
+//            unique counts.  Two synchronisations: the product counts (to size
+//            the staging area) and C's pool top.
 // Sorting by (column, p) makes every sum run in product order, so values are
 // reproducible and match the CPU oracle bit for bit; explicit zeros are kept
 // (reference include/spmm.inl:215-218).
@@ -27,8 +31,13 @@ constexpr int SG_WARP_MAX = 256;   // products per warp-row
 constexpr int SG_CTA_MAX = 4096;   // products per CTA-row
 enum { SG_EMPTY = 0, SG_WARP = 1, SG_CTA = 2, SG_GLOBAL = 3 };
 
+// Per row: its product count P_i, its size class, and the capacity C's
+// layout policy gives a row of P_i entries (an upper bound of the row's
+// capacity, whatever its unique columns); the products of the rows of the
+// global class are added up in *gtotal.
 template <typename V>
-__global__ void k_sg_count(Mat<V> A, Mat<V> B, long long *cnt, unsigned long long *cls, unsigned *rows) {
+__global__ void k_sg_count(Mat<V> A, Mat<V> B, dcsr_opts co, long long *cnt, long long *capub,
+                           unsigned long long *cls, unsigned *rows, unsigned long long *gtotal) {
   const int lane = threadIdx.x & 31;
   const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
   for (int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < A.n_rows; i += nw) {
@@ -39,11 +48,17 @@ __global__ void k_sg_count(Mat<V> A, Mat<V> B, long long *cnt, unsigned long lon
     s = warp_sum(s);
     if (lane == 0) {
       cnt[i] = s;
-      cls[i] = s == 0 ? SG_EMPTY : s <= SG_WARP_MAX ? SG_WARP : s <= SG_CTA_MAX ? SG_CTA : SG_GLOBAL;
+      capub[i] = policy_cap(co, s);
+      const int c = s == 0 ? SG_EMPTY : s <= SG_WARP_MAX ? SG_WARP : s <= SG_CTA_MAX ? SG_CTA : SG_GLOBAL;
+      cls[i] = c;
       rows[i] = (unsigned)i;
+      if (c == SG_GLOBAL) atomicAdd(gtotal, (unsigned long long)s);
     }
   }
-  if (blockIdx.x == 0 && threadIdx.x == 0) cnt[A.n_rows] = 0;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    cnt[A.n_rows] = 0;
+    capub[A.n_rows] = 0;
+  }
 }
 
 // class starts [0..4] from the sorted class keys
@@ -267,20 +282,6 @@ __global__ void k_sg_global_emit(const unsigned long long *gkey, const unsigned 
   }
 }
 
-template <typename V>
-__global__ void k_sg_compact(int32_t n, const long long *ub, const long long *rp, const int32_t *tcol, const V *tval,
-                             int32_t *ccol, V *cval) {
-  const int lane = threadIdx.x & 31;
-  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  for (int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += nw) {
-    const int64_t s = ub[i], d = rp[i], L = rp[i + 1] - rp[i];
-    for (int64_t j = lane; j < L; j += 32) {
-      ccol[d + j] = tcol[s + j];
-      cval[d + j] = tval[s + j];
-    }
-  }
-}
-
 // slot products for the global class: goff[slot] = ub-like offsets of the
 // large rows in a dense staging array
 __global__ void k_sg_global_sizes(const unsigned *rows, const long long *starts, const long long *ub,
@@ -303,27 +304,39 @@ static int spgemm_impl(dcsr_handle hA, dcsr_handle hB, dcsr_handle hC, cudaStrea
   Mat<V> A = hA->view<V>(), B = hB->view<V>();
   Arena ar;
   ar.status = hC->stat + ST_STATUS;  // look-back timeouts reach C's status
-  DCSR_TRY(ar.reserve(arena_bytes(n + 2, 8) * 3 + arena_bytes(n + 2, 4) * 2 + arena_bytes(8, 8) +
+  DCSR_TRY(ar.reserve(arena_bytes(n + 2, 8) * 4 + arena_bytes(n + 2, 4) * 2 + arena_bytes(8, 8) +
                           radix_scratch_bytes(n) + scan_scratch_bytes(n + 2), s));
-  long long *cnt = ar.take<long long>(n + 2);
+  long long *cnt = ar.take<long long>(n + 2), *capub = ar.take<long long>(n + 2);
   unsigned long long *k0 = ar.take<unsigned long long>(n + 2), *k1 = ar.take<unsigned long long>(n + 2);
   unsigned *r0 = ar.take<unsigned>(n + 2), *r1 = ar.take<unsigned>(n + 2);
-  long long *starts = ar.take<long long>(8);
+  long long *starts = ar.take<long long>(8);  // [0..4] class starts, [5] products of the global class
   if (ar.overflow) return DCSR_OOM;  // scratch sizing bug: no kernel sees a null pointer
   long long *ub = cnt;  // scanned in place
+  DCSR_CUDA(cudaMemsetAsync(starts, 0, sizeof(long long) * 8, s));
   if (n > 0) {
-    DCSR_LAUNCH(k_sg_count<V>, grid_for((int64_t)n * 32, SG_THREADS), SG_THREADS, 0, s, A, B, cnt, k0, r0);
+    DCSR_LAUNCH(k_sg_count<V>, grid_for((int64_t)n * 32, SG_THREADS), SG_THREADS, 0, s, A, B, hC->o, cnt, capub, k0,
+                r0, (unsigned long long *)(starts + 5));
     if (n > 1) DCSR_TRY(radix_sort_pairs(&k0, &r0, &k1, &r1, n, 2, ar, s));
   }
   DCSR_LAUNCH(k_sg_classes, 1, 32, 0, s, k0, n, starts);
-  DCSR_TRY(scan_i64(cnt, ub, n + 1, hC->stat + ST_TOTAL, ar, s));
-  long long host[6];
-  DCSR_CUDA(cudaMemcpyAsync(host, starts, sizeof(long long) * 5, cudaMemcpyDeviceToHost, s));
-  DCSR_CUDA(cudaMemcpyAsync(host + 5, hC->stat + ST_TOTAL, sizeof(long long), cudaMemcpyDeviceToHost, s));
+  DCSR_TRY(scan2_i64(cnt, ub, hC->stat + ST_TOTAL, capub, capub, hC->stat + ST_AUX + 1, n + 1, ar, s));
+  // the one read before the numeric pass: staging and C's pool are sized here
+  long long host[8];
+  DCSR_CUDA(cudaMemcpyAsync(host, starts, sizeof(long long) * 6, cudaMemcpyDeviceToHost, s));
+  DCSR_CUDA(cudaMemcpyAsync(host + 6, hC->stat + ST_TOTAL, sizeof(long long), cudaMemcpyDeviceToHost, s));
+  DCSR_CUDA(cudaMemcpyAsync(host + 7, hC->stat + ST_AUX + 1, sizeof(long long), cudaMemcpyDeviceToHost, s));
+  long long st_word = 0;
+  DCSR_CUDA(cudaMemcpyAsync(&st_word, hC->stat + ST_STATUS, sizeof(long long), cudaMemcpyDeviceToHost, s));
   DCSR_CUDA(cudaStreamSynchronize(s));
-  const int64_t P = host[5];
+  if (st_word == DCSR_TIMEOUT) {
+    DCSR_CUDA(cudaMemsetAsync(hC->stat + ST_STATUS, 0, sizeof(long long), s));
+    ar.release(s);
+    return DCSR_TIMEOUT;
+  }
+  const int64_t Pg = host[5], P = host[6], cap_bound = pool_capacity(hC->o, host[7]);
   const int64_t n_global = host[SG_GLOBAL + 1] - host[SG_GLOBAL];
-  // staging: unique columns per row at ub[i]
+  if (Pg > 0xffffffffLL) return DCSR_NOT_SUPPORTED;
+  // staging: row i's unique columns at ub[i]
   int32_t *tcol = nullptr;
   V *tval = nullptr;
   long long *ucnt = nullptr;
@@ -345,29 +358,22 @@ static int spgemm_impl(dcsr_handle hA, dcsr_handle hB, dcsr_handle hC, cudaStrea
     DCSR_LAUNCH(k_sg_warp<V>, g_warp, SG_THREADS, 0, s, A, B, r0, starts, ub, tcol, tval, ucnt);
   if (host[SG_CTA + 1] > host[SG_CTA])
     DCSR_LAUNCH(k_sg_cta<V>, g_cta, SG_THREADS, cta_smem, s, A, B, r0, starts, ub, tcol, tval, ucnt);
+  Arena gg;
   if (n_global > 0) {
     // products of all large rows, laid out densely by slot, then one stable
     // radix sort by (slot, column) keeps every column's products in p order
-    Arena g;
-    g.status = hC->stat + ST_STATUS;  // look-back timeouts reach C's status
-    DCSR_TRY(g.reserve(arena_bytes(n_global + 2, 8) + scan_scratch_bytes(n_global + 2), s));
-    long long *goff = g.take<long long>(n_global + 2);
-    if (g.overflow) return DCSR_OOM;  // scratch sizing bug: no kernel sees a null pointer
-    DCSR_LAUNCH(k_sg_global_sizes, grid_for(n_global + 1, 256), 256, 0, s, r0, starts, ub, goff);
-    DCSR_TRY(scan_i64(goff, goff, n_global + 1, hC->stat + ST_AUX + 1, g, s));
-    long long Pg = 0;
-    DCSR_CUDA(cudaMemcpyAsync(&Pg, hC->stat + ST_AUX + 1, sizeof(Pg), cudaMemcpyDeviceToHost, s));
-    DCSR_CUDA(cudaStreamSynchronize(s));
-    if (Pg > 0xffffffffLL) return DCSR_NOT_SUPPORTED;
-    Arena gg;
     gg.status = hC->stat + ST_STATUS;  // look-back timeouts reach C's status
-    DCSR_TRY(gg.reserve(2 * arena_bytes(Pg, 8) + 2 * arena_bytes(Pg, 4) + arena_bytes(Pg, sizeof(V)) +
-                            arena_bytes(Pg + 1, 8) + radix_scratch_bytes(Pg) + scan_scratch_bytes(Pg + 1), s));
+    DCSR_TRY(gg.reserve(arena_bytes(n_global + 2, 8) + 2 * arena_bytes(Pg, 8) + 2 * arena_bytes(Pg, 4) +
+                            arena_bytes(Pg, sizeof(V)) + arena_bytes(Pg + 1, 8) + radix_scratch_bytes(Pg) +
+                            scan_scratch_bytes(Pg + 1) + scan_scratch_bytes(n_global + 2), s));
+    long long *goff = gg.take<long long>(n_global + 2);
     unsigned long long *gk0 = gg.take<unsigned long long>(Pg), *gk1 = gg.take<unsigned long long>(Pg);
     unsigned *gi0 = gg.take<unsigned>(Pg), *gi1 = gg.take<unsigned>(Pg);
     V *gprod = (V *)gg.take<double>(Pg);
     long long *hpos = gg.take<long long>(Pg + 1);
     if (gg.overflow) return DCSR_OOM;  // scratch sizing bug: no kernel sees a null pointer
+    DCSR_LAUNCH(k_sg_global_sizes, grid_for(n_global + 1, 256), 256, 0, s, r0, starts, ub, goff);
+    DCSR_TRY(scan_i64(goff, goff, n_global + 1, nullptr, gg, s));
     const int cb = bits_for(hB->n_cols);
     DCSR_LAUNCH(k_sg_global_expand<V>, grid_for(n_global * 32, 256), 256, 0, s, A, B, r0, starts, goff, cb, gk0, gi0,
                 gprod);
@@ -376,35 +382,15 @@ static int spgemm_impl(dcsr_handle hA, dcsr_handle hB, dcsr_handle hC, cudaStrea
     DCSR_TRY(scan_i64(hpos, hpos, Pg, nullptr, gg, s));
     DCSR_LAUNCH(k_sg_global_emit<V>, grid_for(Pg, 256), 256, 0, s, gk0, gi0, gprod, Pg, hpos, r0, starts, goff, ub,
                 cb, tcol, tval, ucnt);
-    gg.release(s);
-    g.release(s);
   }
-  // compact staging -> CSR, then lay out C with its policy
-  long long *rp = nullptr;
-  int32_t *ccol = nullptr;
-  V *cval = nullptr;
-  Arena c;
-  c.status = hC->stat + ST_STATUS;  // look-back timeouts reach C's status
-  DCSR_TRY(c.reserve(arena_bytes(n + 2, 8) + scan_scratch_bytes(n + 2), s));
-  rp = c.take<long long>(n + 2);
-  if (c.overflow) return DCSR_OOM;  // scratch sizing bug: no kernel sees a null pointer
-  DCSR_TRY(scan_i64(ucnt, rp, n + 1, hC->stat + ST_TOTAL, c, s));
-  long long nnzc = 0;
-  DCSR_CUDA(cudaMemcpyAsync(&nnzc, hC->stat + ST_TOTAL, sizeof(nnzc), cudaMemcpyDeviceToHost, s));
-  DCSR_CUDA(cudaStreamSynchronize(s));
-  DCSR_CUDA(cudaMallocAsync((void **)&ccol, sizeof(int32_t) * (nnzc + 1), s));
-  DCSR_CUDA(cudaMallocAsync((void **)&cval, sizeof(V) * (nnzc + 1), s));
-  if (n > 0)
-    DCSR_LAUNCH(k_sg_compact<V>, grid_for((int64_t)n * 32, 256), 256, 0, s, n, ub, rp, tcol, tval, ccol, cval);
-  DCSR_TRY(hC->scratch.reserve(load_scratch_bytes(hC), s));
-  int st = load_from_csr64(hC, rp, ccol, cval, s);
-  c.release(s);
+  // C's rows go straight from the staging area into C's pool (policy
+  // capacities); the second and last synchronisation reads C's pool top
+  const int st = load_from_rows(hC, ub, ucnt, tcol, tval, cap_bound, s);
+  gg.release(s);
   ar.release(s);
   cudaFreeAsync(tcol, s);
   cudaFreeAsync(tval, s);
   cudaFreeAsync(ucnt, s);
-  cudaFreeAsync(ccol, s);
-  cudaFreeAsync(cval, s);
   return st;
 }
 

@@ -76,5 +76,5 @@ def write_matrix_market(path: str, n_rows: int, n_cols: int, rows, cols, vals):
     with open(path, "w") as f:
         f.write("%%MatrixMarket matrix coordinate real general\n")
         f.write(f"{n_rows} {n_cols} {rows.size}\n")
-        for r, c, v in zip(rows, cols, vals):
-            f.write(f"{r + 1} {c + 1} {v!r}\n")
+        for r, c, v in zip(rows.tolist(), cols.tolist(), vals.tolist()):
+            f.write(f"{r + 1} {c + 1} {v!r}\n")  # shortest repr that reads back exactly

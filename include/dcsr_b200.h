@@ -116,6 +116,25 @@ int dcsr_from_hyb(dcsr_handle h, const int32_t *ell_cols, const void *ell_vals, 
                   int64_t ell_pitch, const int32_t *coo_rows, const int32_t *coo_cols, const void *coo_vals,
                   int64_t coo_nnz, void *stream);
 
+/* DCSR -> HYB (ELL + COO overflow, the reference's hyb_matrix and its
+ * LoadMatrix(hyb, csr), include/dcsr_matrix.h:149-172, include/load.h:174-205).
+ * Each row's first ell_width entries (in DCSR order) go to the ELL part,
+ * column-major: slot k of row r at ell_cols[k*ell_pitch + r] (ell_pitch >=
+ * n_rows); unused slots get column -1 and value 0.  The remaining entries go
+ * to the COO part in row order; *coo_nnz (host) receives their count, and the
+ * call returns DCSR_BAD_ARG without writing anything when it exceeds coo_cap
+ * (dcsr_hyb_overflow gives the count first).  Synchronises once. */
+int dcsr_hyb_overflow(dcsr_handle h, int32_t ell_width, int64_t *coo_nnz, void *stream);
+int dcsr_to_hyb(dcsr_handle h, int32_t ell_width, int64_t ell_pitch, int32_t *ell_cols, void *ell_vals,
+                int32_t *coo_rows, int32_t *coo_cols, void *coo_vals, int64_t coo_cap, int64_t *coo_nnz, void *stream);
+/* y = alpha*A*x + beta*y for a HYB matrix in that layout (COO part sorted by
+ * row; beta == 0 does not read y).  A row's ELL products are summed in slot
+ * order, then its COO products in order.  Replaces device::spmv(hyb, x, y)
+ * (include/spmv.h:36-94, spmv_hyb include/spmv.inl:105-156). */
+int dcsr_hyb_spmv(int32_t n_rows, int32_t dtype, int32_t ell_width, int64_t ell_pitch, const int32_t *ell_cols,
+                  const void *ell_vals, int64_t coo_nnz, const int32_t *coo_rows, const int32_t *coo_cols,
+                  const void *coo_vals, const void *x, void *y, double alpha, double beta, void *stream);
+
 /* Number of stored entries (synchronises).  Use before dcsr_to_csr. */
 int dcsr_nnz(dcsr_handle h, int64_t *nnz, void *stream);
 /* DCSR -> CSR in row order, any state (chains followed).  Replaces
@@ -194,7 +213,9 @@ int dcsr_row_reduce(dcsr_handle h, int32_t op, void *y, void *stream);
 /* C = A*B.  C must be a handle created with n_rows = A.n_rows, n_cols =
  * B.n_cols and A's dtype; its content is replaced.  Rows sorted, explicit
  * zeros kept, all rows computed.  Replaces device::spmm (include/spmm.h:30-391).
- * Synchronises once (output size). */
+ * Synchronises twice: after counting products (to size the staging area and
+ * an upper bound of C's pool) and at the end (C's pool top); C's rows are
+ * written straight into C's pool. */
 int dcsr_spgemm(dcsr_handle A, dcsr_handle B, dcsr_handle C, void *stream);
 
 /* Conjugate gradient on a symmetric positive definite matrix (square),
@@ -214,8 +235,11 @@ int dcsr_cg(dcsr_handle A, const void *b, void *x, int32_t max_iter, double rel_
 /* X[I[n]] += 1 for a sorted index array I.  Replaces
  * device::count_sorted_indices (include/primitives.h:417-464). */
 int dcsr_count_sorted_indices(const int32_t *I, int64_t n, int32_t *X, void *stream);
-/* Reduce-by-key over sorted int32 keys with left-to-right sums; writes the
- * unique count to *n_out (device pointer).  Replaces the CTA/global
+/* Reduce-by-key over sorted int32 keys; writes the unique count to *n_out
+ * (device pointer).  Each run is summed in a fixed order: left to right
+ * within pieces of at most 256 keys (a piece starts at the run's head or at
+ * a multiple of 256), then the piece sums left to right -- deterministic,
+ * and a long run is summed by many threads.  Replaces the CTA/global
  * reduce-by-key of include/reduce.inl:139-308, include/reduce_global.inl. */
 int dcsr_reduce_by_key(const int32_t *keys, const void *vals, int64_t n, int32_t dtype, int32_t *keys_out,
                        void *vals_out, int64_t *n_out, void *stream);
@@ -362,9 +386,11 @@ int dcsr_server_replay(dcsr_server s, const dcsr_request *requests, const double
  * n is limited to DCSR_NOALLOC_MAX_KEYS (larger n returns DCSR_BAD_ARG
  * without touching the GPU).  The first call on a device looks up the
  * array's device address (cudaGetSymbolAddress) with that device current;
- * make that first call before any stream capture.  All calls share the one
- * array: calls that overlap on the GPU (different streams, or threads
- * without ordering) race and must be serialised by the caller. */
+ * make that first call before any stream capture.  The address is kept for
+ * the life of the process: do not use this entry point on a device after
+ * cudaDeviceReset there.  All calls share the one array: calls that overlap
+ * on the GPU (different streams, or threads without ordering) race and must
+ * be serialised by the caller. */
 #define DCSR_NOALLOC_MAX_KEYS (1 << 20)
 int dcsr_reduce_by_key_noalloc(const int32_t *keys, const void *vals, int64_t n, int32_t dtype, int32_t *keys_out,
                                void *vals_out, int64_t *n_out, void *stream);
@@ -401,6 +427,15 @@ int dcsr_debug_lookback(int32_t spin_limit, int32_t stall_first_tile);
  * cost 2 to several hundred milliseconds per allocation on some machines.
  * Synchronises the stream.  No counterpart in the reference (host memory). */
 int dcsr_pool_reserve(int64_t bytes, void *stream);
+/* Measurement aid for the SpMV roofline (no counterpart in the reference):
+ * reads n (column, value) entries -- e.g. a matrix's CSR export, FP32 --
+ * coalesced and gathers x at every column, summing the products per block
+ * into out[0 .. min(out_len, 8 * SMs)).  The memory traffic of a k = 1 SpMV
+ * of those entries without its row bookkeeping: the time it takes is a floor
+ * for that SpMV on this GPU (the random 4-byte reads of x are the part HBM
+ * bandwidth does not cover).  Asynchronous. */
+int dcsr_measure_gather(const int32_t *cols, const float *vals, int64_t n, const float *x, float *out,
+                        int32_t out_len, void *stream);
 /* Library version string. */
 const char *dcsr_version(void);
 

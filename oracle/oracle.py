@@ -255,6 +255,44 @@ def reduce_by_key(keys, vals, dtype=F64):
 
 # ------------------------------------------------------------ cusp harness
 
+def hyb_from_csr(rp, cols, vals, width, pitch):
+    """The HYB layout restated: each row's first `width` entries in the ELL
+    part (column-major, slot k of row r at [k, r]; unused slots column -1,
+    value 0), the rest in the COO part in row order (the reference's
+    hyb_matrix, include/dcsr_matrix.h:149-172, filled as LoadMatrix(hyb, csr)
+    does, include/load.h:174-205, with a row-ordered COO part)."""
+    rp = np.asarray(rp, np.int64)
+    n = len(rp) - 1
+    ec = np.full((width, pitch), -1, np.int32)
+    ev = np.zeros((width, pitch), np.float64)
+    cr, cc, cv = [], [], []
+    for r in range(n):
+        a, b = rp[r], rp[r + 1]
+        k = min(width, b - a)
+        ec[:k, r] = cols[a:a + k]
+        ev[:k, r] = vals[a:a + k]
+        if b - a > width:
+            cr.append(np.full(b - a - width, r, np.int32))
+            cc.append(np.asarray(cols[a + width:b], np.int32))
+            cv.append(np.asarray(vals[a + width:b], np.float64))
+    cat = lambda xs, dt: np.concatenate(xs).astype(dt) if xs else np.zeros(0, dt)  # noqa: E731
+    return ec, ev, cat(cr, np.int32), cat(cc, np.int32), cat(cv, np.float64)
+
+
+def hyb_spmv(ec, ev, cr, cc, cv, x, n_rows):
+    """FP64 y = A x over a HYB layout: a row's ELL slots in order, then its
+    COO entries in order (reference spmv_hyb, include/spmv.inl:105-156)."""
+    x = np.asarray(x, np.float64)
+    width = ec.shape[0]
+    y = np.zeros(n_rows)
+    for k in range(width):
+        c = ec[k, :n_rows]
+        live = c >= 0
+        y[live] += ev[k, :n_rows][live] * x[c[live]]
+    np.add.at(y, cr, cv * x[cc])
+    return y
+
+
 def ref_read_mtx(path: str, cap: int = 1 << 22):
     """The reference's own ReadMatrixFile<int, double> (oracle/_ref/libref_mtx.so):
     (n_rows, n_cols, rows, cols, vals) with 0-based indices, file order."""

@@ -74,3 +74,23 @@ def test_reduce_by_key_sizes(dcsr, n):
     uk, start = np.unique(keys, return_index=True)
     np.testing.assert_array_equal(ko.cpu().numpy(), uk)
     np.testing.assert_array_equal(vo.cpu().numpy(), np.add.reduceat(vals, start))
+
+
+@pytest.mark.parametrize("runs", ["one_key", "long_runs", "ragged"])
+def test_reduce_by_key_long_runs(dcsr, runs):
+    """Runs longer than a summation piece (256 keys), up to one run of 2^20
+    keys: pieces are summed in parallel and combined in order."""
+    rng = np.random.default_rng(11)
+    if runs == "one_key":
+        keys = np.full(1 << 20, 7, np.int32)
+    elif runs == "long_runs":
+        keys = np.repeat(np.arange(40, dtype=np.int32), rng.integers(200, 60_000, 40))
+    else:
+        keys = np.sort(np.concatenate([rng.integers(0, 50, 300_000), rng.integers(0, 200_000, 5_000)])).astype(np.int32)
+    n = keys.size
+    for dt in (torch.float32, torch.float64):
+        vals = rng.integers(-100, 100, n).astype(np.float64)  # integer-valued: every order of summation is exact
+        ko, vo = dcsr.reduce_by_key(torch.tensor(keys, device="cuda"), torch.tensor(vals, dtype=dt, device="cuda"))
+        uk, start = np.unique(keys, return_index=True)
+        np.testing.assert_array_equal(ko.cpu().numpy(), uk)
+        np.testing.assert_array_equal(vo.cpu().double().numpy(), np.add.reduceat(vals, start))

@@ -71,3 +71,19 @@ def test_reference_fixture_files_live(name):
     # file mode keeps the stored values (tols90 has non-unit values)
     if name == "tols90.mtx":
         assert np.any(mmio.read_matrix_market(path, values="file")[4] != 1.0)
+
+
+def test_writer_round_trip(tmp_path):
+    rng = np.random.default_rng(5)
+    r = rng.integers(0, 50, 200).astype(np.int32)
+    c = rng.integers(0, 60, 200).astype(np.int32)
+    v = rng.standard_normal(200)
+    path = str(tmp_path / "w.mtx")
+    mmio.write_matrix_market(path, 50, 60, r, c, v)
+    nr, nc, r2, c2, v2 = mmio.read_matrix_market(path, values="file")
+    assert (nr, nc) == (50, 60)
+    np.testing.assert_array_equal(r2, r)
+    np.testing.assert_array_equal(c2, c)
+    np.testing.assert_array_equal(v2, np.where(v == 0, 1.0, v))
+    # the reference reader's rule turns every value that ends its line into 1
+    assert np.all(mmio.read_matrix_market(path)[4] == 1.0)
