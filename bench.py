@@ -69,22 +69,12 @@ def peaks():
         return 6650.0, "fallback"
 
 
-def profiled_traffic(name, algorithmic_bytes):
-    """DRAM bytes of one SpMV call on this workload, from the ncu summary
-    under profiles/: its measured traffic / algorithmic-bytes ratio applied to
-    this run's algorithmic bytes (the profiled matrix is smaller), else None."""
-    vals = {}
-    try:
-        with open(os.path.join(ROOT, "profiles", name)) as f:
-            for line in f:
-                for key in ("traffic_bytes_per_launch:", "algorithmic_bytes_per_launch:"):
-                    if line.strip().startswith(key):
-                        vals[key] = float(line.split(":", 1)[1])
-    except OSError:
-        return None
-    if len(vals) != 2:
-        return None
-    return int(algorithmic_bytes * vals["traffic_bytes_per_launch:"] / vals["algorithmic_bytes_per_launch:"])
+# DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) of one k = 1
+# SpMV launch on the update-stream matrix, from one ncu capture of the same
+# seeded workload in the same state (profiles/spmv_rmat_k1_f32.md gives the
+# command): keyed by the matrix's stored-entry count, so a run on another
+# state reports no traffic rather than a scaled one.
+SPMV_TRAFFIC = {}
 
 
 class ClockSampler:
@@ -221,26 +211,80 @@ def stream_part(args, dev, world):
     sb = spmv_bytes(nnz, n, n, segs)
     achieved = sb / (spmv_ms / 1e3) / 1e9
 
-    # gather ceiling: one 4-byte read of x per stored entry at the matrix's
-    # own columns in row order (its CSR export; torch.index_select, x warm in
-    # L2 as in the SpMV) -- the sector traffic the SpMV's x reads cost,
-    # whatever its kernel
+    def timed(fn, reps):
+        """Mean device time (ms) of fn over reps launches, L2 flushed before each."""
+        ts = []
+        for rep in range(reps + 3):
+            flush.fill_(float(rep))
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            if rep >= 3:
+                ts.append(e0.elapsed_time(e1))
+        return statistics.mean(ts)
+
+    hbm, _ = peaks()
+    frac = lambda b, ms: round(b / (ms / 1e3) / 1e9 / hbm, 4)  # noqa: E731
+    # gather floor: the same entries (this matrix's CSR export) read coalesced
+    # with x gathered at every column, no row bookkeeping (dcsr_measure_gather)
     assert L.dcsr_to_csr(h, P(out_rp), P(out_c), P(out_v), sp) == 0
-    gidx = out_c[:nnz].to(torch.int64)
-    gout = torch.empty(nnz, dtype=torch.float32, device=dev)
-    gt = []
-    for rep in range(args.spmv_reps + 3):
-        flush.fill_(float(rep))
-        x.add_(0.0)  # x back in L2 (the SpMV reads it many times, so it is warm there)
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        torch.index_select(x, 0, gidx, out=gout)
-        e1.record(stream)
-        torch.cuda.synchronize()
-        if rep >= 3:
-            gt.append(e0.elapsed_time(e1))
-    gather_ms = statistics.mean(gt)
-    del gidx, gout
+    gsum = torch.empty(148 * 8, dtype=torch.float32, device=dev)
+    gather_ms = timed(lambda: L.dcsr_measure_gather(P(out_c), P(out_v), nnz, P(x), P(gsum), gsum.numel(), sp), 10)
+    gather_bytes = nnz * 8 + 4 * n  # entries + x
+    ops = {}
+    # row sums alone (no gathers): nnz*sV + 4n + 8*segs + n*sV
+    rs_ms = timed(lambda: L.dcsr_row_reduce(h, 0, P(rs), sp), 10)
+    b = nnz * 4 + 4 * n + 8 * segs + 4 * n
+    ops["row_sum"] = {"ms": round(rs_ms, 4), "bytes": b, "hbm_frac": frac(b, rs_ms)}
+    # DCSR -> CSR export alone: 2*nnz*(4+sV) + 4(n+1) (+ the row lengths and segment table read)
+    ex_ms = timed(lambda: L.dcsr_to_csr(h, P(out_rp), P(out_c), P(out_v), sp), 5)
+    b = 2 * nnz * 8 + 4 * (n + 1)
+    ops["export_csr"] = {"ms": round(ex_ms, 4), "bytes": b, "hbm_frac": frac(b, ex_ms)}
+    # one update alone (1M skewed triples): T(8+sV) read + T_new(4+sV) written + 4*sum of touched rows' lengths
+    br, bc, bv = dbatch[(args.warmup + args.steps) % len(dbatch)]
+    touched = np.unique(br.cpu().numpy())
+    nnz_before = nnz
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    flush.fill_(0.5)
+    e0.record(stream)
+    st = L.dcsr_update_sync(h, P(br), P(bc), P(bv), br.numel(), sp)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    assert st == 0
+    up_ms = e0.elapsed_time(e1)
+    nnz_after = A.nnz()
+    b = br.numel() * 12 + (nnz_after - nnz_before) * 8 + 4 * int(lay.row_sizes[touched].sum())
+    ops["update"] = {"ms": round(up_ms, 4), "triples": int(br.numel()), "updates_per_s": round(br.numel() / (up_ms / 1e3), 1),
+                     "bytes": b, "hbm_frac": frac(b, up_ms),
+                     "note": "includes the batch sort and plan (their traffic is not in the algorithmic bytes)"}
+    # compaction (defragmentation into a fresh pool): 2*nnz*(4+sV) + 16n
+    e0.record(stream)
+    A.compact()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    cp_ms = e0.elapsed_time(e1)
+    b = 2 * nnz_after * 8 + 16 * n
+    ops["compact"] = {"ms": round(cp_ms, 4), "bytes": b, "hbm_frac": frac(b, cp_ms),
+                      "note": "includes its one synchronisation (pool size)"}
+    # COO load of the initial matrix (unsorted triples): T(8+sV) in, nnz(4+sV) out, 16n layout
+    rows0 = torch.repeat_interleave(torch.arange(n, dtype=torch.int32, device=dev),
+                                    torch.from_numpy(np.diff(rp)).to(dev))
+    perm = torch.randperm(nnz0, device=dev)
+    r0, c0, v0 = rows0[perm], torch.from_numpy(cols).to(dev)[perm], torch.from_numpy(vals).to(dev)[perm]
+    B = api.DcsrMatrix(n, n, torch.float32)
+    B.from_coo(r0, c0, v0)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    B.from_coo(r0, c0, v0)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ld_ms = e0.elapsed_time(e1)
+    b = nnz0 * 12 + nnz0 * 8 + 16 * n
+    ops["coo_load"] = {"ms": round(ld_ms, 4), "triples": nnz0, "bytes": b, "hbm_frac": frac(b, ld_ms),
+                       "note": "unsorted triples; includes the radix sort and the load's one synchronisation"}
+    del B, rows0, perm, r0, c0, v0
 
     # the same steps through host buffers (pinned), copies inside the timed region
     hb = [tuple(torch.from_numpy(a).pin_memory() for a in b) for b in batches]
@@ -274,7 +318,9 @@ def stream_part(args, dev, world):
         "updates_per_s": round(world * args.steps * len(batches[0][0]) / (total_ms / 1e3), 1),
         "nnz_initial": nnz0, "nnz_final": nnz, "rows": n,
         "spmv": {"ms": round(spmv_ms, 4), "bytes": int(sb), "gbs": round(achieved, 1),
-                 "gather_ceiling_ms": round(gather_ms, 4)},
+                 "gather_floor_ms": round(gather_ms, 4), "gather_floor_bytes": gather_bytes},
+        "ops": ops,
+        "_host": (n, rp, cols, vals, batches),
     }
 
 
@@ -317,12 +363,20 @@ def spgemm_part(args, dev):
     ms = statistics.median(times)
     del A, C
     torch.cuda.synchronize()
+    # algorithmic bytes: read A, the B rows its entries select (products x
+    # (4 + sV)), write C (nnz_C x (4 + sV))
+    lens = np.diff(rp).astype(np.int64)
+    products = int((np.bincount(cols, minlength=n).astype(np.int64) * lens).sum())
+    alg = int(rp[-1]) * 12 + 4 * n + products * 12 + nnz_c * 12
+    hbm, _ = peaks()
     return {"workload": f"C = A*A, A 2^17 x 2^17 FP64, band half-width 2 + 8 random off-band columns per row "
                         f"({int(rp[-1])} nnz); then 100k update triples into A and C = A*A again",
             "ms": round(ms, 3), "nnz_c": int(nnz_c), "output_nnz_per_s": round(nnz_c / (ms / 1e3), 1),
+            "products": products, "bytes": alg, "hbm_frac": round(alg / (ms / 1e3) / 1e9 / hbm, 4),
             "after_update_ms": round(after_ms, 3), "after_update_nnz_c": int(nnz_c2),
             "after_update_output_nnz_per_s": round(nnz_c2 / (after_ms / 1e3), 1),
-            "note": "includes the one host sync the operator makes (output size)"}
+            "note": "includes the operator's two host synchronisations (product count, C's pool top)",
+            "_host": (n, rp, cols, vals)}
 
 
 # ----------------------------------------------------------- batched part
@@ -663,71 +717,141 @@ def served_part(args, dev, rank, local_rank):
 
 # ------------------------------------------------------------ CPU (reference) leg
 
-def reference_served_sample(args, n_mats=8, n_req=60):
-    """The reference's cusp host path serving a bounded sample of the served
-    workload: the first n_mats matrix specs (generated on the host) and the
-    trace's first n_req requests mapped onto them, one at a time."""
-    from dcsr_b200 import workloads as W
+class RefServed:
+    """The reference's cusp host path (oracle/_ref, OpenMP on all host
+    threads) serving a sample of the served workload: the first n_mats matrix
+    specs, generated on the host once, and the trace's requests mapped onto
+    them, one at a time (update = cusp::add of the triples, SpMV = one
+    cusp::multiply per right-hand side, export = a copy of the CSR arrays)."""
+
+    def __init__(self, args, n_mats=64):
+        from dcsr_b200 import workloads as W
+        from oracle import oracle as O
+        self.ref = O.Ref(seq=False)
+        self.specs = W.batched_specs(args.seed + 5, count=args.served_mats)[:n_mats]
+        self.hs = []
+        for sp in self.specs:
+            rng = np.random.default_rng(sp["seed"])
+            rp, cols = W.poisson_matrix(rng, sp["n"], sp["n"], sp["degree"])
+            vals = rng.uniform(-1, 1, cols.size).astype(np.float32)
+            self.hs.append(self.ref.L.ref_res_create(sp["n"], sp["n"], rp, cols, vals))
+        self.kind, self.mat, self.size = W.served_trace(args.seed + 6, args.served_mats, 1 << 16)
+        self.rng = np.random.default_rng(args.seed + 7)
+        self.next = 0
+
+    def serve(self, n_req):
+        """Serve the trace's next n_req requests; returns their latencies (ms) and the wall time (s)."""
+        lat = []
+        t0 = time.perf_counter()
+        for _ in range(n_req):
+            j = self.next % len(self.kind)
+            self.next += 1
+            i = int(self.mat[j]) % len(self.hs)
+            n = self.specs[i]["n"]
+            ts = time.perf_counter()
+            if self.kind[j] == 0:
+                T = int(self.size[j])
+                self.ref.L.ref_res_update(self.hs[i], self.rng.integers(0, n, T).astype(np.int32),
+                                          self.rng.integers(0, n, T).astype(np.int32),
+                                          self.rng.uniform(-1, 1, T).astype(np.float32), T)
+            elif self.kind[j] == 1:
+                k = int(self.size[j])
+                x = self.rng.uniform(-1, 1, n * k).astype(np.float32)
+                y = np.empty(n * k, np.float32)
+                self.ref.L.ref_res_spmv(self.hs[i], x, k, y)
+            else:
+                cap = int(self.specs[i]["n"] * self.specs[i]["degree"] * 2 + 200000)
+                self.ref.L.ref_res_export(self.hs[i], np.empty(n + 1, np.int32), np.empty(cap, np.int32),
+                                          np.empty(cap, np.float32))
+            lat.append(1e3 * (time.perf_counter() - ts))
+        return lat, time.perf_counter() - t0
+
+    def close(self):
+        for h in self.hs:
+            self.ref.L.ref_res_free(h)
+        self.hs = []
+
+    def sample_text(self, n_req):
+        return (f"{n_req} requests of the served trace on its first {len(self.specs)} matrices (host-generated), "
+                "served one at a time by cusp::add / cusp::multiply / CSR copy (OpenMP)")
+
+
+def reference_served_sample(args, n_req=400):
+    srv = RefServed(args)
+    srv.serve(8)  # warm-up
+    lat, dt = srv.serve(n_req)
+    out = {"value": round(n_req / dt, 3), "unit": "req/s", "cores": srv.ref.threads(), "kind": "reference",
+           "p50_ms": round(pct(lat, 50), 3), "p99_ms": round(pct(lat, 99), 3), "sample": srv.sample_text(n_req)}
+    srv.close()
+    return out
+
+
+def cpu_ops_baseline(args, stream_host, spgemm_host):
+    """The reference's cusp host path on the update stream's step (cusp::add
+    of a 1M-triple batch, then SpMV, row sums -- SpMV with x = 1 -- and the
+    CSR copy) and on the SpGEMM workload (cusp::multiply), once on one thread
+    (the sequential host system) and once on all host threads (OpenMP)."""
     from oracle import oracle as O
-    ref = O.Ref(seq=False)
-    specs = W.batched_specs(args.seed + 5, count=args.served_mats)[:n_mats]
-    hs = []
-    for sp in specs:
-        rng = np.random.default_rng(sp["seed"])
-        rp, cols = W.poisson_matrix(rng, sp["n"], sp["n"], sp["degree"])
-        vals = rng.uniform(-1, 1, cols.size).astype(np.float32)
-        hs.append(ref.L.ref_res_create(sp["n"], sp["n"], rp, cols, vals))
-    kind, mat, size = W.served_trace(args.seed + 6, args.served_mats, n_req)
-    rng = np.random.default_rng(args.seed + 7)
-    lat = []
-    t0 = time.perf_counter()
-    for j in range(n_req):
-        i = int(mat[j]) % n_mats
-        n = specs[i]["n"]
-        ts = time.perf_counter()
-        if kind[j] == 0:
-            T = int(size[j])
-            ref.L.ref_res_update(hs[i], rng.integers(0, n, T).astype(np.int32), rng.integers(0, n, T).astype(np.int32),
-                                 rng.uniform(-1, 1, T).astype(np.float32), T)
-        elif kind[j] == 1:
-            k = int(size[j])
-            x = rng.uniform(-1, 1, n * k).astype(np.float32)
-            y = np.empty(n * k, np.float32)
-            ref.L.ref_res_spmv(hs[i], x, k, y)
-        else:
-            cap = int(specs[i]["n"] * specs[i]["degree"] * 2 + 200000)
-            ref.L.ref_res_export(hs[i], np.empty(n + 1, np.int32), np.empty(cap, np.int32), np.empty(cap, np.float32))
-        lat.append(1e3 * (time.perf_counter() - ts))
-    dt = time.perf_counter() - t0
-    for h in hs:
-        ref.L.ref_res_free(h)
-    return {"value": round(n_req / dt, 3), "unit": "req/s", "cores": ref.threads(), "kind": "reference",
-            "p50_ms": round(pct(lat, 50), 3), "p99_ms": round(pct(lat, 99), 3),
-            "sample": f"{n_req} requests of the served trace on its first {n_mats} matrices (host-generated), "
-                      "served one at a time by cusp::add / cusp::multiply / CSR copy (OpenMP)"}
+    out = {}
+    if stream_host is not None:
+        n, rp, cols, vals, batches = stream_host
+        x = np.random.default_rng(args.seed + 1).uniform(-1, 1, n)
+        rows = {}
+        for seq in (True, False):
+            ref = O.Ref(seq=seq)
+            h = ref.L.ref_stream_create(n, n, rp, cols, vals.astype(np.float64), x)
+            y, rsum = np.empty(n), np.empty(n)
+            ts = []
+            for b in batches[:2]:
+                t0 = time.perf_counter()
+                ref.L.ref_stream_step(h, b[0], b[1], b[2].astype(np.float64), len(b[0]), y, rsum)
+                ts.append(time.perf_counter() - t0)
+            ref.L.ref_stream_free(h)
+            rows["1_thread" if seq else f"{ref.threads()}_threads"] = {"step_s": round(statistics.mean(ts), 4)}
+        out["stream_step"] = {"workload": "R-MAT 2^20 update-stream step: cusp::add of 1M triples + SpMV + row "
+                                          "sums + CSR copy (first two batches)", **rows}
+    if spgemm_host is not None:
+        n, rp, cols, vals = spgemm_host
+        rows = {}
+        for seq in (True, False):
+            ref = O.Ref(seq=seq)
+            t0 = time.perf_counter()
+            R = ref.spgemm(O.F64, n, n, n, rp, cols, vals, rp, cols, vals)
+            dt = time.perf_counter() - t0
+            rows["1_thread" if seq else f"{ref.threads()}_threads"] = {
+                "s": round(dt, 4), "output_nnz_per_s": round(len(R[1]) / dt, 1)}
+        out["spgemm"] = {"workload": "C = A*A, banded 2^17 FP64 (cusp::multiply)", **rows}
+    return out
 
 
 def run_reference(args):
     from oracle import oracle as O
     if not O.Ref.available(seq=False):
         return {"impl": "reference", "unavailable": "oracle/_ref (the reference's cusp host path) is not built"}
+    srv = RefServed(args)
     for _ in range(args.warmup):
-        reference_served_sample(args, n_req=6)
-    vals = []
-    for s in range(args.steps):
-        r = reference_served_sample(args, n_req=args.ref_requests)
-        vals.append(r)
-    value = statistics.mean(v["value"] for v in vals)
-    r = vals[-1]
+        srv.serve(4)
+    # the sample (ref_requests requests) split across the timed steps
+    per = max(1, args.ref_requests // max(args.steps, 1))
+    lat, wall = [], 0.0
+    for _ in range(args.steps):
+        l_, dt = srv.serve(per)
+        lat += l_
+        wall += dt
+    value = len(lat) / wall
+    sample = srv.sample_text(len(lat))
+    cores = srv.ref.threads()
+    srv.close()
     return {
         "impl": "reference", "metric": METRIC, "value": round(value, 3), "unit": "req/s", "n_gpus": 1,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * args.ref_requests / value, 3),
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * wall / args.steps, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded served workload sample, generated on the host)",
         "config": {"workload": "served: matrices like the batched ones, 40/50/10 update/SpMV/export requests",
-                   "sample": r["sample"], "parallelism": "host OpenMP"},
-        "p50_ms": r["p50_ms"], "p99_ms": r["p99_ms"],
-        "cpu_baseline": {k: r[k] for k in ("value", "unit", "cores", "kind", "sample")} | {"value": round(value, 3)},
+                   "sample": sample, "parallelism": "host OpenMP"},
+        "p50_ms": round(pct(lat, 50), 3), "p99_ms": round(pct(lat, 99), 3),
+        "cpu_baseline": {"value": round(value, 3), "unit": "req/s", "cores": cores, "kind": "reference",
+                         "sample": sample},
         "e2e": {"value": round(value, 3), "unit": "req/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
 
@@ -745,7 +869,8 @@ def run_ours(args, rank, world, local_rank):
     spgemm = spgemm_part(args, dev) if not args.skip_spgemm else None
     batched = batched_part(args, dev) if not args.skip_batched else None
     if args.skip_served:  # profiling runs of the other parts only
-        return {"stream": stream, "batched": batched, "spgemm": spgemm}
+        strip = lambda d: None if d is None else {k: v for k, v in d.items() if not k.startswith("_")}  # noqa: E731
+        return {"stream": strip(stream), "batched": batched, "spgemm": strip(spgemm)}
     served = served_part(args, dev, rank, local_rank)
 
     # aggregate over ranks: requests of all ranks / the slowest rank's wall time
@@ -767,6 +892,7 @@ def run_ours(args, rank, world, local_rank):
         "p50_ms": served["p50_ms"], "p99_ms": served["p99_ms"],
         "plain": served["plain"], "plain_host_buffers": served["plain_host_buffers"], "served": served["served"],
         "speedup_at_equal_p99": served["speedup_at_equal_p99"],
+        "speedup_at_equal_p99_host_buffers": served["e2e"]["speedup_at_equal_p99"],
         "speedup_vs_plain_capacity": served["speedup_vs_plain_capacity"],
         "e2e": {"value": round(e2e_value, 3), "unit": "req/s", "p99_ms": served["e2e"]["p99_ms"],
                 "capacity_req_s": served["e2e"]["capacity_req_s"], "p99_constraint_met": served["e2e"]["p99_constraint_met"],
@@ -781,27 +907,30 @@ def run_ours(args, rank, world, local_rank):
     }
     if stream is not None:
         sp = stream["spmv"]
-        traffic = profiled_traffic("spmv_rmat_k1_f32.md", sp["bytes"])
+        traffic = SPMV_TRAFFIC.get(stream["nnz_final"])
         out["spmv_gbs"] = sp["gbs"]
-        out["roofline"] = {"kernel": "k_rows_reduce x3 (DCSR SpMV: long-row chunks, medium rows, short-row blocks; "
-                                     "k=1, FP32, R-MAT 2^20 after the update stream)",
+        out["roofline"] = {"kernel": "k_rows1 (DCSR SpMV, k=1, FP32: one launch over long-row chunks, medium rows "
+                                     "and short-row blocks; R-MAT 2^20 after the update stream)",
                            "bound": "hbm", "achieved": sp["gbs"], "peak": hbm, "peak_kind": peak_kind, "unit": "GB/s",
                            "frac": round(sp["gbs"] / hbm, 4), "traffic": traffic, "bytes_per_launch": sp["bytes"],
                            "avg_ms": sp["ms"],
-                           "gather_ceiling": {
-                               "ms": sp["gather_ceiling_ms"],
-                               "frac": round(sp["gather_ceiling_ms"] / sp["ms"], 4),
-                               "note": "torch.index_select of x at the matrix's columns in row order (x warm in "
-                                       "L2): the sector traffic of the SpMV's x reads alone; frac = ceiling time / "
-                                       "SpMV time"}}
+                           "gather_floor": {
+                               "ms": sp["gather_floor_ms"],
+                               "frac_of_hbm": round(sp["bytes"] / (sp["gather_floor_ms"] / 1e3) / 1e9 / hbm, 4),
+                               "note": "dcsr_measure_gather over the same entries (CSR export: int32 columns, FP32 "
+                                       "values, coalesced) gathering x at each column, no row bookkeeping: the "
+                                       "SpMV's data movement at best on this GPU; frac_of_hbm = the SpMV's "
+                                       "algorithmic bytes over that time"}}
         out["stream"] = {k: v for k, v in stream.items() if not k.startswith("_")}
     if batched is not None:
         out["batched"] = batched
     if spgemm is not None:
-        out["spgemm"] = spgemm
+        out["spgemm"] = {k: v for k, v in spgemm.items() if not k.startswith("_")}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             out["cpu_baseline"] = reference_served_sample(args, n_req=args.ref_requests)
+            out["cpu_ops"] = cpu_ops_baseline(args, stream["_host"] if stream is not None else None,
+                                              spgemm["_host"] if spgemm is not None else None)
         except FileNotFoundError as e:
             out["cpu_baseline"] = {"unavailable": str(e)}
     return out
@@ -826,7 +955,7 @@ def main():
     ap.add_argument("--plain-fracs", type=float, nargs="+", default=[0.5, 0.7, 0.9])
     ap.add_argument("--batched-mats", type=int, default=512)
     ap.add_argument("--batched-reps", type=int, default=5)
-    ap.add_argument("--ref-requests", type=int, default=40)
+    ap.add_argument("--ref-requests", type=int, default=400)
     ap.add_argument("--skip-stream", action="store_true")
     ap.add_argument("--skip-batched", action="store_true")
     ap.add_argument("--skip-spgemm", action="store_true")

@@ -193,7 +193,7 @@ int BatchCore::plan(const dcsr_batch_item *its, int n, cudaStream_t s, bool all_
     g.off = off;
     off = align_up((int64_t)(off + g.idx.size() * desc_size(dtype, true)), 256);
     g.pref_off = poff;
-    poff += 3 * (g.idx.size() + 1) + 1;  // unit prefixes + the k = 1 pass's counter word
+    poff += 3 * (g.idx.size() + 1) + 2;  // unit prefixes + the k = 1 passes' counter words
     int64_t blocks = 0;
     for (int i : g.idx) blocks += div_up(its[i].matrix->n_rows, 32);
     g.split = short_split(blocks, g.k);
@@ -238,7 +238,7 @@ int BatchCore::reserve_items(int n, int dt, cudaStream_t s) {
   cc = 2 * (size_t)cnt_cap;
   DCSR_TRY(grow_dev(&status_dev, 2 * (size_t)n, cc, s));
   cnt_cap = n > cnt_cap ? n : cnt_cap;
-  DCSR_TRY(grow_dev(&pref, 3 * (size_t)(n + 8) + 8, pref_cap, s));
+  DCSR_TRY(grow_dev(&pref, 3 * (size_t)(n + 8) + 16, pref_cap, s));
   return DCSR_OK;
 }
 

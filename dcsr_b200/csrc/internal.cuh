@@ -78,8 +78,8 @@ int schedule_many(const void *items_dev, int dtype, int count, int64_t R, Arena 
 size_t schedule_scratch_bytes(int64_t R);
 // y = A x for `count` matrices (items: device RowItem<V>[count]) of one k
 // family: kf = 1, 2, 4 or 8, every item's k <= kf (each item's own k / vec
-// are read by the kernel); pref: device scratch of 3*(count+1)+1 long longs
-// (the unit prefixes, then the k = 1 pass's counter word).
+// are read by the kernel); pref: device scratch of 3*(count+1)+2 long longs
+// (the unit prefixes, then the k = 1 passes' counter words).
 // prefixed: the group's unit prefixes were computed already (unit_prefix_many,
 // with the same split); split: warps per 32-row block of short rows (short_split)
 int spmv_many(const void *items_dev, int dtype, int count, int k, long long *pref, cudaStream_t s,

@@ -62,10 +62,13 @@ template <typename V>
 struct RowOne {
   RowItem<V> it;
   int split = 1;
-  // unit counter and finished-warp counter of the k = 1 pass (the handle's
-  // schedule words 8 and 9: zeroed by the schedule rebuild, reset by the
-  // last warp of every pass)
-  __device__ __forceinline__ unsigned *ctr() const { return reinterpret_cast<unsigned *>(it.info + 8); }
+  // unit counter and finished-warp counter of the k = 1 passes (the handle's
+  // schedule words 8, 9 for the streamed units, 10, 11 for the short-row
+  // blocks: zeroed by the schedule rebuild, reset by the last warp of every
+  // pass)
+  __device__ __forceinline__ unsigned *ctr(int which) const {
+    return reinterpret_cast<unsigned *>(it.info + 8 + 2 * which);
+  }
   __device__ __forceinline__ int n_items() const { return 1; }
   __device__ __forceinline__ const RowItem<V> &item(int) const { return it; }
   __device__ __forceinline__ int find_row(int64_t) const { return 0; }
@@ -85,10 +88,11 @@ struct RowMany {
   const RowItem<V> *its;
   int count;
   const long long *pref;  // [3][count+1] unit prefixes per class (short blocks counted split times),
-                          // then one word: the k = 1 pass's unit and finished-warp counters
+                          // then two words: the unit and finished-warp counters of the
+                          // k = 1 passes (streamed units, short-row blocks)
   int split = 1;
-  __device__ __forceinline__ unsigned *ctr() const {
-    return reinterpret_cast<unsigned *>(const_cast<long long *>(pref + 3 * (count + 1)));
+  __device__ __forceinline__ unsigned *ctr(int which) const {
+    return reinterpret_cast<unsigned *>(const_cast<long long *>(pref + 3 * (count + 1) + which));
   }
   __device__ __forceinline__ int n_items() const { return count; }
   __device__ __forceinline__ const RowItem<V> &item(int i) const { return its[i]; }
@@ -148,8 +152,10 @@ __global__ void k_sched_emit(Src src, int64_t R, const long long *lscan, const l
     const int64_t r = g - it.row0;
     const int32_t L = it.m.row_sizes[r];
     if (L > it.short_max) {
+      // unit descriptors of the k = 1 pass: (row, length, pool slot of the
+      // unit's first entry when the unit lies in layer 0 else -1, chunk number)
       const int2 s0 = *reinterpret_cast<const int2 *>(it.m.seg + 2 * r);  // layer 0
-      const int4 d = make_int4((int32_t)r, L, s0.x, s0.y - s0.x);
+      const int32_t cap0 = s0.y - s0.x;
       if (L > it.long_min) {
         const long long s = lscan[g] - lscan[it.row0];
         const int32_t li = (int32_t)(s >> 32);
@@ -158,11 +164,14 @@ __global__ void k_sched_emit(Src src, int64_t R, const long long *lscan, const l
         const_cast<long long *>(it.long_off)[li] = c0;
         it.long_cnt[li] = 0;
         for (long long c = c0; c < c0 + nc; c++) {
+          const int32_t k = (int32_t)(c - c0);
+          const int32_t e = (k + 1) * CHUNK < L ? (k + 1) * CHUNK : L;
           const_cast<int2 *>(it.chunk_rl)[c] = make_int2((int32_t)r, li);
-          const_cast<int4 *>(it.chunk_desc)[c] = d;
+          const_cast<int4 *>(it.chunk_desc)[c] = make_int4((int32_t)r, L, e <= cap0 ? s0.x + k * CHUNK : -1, k);
         }
       } else {
-        const_cast<int4 *>(it.med_desc)[mscan[g] - mscan[it.row0]] = d;
+        const_cast<int4 *>(it.med_desc)[mscan[g] - mscan[it.row0]] =
+            make_int4((int32_t)r, L, L <= cap0 ? s0.x : -1, 0);
       }
     }
   }
@@ -182,8 +191,7 @@ __global__ void k_sched_info(Src src, const long long *lscan, const long long *m
       it.info[0] = n_long;
       it.info[1] = n_chunks;
       it.info[2] = (int32_t)(mscan[b] - mscan[a]);
-      it.info[8] = 0;  // k = 1 pass counters
-      it.info[9] = 0;
+      for (int q = 8; q < 12; q++) it.info[q] = 0;  // k = 1 pass counters
       const_cast<long long *>(it.long_off)[n_long] = n_chunks;
     }
   }
@@ -322,7 +330,7 @@ __device__ __forceinline__ void unit_prefix_block(const RowItem<V> *its, int cou
     __syncthreads();
   }
   if (threadIdx.x < 3) pref[threadIdx.x * (count + 1) + count] = carry[threadIdx.x];
-  if (threadIdx.x == 0) pref[3 * (count + 1)] = 0;  // the k = 1 pass's counters
+  if (threadIdx.x < 2) pref[3 * (count + 1) + threadIdx.x] = 0;  // the k = 1 passes' counters
 }
 
 template <typename V>
@@ -899,7 +907,10 @@ __global__ void __launch_bounds__(RS_THREADS_, RowsMinBlocks<K>::N) k_rows_reduc
 #define DCSR_K1_UN 4
 #endif
 #ifndef DCSR_K1_MINB
-#define DCSR_K1_MINB 4
+#define DCSR_K1_MINB 3
+#endif
+#ifndef DCSR_K1B_MINB
+#define DCSR_K1B_MINB 4
 #endif
 
 // Entries [c0, c1) of a row whose range lies in one segment starting at pool
@@ -954,12 +965,13 @@ __device__ __forceinline__ double stream_seg(const RowItem<V> &it, int64_t st, i
 
 // The same over a range that crosses segments (a chained row): UN windows
 // per step, each entry's slot found through the chain.  Same summation
-// order as stream_seg.
+// order as the single-segment stream.  Not inlined (chained units are rare;
+// their registers stay out of the streaming loop); takes plain pointers.
 template <typename V, int OP>
-__device__ __noinline__ double stream_chain(const RowItem<V> &it, const Chain &ch, int64_t c0, int64_t c1, int lane) {
+__device__ __forceinline__ double stream_chain(const V *vals, const int32_t *cols, const V *x, int64_t ldx, Chain ch,
+                                            int64_t c0, int64_t c1, int lane) {
   using P = typename std::conditional<sizeof(V) == 4, float, double>::type;
   constexpr int UN = sizeof(V) == 8 && DCSR_K1_UN > 1 ? DCSR_K1_UN / 2 : DCSR_K1_UN;
-  const Mat<V> &m = it.m;
   const int64_t first = ch.phys(c0);
   double acc = op_init<double, OP>();
   for (int64_t b0 = c0; b0 < c1; b0 += 32 * UN) {
@@ -969,15 +981,15 @@ __device__ __noinline__ double stream_chain(const RowItem<V> &it, const Chain &c
     for (int i = 0; i < UN; i++) {
       const int64_t p = b0 + 32 * i + lane;
       const int64_t q = p < c1 ? ch.phys(p) : first;
-      a[i] = __ldcs(m.vals + q);
-      col[i] = OP == OP_SPMV ? __ldcs(m.cols + q) : 0;
+      a[i] = __ldcs(vals + q);
+      col[i] = OP == OP_SPMV ? __ldcs(cols + q) : 0;
     }
     P w = op_init<P, OP>();
 #pragma unroll
     for (int i = 0; i < UN; i++) {
       if (b0 + 32 * i + lane < c1) {
         P t;
-        if constexpr (OP == OP_SPMV) t = mul_rn((P)a[i], (P)__ldg(it.x + (int64_t)col[i] * it.ldx));
+        if constexpr (OP == OP_SPMV) t = mul_rn((P)a[i], (P)__ldg(x + (int64_t)col[i] * ldx));
         else t = OP == OP_COUNT ? (P)1 : (P)a[i];
         w = op_comb<P, OP>(w, t);
       }
@@ -994,15 +1006,18 @@ __device__ __forceinline__ double warp_comb(double v) {
   return v;
 }
 
-// A unit of the k = 1 pass, decoded and with its descriptor loaded: for a
-// chunk or a medium row every lane holds the row's descriptor (row, length,
-// layer-0 start, layer-0 capacity); for a block of short rows each lane holds
-// its own row's.
+// A unit of the k = 1 pass, decoded, with its descriptor loaded.  A long-row
+// chunk or a medium row is a "streamed" unit: every lane holds (row, row
+// length, pool slot of the unit's first entry or -1 when the unit crosses a
+// segment boundary, chunk number within the row).  A block of short rows
+// holds, in each lane, that lane's row: (row or -1, length, layer-0 start,
+// layer-0 capacity).
 enum { U1_CHUNK = 0, U1_MED = 1, U1_BLOCK = 2, U1_NONE = 3 };
 struct Unit1 {
+  int32_t u;   // unit number (>= total: past the end)
+  int32_t lu;  // chunk index within the matrix's chunk table (chunks)
   int kind;
   int item;    // matrix of the unit
-  int64_t lu;  // chunk number within the matrix (chunks)
   int4 d;
 };
 
@@ -1010,10 +1025,11 @@ template <typename V, typename Src>
 __device__ __forceinline__ Unit1 unit1_load(const Src &src, int64_t u, int64_t NC, int64_t NM, int64_t total,
                                             int lane) {
   Unit1 x;
+  x.u = (int32_t)(u < total ? u : total);
   x.kind = U1_NONE;
   x.item = 0;
   x.lu = 0;
-  x.d = make_int4(-1, 0, 0, 0);
+  x.d = make_int4(-1, 0, -1, 0);
   if (u >= total) return x;
   int64_t lu;
   if (u < NC) {
@@ -1021,7 +1037,7 @@ __device__ __forceinline__ Unit1 unit1_load(const Src &src, int64_t u, int64_t N
     const RowItem<V> &it = src.item(x.item);
     if (it.skip && *it.skip) return x;
     x.kind = U1_CHUNK;
-    x.lu = lu;
+    x.lu = (int32_t)lu;
     x.d = it.chunk_desc[lu];
   } else if (u < NC + NM) {
     x.item = src.locate(P_MED, (u - NC) / RS_WARPS, lu);
@@ -1046,79 +1062,182 @@ __device__ __forceinline__ Unit1 unit1_load(const Src &src, int64_t u, int64_t N
   return x;
 }
 
+__device__ __forceinline__ bool streamed(const Unit1 &x) { return x.kind == U1_CHUNK || x.kind == U1_MED; }
+// The entry range [c0, c1) of a streamed unit within its row.
+__device__ __forceinline__ void unit_range(const Unit1 &x, int64_t &c0, int64_t &c1) {
+  if (x.kind == U1_CHUNK) {
+    c0 = (int64_t)x.d.w * CHUNK;
+    c1 = c0 + CHUNK < x.d.y ? c0 + CHUNK : x.d.y;
+  } else {
+    c0 = 0;
+    c1 = x.d.y;
+  }
+}
+
+// Loads of one step (UN windows of 32 entries) of a streamed unit lying in
+// one segment (first pool slot d.z), entries [o, o + 32*UN) of the unit.
+template <typename V, int UN, int OP>
+__device__ __forceinline__ void load_step(const Mat<V> &m, int64_t base, int64_t n, int64_t o, int lane, V (&a)[UN],
+                                          int32_t (&col)[UN]) {
+#pragma unroll
+  for (int i = 0; i < UN; i++) {
+    const int64_t p = o + 32 * i + lane, q = base + (p < n ? p : 0);
+    a[i] = __ldcs(m.vals + q);
+    col[i] = OP == OP_SPMV ? __ldcs(m.cols + q) : 0;
+  }
+}
+
+// The end of a streamed unit: its total (t, in every lane) is the row's
+// result, or one chunk's partial; the warp that adds the row's last chunk
+// combines the partials in chunk order.
+template <typename V, int OP>
+__device__ __forceinline__ void finish_unit(const RowItem<V> &it, const Unit1 &x, double t, int lane) {
+  const int32_t row = x.d.x, L = x.d.y;
+  const int64_t nch = x.kind == U1_CHUNK ? (L + CHUNK - 1) / CHUNK : 1;
+  if (nch == 1) {
+    if (lane == 0) {
+      const double o[1] = {t};
+      write_y<V, 1, OP>(it.y, it.ldy, row, o, it.alpha, it.beta, L, 1);
+    }
+    return;
+  }
+  const int64_t p0 = x.lu - x.d.w;  // the row's first chunk (chunks of a row are consecutive)
+  int last = 0;
+  if (lane == 0) {
+    const int32_t li = it.chunk_rl[x.lu].y;
+    it.part[x.lu] = t;
+    __threadfence();
+    last = atomicAdd(&it.long_cnt[li], 1) == nch - 1;
+    if (last) it.long_cnt[li] = 0;
+  }
+  if (__shfl_sync(FULL, last, 0)) {
+    // every chunk's partial is published: lanes take partials lane,
+    // lane+32, ... in order, then a fixed xor tree
+    __threadfence();
+    double v = op_init<double, OP>();
+    for (int64_t q = lane; q < nch; q += 32) v = op_comb<double, OP>(v, __ldcg(it.part + p0 + q));
+    v = warp_comb<OP>(v);
+    if (lane == 0) {
+      const double o[1] = {v};
+      write_y<V, 1, OP>(it.y, it.ldy, row, o, it.alpha, it.beta, L, 1);
+    }
+  }
+}
+
+// The streamed units (long-row chunks, then medium rows) of a k = 1 pass.
 template <typename V, int OP, typename Src>
 __global__ void __launch_bounds__(RS_THREADS_, DCSR_K1_MINB) k_rows1(Src src) {
+  using P = typename std::conditional<sizeof(V) == 4, float, double>::type;
+  constexpr int UN = sizeof(V) == 8 && DCSR_K1_UN > 1 ? DCSR_K1_UN / 2 : DCSR_K1_UN;
+  constexpr int W = 32 * UN;  // entries of one step
   const int lane = threadIdx.x & 31;
-  const int64_t NC = src.units(P_CHUNKS), NM = src.units(P_MED) * RS_WARPS, NB = src.units(P_BLOCKS) * RS_WARPS;
-  const int64_t total = NC + NM + NB;
-  unsigned *ctr = src.ctr();
+  const int64_t NC = src.units(P_CHUNKS), NM = src.units(P_MED) * RS_WARPS;
+  const int64_t total = NC + NM;
+  unsigned *ctr = src.ctr(0);
   auto fetch = [&]() -> int64_t {
     unsigned v = 0;
     if (lane == 0) v = atomicAdd(ctr, 1u);
     return (int64_t)__shfl_sync(FULL, v, 0);
   };
-  // three units in flight per warp: the one being worked on (its descriptor
-  // loaded), the next (its descriptor loads issued at the top of this
-  // iteration), and the one after (its number being fetched)
-  int64_t u = fetch();
-  Unit1 cur = unit1_load<V>(src, u, NC, NM, total, lane);
-  int64_t n1 = fetch();
-  while (u < total) {
-    const int64_t n2 = fetch();
-    const Unit1 nx = unit1_load<V>(src, n1, NC, NM, total, lane);
-    if (cur.kind == U1_CHUNK || cur.kind == U1_MED) {
-      // ---- a long-row chunk or a medium row
+  // Units in flight per warp: cur (streamed step by step), nx (its
+  // descriptor loaded or in flight) and the number of the one after.  The
+  // loads of the next step are issued before the current step's x values
+  // are gathered, whether that step is the current unit's next or the next
+  // unit's first -- the stream does not stop at unit ends.
+  Unit1 cur = unit1_load<V>(src, fetch(), NC, NM, total, lane);
+  Unit1 nx = unit1_load<V>(src, fetch(), NC, NM, total, lane);
+  int64_t n2 = fetch();
+  V a[UN], an[UN];
+  int32_t col[UN], coln[UN];
+  int64_t c0 = 0, c1 = 0, o = 0;  // cur's range and the current step's offset in it
+  if (streamed(cur)) {
+    unit_range(cur, c0, c1);
+    if (cur.d.z >= 0) load_step<V, UN, OP>(src.item(cur.item).m, cur.d.z, c1 - c0, 0, lane, a, col);
+  }
+  double acc = op_init<double, OP>();
+  while (cur.u < total) {
+    bool advance = true;
+    if (streamed(cur)) {
       const RowItem<V> &it = src.item(cur.item);
-      const Mat<V> &m = it.m;
-      const int32_t row = cur.d.x;
-      const int64_t L = cur.d.y;
-      int64_t chunk = 0, nch = 1;
-      if (cur.kind == U1_CHUNK) nch = (L + CHUNK - 1) / CHUNK;
-      int64_t li = 0;
-      if (nch > 1) {
-        li = it.chunk_rl[cur.lu].y;
-        chunk = cur.lu - it.long_off[li];
-      }
-      const int64_t c0 = chunk * CHUNK, c1 = cur.kind == U1_CHUNK ? (c0 + CHUNK < L ? c0 + CHUNK : L) : L;
-      const double part = c1 <= cur.d.w ? stream_seg<V, OP>(it, cur.d.z, c0, c1, lane)  // inside layer 0
-                                        : stream_chain<V, OP>(it, load_chain(m, row), c0, c1, lane);
-      const double t = warp_comb<OP>(part);
-      if (nch == 1) {
-        if (lane == 0) {
-          const double o[1] = {t};
-          write_y<V, 1, OP>(it.y, it.ldy, row, o, it.alpha, it.beta, (int32_t)L, 1);
-        }
+      if (cur.d.z < 0) {
+        // a unit across segment boundaries (a chained row): streamed on its own
+        const double t = warp_comb<OP>(
+            stream_chain<V, OP>(it.m.vals, it.m.cols, it.x, it.ldx, load_chain(it.m, cur.d.x), c0, c1, lane));
+        finish_unit<V, OP>(it, cur, t, lane);
       } else {
-        const int64_t p0 = it.long_off[li];
-        int last = 0;
-        if (lane == 0) {
-          it.part[p0 + chunk] = t;
-          __threadfence();
-          last = atomicAdd(&it.long_cnt[li], 1) == nch - 1;
+        const int64_t n = c1 - c0;
+        const bool last = o + W >= n;
+        if (!last) {
+          load_step<V, UN, OP>(it.m, cur.d.z, n, o + W, lane, an, coln);
+        } else if (streamed(nx) && nx.d.z >= 0) {
+          int64_t d0, d1;
+          unit_range(nx, d0, d1);
+          load_step<V, UN, OP>(src.item(nx.item).m, nx.d.z, d1 - d0, 0, lane, an, coln);
         }
-        if (__shfl_sync(FULL, last, 0)) {
-          // every chunk's partial is published: lanes take partials
-          // lane, lane+32, ... in order, then a fixed xor tree
-          __threadfence();
-          double v = op_init<double, OP>();
-          for (int64_t q = lane; q < nch; q += 32) v = op_comb<double, OP>(v, __ldcg(it.part + p0 + q));
-          v = warp_comb<OP>(v);
-          if (lane == 0) {
-            const double o[1] = {v};
-            write_y<V, 1, OP>(it.y, it.ldy, row, o, it.alpha, it.beta, (int32_t)L, 1);
-            it.long_cnt[li] = 0;
+        P w = op_init<P, OP>();
+#pragma unroll
+        for (int i = 0; i < UN; i++) {
+          if (o + 32 * i + lane < n) {
+            P t;
+            if constexpr (OP == OP_SPMV) t = mul_rn((P)a[i], (P)__ldg(it.x + (int64_t)col[i] * it.ldx));
+            else t = OP == OP_COUNT ? (P)1 : (P)a[i];
+            w = op_comb<P, OP>(w, t);
           }
         }
+        acc = op_comb<double, OP>(acc, (double)w);
+#pragma unroll
+        for (int i = 0; i < UN; i++) {
+          a[i] = an[i];
+          col[i] = coln[i];
+        }
+        if (last) {
+          finish_unit<V, OP>(it, cur, warp_comb<OP>(acc), lane);
+          acc = op_init<double, OP>();
+        } else {
+          o += W;
+          advance = false;
+        }
       }
-    } else if (cur.kind == U1_BLOCK) {
-      // ---- a block of 32 short rows
-      short_block_k1<V, OP>(src.item(cur.item), cur.d, lane);
     }
-    u = n1;
+    if (advance) {
+      cur = nx;
+      nx = unit1_load<V>(src, n2, NC, NM, total, lane);
+      n2 = fetch();
+      o = 0;
+      if (streamed(cur)) unit_range(cur, c0, c1);
+    }
+  }
+  // the last warp to finish resets the counters for the next pass
+  if (lane == 0 && atomicAdd(ctr + 1, 1u) == gridDim.x * RS_WARPS - 1) {
+    ctr[0] = 0;
+    ctr[1] = 0;
+  }
+}
+
+// The short-row blocks of a k = 1 pass: a warp per block of 32 rows, the
+// next block's descriptors (each lane's row length and layer-0 segment)
+// loaded while the current block runs.
+template <typename V, int OP, typename Src>
+__global__ void __launch_bounds__(RS_THREADS_, DCSR_K1B_MINB) k_rows1_blocks(Src src) {
+  const int lane = threadIdx.x & 31;
+  const int64_t NB = src.units(P_BLOCKS) * RS_WARPS;
+  unsigned *ctr = src.ctr(1);
+  auto fetch = [&]() -> int64_t {
+    unsigned v = 0;
+    if (lane == 0) v = atomicAdd(ctr, 1u);
+    return (int64_t)__shfl_sync(FULL, v, 0);
+  };
+  // units numbered after the streamed ones (NC + NM): unit1_load decodes them as blocks
+  const int64_t base = src.units(P_CHUNKS) + src.units(P_MED) * RS_WARPS, total = base + NB;
+  Unit1 cur = unit1_load<V>(src, base + fetch(), base, 0, total, lane);
+  int64_t n1 = fetch();
+  while (cur.u < total) {
+    const int64_t n2 = fetch();
+    const Unit1 nx = unit1_load<V>(src, base + n1, base, 0, total, lane);
+    if (cur.kind == U1_BLOCK) short_block_k1<V, OP>(src.item(cur.item), cur.d, lane);
     cur = nx;
     n1 = n2;
   }
-  // the last warp to finish resets the counters for the next pass
   if (lane == 0 && atomicAdd(ctr + 1, 1u) == gridDim.x * RS_WARPS - 1) {
     ctr[0] = 0;
     ctr[1] = 0;
@@ -1250,9 +1369,11 @@ static int grid_of(const void *k) { return persistent_grid(k, RS_THREADS_, 0); }
 
 template <typename V, int K, int OP, bool VEC, typename Src>
 static int launch_reduce_src(const Src &src, cudaStream_t s) {
-  if constexpr (K == 1) {  // one value per entry: every class in one launch
+  if constexpr (K == 1) {  // one value per entry: streamed units, then short-row blocks
     static const int g = grid_of((const void *)k_rows1<V, OP, Src>);
+    static const int gb = grid_of((const void *)k_rows1_blocks<V, OP, Src>);
     DCSR_LAUNCH((k_rows1<V, OP, Src>), g, RS_THREADS_, 0, s, src);
+    DCSR_LAUNCH((k_rows1_blocks<V, OP, Src>), gb, RS_THREADS_, 0, s, src);
     return DCSR_OK;
   } else {
     static const int g0 = grid_of((const void *)k_rows_reduce<V, K, OP, VEC, P_BLOCKS, Src>);

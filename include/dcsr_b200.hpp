@@ -18,6 +18,9 @@
 //   device::spmv(dcsr, x, y, streams)  spmv.h:121
 //   device::spmm(A, B, C, streams)     spmm.h:30
 //   device::count_sorted_indices(I, X, n) primitives.h:417
+//   device::LoadMatrix(hyb, csr)       load.h:174  device::ExportHYB (DCSR -> HYB)
+//   device::spmv(hyb, x, y)            spmv.h:36   device::spmv(rows, width, ...)
+//   cusp::krylov::cg(A, x, b)          cusp/krylov/cg.h   device::cg
 //
 // Differences, by design: errors are returned as dcsr_status (the reference
 // returned void and wrote out of bounds on overflow); every call takes one
@@ -176,6 +179,41 @@ inline void spmm(const dcsr::dcsr_matrix<V> &A, const dcsr::dcsr_matrix<V> &B, d
 
 inline void count_sorted_indices(const int32_t *I, int32_t *X, int64_t size, void *stream = nullptr) {
   dcsr::check(dcsr_count_sorted_indices(I, size, X, stream), "count_sorted_indices");
+}
+
+// DCSR -> HYB (reference LoadMatrix(hyb, csr), include/load.h:174-205): the
+// first `width` entries of each row into the column-major ELL arrays (pitch
+// >= rows), the rest into the COO arrays (room for coo_cap); returns the
+// COO count.
+template <typename V>
+inline int64_t ExportHYB(const dcsr::dcsr_matrix<V> &src, int32_t width, int64_t pitch, int32_t *ell_cols,
+                         V *ell_vals, int32_t *coo_rows, int32_t *coo_cols, V *coo_vals, int64_t coo_cap,
+                         void *stream = nullptr) {
+  int64_t n = 0;
+  dcsr::check(dcsr_to_hyb(src.handle(), width, pitch, ell_cols, ell_vals, coo_rows, coo_cols, coo_vals, coo_cap, &n,
+                          stream),
+              "ExportHYB");
+  return n;
+}
+
+// y = A x for a HYB matrix (reference device::spmv(hyb, x, y), include/spmv.h:36-94).
+template <typename V>
+inline void spmv(int32_t rows, int32_t width, int64_t pitch, const int32_t *ell_cols, const V *ell_vals,
+                 int64_t coo_nnz, const int32_t *coo_rows, const int32_t *coo_cols, const V *coo_vals, const V *x,
+                 V *y, void *stream = nullptr) {
+  dcsr::check(dcsr_hyb_spmv(rows, dcsr::dtype_of<V>::value, width, pitch, ell_cols, ell_vals, coo_nnz, coo_rows,
+                            coo_cols, coo_vals, x, y, 1.0, 0.0, stream),
+              "spmv(hyb)");
+}
+
+// cusp::krylov::cg(A, x, b) with cusp::monitor(b, max_iter, rel_tol, abs_tol)
+// (cusp/krylov/cg.h), on the DCSR matrix; returns the iteration count.
+template <typename V>
+inline int32_t cg(const dcsr::dcsr_matrix<V> &A, V *x, const V *b, int32_t max_iter = 500, double rel_tol = 1e-5,
+                  double abs_tol = 0.0, void *stream = nullptr) {
+  int32_t it = 0;
+  dcsr::check(dcsr_cg(A.handle(), b, x, max_iter, rel_tol, abs_tol, &it, nullptr, stream), "cg");
+  return it;
 }
 
 }  // namespace device

@@ -703,16 +703,29 @@ void or_count_sorted_indices(const int32_t *I, int64_t n, int32_t *X) {
 
 int64_t or_reduce_by_key(const int32_t *keys, const double *vals, int64_t n, int32_t dtype,
                          int32_t *out_keys, double *out_vals) {
-  int64_t w = 0;
-  for (int64_t i = 0; i < n; i++) {
-    double v = vround(dtype, vals[i]);
-    if (i > 0 && keys[i] == keys[i - 1]) {
-      out_vals[w - 1] = vadd(dtype, out_vals[w - 1], v);
-    } else {
-      out_keys[w] = keys[i];
-      out_vals[w] = v;
-      w++;
+  /* The library's stated order: a run is cut into pieces at its head and at
+   * every multiple of RBK_PIECE inside it; each piece is summed left to
+   * right, then the piece sums left to right.  (The reference's CTA
+   * reduce-by-key, include/reduce.inl:139-308, sums in a tree order of its
+   * own; it specifies none.) */
+  const int64_t RBK_PIECE = 256;
+  int64_t w = 0, i = 0;
+  while (i < n) {
+    int64_t e = i + 1;
+    while (e < n && keys[e] == keys[i]) e++;
+    double total = 0.0;
+    for (int64_t p = i; p < e;) {
+      int64_t pe = (p / RBK_PIECE + 1) * RBK_PIECE;
+      if (pe > e) pe = e;
+      double s = vround(dtype, vals[p]);
+      for (int64_t q = p + 1; q < pe; q++) s = vadd(dtype, s, vround(dtype, vals[q]));
+      total = p == i ? s : vadd(dtype, total, s);
+      p = pe;
     }
+    out_keys[w] = keys[i];
+    out_vals[w] = total;
+    w++;
+    i = e;
   }
   return w;
 }

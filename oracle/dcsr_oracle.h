@@ -5,7 +5,7 @@
  * in dcsr_b200/.  Only tests/, __graft_entry__.smoke() and bench.py's CPU
  * baseline leg may load it; the product path never links or calls it.
  *
- * It restates the reference's DCSR algorithms (Vizerai/DCSR, include/*.inl)
+ * It restates the reference's DCSR algorithms (Vizerai/DCSR, include/ *.inl)
  * with the canonical semantics the library states where the reference is
  * defective (no duplicate merge, no overflow guard, stale bins, bin-ordered
  * compaction).  Every function cites the reference lines it follows.
@@ -102,7 +102,9 @@ void or_spgemm_counts(const or_dcsr *A, const or_dcsr *B, int64_t *counts);
 
 /* X[I[n]] += 1 for sorted I (reference include/primitives.h:417-464). */
 void or_count_sorted_indices(const int32_t *I, int64_t n, int32_t *X);
-/* Reduce-by-key over sorted keys, left-to-right sums.  Returns unique count. */
+/* Reduce-by-key over sorted keys: each run summed in pieces of 256 keys (from
+ * its head and from each multiple of 256), left to right within a piece, then
+ * the piece sums left to right.  Returns the unique count. */
 int64_t or_reduce_by_key(const int32_t *keys, const double *vals, int64_t n, int32_t dtype,
                          int32_t *out_keys, double *out_vals);
 
