@@ -578,6 +578,26 @@ def replay_point(api, srv, trace, rate, n, seed, repeats, lo=0, hi=None):
     return pick
 
 
+def host_link_gbs(torch, dev, nbytes=1 << 30):
+    """Pinned host <-> device copy bandwidth (GB/s), best of 3 each way."""
+    h = torch.empty(nbytes, dtype=torch.uint8).pin_memory()
+    d = torch.empty(nbytes, dtype=torch.uint8, device=dev)
+    out = {}
+    for name, dst, src in (("h2d_gbs", d, h), ("d2h_gbs", h, d)):
+        best = None
+        for _ in range(3):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            dst.copy_(src, non_blocking=True)
+            e1.record()
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1)
+            best = ms if best is None else min(best, ms)
+        out[name] = round(nbytes / (best / 1e3) / 1e9, 1)
+    del h, d
+    return out
+
+
 def poisson_arrivals(rate_per_s, n, seed):
     rng = np.random.default_rng(seed)
     return np.cumsum(rng.exponential(1e6 / rate_per_s, n))
@@ -710,6 +730,13 @@ def served_part(args, dev, rank, local_rank):
                        "speedup_at_equal_p99": round(e2e["req_s"] / out["plain_host_buffers"]["slo_point"]["req_s"], 2)})
     out["e2e"]["h2d_bytes_per_request"] = int(h2d / N)
     out["e2e"]["d2h_bytes_per_request"] = int(d2h / N)
+    # the host link: pinned copies of 1 GiB each way, and the request rate it
+    # bounds the host-buffer form to (bytes per request / bandwidth, the two
+    # directions overlapping)
+    link = host_link_gbs(torch, dev)
+    bound = min(link["h2d_gbs"] * 1e9 / max(h2d / N, 1), link["d2h_gbs"] * 1e9 / max(d2h / N, 1))
+    out["e2e"]["host_link"] = {**link, "req_s_bound": round(bound, 1),
+                               "capacity_frac_of_bound": round(cap_h["req_s"] / bound, 3)}
     out["launches"] = int(best["kernel_launches"])
     out["clocks"] = clocks
     return out

@@ -1134,28 +1134,35 @@ __global__ void __launch_bounds__(RS_THREADS_, DCSR_K1_MINB) k_rows1(Src src) {
   const int64_t NC = src.units(P_CHUNKS), NM = src.units(P_MED) * RS_WARPS;
   const int64_t total = NC + NM;
   unsigned *ctr = src.ctr(0);
-  auto fetch = [&]() -> int64_t {
-    unsigned v = 0;
-    if (lane == 0) v = atomicAdd(ctr, 1u);
-    return (int64_t)__shfl_sync(FULL, v, 0);
+  // A unit number is taken by lane 0 with an atomic and broadcast only when
+  // it is needed, one unit later: the atomic's round trip overlaps a unit.
+  unsigned pend = 0;
+  auto fetch_issue = [&]() {
+    if (lane == 0) pend = atomicAdd(ctr, 1u);
   };
+  auto fetch_take = [&]() -> int64_t { return (int64_t)__shfl_sync(FULL, pend, 0); };
   // Units in flight per warp: cur (streamed step by step), nx (its
-  // descriptor loaded or in flight) and the number of the one after.  The
-  // loads of the next step are issued before the current step's x values
-  // are gathered, whether that step is the current unit's next or the next
-  // unit's first -- the stream does not stop at unit ends.
-  Unit1 cur = unit1_load<V>(src, fetch(), NC, NM, total, lane);
-  Unit1 nx = unit1_load<V>(src, fetch(), NC, NM, total, lane);
-  int64_t n2 = fetch();
-  V a[UN], an[UN];
-  int32_t col[UN], coln[UN];
+  // descriptor loaded or in flight) and the number of the one after.  Two
+  // register buffers take turns: the loads of the next step go into one
+  // while the current step's x values are gathered from the other (no copy
+  // between them, so nothing waits for a load before its data is used), and
+  // the next step may be the next unit's first -- the stream does not stop at
+  // unit ends.
+  fetch_issue();
+  Unit1 cur = unit1_load<V>(src, fetch_take(), NC, NM, total, lane);
+  fetch_issue();
+  Unit1 nx = unit1_load<V>(src, fetch_take(), NC, NM, total, lane);
+  fetch_issue();
+  V a0[UN], a1[UN];
+  int32_t k0[UN], k1[UN];
   int64_t c0 = 0, c1 = 0, o = 0;  // cur's range and the current step's offset in it
   if (streamed(cur)) {
     unit_range(cur, c0, c1);
-    if (cur.d.z >= 0) load_step<V, UN, OP>(src.item(cur.item).m, cur.d.z, c1 - c0, 0, lane, a, col);
+    if (cur.d.z >= 0) load_step<V, UN, OP>(src.item(cur.item).m, cur.d.z, c1 - c0, 0, lane, a0, k0);
   }
   double acc = op_init<double, OP>();
-  while (cur.u < total) {
+  // One step: consume (ca, cc), loading the following step into (na, nc).
+  auto step = [&](V(&ca)[UN], int32_t(&cc)[UN], V(&na)[UN], int32_t(&nc)[UN]) {
     bool advance = true;
     if (streamed(cur)) {
       const RowItem<V> &it = src.item(cur.item);
@@ -1164,32 +1171,32 @@ __global__ void __launch_bounds__(RS_THREADS_, DCSR_K1_MINB) k_rows1(Src src) {
         const double t = warp_comb<OP>(
             stream_chain<V, OP>(it.m.vals, it.m.cols, it.x, it.ldx, load_chain(it.m, cur.d.x), c0, c1, lane));
         finish_unit<V, OP>(it, cur, t, lane);
+        if (streamed(nx) && nx.d.z >= 0) {  // the next unit's first step, into the buffer consumed next
+          int64_t d0, d1;
+          unit_range(nx, d0, d1);
+          load_step<V, UN, OP>(src.item(nx.item).m, nx.d.z, d1 - d0, 0, lane, na, nc);
+        }
       } else {
         const int64_t n = c1 - c0;
         const bool last = o + W >= n;
         if (!last) {
-          load_step<V, UN, OP>(it.m, cur.d.z, n, o + W, lane, an, coln);
+          load_step<V, UN, OP>(it.m, cur.d.z, n, o + W, lane, na, nc);
         } else if (streamed(nx) && nx.d.z >= 0) {
           int64_t d0, d1;
           unit_range(nx, d0, d1);
-          load_step<V, UN, OP>(src.item(nx.item).m, nx.d.z, d1 - d0, 0, lane, an, coln);
+          load_step<V, UN, OP>(src.item(nx.item).m, nx.d.z, d1 - d0, 0, lane, na, nc);
         }
         P w = op_init<P, OP>();
 #pragma unroll
         for (int i = 0; i < UN; i++) {
           if (o + 32 * i + lane < n) {
             P t;
-            if constexpr (OP == OP_SPMV) t = mul_rn((P)a[i], (P)__ldg(it.x + (int64_t)col[i] * it.ldx));
-            else t = OP == OP_COUNT ? (P)1 : (P)a[i];
+            if constexpr (OP == OP_SPMV) t = mul_rn((P)ca[i], (P)__ldg(it.x + (int64_t)cc[i] * it.ldx));
+            else t = OP == OP_COUNT ? (P)1 : (P)ca[i];
             w = op_comb<P, OP>(w, t);
           }
         }
         acc = op_comb<double, OP>(acc, (double)w);
-#pragma unroll
-        for (int i = 0; i < UN; i++) {
-          a[i] = an[i];
-          col[i] = coln[i];
-        }
         if (last) {
           finish_unit<V, OP>(it, cur, warp_comb<OP>(acc), lane);
           acc = op_init<double, OP>();
@@ -1198,16 +1205,27 @@ __global__ void __launch_bounds__(RS_THREADS_, DCSR_K1_MINB) k_rows1(Src src) {
           advance = false;
         }
       }
+    } else if (streamed(nx) && nx.d.z >= 0) {  // a skipped unit: the next one's first step
+      int64_t d0, d1;
+      unit_range(nx, d0, d1);
+      load_step<V, UN, OP>(src.item(nx.item).m, nx.d.z, d1 - d0, 0, lane, na, nc);
     }
     if (advance) {
       cur = nx;
-      nx = unit1_load<V>(src, n2, NC, NM, total, lane);
-      n2 = fetch();
+      nx = unit1_load<V>(src, fetch_take(), NC, NM, total, lane);
+      fetch_issue();
       o = 0;
       if (streamed(cur)) unit_range(cur, c0, c1);
     }
+  };
+  while (cur.u < total) {
+    step(a0, k0, a1, k1);
+    if (cur.u >= total) break;
+    step(a1, k1, a0, k0);
   }
-  // the last warp to finish resets the counters for the next pass
+  // the last warp to finish resets the counters for the next pass (the
+  // atomic still pending in lane 0 belongs to nobody: every number past
+  // the end is discarded)
   if (lane == 0 && atomicAdd(ctr + 1, 1u) == gridDim.x * RS_WARPS - 1) {
     ctr[0] = 0;
     ctr[1] = 0;
@@ -1222,21 +1240,21 @@ __global__ void __launch_bounds__(RS_THREADS_, DCSR_K1B_MINB) k_rows1_blocks(Src
   const int lane = threadIdx.x & 31;
   const int64_t NB = src.units(P_BLOCKS) * RS_WARPS;
   unsigned *ctr = src.ctr(1);
-  auto fetch = [&]() -> int64_t {
-    unsigned v = 0;
-    if (lane == 0) v = atomicAdd(ctr, 1u);
-    return (int64_t)__shfl_sync(FULL, v, 0);
+  unsigned pend = 0;  // lane 0's atomic, broadcast one block later
+  auto fetch_issue = [&]() {
+    if (lane == 0) pend = atomicAdd(ctr, 1u);
   };
+  auto fetch_take = [&]() -> int64_t { return (int64_t)__shfl_sync(FULL, pend, 0); };
   // units numbered after the streamed ones (NC + NM): unit1_load decodes them as blocks
   const int64_t base = src.units(P_CHUNKS) + src.units(P_MED) * RS_WARPS, total = base + NB;
-  Unit1 cur = unit1_load<V>(src, base + fetch(), base, 0, total, lane);
-  int64_t n1 = fetch();
+  fetch_issue();
+  Unit1 cur = unit1_load<V>(src, base + fetch_take(), base, 0, total, lane);
+  fetch_issue();
   while (cur.u < total) {
-    const int64_t n2 = fetch();
-    const Unit1 nx = unit1_load<V>(src, base + n1, base, 0, total, lane);
+    const Unit1 nx = unit1_load<V>(src, base + fetch_take(), base, 0, total, lane);
+    fetch_issue();
     if (cur.kind == U1_BLOCK) short_block_k1<V, OP>(src.item(cur.item), cur.d, lane);
     cur = nx;
-    n1 = n2;
   }
   if (lane == 0 && atomicAdd(ctr + 1, 1u) == gridDim.x * RS_WARPS - 1) {
     ctr[0] = 0;
