@@ -143,7 +143,8 @@ def stream_part(args, dev, world):
     from dcsr_b200 import api
     from dcsr_b200 import workloads as W
 
-    n, rp, cols, vals, batches = W.rmat_stream(args.seed, rounds=16)
+    sc = args.stream_scale
+    n, rp, cols, vals, batches = W.rmat_stream(args.seed, scale=sc, rounds=16, batch=1 << sc)
     nnz0 = int(rp[-1])
     A = api.DcsrMatrix(n, n, torch.float32)
     A.from_csr(torch.from_numpy(rp).to(dev), torch.from_numpy(cols).to(dev), torch.from_numpy(vals).to(dev))
@@ -307,8 +308,8 @@ def stream_part(args, dev, world):
     del A
     torch.cuda.synchronize()
     return {
-        "workload": "R-MAT 2^20 rows, (a,b,c,d)=(.57,.19,.19,.05), mean degree 16, FP32; 16 batches x 1M triples, "
-                    "rows ~ current row length; step = update_sync + SpMV + row-sum + DCSR->CSR export",
+        "workload": f"R-MAT 2^{sc} rows, (a,b,c,d)=(.57,.19,.19,.05), mean degree 16, FP32; 16 batches x "
+                    f"2^{sc} triples, rows ~ current row length; step = update_sync + SpMV + row-sum + DCSR->CSR export",
         "req_s": round(world * args.steps / (total_ms / 1e3), 3),
         "req_s_host_buffers": round(args.steps / (e2e_ms / 1e3), 3),
         "ms_per_step": round(total_ms / args.steps, 4),
@@ -416,12 +417,15 @@ def batched_part(args, dev):
     api.pool_reserve(16 << 30)  # set-up: room for repairs to grow matrices into
     s = torch.cuda.Stream()
     batch = api.DcsrBatch(work, stream=s)
-    tuned = batch.autotune(s)  # row-class thresholds for this set (outputs untouched)
+    tuned = batch.autotune(s)  # row-class thresholds + short-row split for this set (outputs untouched)
+    split = batch.short_split()
     batch.capture(s)
     T = sum(sp["updates"] for sp in specs)
 
     repaired = [0]
+    grown = [0]
     repair_s = [0.0]
+    rejected = np.zeros(9, np.int64)  # rejections by status code, timed rounds
 
     def batched_round(i):
         for dst, src in zip(live, rounds[i]):
@@ -429,8 +433,10 @@ def batched_part(args, dev):
         batch.launch(s)
         st = batch.status(s)  # synchronises: the graph's work is done here
         t0 = time.perf_counter()
+        rejected[:] += np.bincount(np.asarray(st), minlength=9)[:9]
         if (st != 0).any():
             repaired[0] += batch.repair(st, s)
+        grown[0] += batch.grow(s)  # pools the run left > 7/8 full, ahead of the next round
         s.synchronize()
         repair_s[0] += time.perf_counter() - t0
 
@@ -441,8 +447,9 @@ def batched_part(args, dev):
         launches0 = api.launch_count()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(s)
-        repaired[0] = 0
+        repaired[0] = grown[0] = 0
         repair_s[0] = 0.0
+        rejected[:] = 0
         for i in range(reps):
             batched_round(warm + i)
         e1.record(s)
@@ -476,11 +483,15 @@ def batched_part(args, dev):
         "workload": f"{len(specs)} matrices, rows log-uniform [1k,256k], mean degree U[4,64], FP32, "
                     f"{nnz / 1e6:.0f}M nnz; per matrix an update (log-uniform 100..100k, {T / 1e6:.2f}M triples "
                     "in all) + SpMV with k in {1,2,4,8}",
-        "autotuned_row_classes": {"short_max": tuned[0], "long_min": tuned[1], "spmv_pass_us": round(tuned[2], 1)},
+        "autotuned_row_classes": {"short_max": tuned[0], "long_min": tuned[1], "short_split": split,
+                                  "spmv_pass_us": round(tuned[2], 1)},
         "batched_ms": round(batched_ms, 3), "plain_ms": round(plain_ms, 3),
         "speedup": round(plain_ms / batched_ms, 2),
         "batched_kernel_launches": round(batched_launches, 1), "plain_kernel_launches": round(plain_launches, 1),
         "repairs_per_round": repairs_per_round, "repair_ms_per_round": round(repair_ms_per_round, 3),
+        "pools_grown_ahead_per_round": grown[0] / reps,
+        "rejections_per_round": {"pool_exhausted": round(float(rejected[1]) / reps, 2),
+                                 "layer_overflow": round(float(rejected[2]) / reps, 2)},
         "updates_per_s_batched": round(T / (batched_ms / 1e3), 1),
     }
 
@@ -984,6 +995,7 @@ def main():
     ap.add_argument("--batched-reps", type=int, default=5)
     ap.add_argument("--ref-requests", type=int, default=400)
     ap.add_argument("--skip-stream", action="store_true")
+    ap.add_argument("--stream-scale", type=int, default=20, help="profiling: log2 rows of the update-stream matrix")
     ap.add_argument("--skip-batched", action="store_true")
     ap.add_argument("--skip-spgemm", action="store_true")
     ap.add_argument("--spgemm-reps", type=int, default=5)

@@ -113,6 +113,7 @@ _SIGS = {
     "dcsr_batch_grow": (_i32, [_vp, C.POINTER(_i32), _vp]),
     "dcsr_batch_destroy": (_i32, [_vp]),
     "dcsr_batch_autotune": (_i32, [_vp, _vp, C.POINTER(_i32), C.POINTER(_i32), C.POINTER(C.c_float)]),
+    "dcsr_batch_short_split": (_i32, [_vp, C.POINTER(_i32)]),
     "dcsr_set_row_classes": (_i32, [_vp, _i32, _i32]),
     "dcsr_get_row_classes": (_i32, [_vp, C.POINTER(_i32), C.POINTER(_i32)]),
     "dcsr_server_default_opts": (None, [_vp]),
@@ -519,12 +520,19 @@ class DcsrBatch:
         return st
 
     def autotune(self, stream=None):
-        """Pick the row-class thresholds of the batch's matrices by timing
-        their SpMV passes; returns (short_max, long_min, us per run)."""
+        """Pick the row-class thresholds of the batch's matrices and the
+        short-row split of its k >= 2 passes by timing their SpMV passes;
+        returns (short_max, long_min, us per run).  Capture after this."""
         sm, lm, us = _i32(), _i32(), C.c_float()
         _check(lib().dcsr_batch_autotune(self.h, _stream(stream), C.byref(sm), C.byref(lm), C.byref(us)),
                "dcsr_batch_autotune")
         return sm.value, lm.value, us.value
+
+    def short_split(self) -> int:
+        """Warps per 32-row short-row block chosen by autotune (0: automatic)."""
+        v = _i32(0)
+        _check(lib().dcsr_batch_short_split(self.h, C.byref(v)), "dcsr_batch_short_split")
+        return int(v.value)
 
     def grow(self, stream=None) -> int:
         """After status(): grow pools that the last run left more than 7/8

@@ -196,7 +196,7 @@ int BatchCore::plan(const dcsr_batch_item *its, int n, cudaStream_t s, bool all_
     poff += 3 * (g.idx.size() + 1) + 2;  // unit prefixes + the k = 1 passes' counter words
     int64_t blocks = 0;
     for (int i : g.idx) blocks += div_up(its[i].matrix->n_rows, 32);
-    g.split = short_split(blocks, g.k);
+    g.split = split_force > 0 && g.k >= 2 ? split_force : short_split(blocks, g.k);
   }
   img_bytes = off;
   if (img_bytes > img_cap) {
@@ -373,6 +373,7 @@ struct dcsr_batch_s {
   BatchCore core;
   long long *status_host = nullptr;  // pinned [2*count]
   bool status_read = false;          // status_host holds the last status read (for dcsr_batch_grow)
+  std::vector<long long> last_need;  // per item: pool top needed at the previous grow check (-1: none)
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   uint64_t graph_kernels = 0;  // kernel nodes of the captured graph
@@ -485,13 +486,24 @@ int dcsr_batch_grow(dcsr_batch b, int32_t *grown, void *stream) {
   if (!b) return DCSR_BAD_ARG;
   int n = 0;
   if (b->status_read) {  // the words of the last status read: (status, pool top needed) per update
+    b->last_need.resize(b->core.count, -1);
     for (int i = 0; i < b->core.count; i++) {
       const int j = b->core.upd_of[i];
-      if (j < 0 || b->status_host[2 * j] != DCSR_OK) continue;
+      if (j < 0 || b->status_host[2 * j] != DCSR_OK) {
+        b->last_need[i] = -1;  // repaired per call: its pool top moved outside the batch
+        continue;
+      }
       dcsr_handle h = b->core.items[i].matrix;
       const long long need = b->status_host[2 * j + 1];
-      if (h->pool_cap - need < h->pool_cap / 8) {
-        DCSR_TRY(reserve(h, grow_target(h, need), (cudaStream_t)stream));
+      // room for the larger of an eighth of the pool and two more runs
+      // growing it as much as the last one did (the same item's next update
+      // has as many triples)
+      const long long prev = b->last_need[i];
+      const long long step = prev >= 0 && need > prev ? need - prev : 0;
+      b->last_need[i] = need;
+      const long long room = h->pool_cap / 8 > 2 * step ? h->pool_cap / 8 : 2 * step;
+      if (h->pool_cap - need < room) {
+        DCSR_TRY(reserve(h, grow_target(h, need + room), (cudaStream_t)stream));  // keeps the pool top
         n++;
       }
     }
@@ -544,6 +556,7 @@ int dcsr_batch_autotune(dcsr_batch b, void *stream, int32_t *short_max, int32_t 
     items.push_back(t);
   }
   int32_t best_s = c.items[0].matrix->short_max, best_l = c.items[0].matrix->long_min;
+  int best_split = 0;
   float best = -1.0f;
   int st = DCSR_OK;
   if (!items.empty()) {
@@ -551,26 +564,35 @@ int dcsr_batch_autotune(dcsr_batch b, void *stream, int32_t *short_max, int32_t 
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
+    // three timed runs (after one warm-up) of the SpMV pass under one setting
+    auto measure = [&](int32_t sm, int32_t lm, int split, float &sum) -> int {
+      for (auto &it : items) dcsr_set_row_classes(it.matrix, sm, lm);
+      tmp.split_force = split;
+      DCSR_TRY(tmp.plan(items.data(), (int)items.size(), s, true));
+      DCSR_TRY(tmp.upload(s, true));
+      DCSR_TRY(tmp.reserve_scratch(s));
+      DCSR_TRY(tmp.enqueue(s));
+      sum = 0.0f;
+      for (int rep = 0; rep < 3; rep++) {
+        cudaEventRecord(e0, s);
+        DCSR_TRY(tmp.enqueue(s));
+        cudaEventRecord(e1, s);
+        cudaEventSynchronize(e1);
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        sum += ms;
+      }
+      return DCSR_OK;
+    };
+    // row-class thresholds under the automatic split, then the split of the
+    // k >= 2 groups' short-row blocks under the best thresholds (the split
+    // changes which warp takes a row's lane group, never a row's result)
     const int32_t shorts[] = {32, 64, 128};
     const int32_t longs[] = {512, 1024, 4096, 16384};
     for (int32_t sm : shorts) {
       for (int32_t lm : longs) {
-        for (auto &it : items) dcsr_set_row_classes(it.matrix, sm, lm);
-        if ((st = tmp.plan(items.data(), (int)items.size(), s, true)) != DCSR_OK) break;
-        if ((st = tmp.upload(s, true)) != DCSR_OK) break;
-        if ((st = tmp.reserve_scratch(s)) != DCSR_OK) break;
-        if ((st = tmp.enqueue(s)) != DCSR_OK) break;  // warm-up
         float sum = 0.0f;
-        for (int rep = 0; rep < 3 && st == DCSR_OK; rep++) {
-          cudaEventRecord(e0, s);
-          st = tmp.enqueue(s);
-          cudaEventRecord(e1, s);
-          cudaEventSynchronize(e1);
-          float ms = 0.0f;
-          cudaEventElapsedTime(&ms, e0, e1);
-          sum += ms;
-        }
-        if (st != DCSR_OK) break;
+        if ((st = measure(sm, lm, 0, sum)) != DCSR_OK) break;
         if (best < 0.0f || sum < best) {
           best = sum;
           best_s = sm;
@@ -579,10 +601,27 @@ int dcsr_batch_autotune(dcsr_batch b, void *stream, int32_t *short_max, int32_t 
       }
       if (st != DCSR_OK) break;
     }
+    bool has_k2 = false;
+    for (const auto &g : tmp.groups) has_k2 |= g.k >= 2;
+    for (int split = 1; st == DCSR_OK && has_k2 && split <= 8; split *= 2) {
+      float sum = 0.0f;
+      if ((st = measure(best_s, best_l, split, sum)) != DCSR_OK) break;
+      if (sum < best) {
+        best = sum;
+        best_split = split;
+      }
+    }
     cudaStreamSynchronize(s);
     tmp.release();
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
+  }
+  c.split_force = best_split;
+  for (auto &g : c.groups) {
+    if (g.k < 2) continue;
+    int64_t blocks = 0;
+    for (int i : g.idx) blocks += div_up(c.items[i].matrix->n_rows, 32);
+    g.split = best_split > 0 ? best_split : short_split(blocks, g.k);
   }
   for (auto &it : c.items) dcsr_set_row_classes(it.matrix, best_s, best_l);
   if (yscratch) cudaFreeAsync(yscratch, s);
@@ -591,6 +630,12 @@ int dcsr_batch_autotune(dcsr_batch b, void *stream, int32_t *short_max, int32_t 
   if (short_max) *short_max = best_s;
   if (long_min) *long_min = best_l;
   if (best_us) *best_us = best < 0.0f ? 0.0f : 1e3f * best / 3.0f;
+  return DCSR_OK;
+}
+
+int dcsr_batch_short_split(dcsr_batch b, int32_t *split) {
+  if (!b || !split) return DCSR_BAD_ARG;
+  *split = b->core.split_force;
   return DCSR_OK;
 }
 

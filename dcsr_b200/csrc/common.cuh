@@ -330,6 +330,20 @@ struct Chain {
   }
 };
 
+// The chain of the row owned by lane `owner` (every lane loaded its own row's
+// chain; a pass hands it to the lanes that work on that row).
+__device__ __forceinline__ Chain shfl_chain(const Chain &own, int owner) {
+  Chain c;
+#pragma unroll
+  for (int l = 0; l < MAX_SEGS; l++) {
+    c.st[l] = __shfl_sync(FULL, own.st[l], owner);
+    c.cp[l] = __shfl_sync(FULL, own.cp[l], owner);
+  }
+  c.ns = __shfl_sync(FULL, own.ns, owner);
+  c.total = 0;
+  return c;
+}
+
 // All layer pairs are loaded independently (no dependent load chain), then
 // the chain is the leading run of linked layers.
 template <typename V>

@@ -132,6 +132,7 @@ struct BatchCore {
     size_t pref_off = 0;   // unit-prefix offset in pref
   };
   int count = 0, dtype = 0, mode = 0;
+  int split_force = 0;  // > 0: warps per short-row block of every k >= 2 group (else short_split)
   std::vector<dcsr_batch_item> items;
   int64_t T = 0, R = 0;
   int rb = 1, cb = 1;

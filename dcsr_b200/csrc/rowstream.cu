@@ -390,25 +390,18 @@ __device__ __forceinline__ void next_layer(const Mat<V> &m, const RowBlock &b, i
   }
 }
 
-// Row of each lane's entry in the window [w0, w0+32): M has bit p set where a
-// row starts at w0+p; the lane's row is the k-th starting row (k = starts at
-// positions <= lane) or, before the first start, the row running into the
-// window.  Lanes past the stream's end get the last row (callers mask them).
-struct WinMap {
-  int j;
-  unsigned M;
-};
-__device__ __forceinline__ WinMap window_map(int32_t w0, int32_t excl, int32_t incl, int32_t len, int lane) {
-  const bool starts = len > 0 && excl >= w0 && excl < w0 + 32;
-  const bool runs_in = len > 0 && excl < w0 && incl > w0;
-  const unsigned O = __ballot_sync(FULL, starts);
-  const unsigned M = __reduce_or_sync(FULL, starts ? (1u << (excl - w0)) : 0u);
-  const unsigned C = __ballot_sync(FULL, runs_in);
-  const int k = __popc(M & (0xffffffffu >> (31 - lane)));
-  WinMap r;
-  r.j = k == 0 ? (C ? __ffs(C) - 1 : 0) : (int)__fns(O, 0, k);
-  r.M = M;
-  return r;
+// The lane whose row holds block position p: the last lane whose row starts
+// at or before p (excl, the rows' exclusive offsets, never decreases across
+// the lanes; an empty row shares its offset with the next row, so the last
+// lane found is the non-empty one), by a binary search over the lanes.
+__device__ __forceinline__ int owner_lane(int32_t excl, int32_t p) {
+  int lo = 0;
+#pragma unroll
+  for (int st = 16; st > 0; st >>= 1) {
+    const int c = lo + st;  // <= 31
+    if (__shfl_sync(FULL, excl, c) <= p) lo = c;
+  }
+  return lo;
 }
 
 // Lanes per row for a block of 32 short rows: the largest power of two
@@ -417,20 +410,6 @@ __device__ __forceinline__ WinMap window_map(int32_t w0, int32_t excl, int32_t i
 __device__ __forceinline__ int group_width(int32_t total) {
   const int32_t mean = total >> 5;
   return mean < 8 ? 1 : mean < 16 ? 2 : mean < 32 ? 4 : mean < 64 ? 8 : 16;
-}
-
-// The chain of the row owned by lane `owner` (every lane loaded its own row's
-// chain at the block's start; a pass hands it to the row's group).
-__device__ __forceinline__ Chain shfl_chain(const Chain &own, int owner) {
-  Chain c;
-#pragma unroll
-  for (int l = 0; l < MAX_SEGS; l++) {
-    c.st[l] = __shfl_sync(FULL, own.st[l], owner);
-    c.cp[l] = __shfl_sync(FULL, own.cp[l], owner);
-  }
-  c.ns = __shfl_sync(FULL, own.ns, owner);
-  c.total = 0;
-  return c;
 }
 
 // Visit the logical entries [0, len) of a row: lane j of a G-lane group takes
@@ -618,17 +597,17 @@ __device__ __forceinline__ void short_block_k1(const RowItem<V> &it, int4 d0, in
     const int32_t E = __shfl_sync(FULL, incl, 31);
     for (int32_t base = 0; base < E; base += 32 * U) {
       int32_t q[U];
-      unsigned Mw[U];
+      int32_t rs[U];  // the window lane where the lane's row starts (0: it runs in from before)
       bool ok[U];
 #pragma unroll
       for (int i = 0; i < U; i++) {
-        const int32_t w0 = base + 32 * i;
-        const WinMap wm = window_map(w0, excl, incl, len_l, lane);
-        const int32_t ej = __shfl_sync(FULL, excl, wm.j);
-        const int32_t sj = __shfl_sync(FULL, st_l, wm.j);
-        ok[i] = w0 + lane < E;
-        Mw[i] = wm.M;
-        q[i] = sj + (ok[i] ? w0 + lane - ej : 0);
+        const int32_t w0 = base + 32 * i, p = w0 + lane;
+        const int j = owner_lane(excl, p);
+        const int32_t ej = __shfl_sync(FULL, excl, j);
+        const int32_t sj = __shfl_sync(FULL, st_l, j);
+        ok[i] = p < E;
+        rs[i] = ej > w0 ? ej - w0 : 0;
+        q[i] = sj + (ok[i] ? p - ej : 0);
       }
       V a[U];
       int32_t col[U];
@@ -644,13 +623,12 @@ __device__ __forceinline__ void short_block_k1(const RowItem<V> &it, int4 d0, in
           if constexpr (OP == OP_SPMV) c = mul_rn((P)a[i], (P)__ldg(x + (int64_t)col[i] * it.ldx));
           else c = OP == OP_COUNT ? (P)1 : (P)a[i];
         }
-        // segmented inclusive scan: lanes p-d and p share a row unless a
-        // row starts in (p-d, p] (bit test on the window's start mask)
+        // segmented inclusive scan: lanes p-d and p share a row when p-d is
+        // at or past the start of p's row in this window
 #pragma unroll
         for (int d = 1; d < 32; d <<= 1) {
-          const bool same = lane >= d && ((Mw[i] >> (lane - d + 1)) & ((1u << d) - 1u)) == 0;
           const P co = __shfl_up_sync(FULL, c, d);
-          if (same) c = op_comb<P, OP>(c, co);
+          if (lane - d >= rs[i]) c = op_comb<P, OP>(c, co);
         }
         // lane j collects the tail of its row's run in this window
         const int32_t w0 = base + 32 * i;
@@ -1352,13 +1330,13 @@ __global__ void __launch_bounds__(RS_THREADS_) k_rows_copy(RowItem<V> it, const 
 #pragma unroll
           for (int i = 0; i < U; i++) {
             const int32_t w0 = base + 32 * i;
-            const WinMap wm = window_map(w0, excl, incl, len_l, lane);
-            const int32_t ej = __shfl_sync(FULL, excl, wm.j);
-            const int32_t sj = __shfl_sync(FULL, st_l, wm.j);
-            const int64_t dj = __shfl_sync(FULL, dl, wm.j);
+            const int j = owner_lane(excl, w0 + lane);
+            const int32_t ej = __shfl_sync(FULL, excl, j);
+            const int32_t sj = __shfl_sync(FULL, st_l, j);
+            const int64_t dj = __shfl_sync(FULL, dl, j);
             const bool ok = w0 + lane < E;
             const int32_t off = ok ? w0 + lane - ej : 0;
-            jw[i] = ok ? wm.j : -1;
+            jw[i] = ok ? j : -1;
             q[i] = (int64_t)sj + off;
             dst[i] = dj + off;
           }

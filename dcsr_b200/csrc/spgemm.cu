@@ -102,6 +102,94 @@ __device__ __forceinline__ int64_t sg_expand(const Mat<V> &A, const Mat<V> &B, i
   return pos;
 }
 
+// Sort keys of the warp class: (column, product index p < 256) packed into
+// 32 bits when columns fit in 24 bits, else into 64.
+template <typename K>
+struct SgKey {
+  static constexpr int S = sizeof(K) == 4 ? 8 : 32;
+  __device__ __forceinline__ static K make(int32_t col, int p) { return ((K)(uint32_t)col << S) | (K)p; }
+  __device__ __forceinline__ static int32_t col(K k) { return (int32_t)(k >> S); }
+  __device__ __forceinline__ static uint32_t idx(K k) { return (uint32_t)(k & ((K(1) << S) - 1)); }
+};
+
+// The warp class's expand (P_i <= 256): row i's A entries are taken 32 at
+// a time, one per lane, each lane loading its entry's column k and value,
+// then B row k's length and segments, side by side (no load waits on another
+// entry's); the B-row lengths are scanned into product offsets, and lane l
+// produces products q = l, l + 32, ... of the group: the entry owning q is
+// found by a binary search over the lanes' offsets, and all B loads of the
+// group are issued before the first is used.  Same keys and products as
+// sg_expand (product p = the row's p-th product in A-entry-major order).
+template <typename V, typename K>
+__device__ __forceinline__ int sg_expand_warp(const Mat<V> &A, const Mat<V> &B, int64_t i, int lane, K *key,
+                                              V *prod) {
+  constexpr int H = 4;
+  const int32_t LA = A.row_sizes[i];
+  const Chain ca = load_chain_used(A, (int32_t)i, LA);
+  int base = 0;
+  for (int32_t e0 = 0; e0 < LA; e0 += 32) {
+    const int nE = LA - e0 < 32 ? LA - e0 : 32;
+    int32_t kb = 0, lb = 0;
+    V a = V(0);
+    if (lane < nE) {
+      const int64_t qa = ca.phys(e0 + lane);
+      kb = A.cols[qa];
+      a = A.vals[qa];
+      lb = B.row_sizes[kb];
+    }
+    const Chain cb = load_chain_used(B, kb, lb);
+    const int incl = warp_incl_scan(lb);
+    const int pos = incl - lb;
+    const int tot = __shfl_sync(FULL, incl, 31);  // base + tot <= P_i <= SG_WARP_MAX
+    // products in groups of H per lane: every B load of a group in flight at once
+    for (int t0 = 0; t0 * 32 < tot; t0 += H) {
+      int own[H];
+      int32_t bc[H];
+      V bv[H];
+#pragma unroll
+      for (int h = 0; h < H; h++) {
+        const int q = (t0 + h) * 32 + lane;
+        own[h] = 0;
+        bc[h] = 0;
+        bv[h] = V(0);
+        if ((t0 + h) * 32 < tot) {  // warp-uniform
+          int lo = 0;  // the last entry (< nE) whose offset is <= q: it owns q
+#pragma unroll
+          for (int st = 16; st > 0; st >>= 1) {
+            const int c = lo + st;  // <= 31
+            const int pc = __shfl_sync(FULL, pos, c);
+            if (c < nE && pc <= q) lo = c;
+          }
+          own[h] = lo;
+          const Chain co = shfl_chain(cb, lo);
+          const int pj = __shfl_sync(FULL, pos, lo);
+          if (q < tot) {
+            const int64_t qb = co.phys(q - pj);
+            bc[h] = B.cols[qb];
+            bv[h] = B.vals[qb];
+          }
+        }
+      }
+#pragma unroll
+      for (int h = 0; h < H; h++) {
+        const int q = (t0 + h) * 32 + lane;
+        if ((t0 + h) * 32 < tot) {
+          const V ao = __shfl_sync(FULL, a, own[h]);
+          if (q < tot) {
+            key[base + q] = SgKey<K>::make(bc[h], base + q);
+            V pr;
+            if constexpr (sizeof(V) == 4) pr = __fmul_rn(ao, bv[h]);
+            else pr = __dmul_rn(ao, bv[h]);
+            prod[base + q] = pr;
+          }
+        }
+      }
+    }
+    base += tot;
+  }
+  return base;
+}
+
 __device__ __forceinline__ int next_pow2(int x) {
   int p = 32;
   while (p < x) p <<= 1;
@@ -109,15 +197,15 @@ __device__ __forceinline__ int next_pow2(int x) {
 }
 
 // Bitonic sort of n2 (power of two) keys by `nthr` threads; sync() between steps.
-template <typename Sync>
-__device__ __forceinline__ void bitonic(unsigned long long *key, int n2, int tid, int nthr, Sync sync) {
+template <typename K, typename Sync>
+__device__ __forceinline__ void bitonic(K *key, int n2, int tid, int nthr, Sync sync) {
   for (int k = 2; k <= n2; k <<= 1)
     for (int j = k >> 1; j > 0; j >>= 1) {
       for (int t = tid; t < (n2 >> 1); t += nthr) {
         const int i = ((t & ~(j - 1)) << 1) | (t & (j - 1));
         const int l = i + j;
         const bool up = (i & k) == 0;
-        const unsigned long long a = key[i], b = key[l];
+        const K a = key[i], b = key[l];
         if ((a > b) == up) {
           key[i] = b;
           key[l] = a;
@@ -128,23 +216,24 @@ __device__ __forceinline__ void bitonic(unsigned long long *key, int n2, int tid
 }
 
 // Warp per row, P_i <= 256.
-template <typename V>
+template <typename V, typename K>
 __global__ void __launch_bounds__(SG_THREADS) k_sg_warp(Mat<V> A, Mat<V> B, const unsigned *rows,
                                                         const long long *starts, const long long *ub, int32_t *tcol,
                                                         V *tval, long long *ucnt) {
-  __shared__ unsigned long long skey[SG_THREADS / 32][SG_WARP_MAX];
+  using KO = SgKey<K>;
+  __shared__ K skey[SG_THREADS / 32][SG_WARP_MAX];
   __shared__ V sprod[SG_THREADS / 32][SG_WARP_MAX];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int64_t b = starts[SG_WARP], e = starts[SG_WARP + 1];
   const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
   const unsigned lt = (1u << lane) - 1u;
-  unsigned long long *key = skey[w];
+  K *key = skey[w];
   V *prod = sprod[w];
   for (int64_t it = b + (((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5); it < e; it += nw) {
     const int64_t i = rows[it];
-    const int P = (int)sg_expand(A, B, i, lane, 32, key, prod);
+    const int P = sg_expand_warp(A, B, i, lane, key, prod);
     const int n2 = next_pow2(P);
-    for (int t = P + lane; t < n2; t += 32) key[t] = ~0ull;
+    for (int t = P + lane; t < n2; t += 32) key[t] = ~K(0);
     __syncwarp();
     bitonic(key, n2, lane, 32, []() { __syncwarp(); });
     const int64_t base = ub[i];
@@ -152,14 +241,14 @@ __global__ void __launch_bounds__(SG_THREADS) k_sg_warp(Mat<V> A, Mat<V> B, cons
     for (int c0 = 0; c0 < P; c0 += 32) {
       const int idx = c0 + lane;
       const bool valid = idx < P;
-      const unsigned long long k = valid ? key[idx] : 0;
-      const bool head = valid && (idx == 0 || (key[idx - 1] >> 32) != (k >> 32));
+      const K k = valid ? key[idx] : K(0);
+      const bool head = valid && (idx == 0 || KO::col(key[idx - 1]) != KO::col(k));
       const unsigned hm = __ballot_sync(FULL, head);
       if (head) {
-        V v = prod[(uint32_t)k];
-        for (int j = idx + 1; j < P && (key[j] >> 32) == (k >> 32); j++) v = v + prod[(uint32_t)key[j]];
+        V v = prod[KO::idx(k)];
+        for (int j = idx + 1; j < P && KO::col(key[j]) == KO::col(k); j++) v = v + prod[KO::idx(key[j])];
         const int64_t o = base + heads + __popc(hm & lt);
-        tcol[o] = (int32_t)(k >> 32);
+        tcol[o] = KO::col(k);
         tval[o] = v;
       }
       heads += __popc(hm);
@@ -345,7 +434,7 @@ static int spgemm_impl(dcsr_handle hA, dcsr_handle hB, dcsr_handle hC, cudaStrea
   DCSR_CUDA(cudaMallocAsync((void **)&ucnt, sizeof(long long) * (n + 2), s));
   DCSR_CUDA(cudaMemsetAsync(ucnt, 0, sizeof(long long) * (n + 2), s));
   const size_t cta_smem = SG_CTA_MAX * (sizeof(unsigned long long) + sizeof(V));
-  static const int g_warp = persistent_grid((const void *)k_sg_warp<double>, SG_THREADS, 0);
+  static const int g_warp = persistent_grid((const void *)k_sg_warp<double, unsigned long long>, SG_THREADS, 0);
   static const int g_cta = [] {  // once, thread-safely: the CTA kernels' shared-memory limit, then their grid
     cudaFuncSetAttribute(k_sg_cta<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)(SG_CTA_MAX * (sizeof(unsigned long long) + sizeof(float))));
@@ -354,8 +443,13 @@ static int spgemm_impl(dcsr_handle hA, dcsr_handle hB, dcsr_handle hC, cudaStrea
     return persistent_grid((const void *)k_sg_cta<double>, SG_THREADS,
                            SG_CTA_MAX * (sizeof(unsigned long long) + sizeof(double)));
   }();
-  if (host[SG_WARP + 1] > host[SG_WARP])
-    DCSR_LAUNCH(k_sg_warp<V>, g_warp, SG_THREADS, 0, s, A, B, r0, starts, ub, tcol, tval, ucnt);
+  if (host[SG_WARP + 1] > host[SG_WARP]) {
+    if (hB->n_cols <= (1 << 24))  // (column, p) in 32-bit keys
+      DCSR_LAUNCH((k_sg_warp<V, unsigned>), g_warp, SG_THREADS, 0, s, A, B, r0, starts, ub, tcol, tval, ucnt);
+    else
+      DCSR_LAUNCH((k_sg_warp<V, unsigned long long>), g_warp, SG_THREADS, 0, s, A, B, r0, starts, ub, tcol, tval,
+                  ucnt);
+  }
   if (host[SG_CTA + 1] > host[SG_CTA])
     DCSR_LAUNCH(k_sg_cta<V>, g_cta, SG_THREADS, cta_smem, s, A, B, r0, starts, ub, tcol, tval, ucnt);
   Arena gg;

@@ -15,8 +15,9 @@
 //   check    per matrix: pool / layer / index verdict -> go flag  k_check
 //   apply    existing columns in place (thread per group), then per row
 //            the in-place shift + inserts (8- or 32-lane sub-warps)
-//   relocate rows whose in-place shift would exceed reloc_min are merged
-//            out of place into a fresh segment, tile-parallel      k_relocate
+//   relocate rows whose in-place shift would exceed reloc_min, and rows
+//            that outgrow a chain already max_segs long, are merged out
+//            of place into a fresh segment, tile-parallel          k_relocate
 //   finish   chain reset of relocated rows, new pool tops          k_finish
 // A rejected matrix (status != OK) is left untouched; the others proceed.
 //
@@ -285,10 +286,17 @@ __global__ void k_row_plan(Src src, int64_t T, const long long *gstat, const int
     } else {
       big = mnew > 0 && L - ins0 > SMALL_AFF;
       if (nl > ch.total) {
-        cap = align_up(policy_cap(m.o, nl) - ch.total, m.o.align);
         layer = ch.total == 0 ? 0 : ch.ns;
-        if (layer >= m.max_segs)
-          atomicOr((unsigned long long *)&src.st(i)[ST_AUX], (unsigned long long)AUX_LAYER_OVF);
+        if (layer >= m.max_segs) {
+          // every layer in use: the row is merged out of place into one
+          // fresh segment of policy_cap(nl) (chain reset), as a relocation
+          reloc = 1;
+          layer = 0;
+          big = 0;
+          cap = policy_cap(m.o, nl);
+        } else {
+          cap = align_up(policy_cap(m.o, nl) - ch.total, m.o.align);
+        }
       }
     }
     tcap[t] = cap;

@@ -40,7 +40,7 @@ enum { DCSR_MERGE = 0, DCSR_APPEND = 1 };
 typedef enum {
   DCSR_OK = 0,
   DCSR_POOL_EXHAUSTED = 1, /* update rejected: pool too small (matrix unchanged) */
-  DCSR_LAYER_OVERFLOW = 2, /* update rejected: a row needs > max_segs segments */
+  DCSR_LAYER_OVERFLOW = 2, /* APPEND-mode update rejected: a row needs > max_segs segments */
   DCSR_BAD_INDEX = 3,      /* an input row/column index is out of range */
   DCSR_OOM = 4,            /* device allocation failed */
   DCSR_BAD_ARG = 5,        /* invalid argument (null handle, size, dtype ...) */
@@ -68,8 +68,11 @@ typedef struct {
   int32_t min_spare;  /* minimum pool spare, entries */
   int32_t mode;       /* DCSR_MERGE (canonical) or DCSR_APPEND (reference) */
   int32_t reloc_min;  /* MERGE: a row whose in-place merge would shift more than
-                         reloc_min entries is instead merged out of place into
-                         one fresh segment of policy_cap(new_len) (chain reset) */
+                         reloc_min entries -- or that outgrows a chain already
+                         max_segs segments long -- is instead merged out of
+                         place into one fresh segment of policy_cap(new_len)
+                         (chain reset); MERGE updates therefore never report
+                         LAYER_OVERFLOW */
 } dcsr_opts;
 
 /* Snapshot of a matrix's device layout (device pointers). */
@@ -280,22 +283,33 @@ int dcsr_batch_launch(dcsr_batch b, void *stream);
 /* Per-matrix statuses of the last run (synchronises, clears them). */
 int dcsr_batch_status(dcsr_batch b, int32_t *statuses, void *stream);
 /* After dcsr_batch_status: grow the pool of every matrix whose accepted
- * update left it more than 7/8 full (stream-ordered, the server's rule), so
- * the next run's update is not rejected for space and needs no repair.
- * Contents, row lengths and segment tables are unchanged; only the pool
- * capacity grows.  *grown (may be NULL) = matrices grown. */
+ * update left less room than the larger of an eighth of its pool and twice
+ * the pool top's growth since the previous call (its next update has as
+ * many triples), stream-ordered, so the next run's update is not rejected
+ * for space and needs no repair.  Contents, row lengths, segment tables and
+ * the pool top are unchanged; only the pool capacity grows.  *grown (may be
+ * NULL) = matrices grown. */
 int dcsr_batch_grow(dcsr_batch b, int32_t *grown, void *stream);
 /* For matrices whose update was rejected: apply the repair policy
  * (compact, grow) and redo their update and SpMV per call.  Returns the
  * number of matrices repaired in *repaired (may be NULL). */
 int dcsr_batch_repair(dcsr_batch b, const int32_t *statuses, int32_t *repaired, void *stream);
 int dcsr_batch_destroy(dcsr_batch b);
-/* Autotune the row-class thresholds of the batch's matrices: time the
- * batch's schedule rebuild + SpMV passes for a grid of candidates (outputs to
- * scratch: the matrices' contents and the items' y are not touched), set the
- * fastest on every matrix and return it (best_us: its time per run).
+/* Autotune the batch's row schedule: time the batch's schedule rebuild +
+ * SpMV passes (outputs to scratch: the matrices' contents and the items' y
+ * are not touched) for a grid of row-class thresholds (short_max x long_min),
+ * then, under the best of those, for the warps per 32-row short-row block of
+ * the k >= 2 passes (1, 2, 4, 8 against the automatic rule).  Sets the
+ * fastest thresholds on every matrix and the split on the batch (a captured
+ * graph must be captured again to use them), returns the thresholds
+ * (best_us: the best time per run).  The split never changes a result; the
+ * thresholds move rows between classes, which sum in different orders.
  * Synchronises. */
 int dcsr_batch_autotune(dcsr_batch b, void *stream, int32_t *short_max, int32_t *long_min, float *best_us);
+/* The short-row split the autotuner chose (0: the automatic rule, which
+ * doubles warps per block up to 8 while the blocks stay under 12 warps per
+ * SM). */
+int dcsr_batch_short_split(dcsr_batch b, int32_t *split);
 
 /* ------------------------------------------------------------ serving */
 

@@ -372,9 +372,14 @@ static int update_merge(or_dcsr *m, const int32_t *rows, const int32_t *cols, co
       t[k].layer = 8; /* marker: reset the chain to this segment */
       need += t[k].seg_cap;
     } else if (nl > tot) {
-      t[k].seg_cap = align_up64(or_policy_cap(&m->o, nl) - tot, m->o.align);
       t[k].layer = tot == 0 ? 0 : ns;
-      if (t[k].layer >= m->o.max_segs) st = OR_LAYER_OVERFLOW;
+      if (t[k].layer >= m->o.max_segs) {
+        /* every layer in use: relocation into one fresh segment (chain reset) */
+        t[k].seg_cap = or_policy_cap(&m->o, nl);
+        t[k].layer = 8;
+      } else {
+        t[k].seg_cap = align_up64(or_policy_cap(&m->o, nl) - tot, m->o.align);
+      }
       need += t[k].seg_cap;
     }
   }

@@ -51,7 +51,7 @@ def test_ctypes_match_c_layout(tmp_path):
             assert getattr(cls, f).offset == ref[(cname, f)], f"{cname}.{f}: offset"
 
 
-@pytest.mark.parametrize("name", ["dcsr_batch_autotune", "dcsr_batch_grow", "dcsr_server_replay", "dcsr_set_row_classes",
+@pytest.mark.parametrize("name", ["dcsr_batch_autotune", "dcsr_batch_short_split", "dcsr_batch_grow", "dcsr_server_replay", "dcsr_set_row_classes",
                                   "dcsr_pool_reserve", "dcsr_spin_faults"])
 def test_new_entry_points_declared(name):
     text = open(os.path.join(ROOT, "include", "dcsr_b200.h")).read()

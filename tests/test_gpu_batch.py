@@ -235,6 +235,9 @@ def test_batch_autotune(dcsr):
     batch = dcsr.DcsrBatch(work)
     sm, lm, us = batch.autotune()
     assert (sm, lm) in {(a, b) for a in (32, 64, 128) for b in (512, 1024, 4096, 16384)} and us > 0
+    # the chosen short-row split (if not the automatic rule) must not change
+    # a result: the per-call copies below run under the automatic rule
+    assert batch.short_split() in (0, 1, 2, 4, 8)
     torch.cuda.synchronize()
     for w, y0, ref in zip(work, y_before, refs):
         assert torch.equal(w["y"], y0), "autotune wrote an item's y"
@@ -260,8 +263,9 @@ def test_row_classes_api(dcsr):
 
 
 def test_grow_nearly_full_pools(dcsr):
-    """dcsr_batch_grow after a status read grows exactly the pools that the
-    run left more than 7/8 full (here every pool: 1/16 spare), and only
+    """dcsr_batch_grow after a status read grows the pools that the run left
+    short of room (more than 7/8 full -- here every pool: 1/16 spare -- or
+    with less room than two more runs of the last run's growth), and only
     their capacity: contents, row lengths and segments stay the per-call
     ones round after round."""
     rng = np.random.default_rng(31)

@@ -352,6 +352,30 @@ def test_spgemm_all_size_classes(dcsr):
     assert_content_equal(dC, oC, "C")
 
 
+@pytest.mark.parametrize("dtype", [0, 1])
+def test_spgemm_wide_columns(dcsr, dtype):
+    """C's columns above 2^24 (the warp path's 64-bit sort keys) and at most
+    2^24 (32-bit keys) give the same structure and values as the oracle;
+    B's rows share columns so equal columns are summed."""
+    rng = np.random.default_rng(23)
+    n, k = 64, 64
+    for m in ((1 << 24), (1 << 24) + 100):
+        lensA = rng.integers(0, 12, n)
+        A_rp = np.concatenate([[0], np.cumsum(lensA)]).astype(np.int32)
+        A_c = np.concatenate([np.sort(rng.choice(k, L, replace=False)) for L in lensA]).astype(np.int32)
+        A_v = rng.standard_normal(A_c.size)
+        pool = np.concatenate([rng.choice(m, 40, replace=False), [m - 1, m - 2, 0]])  # shared columns
+        lensB = rng.integers(0, 20, k)
+        B_rp = np.concatenate([[0], np.cumsum(lensB)]).astype(np.int32)
+        B_c = np.concatenate([np.sort(rng.choice(pool, L, replace=False)) for L in lensB]).astype(np.int32)
+        B_v = rng.standard_normal(B_c.size)
+        if dtype == 0:
+            A_v, B_v = A_v.astype(np.float32), B_v.astype(np.float32)
+        dC, oC = _spgemm_pair(dcsr, A_rp, A_c, A_v, B_rp, B_c, B_v, n, k, m, dtype)
+        assert_layout_equal(dC, oC, f"C m={m}")
+        assert_content_equal(dC, oC, f"C m={m}")
+
+
 def test_spgemm_after_updates(dcsr):
     """SpGEMM reads chained (uncompacted) inputs correctly."""
     n, rp, cols, vals, upd = W.banded_spgemm(1, scale=10, n_updates=3000)
@@ -401,3 +425,26 @@ def test_spmv_k1_both_paths(dcsr, n):
     v = rng.uniform(-1, 1, T).astype(np.float32)
     assert dev.update(r, c, v) == orc.update_auto(r, c, v.astype(np.float64)) == 0
     check_spmv(dev, orc, rng)
+
+
+def test_full_chain_relocates_instead_of_overflowing(dcsr):
+    """MERGE: a row that outgrows a chain already max_segs long is merged out
+    of place into one fresh segment (no LAYER_OVERFLOW), exactly as the
+    oracle restates; the asynchronous update is accepted."""
+    rng = np.random.default_rng(31)
+    n, m = 64, 5000
+    rp, cols = W.poisson_matrix(rng, n, m, 4.0)
+    vals = rng.uniform(-1, 1, cols.size).astype(np.float32)
+    dev, orc = make_pair(dcsr, n, m, 0, 0, max_segs=2, factor_x16=16, min_cap=1, align=1, spare_x16=64)
+    dev.from_csr(rp, cols, vals)
+    orc.load_csr(rp, cols, vals.astype(np.float64))
+    for it in range(5):  # the same rows again and again: chains fill, then relocate
+        r = np.repeat(np.arange(0, n, 4, dtype=np.int32), 6)
+        c = rng.integers(0, m, r.size).astype(np.int32)
+        v = rng.uniform(-1, 1, r.size).astype(np.float32)
+        assert dev.update(r, c, v, sync=False) == 0
+        assert dev.get_status() == dcsr.OK, f"round {it}"
+        st, _ = orc.update(r, c, v.astype(np.float64))
+        assert st == 0
+        assert_layout_equal(dev, orc, f"round {it}")
+        assert_content_equal(dev, orc, f"round {it}")
