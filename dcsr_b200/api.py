@@ -134,6 +134,8 @@ _SIGS = {
     "dcsr_hyb_overflow": (_i32, [_vp, _i32, C.POINTER(_i64), _vp]),
     "dcsr_to_hyb": (_i32, [_vp, _i32, _i64, _vp, _vp, _vp, _vp, _vp, _i64, C.POINTER(_i64), _vp]),
     "dcsr_hyb_spmv": (_i32, [_i32, _i32, _i32, _i64, _vp, _vp, _i64, _vp, _vp, _vp, _vp, _vp, _dbl, _dbl, _vp]),
+    "dcsr_hyb_update": (_i32, [_i32, _i32, _i32, _i32, _i64, _vp, _vp, _vp, _vp, _vp, _i64, C.POINTER(_i64), _vp,
+                               _vp, _vp, _i64, _vp]),
     "dcsr_measure_gather": (_i32, [_vp, _vp, _i64, _vp, _vp, _i32, _vp]),
     "dcsr_cg": (_i32, [_vp, _vp, _vp, _i32, _dbl, _dbl, C.POINTER(_i32), C.POINTER(_dbl), _vp]),
     "dcsr_pool_reserve": (C.c_int, [C.c_int64, C.c_void_p]),
@@ -453,6 +455,22 @@ def hyb_spmv(ell_cols, ell_vals, coo_rows, coo_cols, coo_vals, x, y=None, alpha=
                                coo_rows.numel(), _ptr(coo_rows), _ptr(coo_cols), _ptr(coo_vals), _ptr(x), _ptr(y),
                                alpha, beta, _stream(stream)), "dcsr_hyb_spmv")
     return y
+
+
+def hyb_update(ell_cols, ell_vals, coo_rows, coo_cols, coo_vals, coo_nnz: int, rows, cols, vals, n_rows: int,
+               n_cols: int, stream=None):
+    """Append triples to a HYB matrix in place (dcsr_hyb_update).  The COO
+    arrays' length is their capacity and their first coo_nnz entries the
+    COO part.  Returns (status, new coo_nnz): DCSR_BAD_INDEX or
+    DCSR_POOL_EXHAUSTED leave the matrix unchanged."""
+    width, pitch = (ell_cols.shape[0], ell_cols.shape[1]) if ell_cols.dim() == 2 else (0, n_rows)
+    n = _i64(int(coo_nnz))
+    st = lib().dcsr_hyb_update(n_rows, n_cols, _dtype_code(ell_vals.dtype), width, pitch, _ptr(ell_cols),
+                               _ptr(ell_vals), _ptr(coo_rows), _ptr(coo_cols), _ptr(coo_vals), coo_rows.numel(),
+                               C.byref(n), _ptr(rows), _ptr(cols), _ptr(vals), rows.numel(), _stream(stream))
+    if st not in (OK, POOL_EXHAUSTED, BAD_INDEX):
+        _check(st, "dcsr_hyb_update")
+    return st, int(n.value)
 
 
 def count_sorted_indices(I: torch.Tensor, X: torch.Tensor, stream=None) -> torch.Tensor:

@@ -92,6 +92,173 @@ __global__ void k_hyb_spmv(int32_t n_rows, int32_t width, int64_t pitch, const i
   }
 }
 
+// ---- HYB update (the reference's UpdateMatrix(hyb), include/load.h:327-373,
+// kernel UpdateMatrix_hyb, include/sparse_update.inl:321-366): triples in
+// row order (a stable sort by row), each to its row's next free ELL slot or,
+// the ELL part full, to the COO part, which stays sorted by row with a row's
+// earlier COO entries first.
+
+// Sort keys (row) and triple numbers; flags[0] |= 1 for an index out of range.
+__global__ void k_hu_keys(const int32_t *rows, const int32_t *cols, int64_t T, int32_t n_rows, int32_t n_cols,
+                          unsigned long long *key, unsigned *idx, long long *flags) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < T; i += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t r = rows[i], c = cols[i];
+    const bool ok = r >= 0 && r < n_rows && c >= 0 && c < n_cols;
+    if (!ok) atomicOr((unsigned long long *)flags, 1ull);
+    key[i] = ok ? (unsigned long long)r : 0ull;
+    idx[i] = (unsigned)i;
+  }
+}
+
+// Per sorted triple: its rank j among its row's triples and the row's ELL
+// fill f (the filled slots are a prefix: a binary search for the first
+// column -1); ELL slot f + j while it is below the width, else a COO entry
+// (ov = 1, scanned into positions in row order).
+__global__ void k_hu_plan(const unsigned long long *key, int64_t T, int32_t width, int64_t pitch,
+                          const int32_t *ell_cols, int32_t *slot, long long *ov) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i <= T; i += (int64_t)gridDim.x * blockDim.x) {
+    if (i == T) {
+      ov[T] = 0;
+      continue;
+    }
+    const unsigned long long r = key[i];
+    int64_t lo = 0, hi = i;  // first triple of row r
+    while (lo < hi) {
+      const int64_t mid = (lo + hi) >> 1;
+      if (key[mid] < r) lo = mid + 1;
+      else hi = mid;
+    }
+    const int64_t j = i - lo;
+    int32_t a = 0, b = width;  // first free ELL slot of row r
+    while (a < b) {
+      const int32_t mid = (a + b) >> 1;
+      if (ell_cols[(int64_t)mid * pitch + (int64_t)r] >= 0) a = mid + 1;
+      else b = mid;
+    }
+    const bool ell = (int64_t)a + j < (int64_t)width;
+    slot[i] = ell ? (int32_t)(a + j) : -1;
+    ov[i] = ell ? 0 : 1;
+  }
+}
+
+// ELL slots written in place; new COO entries gathered in row order.
+template <typename V>
+__global__ void k_hu_emit(const unsigned long long *key, const unsigned *idx, int64_t T, const int32_t *slot,
+                          const long long *ov, int64_t pitch, const int32_t *cols, const V *vals, int32_t *ell_cols,
+                          V *ell_vals, int32_t *nr, int32_t *nc, V *nv) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < T; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t r = (int64_t)key[i];
+    const unsigned t = idx[i];
+    const int32_t k = slot[i];
+    if (k >= 0) {
+      ell_cols[(int64_t)k * pitch + r] = cols[t];
+      ell_vals[(int64_t)k * pitch + r] = vals[t];
+    } else {
+      const int64_t p = ov[i];
+      nr[p] = (int32_t)r;
+      nc[p] = cols[t];
+      nv[p] = vals[t];
+    }
+  }
+}
+
+// Count of sorted rows[0, n) below r (strict) or at most r.
+__device__ __forceinline__ int64_t rows_before(const int32_t *rows, int64_t n, int32_t r, bool inclusive) {
+  int64_t lo = 0, hi = n;
+  while (lo < hi) {
+    const int64_t mid = (lo + hi) >> 1;
+    const int32_t v = rows[mid];
+    if (v < r || (inclusive && v == r)) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo;
+}
+
+// The merged COO part: old entry a at a + (new rows below its row), new
+// entry b at b + (old rows at or below its row) -- a stable merge by row.
+template <typename V>
+__global__ void k_hu_merge(const int32_t *orow, const int32_t *ocol, const V *oval, int64_t m, const int32_t *nr,
+                           const int32_t *nc, const V *nv, int64_t q, int32_t *coo_rows, int32_t *coo_cols,
+                           V *coo_vals) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m + q; i += (int64_t)gridDim.x * blockDim.x) {
+    if (i < m) {
+      const int32_t r = orow[i];
+      const int64_t p = i + rows_before(nr, q, r, false);
+      coo_rows[p] = r;
+      coo_cols[p] = ocol[i];
+      coo_vals[p] = oval[i];
+    } else {
+      const int64_t b = i - m;
+      const int32_t r = nr[b];
+      const int64_t p = b + rows_before(orow, m, r, true);
+      coo_rows[p] = r;
+      coo_cols[p] = nc[b];
+      coo_vals[p] = nv[b];
+    }
+  }
+}
+
+template <typename V>
+int hyb_update_body(int32_t n_rows, int32_t n_cols, int32_t width, int64_t pitch, int32_t *ell_cols, V *ell_vals,
+                    int32_t *coo_rows, int32_t *coo_cols, V *coo_vals, int64_t coo_cap, int64_t *coo_nnz,
+                    const int32_t *rows, const int32_t *cols, const V *vals, int64_t T, Arena &ar, cudaStream_t s) {
+  const int64_t m = *coo_nnz;
+  const size_t bytes = arena_bytes(4, 8) + 2 * arena_bytes(T, 8) + 2 * arena_bytes(T, 4) + arena_bytes(T, 4) +
+                       arena_bytes(T + 1, 8) + 2 * arena_bytes(T, 4) + arena_bytes(T, sizeof(V)) +
+                       2 * arena_bytes(m, 4) + arena_bytes(m, sizeof(V)) + radix_scratch_bytes(T) +
+                       scan_scratch_bytes(T + 1);
+  DCSR_TRY(ar.reserve(bytes, s));
+  long long *st = ar.take<long long>(4);  // [0] look-back status, [1] bad-index flag, [2] new COO entries
+  ar.status = st;
+  unsigned long long *k0 = ar.take<unsigned long long>(T), *k1 = ar.take<unsigned long long>(T);
+  unsigned *i0 = ar.take<unsigned>(T), *i1 = ar.take<unsigned>(T);
+  int32_t *slot = ar.take<int32_t>(T);
+  long long *ov = ar.take<long long>(T + 1);
+  int32_t *nr = ar.take<int32_t>(T), *nc = ar.take<int32_t>(T);
+  V *nv = ar.take<V>(T);
+  int32_t *orow = ar.take<int32_t>(m), *ocol = ar.take<int32_t>(m);
+  V *oval = ar.take<V>(m);
+  if (ar.overflow) return DCSR_OOM;  // scratch sizing bug: no kernel sees a null pointer
+  DCSR_CUDA(cudaMemsetAsync(st, 0, 4 * sizeof(long long), s));
+  DCSR_LAUNCH(k_hu_keys, grid_for(T, 256), 256, 0, s, rows, cols, T, n_rows, n_cols, k0, i0, st + 1);
+  if (T > 1) DCSR_TRY(radix_sort_pairs(&k0, &i0, &k1, &i1, T, bits_for(n_rows), ar, s));
+  DCSR_LAUNCH(k_hu_plan, grid_for(T + 1, 256), 256, 0, s, k0, T, width, pitch, ell_cols, slot, ov);
+  DCSR_TRY(scan_i64(ov, ov, T + 1, st + 2, ar, s));
+  // the one read: validity and the new COO count (the capacity check comes before any write)
+  long long host[3];
+  DCSR_CUDA(cudaMemcpyAsync(host, st, sizeof(host), cudaMemcpyDeviceToHost, s));
+  DCSR_CUDA(cudaStreamSynchronize(s));
+  if (host[0] == DCSR_TIMEOUT) return DCSR_TIMEOUT;
+  if (host[1]) return DCSR_BAD_INDEX;
+  const int64_t q = host[2];
+  if (m + q > coo_cap) return DCSR_POOL_EXHAUSTED;
+  if (q > 0 && (!coo_rows || !coo_cols || !coo_vals)) return DCSR_BAD_ARG;
+  DCSR_LAUNCH(k_hu_emit<V>, grid_for(T, 256), 256, 0, s, k0, i0, T, slot, ov, pitch, cols, vals, ell_cols, ell_vals,
+              nr, nc, nv);
+  if (q > 0) {
+    if (m > 0) {
+      DCSR_CUDA(cudaMemcpyAsync(orow, coo_rows, 4 * m, cudaMemcpyDeviceToDevice, s));
+      DCSR_CUDA(cudaMemcpyAsync(ocol, coo_cols, 4 * m, cudaMemcpyDeviceToDevice, s));
+      DCSR_CUDA(cudaMemcpyAsync(oval, coo_vals, sizeof(V) * m, cudaMemcpyDeviceToDevice, s));
+    }
+    DCSR_LAUNCH(k_hu_merge<V>, grid_for(m + q, 256), 256, 0, s, orow, ocol, oval, m, nr, nc, nv, q, coo_rows, coo_cols,
+                coo_vals);
+  }
+  *coo_nnz = m + q;
+  return DCSR_OK;
+}
+
+template <typename V>
+int hyb_update_t(int32_t n_rows, int32_t n_cols, int32_t width, int64_t pitch, int32_t *ell_cols, V *ell_vals,
+                 int32_t *coo_rows, int32_t *coo_cols, V *coo_vals, int64_t coo_cap, int64_t *coo_nnz,
+                 const int32_t *rows, const int32_t *cols, const V *vals, int64_t T, cudaStream_t s) {
+  Arena ar;  // scratch of this call, released (stream-ordered) on every path
+  const int rc = hyb_update_body<V>(n_rows, n_cols, width, pitch, ell_cols, ell_vals, coo_rows, coo_cols, coo_vals,
+                                    coo_cap, coo_nnz, rows, cols, vals, T, ar, s);
+  ar.release(s);
+  return rc;
+}
+
 int overflow_scan(dcsr_handle h, int32_t width, cudaStream_t s, long long **ov, int64_t *total) {
   Arena &ar = h->scratch;
   ar.status = h->stat + ST_STATUS;
@@ -166,4 +333,23 @@ extern "C" int dcsr_hyb_spmv(int32_t n_rows, int32_t dtype, int32_t ell_width, i
     DCSR_LAUNCH(k_hyb_spmv<double>, g, 256, 0, s, n_rows, ell_width, ell_pitch, ell_cols, (const double *)ell_vals,
                 coo_nnz, coo_rows, coo_cols, (const double *)coo_vals, (const double *)x, (double *)y, alpha, beta);
   return DCSR_OK;
+}
+
+extern "C" int dcsr_hyb_update(int32_t n_rows, int32_t n_cols, int32_t dtype, int32_t ell_width, int64_t ell_pitch,
+                               int32_t *ell_cols, void *ell_vals, int32_t *coo_rows, int32_t *coo_cols,
+                               void *coo_vals, int64_t coo_cap, int64_t *coo_nnz, const int32_t *rows,
+                               const int32_t *cols, const void *vals, int64_t nnz, void *stream) {
+  if (n_rows < 0 || n_cols < 0 || ell_width < 0 || ell_pitch < n_rows || (dtype != DCSR_F32 && dtype != DCSR_F64) ||
+      !coo_nnz || *coo_nnz < 0 || *coo_nnz > coo_cap || nnz < 0 || (ell_width > 0 && (!ell_cols || !ell_vals)) ||
+      (*coo_nnz > 0 && (!coo_rows || !coo_cols || !coo_vals)) || (nnz > 0 && (!rows || !cols || !vals)))
+    return DCSR_BAD_ARG;
+  if (nnz == 0) return DCSR_OK;
+  if (n_rows == 0 || n_cols == 0) return DCSR_BAD_INDEX;  // no triple can be in range
+  if (nnz > 0xffffffffLL) return DCSR_NOT_SUPPORTED;  // triple numbers are 32-bit
+  cudaStream_t s = (cudaStream_t)stream;
+  if (dtype == DCSR_F32)
+    return hyb_update_t<float>(n_rows, n_cols, ell_width, ell_pitch, ell_cols, (float *)ell_vals, coo_rows, coo_cols,
+                               (float *)coo_vals, coo_cap, coo_nnz, rows, cols, (const float *)vals, nnz, s);
+  return hyb_update_t<double>(n_rows, n_cols, ell_width, ell_pitch, ell_cols, (double *)ell_vals, coo_rows, coo_cols,
+                              (double *)coo_vals, coo_cap, coo_nnz, rows, cols, (const double *)vals, nnz, s);
 }

@@ -599,9 +599,13 @@ __device__ __forceinline__ void short_block_k1(const RowItem<V> &it, int4 d0, in
       int32_t q[U];
       int32_t rs[U];  // the window lane where the lane's row starts (0: it runs in from before)
       bool ok[U];
+      // windows past the block's end (warp-uniform) are skipped whole
 #pragma unroll
       for (int i = 0; i < U; i++) {
         const int32_t w0 = base + 32 * i, p = w0 + lane;
+        q[i] = rs[i] = 0;
+        ok[i] = false;
+        if (w0 >= E) continue;
         const int j = owner_lane(excl, p);
         const int32_t ej = __shfl_sync(FULL, excl, j);
         const int32_t sj = __shfl_sync(FULL, st_l, j);
@@ -613,14 +617,24 @@ __device__ __forceinline__ void short_block_k1(const RowItem<V> &it, int4 d0, in
       int32_t col[U];
 #pragma unroll
       for (int i = 0; i < U; i++) {
+        a[i] = V(0);
+        col[i] = 0;
+        if (base + 32 * i >= E) continue;
         a[i] = __ldcs(m.vals + q[i]);
         col[i] = OP == OP_SPMV ? __ldcs(m.cols + q[i]) : 0;
       }
+      // every window's x gathers issued before the first scan (lanes past
+      // the block's end loaded a valid entry: their columns are valid)
+      V xv[U];
+#pragma unroll
+      for (int i = 0; i < U; i++)
+        xv[i] = OP == OP_SPMV && base + 32 * i < E ? __ldg(x + (int64_t)col[i] * it.ldx) : V(0);
 #pragma unroll
       for (int i = 0; i < U; i++) {
+        if (base + 32 * i >= E) continue;
         P c = op_init<P, OP>();
         if (ok[i]) {
-          if constexpr (OP == OP_SPMV) c = mul_rn((P)a[i], (P)__ldg(x + (int64_t)col[i] * it.ldx));
+          if constexpr (OP == OP_SPMV) c = mul_rn((P)a[i], (P)xv[i]);
           else c = OP == OP_COUNT ? (P)1 : (P)a[i];
         }
         // segmented inclusive scan: lanes p-d and p share a row when p-d is
@@ -1164,12 +1178,17 @@ __global__ void __launch_bounds__(RS_THREADS_, DCSR_K1_MINB) k_rows1(Src src) {
           unit_range(nx, d0, d1);
           load_step<V, UN, OP>(src.item(nx.item).m, nx.d.z, d1 - d0, 0, lane, na, nc);
         }
+        // every x gather of the step issued before the first is used (lanes
+        // past the unit's end loaded its first entry: their columns are valid)
+        V xv[UN];
+#pragma unroll
+        for (int i = 0; i < UN; i++) xv[i] = OP == OP_SPMV ? __ldg(it.x + (int64_t)cc[i] * it.ldx) : V(0);
         P w = op_init<P, OP>();
 #pragma unroll
         for (int i = 0; i < UN; i++) {
           if (o + 32 * i + lane < n) {
             P t;
-            if constexpr (OP == OP_SPMV) t = mul_rn((P)ca[i], (P)__ldg(it.x + (int64_t)cc[i] * it.ldx));
+            if constexpr (OP == OP_SPMV) t = mul_rn((P)ca[i], (P)xv[i]);
             else t = OP == OP_COUNT ? (P)1 : (P)ca[i];
             w = op_comb<P, OP>(w, t);
           }

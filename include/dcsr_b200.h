@@ -138,6 +138,25 @@ int dcsr_hyb_spmv(int32_t n_rows, int32_t dtype, int32_t ell_width, int64_t ell_
                   const void *ell_vals, int64_t coo_nnz, const int32_t *coo_rows, const int32_t *coo_cols,
                   const void *coo_vals, const void *x, void *y, double alpha, double beta, void *stream);
 
+/* Append update triples to a HYB matrix in that layout, in place (replaces
+ * device::UpdateMatrix(hyb, rows, cols, vals, N), include/load.h:327-373,
+ * kernel UpdateMatrix_hyb include/sparse_update.inl:321-366).  The triples
+ * are taken in row order -- a stable sort by row, so a row's triples keep
+ * their input order (the reference requires input sorted by row) -- and each
+ * goes to its row's next free ELL slot (the ELL part's filled slots are a
+ * prefix, as dcsr_to_hyb and this call leave them), or, once the row's ELL
+ * part is full, to the COO part, which stays sorted by row with a row's
+ * earlier COO entries first (the reference appends with atomics, then sorts
+ * the COO part by row).  No duplicate check (the reference's HYB update
+ * appends).  *coo_nnz: the COO part's entries, in and out.  DCSR_BAD_INDEX
+ * for a row outside [0, n_rows) or a column outside [0, n_cols),
+ * DCSR_POOL_EXHAUSTED when the COO part would exceed coo_cap (the reference
+ * writes past its end); both leave the matrix unchanged.  Synchronises once. */
+int dcsr_hyb_update(int32_t n_rows, int32_t n_cols, int32_t dtype, int32_t ell_width, int64_t ell_pitch,
+                    int32_t *ell_cols, void *ell_vals, int32_t *coo_rows, int32_t *coo_cols, void *coo_vals,
+                    int64_t coo_cap, int64_t *coo_nnz, const int32_t *rows, const int32_t *cols, const void *vals,
+                    int64_t nnz, void *stream);
+
 /* Number of stored entries (synchronises).  Use before dcsr_to_csr. */
 int dcsr_nnz(dcsr_handle h, int64_t *nnz, void *stream);
 /* DCSR -> CSR in row order, any state (chains followed).  Replaces

@@ -293,6 +293,50 @@ def hyb_spmv(ec, ev, cr, cc, cv, x, n_rows):
     return y
 
 
+def hyb_update(ec, ev, cr, cc, cv, rows, cols, vals, n_rows, n_cols, coo_cap):
+    """The reference's HYB update restated (UpdateMatrix(hyb), include/load.h:
+    327-373, kernel UpdateMatrix_hyb, include/sparse_update.inl:321-366):
+    triples taken in row order (a stable sort by row; the reference needs its
+    input sorted by row for indices_to_offsets), each appended to its row --
+    the next free ELL slot while the row's ELL part has one (the slot after
+    the row's current entries, sparse_update.inl:350-355), else the COO part
+    (:357-363) -- with no duplicate check; the COO part then sorted by row
+    (load.h:362-363, a stable sort: a row's earlier COO entries first, then
+    its new ones in input order).  Returns (status, ec, ev, cr, cc, cv) as new
+    arrays; status 3 (BAD_INDEX) for a row outside [0, n_rows) or a column
+    outside [0, n_cols), 1 (POOL_EXHAUSTED) for a COO part beyond coo_cap,
+    both with the inputs unchanged."""
+    rows, cols = np.asarray(rows, np.int64), np.asarray(cols, np.int64)
+    vals = np.asarray(vals, np.float64)
+    width = ec.shape[0]
+    unchanged = (ec.copy(), ev.copy(), cr.copy(), cc.copy(), cv.copy())
+    if rows.size and (rows.min() < 0 or rows.max() >= n_rows or cols.min() < 0 or cols.max() >= n_cols):
+        return (3,) + unchanged
+    e_c, e_v = ec.copy(), ev.copy()
+    fill = {}
+    nr, nc, nv = [], [], []
+    for i in np.argsort(rows, kind="stable"):
+        r = int(rows[i])
+        if r not in fill:
+            fill[r] = int((e_c[:, r] >= 0).sum())
+        f = fill[r]
+        if f < width:
+            e_c[f, r] = cols[i]
+            e_v[f, r] = vals[i]
+        else:
+            nr.append(r)
+            nc.append(int(cols[i]))
+            nv.append(float(vals[i]))
+        fill[r] = f + 1
+    if cr.size + len(nr) > coo_cap:
+        return (1,) + unchanged
+    r2 = np.concatenate([cr, np.asarray(nr, np.int32)]).astype(np.int32)
+    c2 = np.concatenate([cc, np.asarray(nc, np.int32)]).astype(np.int32)
+    v2 = np.concatenate([cv, np.asarray(nv, np.float64)])
+    o = np.argsort(r2, kind="stable")
+    return 0, e_c, e_v, r2[o], c2[o], v2[o]
+
+
 def ref_read_mtx(path: str, cap: int = 1 << 22):
     """The reference's own ReadMatrixFile<int, double> (oracle/_ref/libref_mtx.so):
     (n_rows, n_cols, rows, cols, vals) with 0-based indices, file order."""
