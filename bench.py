@@ -936,6 +936,7 @@ def run_ours(args, rank, world, local_rank):
                 "capacity_req_s": served["e2e"]["capacity_req_s"], "p99_constraint_met": served["e2e"]["p99_constraint_met"],
                 "speedup_at_equal_p99": served["e2e"]["speedup_at_equal_p99"],
                 "sweep": served["e2e"]["sweep"],
+                "host_link": served["e2e"].get("host_link"),
                 "h2d_bytes_per_step": served["e2e"]["h2d_bytes_per_request"],
                 "d2h_bytes_per_step": served["e2e"]["d2h_bytes_per_request"],
                 "note": "a step is one request: its triples or x copied in from pinned host memory, its y or CSR "

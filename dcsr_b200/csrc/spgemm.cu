@@ -215,9 +215,59 @@ __device__ __forceinline__ void bitonic(K *key, int n2, int tid, int nthr, Sync 
     }
 }
 
+// Bitonic sort of the 32*E keys held by a warp, E per lane: key i = lane*E + t
+// in v[t].  Steps with partner distance j < E swap within a lane's
+// registers, the others exchange with lane ^ (j / E) by shuffle; nothing
+// goes through shared memory.
+template <int E, typename K>
+__device__ __forceinline__ void warp_bitonic(K (&v)[E], int lane) {
+  constexpr int N = 32 * E;
+#pragma unroll
+  for (int k = 2; k <= N; k <<= 1) {
+#pragma unroll
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      if (j >= E) {
+#pragma unroll
+        for (int t = 0; t < E; t++) {
+          const int i = lane * E + t;
+          const K o = __shfl_xor_sync(FULL, v[t], j / E);
+          // the lower index of a pair keeps the smaller key in an ascending
+          // block (i & k == 0) and the larger in a descending one
+          const bool keep_min = ((i & k) == 0) == ((i & j) == 0);
+          v[t] = keep_min ? (o < v[t] ? o : v[t]) : (o > v[t] ? o : v[t]);
+        }
+      } else {
+#pragma unroll
+        for (int t = 0; t < E; t++) {
+          const int q = t ^ j;
+          if (q > t) {
+            const bool up = ((lane * E + t) & k) == 0;
+            const K a = v[t], b = v[q];
+            const bool sw = up ? (a > b) : (a < b);
+            v[t] = sw ? b : a;
+            v[q] = sw ? a : b;
+          }
+        }
+      }
+    }
+  }
+}
+
+// A warp-row's P keys (in key[0, P), P <= 32*E) sorted in place through
+// registers; slots past P take the largest key and end up past P.
+template <int E, typename K>
+__device__ __forceinline__ void sort_row_keys(K *key, int P, int lane) {
+  K v[E];
+#pragma unroll
+  for (int t = 0; t < E; t++) v[t] = lane * E + t < P ? key[lane * E + t] : ~K(0);
+  warp_bitonic<E>(v, lane);
+#pragma unroll
+  for (int t = 0; t < E; t++) key[lane * E + t] = v[t];
+}
+
 // Warp per row, P_i <= 256.
 template <typename V, typename K>
-__global__ void __launch_bounds__(SG_THREADS) k_sg_warp(Mat<V> A, Mat<V> B, const unsigned *rows,
+__global__ void __launch_bounds__(SG_THREADS, 3) k_sg_warp(Mat<V> A, Mat<V> B, const unsigned *rows,
                                                         const long long *starts, const long long *ub, int32_t *tcol,
                                                         V *tval, long long *ucnt) {
   using KO = SgKey<K>;
@@ -232,10 +282,12 @@ __global__ void __launch_bounds__(SG_THREADS) k_sg_warp(Mat<V> A, Mat<V> B, cons
   for (int64_t it = b + (((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5); it < e; it += nw) {
     const int64_t i = rows[it];
     const int P = sg_expand_warp(A, B, i, lane, key, prod);
-    const int n2 = next_pow2(P);
-    for (int t = P + lane; t < n2; t += 32) key[t] = ~K(0);
     __syncwarp();
-    bitonic(key, n2, lane, 32, []() { __syncwarp(); });
+    if (P <= 32) sort_row_keys<1>(key, P, lane);
+    else if (P <= 64) sort_row_keys<2>(key, P, lane);
+    else if (P <= 128) sort_row_keys<4>(key, P, lane);
+    else sort_row_keys<8>(key, P, lane);
+    __syncwarp();
     const int64_t base = ub[i];
     int heads = 0;
     for (int c0 = 0; c0 < P; c0 += 32) {
