@@ -425,6 +425,7 @@ def batched_part(args, dev):
     repaired = [0]
     grown = [0]
     repair_s = [0.0]
+    grow_s = [0.0]
     rejected = np.zeros(9, np.int64)  # rejections by status code, timed rounds
 
     def batched_round(i):
@@ -436,9 +437,12 @@ def batched_part(args, dev):
         rejected[:] += np.bincount(np.asarray(st), minlength=9)[:9]
         if (st != 0).any():
             repaired[0] += batch.repair(st, s)
-        grown[0] += batch.grow(s)  # pools the run left > 7/8 full, ahead of the next round
+            s.synchronize()
+        t1 = time.perf_counter()
+        grown[0] += batch.grow(s)  # pools left short of room, grown ahead of the next round
         s.synchronize()
-        repair_s[0] += time.perf_counter() - t0
+        repair_s[0] += t1 - t0
+        grow_s[0] += time.perf_counter() - t1
 
     with torch.cuda.stream(s):
         for i in range(warm):
@@ -448,7 +452,7 @@ def batched_part(args, dev):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(s)
         repaired[0] = grown[0] = 0
-        repair_s[0] = 0.0
+        repair_s[0] = grow_s[0] = 0.0
         rejected[:] = 0
         for i in range(reps):
             batched_round(warm + i)
@@ -489,7 +493,7 @@ def batched_part(args, dev):
         "speedup": round(plain_ms / batched_ms, 2),
         "batched_kernel_launches": round(batched_launches, 1), "plain_kernel_launches": round(plain_launches, 1),
         "repairs_per_round": repairs_per_round, "repair_ms_per_round": round(repair_ms_per_round, 3),
-        "pools_grown_ahead_per_round": grown[0] / reps,
+        "pools_grown_ahead_per_round": grown[0] / reps, "grow_ms_per_round": round(1e3 * grow_s[0] / reps, 3),
         "rejections_per_round": {"pool_exhausted": round(float(rejected[1]) / reps, 2),
                                  "layer_overflow": round(float(rejected[2]) / reps, 2)},
         "updates_per_s_batched": round(T / (batched_ms / 1e3), 1),

@@ -138,6 +138,7 @@ __device__ __forceinline__ int sg_expand_warp(const Mat<V> &A, const Mat<V> &B, 
       lb = B.row_sizes[kb];
     }
     const Chain cb = load_chain_used(B, kb, lb);
+    const bool flat = __all_sync(FULL, cb.ns <= 1);  // every B row in its first segment (the common case)
     const int incl = warp_incl_scan(lb);
     const int pos = incl - lb;
     const int tot = __shfl_sync(FULL, incl, 31);  // base + tot <= P_i <= SG_WARP_MAX
@@ -161,10 +162,15 @@ __device__ __forceinline__ int sg_expand_warp(const Mat<V> &A, const Mat<V> &B, 
             if (c < nE && pc <= q) lo = c;
           }
           own[h] = lo;
-          const Chain co = shfl_chain(cb, lo);
           const int pj = __shfl_sync(FULL, pos, lo);
+          int64_t qb;
+          if (flat) {
+            qb = (int64_t)__shfl_sync(FULL, cb.st[0], lo) + (q - pj);
+          } else {
+            const Chain co = shfl_chain(cb, lo);
+            qb = co.phys(q - pj);
+          }
           if (q < tot) {
-            const int64_t qb = co.phys(q - pj);
             bc[h] = B.cols[qb];
             bv[h] = B.vals[qb];
           }

@@ -86,7 +86,7 @@ def _hyb_update_case(dcsr, dtype, width, rows, cols, vals, extra_cap, n=600, see
     if st == 0:  # the updated HYB multiplies like the oracle's
         x = np.random.default_rng(4).uniform(-1, 1, n_)
         xt = torch.tensor(x, dtype=ev.dtype, device="cuda")
-        y = dcsr.hyb_spmv(ec, ev, cr[:m2], cc[:m2], cv[:m2], xt)
+        y = dcsr.hyb_spmv(ec, ev, cr[:m2], cc[:m2], cv[:m2], xt, torch.zeros(n_, dtype=ev.dtype, device="cuda"))
         y_ref = O.hyb_spmv(e_c, e_v, o_r, o_c, o_v, xt.cpu().double().numpy(), n_)
         scale = O.hyb_spmv(np.where(e_c >= 0, e_c, 0), np.abs(e_v), o_r, o_c, np.abs(o_v),
                            np.abs(xt.cpu().double().numpy()), n_)
