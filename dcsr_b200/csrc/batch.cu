@@ -501,7 +501,10 @@ int dcsr_batch_grow(dcsr_batch b, int32_t *grown, void *stream) {
       const long long prev = b->last_need[i];
       const long long step = prev >= 0 && need > prev ? need - prev : 0;
       b->last_need[i] = need;
-      const long long room = h->pool_cap / 8 > 2 * step ? h->pool_cap / 8 : 2 * step;
+      const long long T = b->core.items[i].nnz;  // at most T new entries next run, before relocations
+      long long room = h->pool_cap / 8;
+      if (room < 2 * step) room = 2 * step;
+      if (room < 2 * T) room = 2 * T;
       if (h->pool_cap - need < room) {
         DCSR_TRY(reserve(h, grow_target(h, need + room), (cudaStream_t)stream));  // keeps the pool top
         n++;
@@ -520,8 +523,13 @@ int dcsr_batch_repair(dcsr_batch b, const int32_t *statuses, int32_t *repaired, 
     if (statuses[i] == DCSR_OK) continue;
     const dcsr_batch_item &it = b->core.items[i];
     int st = statuses[i];
-    if (st == DCSR_POOL_EXHAUSTED || st == DCSR_LAYER_OVERFLOW)
+    if (st == DCSR_POOL_EXHAUSTED || st == DCSR_LAYER_OVERFLOW) {
       st = dcsr_update_sync(it.matrix, it.rows, it.cols, it.vals, it.nnz, stream);
+      // room for the next run's update (as many triples) beyond the repaired
+      // layout, so the same matrix is not rejected again next run
+      if (st == DCSR_OK && it.nnz > 0)
+        DCSR_TRY(reserve(it.matrix, grow_target(it.matrix, it.matrix->pool_cap + 2 * it.nnz), (cudaStream_t)stream));
+    }
     // the batch skipped this matrix's SpMV: run it on the repaired (or, for
     // an unrepairable update, unchanged) matrix, as the per-call path would
     if (it.x) DCSR_TRY(dcsr_spmv(it.matrix, it.x, it.k, it.ldx, it.y, it.ldy, it.alpha, it.beta, stream));
