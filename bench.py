@@ -70,11 +70,12 @@ def peaks():
 
 
 # DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) of one k = 1
-# SpMV launch on the update-stream matrix, from one ncu capture of the same
-# seeded workload in the same state (profiles/spmv_rmat_k1_f32.md gives the
-# command): keyed by the matrix's stored-entry count, so a run on another
-# state reports no traffic rather than a scaled one.
-SPMV_TRAFFIC = {}
+# SpMV call (its two launches, k_rows1 + k_rows1_blocks) on the update-stream
+# matrix, from one ncu capture of the same seeded workload in the same state
+# (profiles/spmv_rmat_k1_f32.md gives the command): keyed by the matrix's
+# stored-entry count, so a run on another state reports no traffic rather
+# than a scaled one.
+SPMV_TRAFFIC = {32832123: 235313408 + 3162368 + 118307584 + 831488}
 
 
 class ClockSampler:

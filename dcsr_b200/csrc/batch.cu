@@ -489,11 +489,19 @@ int dcsr_batch_grow(dcsr_batch b, int32_t *grown, void *stream) {
     b->last_need.resize(b->core.count, -1);
     for (int i = 0; i < b->core.count; i++) {
       const int j = b->core.upd_of[i];
-      if (j < 0 || b->status_host[2 * j] != DCSR_OK) {
-        b->last_need[i] = -1;  // repaired per call: its pool top moved outside the batch
+      if (j < 0) continue;
+      dcsr_handle h = b->core.items[i].matrix;
+      if (b->status_host[2 * j] != DCSR_OK) {
+        // rejected (and repaired per call): its pool top moved outside the
+        // batch; room for twice its triples beyond the repaired pool
+        b->last_need[i] = -1;
+        const long long T = b->core.items[i].nnz;
+        if (T > 0) {
+          DCSR_TRY(reserve(h, grow_target(h, h->pool_cap + 2 * T), (cudaStream_t)stream));
+          n++;
+        }
         continue;
       }
-      dcsr_handle h = b->core.items[i].matrix;
       const long long need = b->status_host[2 * j + 1];
       // room for the larger of an eighth of the pool and two more runs
       // growing it as much as the last one did (the same item's next update
@@ -523,13 +531,8 @@ int dcsr_batch_repair(dcsr_batch b, const int32_t *statuses, int32_t *repaired, 
     if (statuses[i] == DCSR_OK) continue;
     const dcsr_batch_item &it = b->core.items[i];
     int st = statuses[i];
-    if (st == DCSR_POOL_EXHAUSTED || st == DCSR_LAYER_OVERFLOW) {
+    if (st == DCSR_POOL_EXHAUSTED || st == DCSR_LAYER_OVERFLOW)
       st = dcsr_update_sync(it.matrix, it.rows, it.cols, it.vals, it.nnz, stream);
-      // room for the next run's update (as many triples) beyond the repaired
-      // layout, so the same matrix is not rejected again next run
-      if (st == DCSR_OK && it.nnz > 0)
-        DCSR_TRY(reserve(it.matrix, grow_target(it.matrix, it.matrix->pool_cap + 2 * it.nnz), (cudaStream_t)stream));
-    }
     // the batch skipped this matrix's SpMV: run it on the repaired (or, for
     // an unrepairable update, unchanged) matrix, as the per-call path would
     if (it.x) DCSR_TRY(dcsr_spmv(it.matrix, it.x, it.k, it.ldx, it.y, it.ldy, it.alpha, it.beta, stream));

@@ -252,15 +252,33 @@ int load_from_csr64(dcsr_handle h, const long long *rp, const int32_t *cols, con
 // pool_capacity(top)), the rows are placed, and one synchronisation reads
 // the pool top to set the pool capacity.
 template <typename V>
-__global__ void k_place_rows(int32_t n, const long long *offs, const long long *src_off, const long long *lens,
-                             const int32_t *scols, const V *svals, int32_t *pcols, V *pvals) {
+__global__ void k_place_rows(int32_t n, const long long *__restrict__ offs, const long long *__restrict__ src_off,
+                             const long long *__restrict__ lens, const int32_t *__restrict__ scols,
+                             const V *__restrict__ svals, int32_t *__restrict__ pcols, V *__restrict__ pvals) {
+  constexpr int U = 4;  // windows of 32 entries whose loads are in flight together
   const int lane = threadIdx.x & 31;
   const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
   for (int64_t r = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < n; r += nw) {
     const int64_t s0 = src_off[r], L = lens[r], d = offs[r];
-    for (int64_t j = lane; j < L; j += 32) {
-      pcols[d + j] = scols[s0 + j];
-      pvals[d + j] = svals[s0 + j];
+    for (int64_t j0 = 0; j0 < L; j0 += 32 * U) {
+      int32_t c[U];
+      V v[U];
+#pragma unroll
+      for (int u = 0; u < U; u++) {
+        const int64_t j = j0 + 32 * u + lane;
+        if (j < L) {
+          c[u] = __ldcs(scols + s0 + j);
+          v[u] = __ldcs(svals + s0 + j);
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < U; u++) {
+        const int64_t j = j0 + 32 * u + lane;
+        if (j < L) {
+          pcols[d + j] = c[u];
+          pvals[d + j] = v[u];
+        }
+      }
     }
   }
 }

@@ -42,20 +42,6 @@ namespace {
 
 using Clock = std::chrono::steady_clock;
 
-// The device address of a host buffer that kernels can write directly:
-// pinned memory mapped into the device's address space (any cudaHostAlloc or
-// mapped cudaHostRegister memory under unified addressing); nullptr for
-// pageable memory, which goes through device staging.
-void *device_view(const void *p) {
-  if (!p) return nullptr;
-  cudaPointerAttributes a;
-  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
-    cudaGetLastError();  // an unrecognised pointer is not an error of the server
-    return nullptr;
-  }
-  return a.type == cudaMemoryTypeHost ? a.devicePointer : nullptr;
-}
-
 struct Req {
   dcsr_request r;
   uint64_t ticket = 0;
@@ -63,9 +49,7 @@ struct Req {
   int64_t cost = 0;
   size_t off[3] = {0, 0, 0};  // staging offsets: update rows/cols/vals | spmv x/y | export rp/cols/vals
   int item = -1;              // batch item of its matrix (update / SpMV), export number (export)
-  bool direct = false;        // export written straight into the caller's buffers (device, or mapped host)
-  int32_t *d_rp = nullptr, *d_cols = nullptr;  // a direct export's buffers as device addresses
-  void *d_vals = nullptr;
+  bool direct = false;        // export written straight into the caller's device buffers
   int32_t status = DCSR_OK;
   int64_t nnz = 0;
 };
@@ -269,22 +253,8 @@ int launch(dcsr_server s, Slot &sl, std::vector<Req> &take) {
       q.off[1] = bytes;
       bytes = al256(bytes + vs * q.r.k * h->n_rows);
     } else if (q.r.kind == DCSR_REQ_EXPORT) {
-      // device buffers, or pinned host buffers mapped into the device's
-      // address space, take the export directly (bounded by cap on the
-      // device): no staging, and no second copy once the entry count is known
+      // device buffers take the export directly (bounded by cap on the device)
       q.direct = q.r.on_device;
-      q.d_rp = q.r.row_ptr;
-      q.d_cols = q.r.out_cols;
-      q.d_vals = q.r.out_vals;
-      if (!q.direct) {
-        void *rp = device_view(q.r.row_ptr), *oc = device_view(q.r.out_cols), *ov = device_view(q.r.out_vals);
-        if (rp && (q.r.cap == 0 || (oc && ov))) {
-          q.direct = true;
-          q.d_rp = (int32_t *)rp;
-          q.d_cols = (int32_t *)oc;
-          q.d_vals = ov;
-        }
-      }
       if (!q.direct) {
         q.off[0] = bytes;
         bytes = al256(bytes + 4 * ((size_t)h->n_rows + 1));
@@ -421,11 +391,11 @@ int launch(dcsr_server s, Slot &sl, std::vector<Req> &take) {
     if (q.r.kind == DCSR_REQ_SPMV && !q.r.on_device) {
       DCSR_CUDA(cudaMemcpyAsync(q.r.y, b + q.off[1], vs * q.r.k * h->n_rows, cudaMemcpyDeviceToHost, st));
     } else if (q.r.kind == DCSR_REQ_EXPORT) {
-      int32_t *rp = q.direct ? q.d_rp : (int32_t *)(b + q.off[0]);
-      int32_t *oc = q.direct ? q.d_cols : (int32_t *)(b + q.off[1]);
-      void *ov = q.direct ? q.d_vals : b + q.off[2];
+      int32_t *rp = q.direct ? q.r.row_ptr : (int32_t *)(b + q.off[0]);
+      int32_t *oc = q.direct ? q.r.out_cols : (int32_t *)(b + q.off[1]);
+      void *ov = q.direct ? q.r.out_vals : b + q.off[2];
       DCSR_TRY(export_csr(h, rp, oc, ov, q.direct ? q.r.cap : INT64_MAX, st, &sl.core.ar));
-      DCSR_CUDA(cudaMemcpyAsync(sl.nnz_host + q.item, rp + h->n_rows, 4, cudaMemcpyDefault, st));
+      DCSR_CUDA(cudaMemcpyAsync(sl.nnz_host + q.item, rp + h->n_rows, 4, cudaMemcpyDeviceToHost, st));
       // a staged export's row pointer now; its entries once their count is known
       if (!q.direct)
         DCSR_CUDA(cudaMemcpyAsync(q.r.row_ptr, rp, 4 * ((size_t)h->n_rows + 1), cudaMemcpyDefault, st));
