@@ -21,6 +21,12 @@ constexpr unsigned FULL = 0xffffffffu;
 extern std::atomic<uint64_t> g_launches;
 inline void count_launch(uint64_t n = 1) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 
+// Debugging aid: with DCSR_DEBUG_SYNC=1 in the environment every launch
+// outside stream capture is followed by a synchronisation of its stream,
+// and a failing kernel is named (file:line) on stderr.
+bool debug_sync();
+void debug_check(cudaStream_t s, const char *kernel, const char *file, int line);
+
 #define DCSR_CUDA(call)                                                                         \
   do {                                                                                          \
     cudaError_t _e = (call);                                                                    \
@@ -37,11 +43,12 @@ inline void count_launch(uint64_t n = 1) { g_launches.fetch_add(n, std::memory_o
   } while (0)
 
 // Launch with the launch counter and an error check.
-#define DCSR_LAUNCH(kernel, grid, block, smem, stream, ...)          \
-  do {                                                               \
-    kernel<<<(grid), (block), (smem), (stream)>>>(__VA_ARGS__);      \
-    ::dcsr::count_launch();                                          \
-    DCSR_CUDA(cudaGetLastError());                                   \
+#define DCSR_LAUNCH(kernel, grid, block, smem, stream, ...)                          \
+  do {                                                                               \
+    kernel<<<(grid), (block), (smem), (stream)>>>(__VA_ARGS__);                      \
+    ::dcsr::count_launch();                                                          \
+    DCSR_CUDA(cudaGetLastError());                                                   \
+    if (::dcsr::debug_sync()) ::dcsr::debug_check((stream), #kernel, __FILE__, __LINE__); \
   } while (0)
 
 __host__ __device__ inline int64_t align_up(int64_t x, int64_t a) { return (x + a - 1) / a * a; }

@@ -10,6 +10,21 @@ namespace dcsr {
 
 std::atomic<uint64_t> g_launches{0};
 
+bool debug_sync() {
+  static const bool on = [] {
+    const char *e = getenv("DCSR_DEBUG_SYNC");
+    return e && e[0] == '1';
+  }();
+  return on;
+}
+
+void debug_check(cudaStream_t s, const char *kernel, const char *file, int line) {
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) return;
+  const cudaError_t e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) fprintf(stderr, "dcsr: kernel %s (%s:%d) failed: %s\n", kernel, file, line, cudaGetErrorString(e));
+}
+
 int sm_count() {
   // function-local statics are initialised once, thread-safely (the server
   // launches from several threads)

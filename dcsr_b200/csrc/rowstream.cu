@@ -568,7 +568,7 @@ __device__ __forceinline__ void write_y(V *y, int64_t ldy, int32_t row, const do
 // over the window's row starts, sums use a segmented warp scan.
 // d0: the lane's row, its length and its layer-0 segment (start, capacity),
 // loaded ahead by the caller (row -1 past the matrix's end).
-template <typename V, int OP>
+template <typename V, int OP, bool XU>
 __device__ __forceinline__ void short_block_k1(const RowItem<V> &it, int4 d0, int lane) {
   using P = typename std::conditional<sizeof(V) == 4, float, double>::type;  // window partials
   constexpr int U = 4;
@@ -628,7 +628,9 @@ __device__ __forceinline__ void short_block_k1(const RowItem<V> &it, int4 d0, in
       V xv[U];
 #pragma unroll
       for (int i = 0; i < U; i++)
-        xv[i] = OP == OP_SPMV && base + 32 * i < E ? __ldg(x + (int64_t)col[i] * it.ldx) : V(0);
+        xv[i] = OP != OP_SPMV || base + 32 * i >= E ? V(0)
+                : XU                                ? __ldg(x + col[i])
+                                                    : __ldg(x + (int64_t)col[i] * it.ldx);
 #pragma unroll
       for (int i = 0; i < U; i++) {
         if (base + 32 * i >= E) continue;
@@ -835,7 +837,7 @@ __global__ void __launch_bounds__(RS_THREADS_, RowsMinBlocks<K>::N) k_rows_reduc
           const int2 s0 = __ldg(reinterpret_cast<const int2 *>(m.seg + 2 * r));
           d0 = make_int4((int32_t)r, __ldg(m.row_sizes + r), s0.x, s0.y - s0.x);
         }
-        short_block_k1<V, OP>(it, d0, lane);
+        short_block_k1<V, OP, false>(it, d0, lane);
       } else {
         // K values per entry: G lanes per row
         const RowBlock rb = load_block(m, blk * 32, lane, it.short_max);
@@ -1069,11 +1071,11 @@ __device__ __forceinline__ void unit_range(const Unit1 &x, int64_t &c0, int64_t 
 // Loads of one step (UN windows of 32 entries) of a streamed unit lying in
 // one segment (first pool slot d.z), entries [o, o + 32*UN) of the unit.
 template <typename V, int UN, int OP>
-__device__ __forceinline__ void load_step(const Mat<V> &m, int64_t base, int64_t n, int64_t o, int lane, V (&a)[UN],
+__device__ __forceinline__ void load_step(const Mat<V> &m, int32_t base, int32_t n, int32_t o, int lane, V (&a)[UN],
                                           int32_t (&col)[UN]) {
 #pragma unroll
   for (int i = 0; i < UN; i++) {
-    const int64_t p = o + 32 * i + lane, q = base + (p < n ? p : 0);
+    const int32_t p = o + 32 * i + lane, q = base + (p < n ? p : 0);  // pool slots are below 2^31
     a[i] = __ldcs(m.vals + q);
     col[i] = OP == OP_SPMV ? __ldcs(m.cols + q) : 0;
   }
@@ -1117,7 +1119,7 @@ __device__ __forceinline__ void finish_unit(const RowItem<V> &it, const Unit1 &x
 }
 
 // The streamed units (long-row chunks, then medium rows) of a k = 1 pass.
-template <typename V, int OP, typename Src>
+template <typename V, int OP, typename Src, bool XU>
 __global__ void __launch_bounds__(RS_THREADS_, DCSR_K1_MINB) k_rows1(Src src) {
   using P = typename std::conditional<sizeof(V) == 4, float, double>::type;
   constexpr int UN = sizeof(V) == 8 && DCSR_K1_UN > 1 ? DCSR_K1_UN / 2 : DCSR_K1_UN;
@@ -1147,10 +1149,11 @@ __global__ void __launch_bounds__(RS_THREADS_, DCSR_K1_MINB) k_rows1(Src src) {
   fetch_issue();
   V a0[UN], a1[UN];
   int32_t k0[UN], k1[UN];
-  int64_t c0 = 0, c1 = 0, o = 0;  // cur's range and the current step's offset in it
+  int64_t c0 = 0, c1 = 0;  // cur's range
+  int32_t o = 0;           // the current step's offset in it
   if (streamed(cur)) {
     unit_range(cur, c0, c1);
-    if (cur.d.z >= 0) load_step<V, UN, OP>(src.item(cur.item).m, cur.d.z, c1 - c0, 0, lane, a0, k0);
+    if (cur.d.z >= 0) load_step<V, UN, OP>(src.item(cur.item).m, cur.d.z, (int32_t)(c1 - c0), 0, lane, a0, k0);
   }
   double acc = op_init<double, OP>();
   // One step: consume (ca, cc), loading the following step into (na, nc).
@@ -1166,23 +1169,24 @@ __global__ void __launch_bounds__(RS_THREADS_, DCSR_K1_MINB) k_rows1(Src src) {
         if (streamed(nx) && nx.d.z >= 0) {  // the next unit's first step, into the buffer consumed next
           int64_t d0, d1;
           unit_range(nx, d0, d1);
-          load_step<V, UN, OP>(src.item(nx.item).m, nx.d.z, d1 - d0, 0, lane, na, nc);
+          load_step<V, UN, OP>(src.item(nx.item).m, nx.d.z, (int32_t)(d1 - d0), 0, lane, na, nc);
         }
       } else {
-        const int64_t n = c1 - c0;
+        const int32_t n = (int32_t)(c1 - c0);
         const bool last = o + W >= n;
         if (!last) {
           load_step<V, UN, OP>(it.m, cur.d.z, n, o + W, lane, na, nc);
         } else if (streamed(nx) && nx.d.z >= 0) {
           int64_t d0, d1;
           unit_range(nx, d0, d1);
-          load_step<V, UN, OP>(src.item(nx.item).m, nx.d.z, d1 - d0, 0, lane, na, nc);
+          load_step<V, UN, OP>(src.item(nx.item).m, nx.d.z, (int32_t)(d1 - d0), 0, lane, na, nc);
         }
         // every x gather of the step issued before the first is used (lanes
         // past the unit's end loaded its first entry: their columns are valid)
         V xv[UN];
 #pragma unroll
-        for (int i = 0; i < UN; i++) xv[i] = OP == OP_SPMV ? __ldg(it.x + (int64_t)cc[i] * it.ldx) : V(0);
+        for (int i = 0; i < UN; i++)
+          xv[i] = OP != OP_SPMV ? V(0) : XU ? __ldg(it.x + cc[i]) : __ldg(it.x + (int64_t)cc[i] * it.ldx);
         P w = op_init<P, OP>();
 #pragma unroll
         for (int i = 0; i < UN; i++) {
@@ -1205,7 +1209,7 @@ __global__ void __launch_bounds__(RS_THREADS_, DCSR_K1_MINB) k_rows1(Src src) {
     } else if (streamed(nx) && nx.d.z >= 0) {  // a skipped unit: the next one's first step
       int64_t d0, d1;
       unit_range(nx, d0, d1);
-      load_step<V, UN, OP>(src.item(nx.item).m, nx.d.z, d1 - d0, 0, lane, na, nc);
+      load_step<V, UN, OP>(src.item(nx.item).m, nx.d.z, (int32_t)(d1 - d0), 0, lane, na, nc);
     }
     if (advance) {
       cur = nx;
@@ -1232,7 +1236,7 @@ __global__ void __launch_bounds__(RS_THREADS_, DCSR_K1_MINB) k_rows1(Src src) {
 // The short-row blocks of a k = 1 pass: a warp per block of 32 rows, the
 // next block's descriptors (each lane's row length and layer-0 segment)
 // loaded while the current block runs.
-template <typename V, int OP, typename Src>
+template <typename V, int OP, typename Src, bool XU>
 __global__ void __launch_bounds__(RS_THREADS_, DCSR_K1B_MINB) k_rows1_blocks(Src src) {
   const int lane = threadIdx.x & 31;
   const int64_t NB = src.units(P_BLOCKS) * RS_WARPS;
@@ -1250,7 +1254,7 @@ __global__ void __launch_bounds__(RS_THREADS_, DCSR_K1B_MINB) k_rows1_blocks(Src
   while (cur.u < total) {
     const Unit1 nx = unit1_load<V>(src, base + fetch_take(), base, 0, total, lane);
     fetch_issue();
-    if (cur.kind == U1_BLOCK) short_block_k1<V, OP>(src.item(cur.item), cur.d, lane);
+    if (cur.kind == U1_BLOCK) short_block_k1<V, OP, XU>(src.item(cur.item), cur.d, lane);
     cur = nx;
   }
   if (lane == 0 && atomicAdd(ctr + 1, 1u) == gridDim.x * RS_WARPS - 1) {
@@ -1385,10 +1389,12 @@ static int grid_of(const void *k) { return persistent_grid(k, RS_THREADS_, 0); }
 template <typename V, int K, int OP, bool VEC, typename Src>
 static int launch_reduce_src(const Src &src, cudaStream_t s) {
   if constexpr (K == 1) {  // one value per entry: streamed units, then short-row blocks
-    static const int g = grid_of((const void *)k_rows1<V, OP, Src>);
-    static const int gb = grid_of((const void *)k_rows1_blocks<V, OP, Src>);
-    DCSR_LAUNCH((k_rows1<V, OP, Src>), g, RS_THREADS_, 0, s, src);
-    DCSR_LAUNCH((k_rows1_blocks<V, OP, Src>), gb, RS_THREADS_, 0, s, src);
+    // VEC (k = 1): x has unit stride, gathered without the stride multiply
+    constexpr bool XU = VEC && OP == OP_SPMV;
+    static const int g = grid_of((const void *)k_rows1<V, OP, Src, XU>);
+    static const int gb = grid_of((const void *)k_rows1_blocks<V, OP, Src, XU>);
+    DCSR_LAUNCH((k_rows1<V, OP, Src, XU>), g, RS_THREADS_, 0, s, src);
+    DCSR_LAUNCH((k_rows1_blocks<V, OP, Src, XU>), gb, RS_THREADS_, 0, s, src);
     return DCSR_OK;
   } else {
     static const int g0 = grid_of((const void *)k_rows_reduce<V, K, OP, VEC, P_BLOCKS, Src>);
@@ -1424,7 +1430,8 @@ template <typename V, int K>
 static int spmv_k(dcsr_handle h, const V *x, int64_t ldx, V *y, int64_t ldy, double alpha, double beta,
                   cudaStream_t s) {
   const size_t rb = K * sizeof(V), al = (rb & (0 - rb)) >= 32 ? 32 : (rb & (0 - rb));  // row alignment
-  const bool vec = K > 1 && (K % 2 == 0) && ldx == K && ((uintptr_t)x % al) == 0;
+  // k >= 2: packed, aligned rows of x (vector loads); k = 1: x of unit stride
+  const bool vec = K == 1 ? ldx == 1 : (K % 2 == 0) && ldx == K && ((uintptr_t)x % al) == 0;
   if (vec) return launch_reduce<V, K, OP_SPMV, true>(h, x, ldx, y, ldy, alpha, beta, s);
   return launch_reduce<V, K, OP_SPMV, false>(h, x, ldx, y, ldy, alpha, beta, s);
 }

@@ -498,7 +498,11 @@ int retire(dcsr_server s, Slot &sl) {
       copies = true;
     }
   }
-  if (copies) {
+  // staged exports' copies, and pools grown ahead (a new pool filled by a
+  // copy on this stream), must complete before the batch finishes: finish
+  // releases the matrices, and the next batch using one may run on another
+  // stream
+  if (copies || sl.grows > 0) {
     DCSR_CUDA(cudaEventRecord(sl.done, st));
     sl.phase = 2;
     return DCSR_OK;
