@@ -503,18 +503,19 @@ int dcsr_batch_grow(dcsr_batch b, int32_t *grown, void *stream) {
         continue;
       }
       const long long need = b->status_host[2 * j + 1];
-      // room for the larger of an eighth of the pool and two more runs
-      // growing it as much as the last one did (the same item's next update
-      // has as many triples)
+      // grown when less room is left than the larger of an eighth of the
+      // pool and two more runs growing it as much as the last one did (or
+      // adding all of the item's triples: its next update has as many), then
+      // to room for four such runs, so a growing matrix is grown every few
+      // runs rather than every run (each growth allocates and copies a pool)
       const long long prev = b->last_need[i];
       const long long step = prev >= 0 && need > prev ? need - prev : 0;
       b->last_need[i] = need;
       const long long T = b->core.items[i].nnz;  // at most T new entries next run, before relocations
-      long long room = h->pool_cap / 8;
-      if (room < 2 * step) room = 2 * step;
-      if (room < 2 * T) room = 2 * T;
+      const long long run = step > T ? step : T;
+      const long long room = h->pool_cap / 8 > 2 * run ? h->pool_cap / 8 : 2 * run;
       if (h->pool_cap - need < room) {
-        DCSR_TRY(reserve(h, grow_target(h, need + room), (cudaStream_t)stream));  // keeps the pool top
+        DCSR_TRY(reserve(h, grow_target(h, need + 2 * room), (cudaStream_t)stream));  // keeps the pool top
         n++;
       }
     }

@@ -301,14 +301,15 @@ int dcsr_batch_capture(dcsr_batch b, void *stream);
 int dcsr_batch_launch(dcsr_batch b, void *stream);
 /* Per-matrix statuses of the last run (synchronises, clears them). */
 int dcsr_batch_status(dcsr_batch b, int32_t *statuses, void *stream);
-/* After dcsr_batch_status (and dcsr_batch_repair): grow the pool of every
- * matrix whose accepted update left less room than the largest of an eighth
- * of its pool, twice the pool top's growth since the previous call and twice
- * its triple count (its next update has as many triples), and of every
- * rejected (repaired) one by twice its triple count, stream-ordered, so the
- * next run's update is not rejected for space and needs no repair.  Contents, row lengths, segment tables and
- * the pool top are unchanged; only the pool capacity grows.  *grown (may be
- * NULL) = matrices grown. */
+/* After dcsr_batch_status (and dcsr_batch_repair): grow, stream-ordered, the
+ * pool of every matrix whose accepted update left less room than
+ * max(pool / 8, 2 x run), run = the larger of the pool top's growth since the
+ * previous call and its triple count (its next update has as many triples),
+ * to twice that room, and the pool of every rejected (repaired) one by twice
+ * its triple count, so the next runs' updates are not rejected for space and
+ * need no repair.  Contents, row lengths, segment tables and the pool top
+ * are unchanged; only the pool capacity grows.  *grown (may be NULL) =
+ * matrices grown. */
 int dcsr_batch_grow(dcsr_batch b, int32_t *grown, void *stream);
 /* For matrices whose update was rejected: apply the repair policy
  * (compact, grow) and redo their update and SpMV per call.  Returns the
