@@ -38,15 +38,21 @@ enum { SG_EMPTY = 0, SG_WARP = 1, SG_CTA = 2, SG_GLOBAL = 3 };
 template <typename V>
 __global__ void k_sg_count(Mat<V> A, Mat<V> B, dcsr_opts co, long long *cnt, long long *capub,
                            unsigned long long *cls, unsigned *rows, unsigned long long *gtotal) {
-  const int lane = threadIdx.x & 31;
+  constexpr int G = 8;  // lanes per row: a warp has four rows' loads in flight
+  const int lane = threadIdx.x & 31, j = lane & (G - 1);
   const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  for (int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < A.n_rows; i += nw) {
-    const Chain ch = load_chain(A, (int32_t)i);
-    const int64_t L = A.row_sizes[i];
+  for (int64_t i0 = (((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * (32 / G); i0 < A.n_rows;
+       i0 += nw * (32 / G)) {
+    const int64_t i = i0 + lane / G;
     long long s = 0;
-    for (int64_t p = lane; p < L; p += 32) s += B.row_sizes[A.cols[ch.phys(p)]];
-    s = warp_sum(s);
-    if (lane == 0) {
+    if (i < A.n_rows) {
+      const Chain ch = load_chain(A, (int32_t)i);
+      const int64_t L = A.row_sizes[i];
+      for (int64_t p = j; p < L; p += G) s += B.row_sizes[A.cols[ch.phys(p)]];
+    }
+#pragma unroll
+    for (int o = G / 2; o > 0; o >>= 1) s += __shfl_xor_sync(FULL, s, o);
+    if (j == 0 && i < A.n_rows) {
       cnt[i] = s;
       capub[i] = policy_cap(co, s);
       const int c = s == 0 ? SG_EMPTY : s <= SG_WARP_MAX ? SG_WARP : s <= SG_CTA_MAX ? SG_CTA : SG_GLOBAL;
@@ -461,7 +467,7 @@ static int spgemm_impl(dcsr_handle hA, dcsr_handle hB, dcsr_handle hC, cudaStrea
   long long *ub = cnt;  // scanned in place
   DCSR_CUDA(cudaMemsetAsync(starts, 0, sizeof(long long) * 8, s));
   if (n > 0) {
-    DCSR_LAUNCH(k_sg_count<V>, grid_for((int64_t)n * 32, SG_THREADS), SG_THREADS, 0, s, A, B, hC->o, cnt, capub, k0,
+    DCSR_LAUNCH(k_sg_count<V>, grid_for((int64_t)n * 8, SG_THREADS), SG_THREADS, 0, s, A, B, hC->o, cnt, capub, k0,
                 r0, (unsigned long long *)(starts + 5));
     if (n > 1) DCSR_TRY(radix_sort_pairs(&k0, &r0, &k1, &r1, n, 2, ar, s));
   }
