@@ -8,9 +8,10 @@
 //          one value per entry (SpMV k=1, row reductions, the copy pass) it
 //          streams each segment layer's entries across its lanes, U windows
 //          of 32 entries at a time with every window's loads issued first; a
-//          lane's row comes from ballots over the window's row starts
-//          (__fns) and sums use a segmented scan whose segment tests are bit
-//          operations on that start mask -- uneven rows cost nothing extra.
+//          lane's row is found by a binary search over the lanes' row
+//          offsets and sums use a segmented scan whose segment test is one
+//          compare with the start of the lane's row in the window -- uneven
+//          rows cost nothing extra.
 //          With k >= 2 values per entry (where the scan's k shuffles per
 //          step would dominate) the warp splits into groups of G lanes, G in
 //          {1..16} from the block's mean row length; a group walks one row
@@ -564,8 +565,9 @@ __device__ __forceinline__ void write_y(V *y, int64_t ldy, int32_t row, const do
 // ------------------------------------------------- k = 1 short-row block
 // One warp, one block of 32 consecutive rows: one value per entry (SpMV
 // k = 1, row reductions), the block's entries streamed across the lanes in
-// windows of 32, U windows' loads in flight; a lane's row comes from ballots
-// over the window's row starts, sums use a segmented warp scan.
+// windows of 32, U windows' loads in flight (windows past the block's end
+// skipped); a lane's row comes from a binary search over the lanes' row
+// offsets, sums use a segmented warp scan.
 // d0: the lane's row, its length and its layer-0 segment (start, capacity),
 // loaded ahead by the caller (row -1 past the matrix's end).
 template <typename V, int OP, bool XU>
