@@ -1,7 +1,7 @@
 // batch.cu -- the batched form: many matrices, each with an update batch and
 // an SpMV, run as one merged update (one key sort, one plan, one apply over
 // the union of their triples), one schedule rebuild over all their rows and
-// one SpMV pass per distinct RHS count -- about thirty kernels for the whole
+// one SpMV pass per distinct RHS count -- about fifty kernels for the whole
 // set, whatever its size, optionally replayed as one CUDA graph.
 //
 // Kernels read the matrices through device-resident descriptor arrays
