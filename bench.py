@@ -996,7 +996,8 @@ def main():
     ap.add_argument("--depth", type=int, default=8)
     ap.add_argument("--workers", type=int, default=2)
     ap.add_argument("--repeats", type=int, default=3, help="Poisson replays per served load point (median p99)")
-    ap.add_argument("--load-fracs", type=float, nargs="+", default=[0.3, 0.4, 0.5, 0.55, 0.6, 0.65, 0.7, 0.75, 0.85])
+    ap.add_argument("--load-fracs", type=float, nargs="+",
+                    default=[0.3, 0.4, 0.5, 0.55, 0.6, 0.625, 0.65, 0.675, 0.7, 0.725, 0.75, 0.8, 0.85])
     ap.add_argument("--plain-fracs", type=float, nargs="+", default=[0.5, 0.7, 0.9])
     ap.add_argument("--batched-mats", type=int, default=512)
     ap.add_argument("--batched-reps", type=int, default=5)
