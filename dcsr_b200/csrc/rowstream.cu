@@ -47,7 +47,10 @@ constexpr int RS_WARPS = RS_THREADS_ / 32;
 // (k_rows1), one CTA's in the k >= 2 and copy passes.  Small enough that a
 // power-law matrix's hottest rows spread over many warps; multi-chunk rows
 // combine their partials in chunk order.
-constexpr int CHUNK = 2048;
+#ifndef DCSR_CHUNK
+#define DCSR_CHUNK 2048
+#endif
+constexpr int CHUNK = DCSR_CHUNK;
 constexpr int STEP = 4096;    // entries a CTA has in flight per step
 enum { P_BLOCKS = 0, P_CHUNKS = 1, P_MED = 2 };
 
