@@ -72,9 +72,9 @@ def peaks():
 # DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) of one k = 1
 # SpMV call (its two launches, k_rows1 + k_rows1_blocks) on the update-stream
 # matrix, from one ncu capture of the same seeded workload in the same state
-# (profiles/spmv_rmat_k1_f32.md gives the command): keyed by the matrix's
-# stored-entry count, so a run on another state reports no traffic rather
-# than a scaled one.
+# (this file's stream part with --skip-batched --skip-spgemm --skip-served,
+# the 4th roofline call): keyed by the matrix's stored-entry count, so a run
+# on another state reports no traffic rather than a scaled one.
 SPMV_TRAFFIC = {32832123: 235237120 + 3247104 + 118304256 + 560384}
 
 
