@@ -12,7 +12,7 @@
 //            APPEND: the reference's segment walk per touched row
 //   alloc    exclusive scan of new segment sizes (row order, per matrix
 //            offsets taken relative to its first touched row)
-//   check    per matrix: pool / layer / index verdict -> go flag  k_check
+//   check    per matrix: pool / layer / index status -> go flag   k_check
 //   apply    existing columns in place (thread per group), then per row
 //            the in-place shift + inserts (8- or 32-lane sub-warps)
 //   relocate rows whose in-place shift would exceed reloc_min, and rows
@@ -361,7 +361,7 @@ __global__ void k_plan_append(Src src, int64_t T, const long long *gstat, const 
   }
 }
 
-// Per matrix: requirement from the scanned capacities, verdict and go flag.
+// Per matrix: requirement from the scanned capacities, status and go flag.
 template <typename V, typename Src>
 __global__ void k_check(Src src, int count, const long long *addr) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
