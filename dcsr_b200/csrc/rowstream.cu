@@ -51,6 +51,21 @@ constexpr int RS_WARPS = RS_THREADS_ / 32;
 #define DCSR_CHUNK 2048
 #endif
 constexpr int CHUNK = DCSR_CHUNK;
+// Windows of 32 entries a warp has in flight per step, and blocks per SM the
+// k = 1 pass is compiled for.
+#ifndef DCSR_K1_UN
+#define DCSR_K1_UN 4
+#endif
+#ifndef DCSR_K1_MINB
+#define DCSR_K1_MINB 3
+#endif
+#ifndef DCSR_K1B_MINB
+#define DCSR_K1B_MINB 4
+#endif
+// Windows of 32 entries whose loads a short-row block has in flight.
+#ifndef DCSR_K1B_U
+#define DCSR_K1B_U 4
+#endif
 constexpr int STEP = 4096;    // entries a CTA has in flight per step
 enum { P_BLOCKS = 0, P_CHUNKS = 1, P_MED = 2 };
 
@@ -576,7 +591,7 @@ __device__ __forceinline__ void write_y(V *y, int64_t ldy, int32_t row, const do
 template <typename V, int OP, bool XU>
 __device__ __forceinline__ void short_block_k1(const RowItem<V> &it, int4 d0, int lane) {
   using P = typename std::conditional<sizeof(V) == 4, float, double>::type;  // window partials
-  constexpr int U = 4;
+  constexpr int U = DCSR_K1B_U;
   const Mat<V> &m = it.m;
   const V *__restrict__ x = it.x;
   RowBlock rb;
@@ -900,17 +915,7 @@ __global__ void __launch_bounds__(RS_THREADS_, RowsMinBlocks<K>::N) k_rows_reduc
 
 // Entries [c0, c1) of a row (chain ch) streamed across the warp; returns the
 // lane's partial.
-// Windows of 32 entries a warp has in flight per step, and blocks per SM the
-// k = 1 pass is compiled for.
-#ifndef DCSR_K1_UN
-#define DCSR_K1_UN 4
-#endif
-#ifndef DCSR_K1_MINB
-#define DCSR_K1_MINB 3
-#endif
-#ifndef DCSR_K1B_MINB
-#define DCSR_K1B_MINB 4
-#endif
+
 
 // Entries [c0, c1) of a row whose range lies in one segment starting at pool
 // slot st: two sets of UN windows, the loads of the next set in flight while
