@@ -994,7 +994,7 @@ def main():
     ap.add_argument("--plain-requests", type=int, default=6000)
     ap.add_argument("--max-batch", type=int, default=256)
     ap.add_argument("--depth", type=int, default=8)
-    ap.add_argument("--workers", type=int, default=2)
+    ap.add_argument("--workers", type=int, default=4)
     ap.add_argument("--repeats", type=int, default=3, help="Poisson replays per served load point (median p99)")
     ap.add_argument("--load-fracs", type=float, nargs="+",
                     default=[0.3, 0.4, 0.5, 0.55, 0.6, 0.625, 0.65, 0.675, 0.7, 0.725, 0.75, 0.8, 0.85])
