@@ -375,7 +375,10 @@ constexpr int RS_WARPS = RS_THREADS / 32;
 constexpr int RS_BINS = 256;
 // items per lane: 16 for large inputs (three kernels per pass), 8 up to RS_MID
 // items (single-pass scatter)
-constexpr int64_t RS_MID = 1 << 18;
+#ifndef DCSR_RS_MID_LOG2
+#define DCSR_RS_MID_LOG2 18
+#endif
+constexpr int64_t RS_MID = int64_t(1) << DCSR_RS_MID_LOG2;
 
 __device__ __forceinline__ unsigned lanemask_lt() {
   unsigned m;
