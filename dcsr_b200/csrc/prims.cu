@@ -357,9 +357,9 @@ int scan2_i64(const long long *in0, long long *out0, long long *total0, const lo
 
 // ------------------------------------------------------------ radix sort
 //
-// Stable LSD radix sort, 8-bit digits.  Up to RS_MID keys (where the launch
-// count of a sort matters more than its bandwidth), one pass over the keys per
-// digit plus one histogram pass: (1) one kernel counts the digits of every
+// Stable LSD radix sort, 8-bit digits.  Up to RS_MID = 2^22 keys, one pass
+// over the keys per digit plus one histogram pass (a 1M-triple update's sort
+// ran 12 % faster this way than with the three-kernel passes below): (1) one kernel counts the digits of every
 // pass at once into per-pass histograms; (2) per pass, one scatter kernel:
 // each block takes the next tile, ranks its items per warp with match_any
 // (ties keep input order), orders its warps by a per-digit prefix, and finds
@@ -368,7 +368,8 @@ int scan2_i64(const long long *in0, long long *out0, long long *total0, const lo
 // the exclusive scan of the pass's histogram.  Larger inputs use three
 // kernels per pass (tile histograms, the exclusive scan of the digit-major
 // histogram table, a scatter with the same ranking and the scanned offsets),
-// which keeps look-back latency off the critical path.
+// which bounds the look-back area (one slot per tile and digit) for the
+// largest sorts.
 
 constexpr int RS_THREADS = 256;
 constexpr int RS_WARPS = RS_THREADS / 32;
@@ -376,7 +377,7 @@ constexpr int RS_BINS = 256;
 // items per lane: 16 for large inputs (three kernels per pass), 8 up to RS_MID
 // items (single-pass scatter)
 #ifndef DCSR_RS_MID_LOG2
-#define DCSR_RS_MID_LOG2 18
+#define DCSR_RS_MID_LOG2 22
 #endif
 constexpr int64_t RS_MID = int64_t(1) << DCSR_RS_MID_LOG2;
 

@@ -1,7 +1,7 @@
 """The single-pass scan and radix sort (decoupled look-back) at the sizes
 where they take over from the one-block kernels (scans above 4096 values,
 sorts above 8192 keys) and where sorts switch to three kernels per pass
-(above 2^18 keys), against the oracle: COO loads (stable sort of (row,
+(above 2^22 keys), against the oracle: COO loads (stable sort of (row,
 column) keys, merge of duplicates), updates (a sort and four scans per
 batch), reduce-by-key (a scan), in place and repeated on one handle so the
 look-back epochs advance; and no look-back wait ever gave up."""
@@ -30,7 +30,7 @@ def no_new_faults(dcsr):
     assert spin_faults(dcsr) == before
 
 
-@pytest.mark.parametrize("T", [8193, 2048 * 37 + 5, 262_144, 262_145, 1_500_000])
+@pytest.mark.parametrize("T", [8193, 2048 * 37 + 5, 262_145, 1_500_000, 4_194_304, 4_194_305])
 @pytest.mark.parametrize("mode", [0, 1])
 def test_coo_load_sizes(dcsr, T, mode):
     rng = np.random.default_rng(T + mode)
