@@ -932,6 +932,9 @@ def run_ours(args, rank, world, local_rank):
                                "server's p99 at its highest load (90% of its capacity); device-resident request "
                                f"buffers; each load point the median-p99 of {args.repeats} replays",
                    "parallelism": f"matrix shards x{world} (no data-path collective)",
+                   "step": f"one served request (ms_per_step = 1/value); `steps`/`warmup` are the update-stream "
+                           f"part's; the served sweep replays {args.served_requests} requests per load point, "
+                           f"{len(args.load_fracs)} load points x {args.repeats} replays, after a warm-up pass",
                    "l2": "working sets > L2 (60 GB resident; SpMV roofline flushes L2 between launches)"},
         "p50_ms": served["p50_ms"], "p99_ms": served["p99_ms"],
         "plain": served["plain"], "plain_host_buffers": served["plain_host_buffers"], "served": served["served"],
