@@ -139,6 +139,7 @@ _SIGS = {
     "dcsr_measure_gather": (_i32, [_vp, _vp, _i64, _vp, _vp, _i32, _vp]),
     "dcsr_cg": (_i32, [_vp, _vp, _vp, _i32, _dbl, _dbl, C.POINTER(_i32), C.POINTER(_dbl), _vp]),
     "dcsr_pool_reserve": (C.c_int, [C.c_int64, C.c_void_p]),
+    "dcsr_pool_usage": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     "dcsr_version": (C.c_char_p, []),
 }
 
@@ -179,9 +180,18 @@ def debug_lookback(spin_limit: int = 0, stall_first_tile: bool = False):
 
 
 def pool_reserve(nbytes: int, stream=None):
-    """Pre-grow the device memory pool the library allocates from (kept for
-    later growth of matrices, scratch and staging)."""
+    """Make sure `nbytes` of device memory reserved for the library are free
+    (mapped up front; later growth of matrices, scratch and staging is carved
+    from it with no driver allocation)."""
     _check(lib().dcsr_pool_reserve(int(nbytes), _stream(stream)), "dcsr_pool_reserve")
+
+
+def pool_usage():
+    """(reserved bytes, free bytes, allocations made outside the reserve) of
+    the current device."""
+    r, f, n = C.c_int64(), C.c_int64(), C.c_int64()
+    _check(lib().dcsr_pool_usage(C.byref(r), C.byref(f), C.byref(n)), "dcsr_pool_usage")
+    return r.value, f.value, n.value
 
 
 def _check(st: int, what: str):

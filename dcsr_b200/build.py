@@ -32,7 +32,8 @@ def nvcc() -> str:
 
 
 def _headers():
-    return glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(ROOT, "include", "*.h"))
+    return (glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(CSRC, "*.hpp")) +
+            glob.glob(os.path.join(ROOT, "include", "*.h")))
 
 
 def _compile(src: str, extra: list[str]) -> str:

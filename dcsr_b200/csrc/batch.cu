@@ -92,10 +92,10 @@ void fill_image(const BatchCore &b, unsigned char *img) {
 template <typename T>
 int grow_dev(T **p, size_t n, size_t &cap, cudaStream_t s) {
   if (n <= cap && *p) return DCSR_OK;
-  if (*p) DCSR_CUDA(cudaFreeAsync(*p, s));
+  if (*p) DCSR_CUDA(dcsr::dev_free(*p, s));
   *p = nullptr;
   cap = 0;
-  DCSR_CUDA(cudaMallocAsync((void **)p, sizeof(T) * (n ? n : 1), s));
+  DCSR_CUDA(dcsr::dev_alloc((void **)p, sizeof(T) * (n ? n : 1), s));
   cap = n;
   return DCSR_OK;
 }
@@ -214,7 +214,7 @@ int BatchCore::plan(const dcsr_batch_item *its, int n, cudaStream_t s, bool all_
   cnt_cap = n > cnt_cap ? n : cnt_cap;
   DCSR_TRY(grow_dev(&pref, poff, pref_cap, s));
   if (!gstat) {
-    DCSR_CUDA(cudaMallocAsync((void **)&gstat, sizeof(long long) * ST_WORDS, s));
+    DCSR_CUDA(dcsr::dev_alloc((void **)&gstat, sizeof(long long) * ST_WORDS, s));
     DCSR_CUDA(cudaMemsetAsync(gstat, 0, sizeof(long long) * ST_WORDS, s));
   }
   return DCSR_OK;
@@ -348,11 +348,11 @@ void BatchCore::release() {
   // Device buffers: stream-ordered frees on the legacy default stream (after
   // the work queued on blocking streams; the host does not wait).  The pinned
   // image: once its last upload has been copied.
-  if (img_dev) cudaFreeAsync(img_dev, 0);
-  if (skip) cudaFreeAsync(skip, 0);
-  if (status_dev) cudaFreeAsync(status_dev, 0);
-  if (pref) cudaFreeAsync(pref, 0);
-  if (gstat) cudaFreeAsync(gstat, 0);
+  if (img_dev) dcsr::dev_free(img_dev, 0);
+  if (skip) dcsr::dev_free(skip, 0);
+  if (status_dev) dcsr::dev_free(status_dev, 0);
+  if (pref) dcsr::dev_free(pref, 0);
+  if (gstat) dcsr::dev_free(gstat, 0);
   ar.release(0);
   if (up_ev) {
     cudaEventSynchronize(up_ev);
@@ -553,7 +553,7 @@ int dcsr_batch_autotune(dcsr_batch b, void *stream, int32_t *short_max, int32_t 
   for (const auto &it : c.items)
     if (it.x && it.matrix->n_rows > 0) ybytes += align_up((int64_t)(it.matrix->vsize() * it.k * it.matrix->n_rows), 256);
   unsigned char *yscratch = nullptr;
-  if (ybytes) DCSR_CUDA(cudaMallocAsync((void **)&yscratch, ybytes, s));
+  if (ybytes) DCSR_CUDA(dcsr::dev_alloc((void **)&yscratch, ybytes, s));
   size_t off = 0;
   for (const auto &it : c.items) {
     if (!it.x || it.matrix->n_rows == 0) continue;
@@ -636,7 +636,7 @@ int dcsr_batch_autotune(dcsr_batch b, void *stream, int32_t *short_max, int32_t 
     g.split = best_split > 0 ? best_split : short_split(blocks, g.k);
   }
   for (auto &it : c.items) dcsr_set_row_classes(it.matrix, best_s, best_l);
-  if (yscratch) cudaFreeAsync(yscratch, s);
+  if (yscratch) dcsr::dev_free(yscratch, s);
   DCSR_CUDA(cudaStreamSynchronize(s));
   if (st != DCSR_OK) return st;
   if (short_max) *short_max = best_s;

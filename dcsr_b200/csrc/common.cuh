@@ -27,6 +27,21 @@ inline void count_launch(uint64_t n = 1) { g_launches.fetch_add(n, std::memory_o
 bool debug_sync();
 void debug_check(cudaStream_t s, const char *kernel, const char *file, int line);
 
+// The library's device memory (devmem.cu): a block of the regions that
+// dcsr_pool_reserve mapped, ordered after its previous user's work on
+// another stream, else the driver's stream-ordered allocation.  Every
+// buffer the library allocates goes through these two calls.
+cudaError_t dev_alloc_raw(void **p, size_t bytes, cudaStream_t s);
+cudaError_t dev_free(void *p, cudaStream_t s);
+template <typename T>
+inline cudaError_t dev_alloc(T **p, size_t bytes, cudaStream_t s) {
+  return dev_alloc_raw(reinterpret_cast<void **>(p), bytes, s);
+}
+// Maps a region so that at least `bytes` of the current device's regions
+// are free; region usage of the current device.
+int reserve_regions(int64_t bytes, cudaStream_t s);
+int region_usage(int64_t *reserved, int64_t *free_bytes, int64_t *fallback);
+
 #define DCSR_CUDA(call)                                                                         \
   do {                                                                                          \
     cudaError_t _e = (call);                                                                    \
@@ -141,12 +156,12 @@ struct Arena {
       cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
       DCSR_CUDA(cudaStreamIsCapturing(s, &cs));
       if (cs != cudaStreamCaptureStatusNone) return DCSR_NOT_SUPPORTED;
-      if (lb) DCSR_CUDA(cudaFreeAsync(lb, s));
+      if (lb) DCSR_CUDA(dcsr::dev_free(lb, s));
       lb = nullptr;
       lb_slots = 0;
       const size_t want = slots + slots / 4 + 1024;
       const size_t bytes = LB_HEADER + 8 * want;
-      DCSR_CUDA(cudaMallocAsync((void **)&lb, bytes, s));
+      DCSR_CUDA(dcsr::dev_alloc((void **)&lb, bytes, s));
       DCSR_CUDA(cudaMemsetAsync(lb, 0, bytes, s));
       lb_slots = want;
     }
@@ -164,11 +179,11 @@ struct Arena {
     used = 0;
     overflow = false;
     if (bytes <= cap) return DCSR_OK;
-    if (base) DCSR_CUDA(cudaFreeAsync(base, s));
+    if (base) DCSR_CUDA(dcsr::dev_free(base, s));
     base = nullptr;
     cap = 0;
     size_t want = bytes + bytes / 4 + (1 << 20);
-    DCSR_CUDA(cudaMallocAsync((void **)&base, want, s));
+    DCSR_CUDA(dcsr::dev_alloc((void **)&base, want, s));
     cap = want;
     return DCSR_OK;
   }
@@ -187,8 +202,8 @@ struct Arena {
     return (T *)(base + off);
   }
   void release(cudaStream_t s) {
-    if (base) cudaFreeAsync(base, s);
-    if (lb) cudaFreeAsync(lb, s);
+    if (base) dcsr::dev_free(base, s);
+    if (lb) dcsr::dev_free(lb, s);
     base = nullptr;
     lb = nullptr;
     cap = used = lb_slots = 0;

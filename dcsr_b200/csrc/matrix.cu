@@ -144,8 +144,8 @@ static int64_t pool_bytes(dcsr_handle h, int64_t cap) { return cap * (int64_t)(s
 
 static void drop_spare(dcsr_handle h, cudaStream_t s) {
   if (!h->spare_cols) return;
-  cudaFreeAsync(h->spare_cols, s);
-  cudaFreeAsync(h->spare_vals, s);
+  dcsr::dev_free(h->spare_cols, s);
+  dcsr::dev_free(h->spare_vals, s);
   g_spare_bytes -= pool_bytes(h, h->spare_cap);
   h->spare_cols = nullptr;
   h->spare_vals = nullptr;
@@ -167,8 +167,8 @@ static int alloc_pool(dcsr_handle h, int64_t cap, int32_t **cols, void **vals, i
     h->spare_cap = 0;
     return DCSR_OK;
   }
-  DCSR_CUDA(cudaMallocAsync((void **)cols, cap * sizeof(int32_t), s));
-  DCSR_CUDA(cudaMallocAsync(vals, cap * h->vsize(), s));
+  DCSR_CUDA(dcsr::dev_alloc((void **)cols, cap * sizeof(int32_t), s));
+  DCSR_CUDA(dcsr::dev_alloc(vals, cap * h->vsize(), s));
   *got = cap;
   return DCSR_OK;
 }
@@ -187,8 +187,8 @@ static void free_pool(dcsr_handle h, cudaStream_t s) {
       h->spare_cap = h->buf_cap;
       g_spare_bytes += b;
     } else {
-      cudaFreeAsync(h->cols, s);
-      cudaFreeAsync(h->vals, s);
+      dcsr::dev_free(h->cols, s);
+      dcsr::dev_free(h->vals, s);
     }
   }
   h->cols = nullptr;
@@ -361,9 +361,10 @@ int reserve(dcsr_handle h, int64_t cap, cudaStream_t s) {
   return DCSR_OK;
 }
 
-// Pools and scratch use stream-ordered allocation; keep freed blocks in the
-// device's default pool instead of returning them at every sync, so a
-// compaction's fresh pool does not re-map memory each time (once per device).
+// Allocations the reserved regions cannot hold use stream-ordered
+// allocation; keep freed blocks in the device's default pool instead of
+// returning them at every sync, so a compaction's fresh pool does not re-map
+// memory each time (once per device).
 void keep_pool_memory() {
   static std::mutex mu;
   static bool configured[64] = {};
@@ -493,14 +494,14 @@ int dcsr_create(dcsr_handle *out, int32_t n_rows, int32_t n_cols, int32_t dtype,
   // non-blocking stream, then a wait for that stream only: creating a matrix
   // does not stall work on other streams.
   int st = DCSR_OK;
-  if (cudaMallocAsync((void **)&h->row_sizes, sizeof(int32_t) * (n_rows + 1), ls) != cudaSuccess ||
-      cudaMallocAsync((void **)&h->seg, sizeof(int32_t) * (nseg ? nseg : 1), ls) != cudaSuccess ||
-      cudaMallocAsync((void **)&h->stat, sizeof(long long) * ST_WORDS, ls) != cudaSuccess ||
-      cudaMallocAsync((void **)&h->long_rows, sizeof(int32_t) * (n_rows + 1), ls) != cudaSuccess ||
-      cudaMallocAsync((void **)&h->long_off, sizeof(long long) * (n_rows + 2), ls) != cudaSuccess ||
-      cudaMallocAsync((void **)&h->long_cnt, sizeof(int32_t) * (n_rows + 1), ls) != cudaSuccess ||
-      cudaMallocAsync((void **)&h->med_desc, sizeof(int4) * (n_rows + 1), ls) != cudaSuccess ||
-      cudaMallocAsync((void **)&h->sched_info, sizeof(int32_t) * 32, ls) != cudaSuccess)
+  if (dcsr::dev_alloc((void **)&h->row_sizes, sizeof(int32_t) * (n_rows + 1), ls) != cudaSuccess ||
+      dcsr::dev_alloc((void **)&h->seg, sizeof(int32_t) * (nseg ? nseg : 1), ls) != cudaSuccess ||
+      dcsr::dev_alloc((void **)&h->stat, sizeof(long long) * ST_WORDS, ls) != cudaSuccess ||
+      dcsr::dev_alloc((void **)&h->long_rows, sizeof(int32_t) * (n_rows + 1), ls) != cudaSuccess ||
+      dcsr::dev_alloc((void **)&h->long_off, sizeof(long long) * (n_rows + 2), ls) != cudaSuccess ||
+      dcsr::dev_alloc((void **)&h->long_cnt, sizeof(int32_t) * (n_rows + 1), ls) != cudaSuccess ||
+      dcsr::dev_alloc((void **)&h->med_desc, sizeof(int4) * (n_rows + 1), ls) != cudaSuccess ||
+      dcsr::dev_alloc((void **)&h->sched_info, sizeof(int32_t) * 32, ls) != cudaSuccess)
     st = DCSR_OOM;
   if (st == DCSR_OK) {
     h->scratch.status = h->stat + ST_STATUS;  // look-back timeouts of this matrix's operations
@@ -533,7 +534,7 @@ int dcsr_destroy(dcsr_handle h) {
   void *bufs[] = {h->cols, h->vals, h->row_sizes, h->seg, h->stat, h->long_rows, h->long_off,
                   h->long_cnt, h->med_desc, h->sched_info, h->part, h->chunk_rl, h->chunk_desc};
   for (void *p : bufs)
-    if (p) cudaFreeAsync(p, s0);
+    if (p) dcsr::dev_free(p, s0);
   if (h->spare_ev) cudaEventDestroy(h->spare_ev);
   delete h;
   return DCSR_OK;
@@ -634,10 +635,10 @@ int dcsr_from_hyb(dcsr_handle h, const int32_t *ell_cols, const void *ell_vals, 
   int32_t *rows = nullptr, *cols = nullptr;
   void *vals = nullptr;
   long long *flag = nullptr;
-  DCSR_CUDA(cudaMallocAsync((void **)&rows, sizeof(int32_t) * (T + 1), s));
-  DCSR_CUDA(cudaMallocAsync((void **)&cols, sizeof(int32_t) * (T + 1), s));
-  DCSR_CUDA(cudaMallocAsync(&vals, h->vsize() * (T + 1), s));
-  DCSR_CUDA(cudaMallocAsync((void **)&flag, sizeof(long long) * (slots + 1), s));
+  DCSR_CUDA(dcsr::dev_alloc((void **)&rows, sizeof(int32_t) * (T + 1), s));
+  DCSR_CUDA(dcsr::dev_alloc((void **)&cols, sizeof(int32_t) * (T + 1), s));
+  DCSR_CUDA(dcsr::dev_alloc(&vals, h->vsize() * (T + 1), s));
+  DCSR_CUDA(dcsr::dev_alloc((void **)&flag, sizeof(long long) * (slots + 1), s));
   Arena tmp;
   tmp.status = h->stat + ST_STATUS;
   DCSR_TRY(tmp.reserve(scan_scratch_bytes(slots + 1), s));
@@ -662,10 +663,10 @@ int dcsr_from_hyb(dcsr_handle h, const int32_t *ell_cols, const void *ell_vals, 
   }
   int st = dcsr_from_coo(h, rows, cols, vals, nell + coo_nnz, stream);
   tmp.release(s);
-  cudaFreeAsync(rows, s);
-  cudaFreeAsync(cols, s);
-  cudaFreeAsync(vals, s);
-  cudaFreeAsync(flag, s);
+  dcsr::dev_free(rows, s);
+  dcsr::dev_free(cols, s);
+  dcsr::dev_free(vals, s);
+  dcsr::dev_free(flag, s);
   return st;
 }
 
@@ -921,13 +922,12 @@ uint64_t dcsr_launch_count(void) { return g_launches.load(); }
 int dcsr_pool_reserve(int64_t bytes, void *stream) {
   if (bytes < 0) return DCSR_BAD_ARG;
   if (bytes == 0) return DCSR_OK;
-  cudaStream_t s = (cudaStream_t)stream;
   keep_pool_memory();
-  void *p = nullptr;
-  DCSR_CUDA(cudaMallocAsync(&p, (size_t)bytes, s));
-  DCSR_CUDA(cudaFreeAsync(p, s));
-  DCSR_CUDA(cudaStreamSynchronize(s));
-  return DCSR_OK;
+  return dcsr::reserve_regions(bytes, (cudaStream_t)stream);
+}
+
+int dcsr_pool_usage(int64_t *reserved, int64_t *free_bytes, int64_t *fallback_allocs) {
+  return dcsr::region_usage(reserved, free_bytes, fallback_allocs);
 }
 
 int dcsr_debug_lookback(int32_t spin_limit, int32_t stall_first_tile) {

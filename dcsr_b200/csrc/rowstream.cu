@@ -220,20 +220,20 @@ static int64_t max_chunks(dcsr_handle h) { return h->pool_cap / CHUNK + h->pool_
 
 int ensure_part(dcsr_handle h, int K, cudaStream_t s) {
   if (max_chunks(h) > h->chunk_cap) {
-    if (h->chunk_rl) DCSR_CUDA(cudaFreeAsync(h->chunk_rl, s));
-    if (h->chunk_desc) DCSR_CUDA(cudaFreeAsync(h->chunk_desc, s));
+    if (h->chunk_rl) DCSR_CUDA(dcsr::dev_free(h->chunk_rl, s));
+    if (h->chunk_desc) DCSR_CUDA(dcsr::dev_free(h->chunk_desc, s));
     h->chunk_rl = nullptr;
     h->chunk_desc = nullptr;
-    DCSR_CUDA(cudaMallocAsync((void **)&h->chunk_rl, sizeof(int2) * max_chunks(h), s));
-    DCSR_CUDA(cudaMallocAsync((void **)&h->chunk_desc, sizeof(int4) * max_chunks(h), s));
+    DCSR_CUDA(dcsr::dev_alloc((void **)&h->chunk_rl, sizeof(int2) * max_chunks(h), s));
+    DCSR_CUDA(dcsr::dev_alloc((void **)&h->chunk_desc, sizeof(int4) * max_chunks(h), s));
     h->chunk_cap = max_chunks(h);
     h->bins_valid = false;  // the chunk table is gone
   }
   const int64_t need = max_chunks(h) * K;
   if (need <= h->part_cap) return DCSR_OK;
-  if (h->part) DCSR_CUDA(cudaFreeAsync(h->part, s));
+  if (h->part) DCSR_CUDA(dcsr::dev_free(h->part, s));
   h->part = nullptr;
-  DCSR_CUDA(cudaMallocAsync((void **)&h->part, sizeof(double) * need, s));
+  DCSR_CUDA(dcsr::dev_alloc((void **)&h->part, sizeof(double) * need, s));
   h->part_cap = need;
   return DCSR_OK;
 }

@@ -292,7 +292,7 @@ int launch(dcsr_server s, Slot &sl, std::vector<Req> &take) {
     sl.nnz_cap = n_exp;
   }
   sl.stage = nullptr;
-  if (bytes) DCSR_CUDA(cudaMallocAsync((void **)&sl.stage, bytes, st));
+  if (bytes) DCSR_CUDA(dcsr::dev_alloc((void **)&sl.stage, bytes, st));
   // inputs host -> device; batch items over the staged (or the caller's device) buffers
   for (auto &q : sl.reqs) {
     dcsr_handle h = s->mats[q.r.matrix];
@@ -431,7 +431,7 @@ int finish(dcsr_server s, Slot &sl) {
     std::lock_guard<std::mutex> lk(s->mu);
     s->trace.push_back(t);
   }
-  if (sl.stage) DCSR_CUDA(cudaFreeAsync(sl.stage, sl.s));
+  if (sl.stage) DCSR_CUDA(dcsr::dev_free(sl.stage, sl.s));
   sl.stage = nullptr;
   sl.busy = false;
   sl.phase = 0;
@@ -517,7 +517,7 @@ void fail_slot(dcsr_server s, Slot &sl, int status) {
   for (auto &q : sl.reqs) q.status = status;
   sl.phase = 0;
   if (sl.busy) {
-    if (sl.stage) cudaFreeAsync(sl.stage, sl.s);
+    if (sl.stage) dcsr::dev_free(sl.stage, sl.s);
     sl.stage = nullptr;
     std::lock_guard<std::mutex> lk(s->mu);
     s->in_use -= sl.cost;

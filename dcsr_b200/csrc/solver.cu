@@ -150,8 +150,8 @@ int cg_t(dcsr_handle h, const V *b, V *x, int32_t max_iter, double rel, double a
   const int grid = (int)std::min<int64_t>(std::max<int64_t>(div_up(n, CG_THREADS * 8), 1), CG_MAX_BLOCKS);
   V *work = nullptr;
   CgState *st = nullptr;
-  DCSR_CUDA(cudaMallocAsync((void **)&work, sizeof(V) * 3 * (size_t)(n > 0 ? n : 1), s));
-  DCSR_CUDA(cudaMallocAsync((void **)&st, sizeof(CgState), s));
+  DCSR_CUDA(dcsr::dev_alloc((void **)&work, sizeof(V) * 3 * (size_t)(n > 0 ? n : 1), s));
+  DCSR_CUDA(dcsr::dev_alloc((void **)&st, sizeof(CgState), s));
   V *r = work, *p = work + n, *y = work + 2 * n;
   int rc = DCSR_OK;
   auto run = [&]() -> int {
@@ -181,8 +181,8 @@ int cg_t(dcsr_handle h, const V *b, V *x, int32_t max_iter, double rel, double a
     return DCSR_OK;
   };
   rc = run();
-  cudaFreeAsync(work, s);
-  cudaFreeAsync(st, s);
+  dcsr::dev_free(work, s);
+  dcsr::dev_free(st, s);
   return rc;
 }
 

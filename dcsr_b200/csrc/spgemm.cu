@@ -322,6 +322,91 @@ __global__ void __launch_bounds__(SG_THREADS, 3) k_sg_warp(Mat<V> A, Mat<V> B, c
   }
 }
 
+// The CTA class's expand (256 < P_i <= 4096): row i's A entries are taken
+// 256 at a time, one per thread (column, value, B row length and first
+// segment loaded side by side), the lengths scanned across the block into
+// product offsets, then each thread produces products q = tid, tid + 256,
+// ... of the group -- the owning entry found by a binary search over the
+// offsets in shared memory, four products' B loads in flight at a time.  A
+// B row that does not lie in its first segment is read through its chain.
+// Same keys and products as the warp class (product p = the row's p-th
+// product in A-entry-major order).
+template <typename V>
+__device__ __forceinline__ int sg_expand_cta(const Mat<V> &A, const Mat<V> &B, int64_t i, int tid,
+                                             unsigned long long *key, V *prod, int *soff, int32_t *sk, V *sa,
+                                             int32_t *sst, int *wsum) {
+  constexpr int H = 4;
+  const int32_t LA = A.row_sizes[i];
+  const Chain ca = load_chain_used(A, (int32_t)i, LA);
+  int base = 0;
+  for (int32_t e0 = 0; e0 < LA; e0 += SG_THREADS) {
+    const int nE = LA - e0 < SG_THREADS ? LA - e0 : SG_THREADS;
+    int32_t kb = 0, lb = 0, st0 = -1;
+    V a = V(0);
+    if (tid < nE) {
+      const int64_t qa = ca.phys(e0 + tid);
+      kb = A.cols[qa];
+      a = A.vals[qa];
+      lb = B.row_sizes[kb];
+      const int2 s0 = __ldg(reinterpret_cast<const int2 *>(B.seg + 2 * (int64_t)kb));
+      st0 = s0.x >= 0 && s0.y - s0.x >= lb ? s0.x : -1;  // all of the row in its first segment
+    }
+    const int incl = warp_incl_scan(lb);
+    if ((tid & 31) == 31) wsum[tid >> 5] = incl;
+    __syncthreads();
+    int pre = 0, tot = 0;
+#pragma unroll
+    for (int q = 0; q < SG_THREADS / 32; q++) {
+      if (q < (tid >> 5)) pre += wsum[q];
+      tot += wsum[q];
+    }
+    soff[tid] = pre + incl - lb;
+    sk[tid] = kb;
+    sa[tid] = a;
+    sst[tid] = st0;
+    __syncthreads();
+    for (int q0 = tid; q0 < tot; q0 += H * SG_THREADS) {
+      int own[H];
+      int32_t bc[H];
+      V bv[H];
+#pragma unroll
+      for (int h = 0; h < H; h++) {
+        const int q = q0 + h * SG_THREADS;
+        own[h] = 0;
+        bc[h] = 0;
+        bv[h] = V(0);
+        if (q < tot) {
+          int lo = 0, hi = nE - 1;  // the last entry whose offset is <= q owns q
+          while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (soff[mid] <= q) lo = mid;
+            else hi = mid - 1;
+          }
+          own[h] = lo;
+          const int32_t j = q - soff[lo];
+          const int64_t qb = sst[lo] >= 0 ? (int64_t)sst[lo] + j : load_chain(B, sk[lo]).phys(j);
+          bc[h] = B.cols[qb];
+          bv[h] = B.vals[qb];
+        }
+      }
+#pragma unroll
+      for (int h = 0; h < H; h++) {
+        const int q = q0 + h * SG_THREADS;
+        if (q < tot) {
+          key[base + q] = ((unsigned long long)(uint32_t)bc[h] << 32) | (unsigned long long)(base + q);
+          V pr;
+          if constexpr (sizeof(V) == 4) pr = __fmul_rn(sa[own[h]], bv[h]);
+          else pr = __dmul_rn(sa[own[h]], bv[h]);
+          prod[base + q] = pr;
+        }
+      }
+    }
+    base += tot;
+    __syncthreads();  // the group's tables are reused by the next group
+  }
+  return base;
+}
+
 // CTA per row, 256 < P_i <= 4096 (dynamic shared memory).
 template <typename V>
 __global__ void __launch_bounds__(SG_THREADS) k_sg_cta(Mat<V> A, Mat<V> B, const unsigned *rows,
@@ -331,11 +416,14 @@ __global__ void __launch_bounds__(SG_THREADS) k_sg_cta(Mat<V> A, Mat<V> B, const
   unsigned long long *key = sg_smem;
   V *prod = reinterpret_cast<V *>(sg_smem + SG_CTA_MAX);
   __shared__ int wheads[SG_THREADS / 32 + 1];
+  __shared__ int soff[SG_THREADS], wsum[SG_THREADS / 32];
+  __shared__ int32_t sk[SG_THREADS], sst[SG_THREADS];
+  __shared__ V sa[SG_THREADS];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int64_t b = starts[SG_CTA], e = starts[SG_CTA + 1];
   for (int64_t it = b + blockIdx.x; it < e; it += gridDim.x) {
     const int64_t i = rows[it];
-    const int P = (int)sg_expand(A, B, i, threadIdx.x, SG_THREADS, key, prod);
+    const int P = sg_expand_cta(A, B, i, threadIdx.x, key, prod, soff, sk, sa, sst, wsum);
     const int n2 = next_pow2(P);
     for (int t = P + threadIdx.x; t < n2; t += SG_THREADS) key[t] = ~0ull;
     __syncthreads();
@@ -493,9 +581,9 @@ static int spgemm_impl(dcsr_handle hA, dcsr_handle hB, dcsr_handle hC, cudaStrea
   int32_t *tcol = nullptr;
   V *tval = nullptr;
   long long *ucnt = nullptr;
-  DCSR_CUDA(cudaMallocAsync((void **)&tcol, sizeof(int32_t) * (P + 1), s));
-  DCSR_CUDA(cudaMallocAsync((void **)&tval, sizeof(V) * (P + 1), s));
-  DCSR_CUDA(cudaMallocAsync((void **)&ucnt, sizeof(long long) * (n + 2), s));
+  DCSR_CUDA(dcsr::dev_alloc((void **)&tcol, sizeof(int32_t) * (P + 1), s));
+  DCSR_CUDA(dcsr::dev_alloc((void **)&tval, sizeof(V) * (P + 1), s));
+  DCSR_CUDA(dcsr::dev_alloc((void **)&ucnt, sizeof(long long) * (n + 2), s));
   DCSR_CUDA(cudaMemsetAsync(ucnt, 0, sizeof(long long) * (n + 2), s));
   const size_t cta_smem = SG_CTA_MAX * (sizeof(unsigned long long) + sizeof(V));
   static const int g_warp = persistent_grid((const void *)k_sg_warp<double, unsigned long long>, SG_THREADS, 0);
@@ -546,9 +634,9 @@ static int spgemm_impl(dcsr_handle hA, dcsr_handle hB, dcsr_handle hC, cudaStrea
   const int st = load_from_rows(hC, ub, ucnt, tcol, tval, cap_bound, s);
   gg.release(s);
   ar.release(s);
-  cudaFreeAsync(tcol, s);
-  cudaFreeAsync(tval, s);
-  cudaFreeAsync(ucnt, s);
+  dcsr::dev_free(tcol, s);
+  dcsr::dev_free(tval, s);
+  dcsr::dev_free(ucnt, s);
   return st;
 }
 

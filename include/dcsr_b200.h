@@ -453,15 +453,26 @@ int dcsr_spin_faults(int64_t *count);
  * For tests only; synchronises the device; not thread-safe with running
  * operations. */
 int dcsr_debug_lookback(int32_t spin_limit, int32_t stall_first_tile);
-/* Pre-grow the current device's stream-ordered memory pool, from which
- * every matrix pool, scratch arena and staging buffer of this library is
- * allocated, by `bytes` (allocated and freed on `stream`, then kept by the
- * pool; the library sets the pool never to release memory it holds).
- * Growing a matrix (compaction, repair) or staging a large batch then takes
- * memory the pool already maps: mapping new device memory inside the loop
- * cost 2 to several hundred milliseconds per allocation on some machines.
- * Synchronises the stream.  No counterpart in the reference (host memory). */
+/* Make sure at least `bytes` of device memory reserved for this library are
+ * free on the current device: when the reserved regions have less free, a
+ * new region of the difference is mapped (on `stream`, then synchronised)
+ * and kept for the life of the process.  Every matrix pool, schedule,
+ * scratch arena and staging buffer of the library is then carved from the
+ * regions (best fit, 256-byte aligned); a block freed on one stream is
+ * reused on another after an event wait on the device, with no host sync.
+ * Only a request the regions cannot hold goes to the driver's
+ * stream-ordered allocator (counted by dcsr_pool_usage).  Growing a matrix
+ * (compaction, repair, grow-ahead) or staging a large batch then maps no
+ * device memory: a driver allocation that maps new memory measured from 2 to
+ * several hundred milliseconds on busy hosts.  Without a call, all
+ * allocations go to the driver's allocator.  Regions are not used inside a
+ * stream capture.  No counterpart in the reference (host memory). */
 int dcsr_pool_reserve(int64_t bytes, void *stream);
+/* The current device's reserved regions: bytes mapped, bytes free (blocks
+ * whose last user's work may still be running count as free), and how many
+ * allocations the regions could not hold and the driver's allocator made
+ * instead.  Any pointer may be null.  No counterpart in the reference. */
+int dcsr_pool_usage(int64_t *reserved, int64_t *free_bytes, int64_t *fallback_allocs);
 /* Measurement aid for the SpMV roofline (no counterpart in the reference):
  * reads n (column, value) entries -- e.g. a matrix's CSR export, FP32 --
  * coalesced and gathers x at every column, summing the products per block

@@ -52,7 +52,7 @@ def test_ctypes_match_c_layout(tmp_path):
 
 
 @pytest.mark.parametrize("name", ["dcsr_batch_autotune", "dcsr_batch_short_split", "dcsr_batch_grow", "dcsr_server_replay", "dcsr_set_row_classes",
-                                  "dcsr_pool_reserve", "dcsr_spin_faults"])
+                                  "dcsr_pool_reserve", "dcsr_pool_usage", "dcsr_spin_faults"])
 def test_new_entry_points_declared(name):
     text = open(os.path.join(ROOT, "include", "dcsr_b200.h")).read()
     assert f" {name}(" in text
