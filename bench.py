@@ -683,6 +683,9 @@ def served_part(args, dev, rank, local_rank):
     tr_dev = ServedTrace(api, torch, dev, specs, kind, mat, size, args.seed + 7, export_cap, True)
     tr_host = ServedTrace(api, torch, dev, specs, kind, mat, size, args.seed + 7, export_cap, False)
     torch.cuda.synchronize()
+    # set-up: free reserved regions for the pools that grow during the trace
+    api.pool_reserve(16 << 30)
+    fallback0 = api.pool_usage()[2]
     out = {"workload": f"{len(specs)} resident matrices like the batched ones ({nnz / 1e9:.2f}G nnz, "
                        f"{resident / 2**30:.1f} GiB resident); {N} requests: 40% update (log-uniform 10..100k "
                        "triples), 50% SpMV (k uniform 1..8), 10% DCSR->CSR export; matrices uniform"}
@@ -706,6 +709,7 @@ def served_part(args, dev, rank, local_rank):
 
     out["plain"] = plain_sweep(tr_dev)
     out["plain_host_buffers"] = plain_sweep(tr_host)
+    fallback1 = api.pool_usage()[2]
     ref_p = out["plain"]["slo_point"]
     cap_p = {"req_s": out["plain"]["capacity_req_s"]}
     p99_plain = ref_p["p99_ms"]
@@ -737,6 +741,7 @@ def served_part(args, dev, rank, local_rank):
     # results copied out per request; exports move whole matrices to the host)
     cap_h, sweep_h, e2e, e2e_f, e2e_met = sweep_at(tr_host, out["plain_host_buffers"]["slo_point"]["p99_ms"])
     st = srv.stats()
+    fallback2 = api.pool_usage()[2]
     srv.close()
     # bytes each request of the host-buffer run moved (mean over the trace)
     n_of = np.array([sp["n"] for sp in specs], np.int64)
@@ -751,6 +756,8 @@ def served_part(args, dev, rank, local_rank):
                      "sweep": sweep, "chosen_load_frac": best_f, "p99_constraint_met": met,
                      "batches": st["batches"], "max_batch": args.max_batch, "depth": args.depth,
                      "workers": args.workers,
+                     "allocations_outside_regions": {"plain": int(fallback1 - fallback0),
+                                                     "batched": int(fallback2 - fallback1)},
                      "row_classes": None if tuned is None else {"short_max": tuned[0], "long_min": tuned[1]}}
     out["value"] = best["req_s"]
     out["chosen"] = {"requests": best["requests"], "wall_ms": best["wall_ms"]}

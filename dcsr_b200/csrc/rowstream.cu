@@ -56,6 +56,12 @@ constexpr int CHUNK = DCSR_CHUNK;
 #ifndef DCSR_K1_UN
 #define DCSR_K1_UN 4
 #endif
+// The same for the k = 1 row reductions (sum, max, min, count), which hold
+// no columns: twice the SpMV's (149 against 156 us for the row sums of the
+// R-MAT 2^20 stream matrix; 16 spills).
+#ifndef DCSR_K1_UN_RED
+#define DCSR_K1_UN_RED 8
+#endif
 #ifndef DCSR_K1_MINB
 #define DCSR_K1_MINB 3
 #endif
@@ -1132,7 +1138,8 @@ __device__ __forceinline__ void finish_unit(const RowItem<V> &it, const Unit1 &x
 template <typename V, int OP, typename Src, bool XU>
 __global__ void __launch_bounds__(RS_THREADS_, DCSR_K1_MINB) k_rows1(Src src) {
   using P = typename std::conditional<sizeof(V) == 4, float, double>::type;
-  constexpr int UN = sizeof(V) == 8 && DCSR_K1_UN > 1 ? DCSR_K1_UN / 2 : DCSR_K1_UN;
+  constexpr int UNO = OP == OP_SPMV ? DCSR_K1_UN : DCSR_K1_UN_RED;
+  constexpr int UN = sizeof(V) == 8 && UNO > 1 ? UNO / 2 : UNO;
   constexpr int W = 32 * UN;  // entries of one step
   const int lane = threadIdx.x & 31;
   const int64_t NC = src.units(P_CHUNKS), NM = src.units(P_MED) * RS_WARPS;

@@ -466,7 +466,9 @@ int dcsr_debug_lookback(int32_t spin_limit, int32_t stall_first_tile);
  * device memory: a driver allocation that maps new memory measured from 2 to
  * several hundred milliseconds on busy hosts.  Without a call, all
  * allocations go to the driver's allocator.  Regions are not used inside a
- * stream capture.  No counterpart in the reference (host memory). */
+ * stream capture, and are kept for the life of the process: do not use the
+ * library on a device after cudaDeviceReset there.  No counterpart in the
+ * reference (host memory). */
 int dcsr_pool_reserve(int64_t bytes, void *stream);
 /* The current device's reserved regions: bytes mapped, bytes free (blocks
  * whose last user's work may still be running count as free), and how many
