@@ -72,6 +72,14 @@ constexpr int CHUNK = DCSR_CHUNK;
 #ifndef DCSR_K1B_U
 #define DCSR_K1B_U 4
 #endif
+// Blocks per SM the copy pass (export, compaction) is compiled for.
+#ifndef DCSR_COPY_MINB
+#define DCSR_COPY_MINB 3
+#endif
+// Entries a thread copies per unit and pass (FP64: half).
+#ifndef DCSR_COPY_EPT
+#define DCSR_COPY_EPT 8
+#endif
 constexpr int STEP = 4096;    // entries a CTA has in flight per step
 enum { P_BLOCKS = 0, P_CHUNKS = 1, P_MED = 2 };
 
@@ -1285,7 +1293,7 @@ __global__ void __launch_bounds__(RS_THREADS_, DCSR_K1B_MINB) k_rows1_blocks(Src
 // optionally writing COO row ids and an int32 row pointer (one matrix).
 
 template <typename V, int PART>
-__global__ void __launch_bounds__(RS_THREADS_) k_rows_copy(RowItem<V> it, const long long *__restrict__ dst_off,
+__global__ void __launch_bounds__(RS_THREADS_, DCSR_COPY_MINB) k_rows_copy(RowItem<V> it, const long long *__restrict__ dst_off,
                                                            int32_t *__restrict__ out_cols, V *__restrict__ out_vals,
                                                            int32_t *__restrict__ out_rows,
                                                            int32_t *__restrict__ out_rowptr, int64_t limit) {
@@ -1296,59 +1304,88 @@ __global__ void __launch_bounds__(RS_THREADS_) k_rows_copy(RowItem<V> it, const 
   const int64_t units = src.units(PART);
   if (PART == P_BLOCKS && out_rowptr && blockIdx.x == 0 && threadIdx.x == 0)
     out_rowptr[m.n_rows] = (int32_t)dst_off[m.n_rows];
-  for (int64_t u = blockIdx.x; u < units; u += gridDim.x) {
-    if constexpr (PART == P_CHUNKS || PART == P_MED) {
-      // long-row chunk (whole CTA) or medium row (one warp)
-      int32_t row;
-      int64_t c0, c1, L;
-      int tid, nthr;
-      if (PART == P_CHUNKS) {
-        const int2 rl = it.chunk_rl[u];
-        row = rl.x;
-        L = m.row_sizes[row];
-        const int64_t chunk = L <= CHUNK ? 0 : u - it.long_off[rl.y];
-        c0 = chunk * CHUNK;
-        c1 = c0 + CHUNK < L ? c0 + CHUNK : L;
-        tid = threadIdx.x;
-        nthr = RS_THREADS_;
-      } else {
-        const int64_t mi = u * RS_WARPS + w;
-        if (mi >= it.info[2]) continue;
-        row = it.med_desc[mi].x;
-        L = m.row_sizes[row];
-        c0 = 0;
-        c1 = L;
-        tid = lane;
-        nthr = 32;
-      }
-      const Chain ch = load_chain(m, row);
-      const int64_t d = dst_off[row];
-      if (out_rowptr && c0 == 0 && tid == 0) out_rowptr[row] = (int32_t)d;
-      const bool fast = ch.cp[0] >= c1;
-      constexpr int G = 16;
-      for (int64_t s0 = c0; s0 < c1; s0 += (int64_t)G * nthr) {
-        int32_t cv[G];
-        V vv[G];
+  if constexpr (PART == P_CHUNKS || PART == P_MED) {
+    // Long-row chunks (a CTA each) or medium rows (a warp each), two per
+    // step (unit u and the one a grid stride later): both units' descriptor
+    // chains (unit -> row -> length, segments, destination) and then all
+    // their entries are in flight together -- one unit alone left the warps
+    // waiting on its chain for a fraction of the data.
+    static_assert(CHUNK % RS_THREADS_ == 0, "whole chunks per thread");
+    constexpr bool CH = PART == P_CHUNKS;
+    constexpr int NTHR = CH ? RS_THREADS_ : 32;
+    // a thread's entries per unit and pass: chunks DCSR_COPY_EPT, medium rows
+    // (shorter, a warp each) half that, FP64 half again (8 / 4 measured
+    // 217 us for the R-MAT 2^20 stream matrix's export, 8 / 8 with spills
+    // 267 us, 4 / 4 219 us; one unit per step 244 us)
+    constexpr int EMAX = (CH ? DCSR_COPY_EPT : DCSR_COPY_EPT / 2) / (sizeof(V) == 8 ? 2 : 1);
+    constexpr int EPT = CH && CHUNK / RS_THREADS_ < EMAX ? CHUNK / RS_THREADS_ : EMAX;
+    const int tid = CH ? threadIdx.x : lane;
+    // unit numbers: chunks per CTA, medium rows per warp
+    const int64_t n_units = CH ? units : it.info[2];
+    const int64_t first = CH ? blockIdx.x : (int64_t)blockIdx.x * RS_WARPS + w;
+    const int64_t stride = CH ? gridDim.x : (int64_t)gridDim.x * RS_WARPS;
+    for (int64_t u = first; u < n_units; u += 2 * stride) {
+      int32_t row[2];
+      int64_t c0[2], c1[2], d[2];
+      Chain ch[2];
+      bool fast[2];
 #pragma unroll
-        for (int g = 0; g < G; g++) {
-          const int64_t p = s0 + tid + (int64_t)g * nthr;
-          if (p < c1) {
-            const int64_t q = fast ? (int64_t)ch.st[0] + p : ch.phys(p);
-            cv[g] = __ldcs(m.cols + q);
-            vv[g] = __ldcs(m.vals + q);
+      for (int h = 0; h < 2; h++) {
+        const int64_t uu = u + h * stride;
+        row[h] = -1;
+        c0[h] = c1[h] = d[h] = 0;
+        fast[h] = true;
+        ch[h].ns = 0;
+        if (uu < n_units) {
+          int64_t L;
+          if (CH) {
+            const int2 rl = it.chunk_rl[uu];
+            row[h] = rl.x;
+            L = m.row_sizes[rl.x];
+            const int64_t chunk = L <= CHUNK ? 0 : uu - it.long_off[rl.y];
+            c0[h] = chunk * CHUNK;
+            c1[h] = c0[h] + CHUNK < L ? c0[h] + CHUNK : L;
+          } else {
+            row[h] = it.med_desc[uu].x;
+            L = m.row_sizes[row[h]];
+            c1[h] = L;
           }
-        }
-#pragma unroll
-        for (int g = 0; g < G; g++) {
-          const int64_t p = s0 + tid + (int64_t)g * nthr;
-          if (p < c1 && d + p < limit) {
-            out_cols[d + p] = cv[g];
-            out_vals[d + p] = vv[g];
-            if (out_rows) out_rows[d + p] = row;
-          }
+          ch[h] = load_chain(m, row[h]);
+          d[h] = dst_off[row[h]];
+          fast[h] = ch[h].cp[0] >= c1[h];
+          if (out_rowptr && c0[h] == 0 && tid == 0) out_rowptr[row[h]] = (int32_t)d[h];
         }
       }
-    } else {
+      const int64_t span = CH ? CHUNK : (c1[0] > c1[1] ? c1[0] : c1[1]);  // medium rows start at 0
+      for (int64_t s0 = 0; s0 < span; s0 += (int64_t)EPT * NTHR) {
+        int32_t cv[2 * EPT];
+        V vv[2 * EPT];
+#pragma unroll
+        for (int h = 0; h < 2; h++)
+#pragma unroll
+          for (int g = 0; g < EPT; g++) {
+            const int64_t p = c0[h] + s0 + tid + (int64_t)g * NTHR;
+            if (p < c1[h]) {
+              const int64_t q = fast[h] ? (int64_t)ch[h].st[0] + p : ch[h].phys(p);
+              cv[h * EPT + g] = __ldcs(m.cols + q);
+              vv[h * EPT + g] = __ldcs(m.vals + q);
+            }
+          }
+#pragma unroll
+        for (int h = 0; h < 2; h++)
+#pragma unroll
+          for (int g = 0; g < EPT; g++) {
+            const int64_t p = c0[h] + s0 + tid + (int64_t)g * NTHR;
+            if (p < c1[h] && d[h] + p < limit) {
+              out_cols[d[h] + p] = cv[h * EPT + g];
+              out_vals[d[h] + p] = vv[h * EPT + g];
+              if (out_rows) out_rows[d[h] + p] = row[h];
+            }
+          }
+      }
+    }
+  } else {
+    for (int64_t u = blockIdx.x; u < units; u += gridDim.x) {  // a block of 32 short rows per warp
       const int64_t blk = u * RS_WARPS + w;
       if (blk * 32 >= m.n_rows) continue;
       const int64_t r0 = blk * 32;
