@@ -43,16 +43,77 @@ __global__ void k_layout(int32_t *seg, int32_t *row_sizes, int32_t n, int32_t pi
 }
 
 // Copy CSR rows into their new layer-0 segments (warp per row, grid-stride).
+// CSR rows into their pool segments: a warp per row, four windows of 32
+// entries in flight.  A row longer than COPY_LONG entries is left to
+// k_copy_csr_long (listed here): one warp would copy a power-law graph's
+// hottest rows alone, and the whole load would wait for it.
+constexpr int COPY_LONG = 4096;
 template <typename V>
-__global__ void k_copy_csr(int32_t n, const long long *offs, const long long *rp, const int32_t *cols,
-                           const V *vals, int32_t *pcols, V *pvals) {
+__global__ void k_copy_csr(int32_t n, const long long *__restrict__ offs, const long long *__restrict__ rp,
+                           const int32_t *__restrict__ cols, const V *__restrict__ vals, int32_t *__restrict__ pcols,
+                           V *__restrict__ pvals, int32_t *long_rows, int32_t *long_count) {
+  constexpr int U = 4;
   const int lane = threadIdx.x & 31;
   const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
   for (int64_t r = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < n; r += nw) {
-    const int64_t s = rp[r], e = rp[r + 1], d = offs[r];
-    for (int64_t j = s + lane; j < e; j += 32) {
-      pcols[d + (j - s)] = cols[j];
-      pvals[d + (j - s)] = vals[j];
+    const int64_t s = rp[r], L = rp[r + 1] - s, d = offs[r];
+    if (L > COPY_LONG) {
+      if (lane == 0) long_rows[atomicAdd(long_count, 1)] = (int32_t)r;
+      continue;
+    }
+    for (int64_t j0 = 0; j0 < L; j0 += 32 * U) {
+      int32_t c[U];
+      V v[U];
+#pragma unroll
+      for (int u = 0; u < U; u++) {
+        const int64_t j = j0 + 32 * u + lane;
+        if (j < L) {
+          c[u] = __ldcs(cols + s + j);
+          v[u] = __ldcs(vals + s + j);
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < U; u++) {
+        const int64_t j = j0 + 32 * u + lane;
+        if (j < L) {
+          pcols[d + j] = c[u];
+          pvals[d + j] = v[u];
+        }
+      }
+    }
+  }
+}
+
+// The listed long rows, one after another, each spread over the whole grid.
+template <typename V>
+__global__ void k_copy_csr_long(const int32_t *long_rows, const int32_t *long_count, const long long *__restrict__ offs,
+                                const long long *__restrict__ rp, const int32_t *__restrict__ cols,
+                                const V *__restrict__ vals, int32_t *__restrict__ pcols, V *__restrict__ pvals) {
+  constexpr int U = 4;
+  const int64_t nt = (int64_t)gridDim.x * blockDim.x, t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int32_t cnt = *long_count;
+  for (int32_t i = 0; i < cnt; i++) {
+    const int32_t r = long_rows[i];
+    const int64_t s = rp[r], L = rp[r + 1] - s, d = offs[r];
+    for (int64_t j0 = t; j0 < L; j0 += U * nt) {
+      int32_t c[U];
+      V v[U];
+#pragma unroll
+      for (int u = 0; u < U; u++) {
+        const int64_t j = j0 + u * nt;
+        if (j < L) {
+          c[u] = __ldcs(cols + s + j);
+          v[u] = __ldcs(vals + s + j);
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < U; u++) {
+        const int64_t j = j0 + u * nt;
+        if (j < L) {
+          pcols[d + j] = c[u];
+          pvals[d + j] = v[u];
+        }
+      }
     }
   }
 }
@@ -198,13 +259,18 @@ static void free_pool(dcsr_handle h, cudaStream_t s) {
 
 static int clear_status(dcsr_handle h, cudaStream_t s);
 
-size_t load_scratch_bytes(dcsr_handle h) { return arena_bytes(h->n_rows + 2, 8) + scan_scratch_bytes(h->n_rows + 1); }
+size_t load_scratch_bytes(dcsr_handle h) {
+  return arena_bytes(h->n_rows + 2, 8) + arena_bytes(h->n_rows + 2, 4) + scan_scratch_bytes(h->n_rows + 1);
+}
 
 int load_from_csr64(dcsr_handle h, const long long *rp, const int32_t *cols, const void *vals, cudaStream_t s) {
   Arena &ar = h->scratch;  // caller reserved load_scratch_bytes() beyond its own use
   const int32_t n = h->n_rows;
   long long *caps = ar.take<long long>(n + 2);
+  int32_t *long_rows = ar.take<int32_t>(n + 2);  // rows for k_copy_csr_long, then their count
   if (ar.overflow) return DCSR_OOM;  // scratch sizing bug: no kernel sees a null pointer
+  int32_t *long_count = long_rows + n + 1;
+  DCSR_CUDA(cudaMemsetAsync(long_count, 0, sizeof(int32_t), s));
   DCSR_LAUNCH(k_caps_from_rp, grid_for(n + 1, 256), 256, 0, s, rp, n, h->o, caps);
   DCSR_TRY(scan_i64(caps, caps, n + 1, h->stat + ST_TOTAL, ar, s));
   long long host[ST_WORDS];
@@ -232,12 +298,18 @@ int load_from_csr64(dcsr_handle h, const long long *rp, const int32_t *cols, con
   h->buf_cap = got;
   h->pool_cap = cap;
   DCSR_LAUNCH(k_layout, grid_for(n + 1, 256), 256, 0, s, h->seg, h->row_sizes, n, h->pitch, h->o.max_segs, caps, rp);
-  if (h->dtype == DCSR_F32)
+  const unsigned gl = (unsigned)(8 * sm_count());  // the long rows' grid
+  if (h->dtype == DCSR_F32) {
     DCSR_LAUNCH(k_copy_csr<float>, grid_for((int64_t)n * 32, 256), 256, 0, s, n, caps, rp, cols, (const float *)vals,
+                h->cols, (float *)h->vals, long_rows, long_count);
+    DCSR_LAUNCH(k_copy_csr_long<float>, gl, 256, 0, s, long_rows, long_count, caps, rp, cols, (const float *)vals,
                 h->cols, (float *)h->vals);
-  else
+  } else {
     DCSR_LAUNCH(k_copy_csr<double>, grid_for((int64_t)n * 32, 256), 256, 0, s, n, caps, rp, cols,
-                (const double *)vals, h->cols, (double *)h->vals);
+                (const double *)vals, h->cols, (double *)h->vals, long_rows, long_count);
+    DCSR_LAUNCH(k_copy_csr_long<double>, gl, 256, 0, s, long_rows, long_count, caps, rp, cols, (const double *)vals,
+                h->cols, (double *)h->vals);
+  }
   h->bins_valid = false;
   // A load is a one-off: a resident matrix keeps no load-sized scratch (the
   // stream-ordered pool keeps the memory for the next allocation).
