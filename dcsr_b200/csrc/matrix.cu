@@ -44,21 +44,26 @@ __global__ void k_layout(int32_t *seg, int32_t *row_sizes, int32_t n, int32_t pi
 
 // Copy CSR rows into their new layer-0 segments (warp per row, grid-stride).
 // CSR rows into their pool segments: a warp per row, four windows of 32
-// entries in flight.  A row longer than COPY_LONG entries is left to
-// k_copy_csr_long (listed here): one warp would copy a power-law graph's
+// entries in flight.  A row longer than COPY_LONG entries is cut into pieces
+// of COPY_LONG entries, listed here as (row, piece) and copied a CTA per
+// piece by k_copy_csr_pieces: one warp would copy a power-law graph's
 // hottest rows alone, and the whole load would wait for it.
 constexpr int COPY_LONG = 4096;
 template <typename V>
 __global__ void k_copy_csr(int32_t n, const long long *__restrict__ offs, const long long *__restrict__ rp,
                            const int32_t *__restrict__ cols, const V *__restrict__ vals, int32_t *__restrict__ pcols,
-                           V *__restrict__ pvals, int32_t *long_rows, int32_t *long_count) {
+                           V *__restrict__ pvals, unsigned long long *pieces, int32_t *piece_count) {
   constexpr int U = 4;
   const int lane = threadIdx.x & 31;
   const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
   for (int64_t r = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < n; r += nw) {
     const int64_t s = rp[r], L = rp[r + 1] - s, d = offs[r];
     if (L > COPY_LONG) {
-      if (lane == 0) long_rows[atomicAdd(long_count, 1)] = (int32_t)r;
+      const int np = (int)((L + COPY_LONG - 1) / COPY_LONG);
+      int base = 0;
+      if (lane == 0) base = atomicAdd(piece_count, np);
+      base = __shfl_sync(FULL, base, 0);
+      for (int q = lane; q < np; q += 32) pieces[base + q] = ((unsigned long long)(uint32_t)r << 32) | (uint32_t)q;
       continue;
     }
     for (int64_t j0 = 0; j0 < L; j0 += 32 * U) {
@@ -84,32 +89,36 @@ __global__ void k_copy_csr(int32_t n, const long long *__restrict__ offs, const 
   }
 }
 
-// The listed long rows, one after another, each spread over the whole grid.
+// The listed pieces of long rows, a CTA per piece.
 template <typename V>
-__global__ void k_copy_csr_long(const int32_t *long_rows, const int32_t *long_count, const long long *__restrict__ offs,
-                                const long long *__restrict__ rp, const int32_t *__restrict__ cols,
-                                const V *__restrict__ vals, int32_t *__restrict__ pcols, V *__restrict__ pvals) {
+__global__ void k_copy_csr_pieces(const unsigned long long *pieces, const int32_t *piece_count,
+                                  const long long *__restrict__ offs, const long long *__restrict__ rp,
+                                  const int32_t *__restrict__ cols, const V *__restrict__ vals,
+                                  int32_t *__restrict__ pcols, V *__restrict__ pvals) {
   constexpr int U = 4;
-  const int64_t nt = (int64_t)gridDim.x * blockDim.x, t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const int32_t cnt = *long_count;
-  for (int32_t i = 0; i < cnt; i++) {
-    const int32_t r = long_rows[i];
+  const int32_t cnt = *piece_count;
+  const int nt = blockDim.x;
+  for (int64_t b = blockIdx.x; b < cnt; b += gridDim.x) {
+    const unsigned long long pc = pieces[b];
+    const int32_t r = (int32_t)(pc >> 32);
+    const int64_t q = (int64_t)(uint32_t)pc;
     const int64_t s = rp[r], L = rp[r + 1] - s, d = offs[r];
-    for (int64_t j0 = t; j0 < L; j0 += U * nt) {
+    const int64_t j1 = (q + 1) * COPY_LONG < L ? (q + 1) * COPY_LONG : L;
+    for (int64_t jb = q * COPY_LONG + threadIdx.x; jb < j1; jb += (int64_t)U * nt) {
       int32_t c[U];
       V v[U];
 #pragma unroll
       for (int u = 0; u < U; u++) {
-        const int64_t j = j0 + u * nt;
-        if (j < L) {
+        const int64_t j = jb + (int64_t)u * nt;
+        if (j < j1) {
           c[u] = __ldcs(cols + s + j);
           v[u] = __ldcs(vals + s + j);
         }
       }
 #pragma unroll
       for (int u = 0; u < U; u++) {
-        const int64_t j = j0 + u * nt;
-        if (j < L) {
+        const int64_t j = jb + (int64_t)u * nt;
+        if (j < j1) {
           pcols[d + j] = c[u];
           pvals[d + j] = v[u];
         }
@@ -260,17 +269,16 @@ static void free_pool(dcsr_handle h, cudaStream_t s) {
 static int clear_status(dcsr_handle h, cudaStream_t s);
 
 size_t load_scratch_bytes(dcsr_handle h) {
-  return arena_bytes(h->n_rows + 2, 8) + arena_bytes(h->n_rows + 2, 4) + scan_scratch_bytes(h->n_rows + 1);
+  return arena_bytes(h->n_rows + 2, 8) + arena_bytes(1, 8) + scan_scratch_bytes(h->n_rows + 1);
 }
 
 int load_from_csr64(dcsr_handle h, const long long *rp, const int32_t *cols, const void *vals, cudaStream_t s) {
   Arena &ar = h->scratch;  // caller reserved load_scratch_bytes() beyond its own use
   const int32_t n = h->n_rows;
   long long *caps = ar.take<long long>(n + 2);
-  int32_t *long_rows = ar.take<int32_t>(n + 2);  // rows for k_copy_csr_long, then their count
+  int32_t *piece_count = ar.take<int32_t>(1);  // pieces of long rows listed by k_copy_csr
   if (ar.overflow) return DCSR_OOM;  // scratch sizing bug: no kernel sees a null pointer
-  int32_t *long_count = long_rows + n + 1;
-  DCSR_CUDA(cudaMemsetAsync(long_count, 0, sizeof(int32_t), s));
+  DCSR_CUDA(cudaMemsetAsync(piece_count, 0, sizeof(int32_t), s));
   DCSR_LAUNCH(k_caps_from_rp, grid_for(n + 1, 256), 256, 0, s, rp, n, h->o, caps);
   DCSR_TRY(scan_i64(caps, caps, n + 1, h->stat + ST_TOTAL, ar, s));
   long long host[ST_WORDS];
@@ -298,18 +306,22 @@ int load_from_csr64(dcsr_handle h, const long long *rp, const int32_t *cols, con
   h->buf_cap = got;
   h->pool_cap = cap;
   DCSR_LAUNCH(k_layout, grid_for(n + 1, 256), 256, 0, s, h->seg, h->row_sizes, n, h->pitch, h->o.max_segs, caps, rp);
-  const unsigned gl = (unsigned)(8 * sm_count());  // the long rows' grid
+  // pieces of rows longer than COPY_LONG: at most 2 * top / COPY_LONG
+  unsigned long long *pieces = nullptr;
+  DCSR_CUDA(dcsr::dev_alloc(&pieces, sizeof(unsigned long long) * (size_t)(2 * top / COPY_LONG + 1), s));
+  const unsigned gp = (unsigned)(8 * sm_count());  // the pieces' grid
   if (h->dtype == DCSR_F32) {
     DCSR_LAUNCH(k_copy_csr<float>, grid_for((int64_t)n * 32, 256), 256, 0, s, n, caps, rp, cols, (const float *)vals,
-                h->cols, (float *)h->vals, long_rows, long_count);
-    DCSR_LAUNCH(k_copy_csr_long<float>, gl, 256, 0, s, long_rows, long_count, caps, rp, cols, (const float *)vals,
+                h->cols, (float *)h->vals, pieces, piece_count);
+    DCSR_LAUNCH(k_copy_csr_pieces<float>, gp, 256, 0, s, pieces, piece_count, caps, rp, cols, (const float *)vals,
                 h->cols, (float *)h->vals);
   } else {
     DCSR_LAUNCH(k_copy_csr<double>, grid_for((int64_t)n * 32, 256), 256, 0, s, n, caps, rp, cols,
-                (const double *)vals, h->cols, (double *)h->vals, long_rows, long_count);
-    DCSR_LAUNCH(k_copy_csr_long<double>, gl, 256, 0, s, long_rows, long_count, caps, rp, cols, (const double *)vals,
+                (const double *)vals, h->cols, (double *)h->vals, pieces, piece_count);
+    DCSR_LAUNCH(k_copy_csr_pieces<double>, gp, 256, 0, s, pieces, piece_count, caps, rp, cols, (const double *)vals,
                 h->cols, (double *)h->vals);
   }
+  DCSR_CUDA(dcsr::dev_free(pieces, s));
   h->bins_valid = false;
   // A load is a one-off: a resident matrix keeps no load-sized scratch (the
   // stream-ordered pool keeps the memory for the next allocation).

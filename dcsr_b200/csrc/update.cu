@@ -770,18 +770,29 @@ __global__ void k_group_emit(const unsigned long long *keys, const unsigned *per
                              int32_t *ocols, V *ovals, long long *rowcnt) {
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
   const unsigned long long cmask = (1ull << cb) - 1;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
-    const unsigned long long k = keys[i];
-    if (merge && i > 0 && keys[i - 1] == k) continue;
-    V v = vals[perm[i]];
-    if (merge)
-      for (int64_t j = i + 1; j < n && keys[j] == k; j++) v = v + vals[perm[j]];
-    int32_t c = merge ? (int32_t)(k & cmask) : cols[perm[i]];
-    if (c < 0 || c >= n_cols) c = 0;
-    ocols[pos[i]] = c;
-    ovals[pos[i]] = v;
-    const int32_t r = merge ? (int32_t)(k >> cb) : (int32_t)k;
-    atomicAdd((unsigned long long *)&rowcnt[r], 1ull);
+  const int lane = threadIdx.x & 31;
+  // block-uniform trip count, so whole warps take part in the count below
+  for (int64_t i0 = (int64_t)blockIdx.x * blockDim.x; i0 < n; i0 += stride) {
+    const int64_t i = i0 + threadIdx.x;
+    int32_t r = -1;  // the row of the entry this thread emits
+    if (i < n) {
+      const unsigned long long k = keys[i];
+      if (!(merge && i > 0 && keys[i - 1] == k)) {
+        V v = vals[perm[i]];
+        if (merge)
+          for (int64_t j = i + 1; j < n && keys[j] == k; j++) v = v + vals[perm[j]];
+        int32_t c = merge ? (int32_t)(k & cmask) : cols[perm[i]];
+        if (c < 0 || c >= n_cols) c = 0;
+        ocols[pos[i]] = c;
+        ovals[pos[i]] = v;
+        r = merge ? (int32_t)(k >> cb) : (int32_t)k;
+      }
+    }
+    // row counts, one atomic per row and warp: the keys are sorted, so a
+    // warp's entries are a few runs of one row each (a power-law graph's
+    // hottest rows otherwise took one atomic per entry on a single word)
+    const unsigned peers = __match_any_sync(FULL, r);
+    if (r >= 0 && __ffs(peers) - 1 == lane) atomicAdd((unsigned long long *)&rowcnt[r], (unsigned long long)__popc(peers));
   }
 }
 
