@@ -1,6 +1,7 @@
 """Host-side helpers of bench.py that shape the reported numbers: the
-median-p99 pick of a served load point over repeated replays, Poisson
-arrivals, and the roofline traffic taken from the committed ncu summary."""
+median-p99 pick of a served load point over repeated replays, the median
+capacity over closed-loop replays, Poisson arrivals, and the roofline
+traffic taken from the committed ncu summary."""
 import os
 import sys
 
@@ -35,6 +36,24 @@ def test_replay_point_takes_the_median_p99_run(monkeypatch):
     assert r["p99_ms_runs"] == [3.0, 1.0, 2.0]
     assert r["offered_req_s"] == 5000.0
     assert r["kernel_launches"] == 10
+
+
+def test_capacity_takes_the_median_replay(monkeypatch):
+    """One replay slowed by an allocation stall does not set the capacity."""
+    rates = iter([12000.0, 4000.0, 11800.0])
+    seen = []
+
+    def fake_replay(api, srv, trace, arrivals, lo=0, hi=None):
+        assert np.all(np.asarray(arrivals) == 0)  # closed loop: all queued at once
+        seen.append((lo, hi))
+        return {"requests": 100, "wall_ms": 1.0, "req_s": next(rates), "p50_ms": 1.0, "p99_ms": 2.0,
+                "errors": 0, "mean_batch": 3.0}
+
+    monkeypatch.setattr(bench, "replay", fake_replay)
+    r = bench.capacity(_FakeApi(), None, None, 100, 0, 100)
+    assert r["req_s"] == 11800.0
+    assert r["req_s_runs"] == [4000.0, 11800.0, 12000.0]
+    assert seen == [(0, 100)] * 3
 
 
 def test_poisson_arrivals_rate_and_seed():
