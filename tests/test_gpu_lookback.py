@@ -1,7 +1,8 @@
 """The single-pass scan and radix sort (decoupled look-back) at the sizes
 where they take over from the one-block kernels (scans above 4096 values,
 sorts above 8192 keys) and where sorts switch to three kernels per pass
-(above 2^22 keys), against the oracle: COO loads (stable sort of (row,
+(above 2^22 keys inside a stream capture, above 2^25 outside one), against
+the oracle: COO loads (stable sort of (row,
 column) keys, merge of duplicates), updates (a sort and four scans per
 batch), reduce-by-key (a scan), in place and repeated on one handle so the
 look-back epochs advance; and no look-back wait ever gave up."""
@@ -43,6 +44,22 @@ def test_coo_load_sizes(dcsr, T, mode):
     assert orc.load_coo(r, c, v) == 0
     assert_layout_equal(dev, orc, f"coo load T={T}")
     assert_content_equal(dev, orc, f"coo load T={T}")
+
+
+def test_coo_load_three_kernel_sort(dcsr):
+    """A COO load of 2^25 + 1 triples: its sort takes three kernels per pass
+    (the single-pass tier stops at 2^25 keys outside a capture)."""
+    T = (1 << 25) + 1
+    rng = np.random.default_rng(25)
+    n, m = 50_000, 40_000
+    r = rng.integers(0, n, T).astype(np.int32)
+    c = rng.integers(0, m, T).astype(np.int32)
+    v = rng.uniform(-1, 1, T)
+    dev, orc = make_pair(dcsr, n, m, 1, 0)
+    dev.from_coo(r, c, v)
+    assert orc.load_coo(r, c, v) == 0
+    assert_layout_equal(dev, orc, "coo load T=2^25+1")
+    assert_content_equal(dev, orc, "coo load T=2^25+1")
 
 
 def test_update_sizes_repeated(dcsr):
